@@ -1,0 +1,424 @@
+"""Benchmark of the structure-factor + detector-chain path.
+
+Workload (one step): the 50,000-atom precision-stress particle (C 62 % N 17 %
+O 20 % S 1 %, uniform in a 12 nm ball, 1.2 A minimum separation, seeded) on a
+1024 x 1024 detector of 75 um pixels at 0.1 m, wavelength 0.15 nm, compensated
+FP32 structure factor followed by the full detector chain (Thomson, solid
+angle, photons, Poisson, electrons, readout noise 10 e-, ADC with a clamp at
+65535).  Inputs are device-resident for `value`; `e2e` runs the reference-
+facing simulate_shot call with host buffers.  Under torchrun every rank
+simulates its own orientation of the particle (weak scaling, no data-path
+collective); the timing is the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom·pixel terms/s at ≤1e-5 rel |F|² err vs FP64; backward/forward time ratio"
+UNIT = "terms/s"
+WORKLOAD = "precision_50k"
+MUFU_PER_SM_CLK = 16          # sin/cos (MUFU) results per SM per clock, nominal
+FMA_PER_SM_CLK = 128          # FP32 FMA lanes per SM per clock, nominal
+OPS_PER_TERM_MUFU = 2         # canonical term: 2 MUFU (sin, cos)
+OPS_PER_TERM_FMA = 5          # canonical term: 3 FMA (q.r) + 2 FMA (accumulate)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload_desc():
+    return ("precision_50k: 50,000 atoms (C 62% N 17% O 20% S 1%, 12 nm ball), 1024x1024 pixels of 75 um at 0.1 m, "
+            "lambda 0.15 nm, compensated FP32 structure factor + detector chain (readout 10 e-, clamp 65535)")
+
+
+# ----------------------------------------------------------------- CPU reference
+
+def _ref_worker(args):
+    """spsim's own CPU path on one pixel slab (runs in a spawned process)."""
+    Z, pos, hkl, vector = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+
+    t = time.perf_counter()
+    O.ref_pattern(Z, pos, hkl, vector=vector)
+    return time.perf_counter() - t
+
+
+def _ref_kind():
+    from oracle import oracle as O
+
+    return "reference" if O.ref_available() else "port"
+
+
+def _cpu_sample(Z, pos, hkl_all, pool, nproc, target_s, vector=True):
+    """Time spsim's CPU structure factor on an evenly spread pixel sample sized to
+    about target_s of wall time over nproc processes; returns (terms/s, desc)."""
+    from oracle import oracle as O
+
+    n_atoms = int(np.count_nonzero(Z))
+    if O.ref_available():
+        t = time.perf_counter()
+        O.ref_pattern(Z, pos, hkl_all[:64], vector=vector)
+        per_pix = (time.perf_counter() - t) / 64
+    else:
+        per_pix = n_atoms * 30e-9
+    npix = int(min(len(hkl_all), max(nproc, target_s * nproc / max(per_pix, 1e-9))))
+    idx = np.linspace(0, len(hkl_all) - 1, npix).astype(np.int64)
+    sample = hkl_all[idx]
+    slabs = np.array_split(sample, nproc)
+    if O.ref_available():
+        t = time.perf_counter()
+        pool.map(_ref_worker, [(Z, pos, s, vector) for s in slabs])
+        wall = time.perf_counter() - t
+    else:  # the oracle port, FP64, threaded
+        t = time.perf_counter()
+        O.structure_factor(Z, pos.astype(np.float64), sample.astype(np.float64), nthreads=nproc)
+        wall = time.perf_counter() - t
+    path = "vector_compute_pattern_on_list" if vector else "compute_pattern_on_list"
+    desc = "%d evenly spaced pixels of the 1024x1024 detector x %d atoms, %s, %d processes over contiguous " \
+           "slabs (src/mpi.c:30-48)" % (npix, n_atoms, path, nproc)
+    return npix * n_atoms / wall, desc
+
+
+def _make_workload(rank=0):
+    from spsim_b200 import synth
+
+    w = synth.WORKLOADS[WORKLOAD]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    return w, Z, pos
+
+
+def _hkl_host(w):
+    from oracle import oracle as O
+
+    d = w["det"]
+    return O.hkl_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"]).astype(
+        np.float32)
+
+
+def run_reference(args):
+    """--impl reference: spsim's own CPU path on this box's host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+
+    nproc = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    w, Z, pos = _make_workload()
+    hkl = _hkl_host(w)
+    with ctx.Pool(nproc) as pool:
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, desc = _cpu_sample(Z, pos, hkl, pool, nproc, target_s=2.0)
+            if i >= args.warmup:
+                vals.append(v)
+    value = float(statistics.median(vals))
+    terms = float(w["natoms"]) * w["det"]["nx"] * w["det"]["ny"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": terms / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_desc(), "precision": "reference float path (SSE sincos_ps)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": _ref_kind(), "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- GPU
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+        return False
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+def _peaks(props):
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    src = "nominal"
+    sm_max = 1965.0
+    if os.path.exists(path):
+        try:
+            mp = json.load(open(path))
+            sm_max = float(mp.get("sm_max_mhz", sm_max))
+            src = "MEASURED_PEAKS.json sm_max_mhz"
+        except (ValueError, OSError):
+            pass
+    sms = props.multi_processor_count
+    p_mufu = sms * MUFU_PER_SM_CLK * sm_max * 1e6
+    p_fma = sms * FMA_PER_SM_CLK * sm_max * 1e6
+    return min(p_fma / OPS_PER_TERM_FMA, p_mufu / OPS_PER_TERM_MUFU), p_mufu, p_fma, sm_max, src
+
+
+def _traffic_per_launch():
+    p = os.path.join(ROOT, "profiles", "sf_f32_precision50k_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("dram_bytes_per_launch")
+        except (ValueError, OSError):
+            return None
+    return None
+
+
+def run_b200(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pool = None
+    nproc = os.cpu_count() or 1
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import multiprocessing as mp
+
+        pool = mp.get_context("spawn").Pool(nproc)  # before the first CUDA call
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from spsim_b200 import core, synth
+
+    w, Z, pos = _make_workload()
+    d = w["det"]
+    prec = args.precision
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+    rot = synth.haar_rotations(world, 77)[rank] if world > 1 else None
+    npix = d["nx"] * d["ny"]
+    terms = float(np.count_nonzero(Z)) * npix
+    chain = core.chain_params(nx=d["nx"], ny=d["ny"], width=d["width"], height=d["height"], distance=d["distance"],
+                              pixel_width=d["width"] / d["nx"], pixel_height=d["height"] / d["ny"],
+                              wavelength=d["wavelength"], beam_intensity=1e30, quantum_efficiency=1.0,
+                              electron_hole_production_energy=5.8e-19, readout_noise=w["readout_noise"],
+                              linear_full_well=2e5, maximum_value=w["full_well_clamp"], clamp_to_maximum=1,
+                              exposure_time=1e-3, dark_current=0.0, seed=1234 + rank)
+    F = torch.empty(npix, dtype=torch.complex64, device="cuda")
+    I = torch.empty(npix, dtype=torch.float32, device="cuda")
+    outs = ["photon_count", "real_output", "noiseless_output"]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step(pattern):
+        chain.pattern_index = pattern
+        core.forward(mol, qs, rot=rot, precision=prec, F=F, I=I)
+        return core.detector_chain(chain, I, outputs=outs)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    core.synchronize()
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with core.timing() as kt, ClockSampler(local) as clocks:
+        for i, (a, b) in enumerate(evs):
+            flush.zero_()  # L2 flush between timed steps, outside the events
+            a.record()
+            step(args.warmup + i)
+            b.record()
+        torch.cuda.synchronize()
+        kt.read()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    core.synchronize()
+    elapsed_ms = sum(a.elapsed_time(b) for a, b in evs)
+    if dist:
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = world * args.steps * terms / (elapsed_ms * 1e-3)
+    sf_ms = kt.ms[-args.steps:] if kt.ms else []
+    sf_avg = statistics.mean(sf_ms) if sf_ms else None
+
+    line = None
+    if rank == 0:
+        props = torch.cuda.get_device_properties(local)
+        R, p_mufu, p_fma, sm_max, src = _peaks(props)
+        achieved = terms / (sf_avg * 1e-3) if sf_avg else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec != "fp64" else "f64",
+            "data": "synthetic (seeded molecule; no dataset)",
+            "config": {"workload": workload_desc(), "precision": prec,
+                       "parallelism": "one orientation per rank" if world > 1 else "single GPU",
+                       "l2": "flushed between timed steps (256 MiB write outside the timed events)"},
+            "roofline": {
+                "bound": "sfu", "achieved": achieved, "peak": R, "unit": UNIT,
+                "frac": achieved / R if achieved else None, "traffic": _traffic_per_launch(),
+                "kernel": "sf_f32_kernel" if prec != "fp64" else "sf_f64_kernel",
+                "kernel_ms": sf_avg,
+                "peak_source": "min(P_FMA/5, P_MUFU/2) terms/s with %d SMs x %d MUFU and %d FMA lanes per clock at "
+                               "%.0f MHz (%s); MEASURED_PEAKS.json has no FMA/MUFU figure" %
+                               (props.multi_processor_count, MUFU_PER_SM_CLK, FMA_PER_SM_CLK, sm_max, src),
+            },
+            "clocks": clocks.summary(),
+            "gpu_launches": 3 * args.steps,
+        }
+    # end to end through the reference-facing simulate_shot (host buffers)
+    if rank == 0 and not args.no_e2e:
+        line["e2e"] = _e2e(args, w, Z, pos, terms, world)
+    if rank == 0 and pool is not None:
+        v, desc = _cpu_sample(Z, pos, _hkl_host(w), pool, nproc, target_s=12.0)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nproc, "kind": _ref_kind(), "sample": desc}
+        pool.close()
+    if rank == 0:
+        line["backward_forward_ratio"] = _adjoint_ratio(prec) if not args.no_adjoint else None
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _e2e(args, w, Z, pos, terms, world):
+    """simulate_shot (src/spsim.c:281) with host buffers: geometry, structure factor
+    and the detector chain, every host<->device copy inside the timed region."""
+    import torch
+
+    from spsim_b200 import spsim as S
+
+    d = w["det"]
+    opts = S.set_defaults()
+    o = opts.contents
+    det, exp = o.detector.contents, o.experiment.contents
+    det.nx, det.ny, det.nz = d["nx"], d["ny"], 1
+    det.width, det.height, det.distance = d["width"], d["height"], d["distance"]
+    det.pixel_width = det.pixel_height = d["width"] / d["nx"]
+    det.quantum_efficiency, det.electron_hole_production_energy = 1.0, 5.8e-19
+    det.readout_noise, det.linear_full_well, det.maximum_value = w["readout_noise"], 2e5, w["full_well_clamp"]
+    exp.wavelength, exp.beam_intensity, exp.exposure_time = d["wavelength"], 1e30, 1e-3
+    o.verbosity_level = 0
+    o.random_seed = 99
+    mol = S.get_molecule_from_atoms(Z, pos)
+    n = d["nx"] * d["ny"]
+    nsteps = max(2, min(args.steps, 5))
+    for _ in range(1):
+        S.free_stuff(S.simulate_shot(mol, opts), opts)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(nsteps):
+        S.free_stuff(S.simulate_shot(mol, opts), opts)
+    wall = (time.perf_counter() - t) / nsteps
+    S.free_mol(mol)
+    natoms = len(Z)
+    return {"value": world * terms / wall, "unit": UNIT,
+            "h2d_bytes_per_step": 12 * n + 16 * natoms + 4 * n,
+            "d2h_bytes_per_step": 12 * n + 12 * n + 7 * 4 * n,
+            "call": "simulate_shot (reference-facing C ABI, host buffers)", "steps": nsteps,
+            "note": "reference semantics: no ADC clamp (extension) in this call"}
+
+
+def _adjoint_ratio(prec):
+    """Adjoint / forward time on the refinement shape (5,000 atoms, 512^2 pixels,
+    8 orientations), both timed with CUDA events."""
+    import torch
+
+    from spsim_b200 import core, synth
+
+    w = synth.WORKLOADS["adjoint_5k"]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    d = w["det"]
+    mol = core.Molecule(Z, pos, occ=np.ones(len(Z), np.float32))
+    qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+    R = synth.haar_rotations(8, w["rot_seed"])
+    F, I = core.forward_batch([mol] * 8, [qs] * 8, rots=R, precision=prec)
+    Fc = torch.cat(F)
+    G = torch.rand(Fc.numel(), device="cuda")
+    ta, tb = [], []
+    for it in range(4):
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record()
+        core.forward_batch([mol] * 8, [qs] * 8, rots=R, precision=prec, F=F, I=I)
+        b.record()
+        core.adjoint(mol, qs, Fc, G, rots=R, precision=prec)
+        c.record()
+        torch.cuda.synchronize()
+        if it:
+            ta.append(a.elapsed_time(b))
+            tb.append(b.elapsed_time(c))
+    return statistics.median(tb) / statistics.median(ta)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f32_fast", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

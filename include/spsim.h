@@ -1,0 +1,82 @@
+/*
+ * spsim.h — the reference-shaped C entry points of libspsim_b200.so.
+ *
+ * Same names, signatures, ownership and error behaviour as spsim's own
+ * (the file:line after each names the reference declaration it replaces);
+ * the structure factor and the detector chain run on the GPU through the
+ * native ABI in spsim_b200.h.  Ownership is the reference's: the callee
+ * mallocs returned patterns and the CCD output arrays; free them with
+ * free_diffraction_pattern / free_output_in_options.  Like the reference,
+ * these functions have no status return: on a failure they print the reason
+ * to stderr and abort() (no silent CPU fallback).
+ */
+#ifndef SPSIM_B200_SPSIM_H
+#define SPSIM_B200_SPSIM_H
+
+#include "spsim_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- configuration: include/config.h:184-187 ---- */
+Options *set_defaults(void);                                     /* src/config.c:30 */
+void read_options_file(char *filename, Options *opt);            /* src/config.c:89 */
+void write_options_file(char *filename, Options *opt);           /* src/config.c:433 */
+
+/* ---- geometry: include/diffraction.h:72-73, :104 ---- */
+float *get_HKL_list_for_detector(CCD *det, Experiment *exp, int *HKL_list_size);  /* src/diffraction.c:237 */
+float *get_HKL_list_for_3d_detector(CCD *det, Experiment *exp, int *HKL_list_size); /* src/diffraction.c:325 */
+SpRotation *apply_orientation_to_HKL_list(float **HKL_list, int *HKL_list_size, Options *opts); /* :300 */
+float *get_HKL_list(Options *opts, int *HKL_list_size);          /* include/spsim.h:44, src/spsim.c:98 */
+
+/* ---- structure factor: include/diffraction.h:76-83 ---- */
+Diffraction_Pattern *compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
+                                             Experiment *exp, Options *opts);        /* src/diffraction.c:770 */
+Diffraction_Pattern *vector_compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
+                                                    Experiment *exp, Options *opts); /* src/diffraction.c:856 */
+Diffraction_Pattern *cuda_compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
+                                                  Experiment *exp, Options *opts);   /* src/diffraction.cu:135 */
+Diffraction_Pattern *cuda_compute_pattern_on_list2(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
+                                                   Experiment *exp, Options *opts);  /* src/diffraction.cu:235 */
+Diffraction_Pattern *compute_sf(Molecule *mol, float *HKL_list, int HKL_list_size, Options *opts); /* src/spsim.c:110 */
+
+/* ---- detector chain: include/diffraction.h:85-89, include/noise.h:33, include/amplification.h:24-26 ---- */
+void calculate_thomson_correction(CCD *det, Experiment *exp);            /* src/diffraction.c:1109 */
+void calculate_pixel_solid_angle(CCD *det);                              /* src/diffraction.c:1146 */
+void calculate_photons_per_pixel(Diffraction_Pattern *pattern, Options *opts); /* src/diffraction.c:1190 */
+void generate_poisson_noise(CCD *det);                                   /* src/noise.c:32 */
+void calculate_electrons_per_pixel(CCD *det, Experiment *experiment);    /* src/amplification.c:54 */
+void calculate_real_detector_output(CCD *det, Experiment *experiment);   /* src/amplification.c:77 */
+void calculate_noiseless_detector_output(CCD *det, Experiment *experiment); /* src/amplification.c:119 */
+
+/* ---- orchestration: include/spsim.h:45-59 ---- */
+Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts);        /* src/spsim.c:281 */
+void free_stuff(Diffraction_Pattern *pattern, Options *opts);            /* src/spsim.c:348 */
+void free_diffraction_pattern(Diffraction_Pattern *pattern);             /* src/spsim.c:353 */
+void free_output_in_options(Options *opts);                              /* src/spsim.c:363 */
+
+/* ---- molecules: include/molecule.h:25-28 ---- */
+Molecule *alloc_mol(void);                                               /* src/molecule.c:394 */
+void add_atom_to_mol(Molecule *mol, int atomic_number, float x, float y, float z); /* src/molecule.c:402 */
+void free_mol(Molecule *mol);                                            /* src/molecule.c:413 */
+
+/* ---- distribution: include/mpi_comm.h:30-32 (single-process semantics;
+ *      multi-GPU sharding lives in the Python layer over torch.distributed) ---- */
+void get_my_loop_start_and_end(int size, int *start, int *end);          /* src/mpi.c:30 */
+void syncronize_patterns(Diffraction_Pattern *pat);                      /* src/mpi.c:50 */
+void sum_patterns(Diffraction_Pattern *pat);                             /* src/mpi.c:62 */
+
+/* ---- library controls (no counterpart in the reference) ----
+ * Precision used by the reference-shaped structure-factor calls above
+ * (SPSIM_PREC_* of spsim_b200.h; default SPSIM_PREC_F32), and the Philox key
+ * of the noise stages (simulate_shot sets it from opts->random_seed). */
+void spsim_b200_set_legacy_precision(int precision);
+int spsim_b200_get_legacy_precision(void);
+void spsim_b200_set_noise_seed(unsigned long long seed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

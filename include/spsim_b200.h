@@ -1,0 +1,245 @@
+/*
+ * spsim_b200.h — native C ABI of the B200 structure-factor and detector-chain
+ * library (libspsim_b200.so).
+ *
+ * Everything is plain C: opaque handles, pointers and sizes.  Every function
+ * returns an int status (SPSIM_OK == 0); spsim_b200_last_error() gives the
+ * message of the last failure on the calling thread.  The reference-shaped
+ * entry points (compute_pattern_on_list, simulate_shot, read_options_file, ...)
+ * live in spsim.h and are implemented on top of these.
+ *
+ * Units follow spsim: lengths in metres, scattering vectors q in 1/m (the
+ * reference's HKL list, src/diffraction.c:237-297), B factors in Angstrom^2.
+ * Sign convention: F(q) = sum_j f_j exp(-2 pi i q . r_j) (src/diffraction.c:836).
+ */
+#ifndef SPSIM_B200_H
+#define SPSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SPSIM_OK 0
+#define SPSIM_ERR_INVALID_ARG 1
+#define SPSIM_ERR_CUDA 2
+#define SPSIM_ERR_NO_DEVICE 3
+#define SPSIM_ERR_OUT_OF_MEMORY 4
+#define SPSIM_ERR_RANGE 5       /* phase range beyond the compensated FP32 kernel's domain */
+#define SPSIM_ERR_TIMEOUT 6     /* a bounded device-side wait gave up (kernel returned early) */
+#define SPSIM_ERR_UNSUPPORTED 7
+
+/* ---- precision of the structure-factor sum ----------------------------- */
+#define SPSIM_PREC_FP64 0        /* plain FP64 per-pixel kernel (FP64 phase, sincos, sum)      */
+#define SPSIM_PREC_F32 1         /* compensated FP32 phase, FMA-pipe minimax sin/cos,          */
+                                 /* float-float segment sums, FP64 cross-tile/element sum      */
+#define SPSIM_PREC_F32_FAST 2    /* compensated FP32 phase, MUFU sin/cos, same summation        */
+
+/* ---- where caller buffers live ----------------------------------------- */
+#define SPSIM_MEM_HOST 0
+#define SPSIM_MEM_DEVICE 1
+
+/* Detector-chain polarisation codes (include/config.h:36-39 of spsim). */
+#define SPSIM_POL_IGNORE 0
+#define SPSIM_POL_VERTICAL 1
+#define SPSIM_POL_HORIZONTAL 2
+#define SPSIM_POL_UNPOLARIZED 3
+
+const char *spsim_b200_status_string(int status);
+const char *spsim_b200_last_error(void);
+/* Library version string. */
+const char *spsim_b200_version(void);
+
+/* Selects the CUDA device for the calling thread's later calls and checks it
+ * is present (the reference's device probe, src/config.c:344-356, but as an
+ * error instead of a silent CPU fallback). */
+int spsim_b200_init(int device);
+/* Number of visible CUDA devices (0 when none; never an error). */
+int spsim_b200_device_count(int *count);
+
+/* ---- molecules ----------------------------------------------------------
+ * A molecule handle owns device-resident atom records: atoms with Z == 0 are
+ * dropped (src/diffraction.c:830-832), the rest are sorted by element,
+ * centred, and split into a coarse grid part and a remainder for the
+ * compensated phase.  Weights are occ_j * sqrt(illumination_j)
+ * (src/diffraction.c:223-235, :834), or 1 under delta_atoms.
+ * pos: xyz per atom (metres), host memory.  occ / bfac may be NULL (1 / 0).
+ * beam: {fwhm, centre_x, centre_y} in metres, or NULL for a plane wave.
+ * bfac != NULL selects per-atom Debye-Waller factors exp(-B_j |q|^2/4). */
+typedef struct spsim_b200_molecule spsim_b200_molecule;
+int spsim_b200_molecule_create(int natoms, const int32_t *Z, const float *pos, const float *occ,
+                               const float *bfac, int delta_atoms, const float *beam,
+                               spsim_b200_molecule **out);
+/* Same from FP64 positions (host). */
+int spsim_b200_molecule_create_f64(int natoms, const int32_t *Z, const double *pos, const float *occ,
+                                   const float *bfac, int delta_atoms, const float *beam,
+                                   spsim_b200_molecule **out);
+/* Refinement: rewrites positions / occupancies / B factors from DEVICE arrays
+ * in the caller's original atom order, on `stream`, keeping the element
+ * order and grid chosen at creation.  pos_dev is float (pos_is_f64 == 0) or
+ * double; occ_dev / bfac_dev may be NULL (unchanged).  Positions that leave the
+ * creation-time bounds raise SPSIM_ERR_RANGE at the next forward. */
+int spsim_b200_molecule_update_device(spsim_b200_molecule *m, const void *pos_dev, int pos_is_f64,
+                                      const float *occ_dev, const float *bfac_dev, void *stream);
+int spsim_b200_molecule_natoms(const spsim_b200_molecule *m, int *natoms);
+int spsim_b200_molecule_destroy(spsim_b200_molecule *m);
+
+/* ---- pixel q sets -------------------------------------------------------
+ * A q set owns the device-resident scattering vectors of one detector.
+ * from_list: the reference's float HKL list (3 floats per pixel), in host or
+ * device memory (src/diffraction.c:770, HKL_list argument).
+ * from_detector: the Ewald-sphere geometry of src/diffraction.c:237-297
+ * evaluated on the device in FP64 and kept in FP64 (flat or spherical). */
+typedef struct spsim_b200_qset spsim_b200_qset;
+int spsim_b200_qset_from_list(int64_t npix, const float *hkl, int memory, spsim_b200_qset **out);
+int spsim_b200_qset_from_detector(int nx, int ny, float width, float height, float distance,
+                                  float center_x, float center_y, float wavelength, int spherical,
+                                  spsim_b200_qset **out);
+int spsim_b200_qset_npix(const spsim_b200_qset *qs, int64_t *npix);
+/* Copies the set's q vectors (3 per pixel, float) to host memory. */
+int spsim_b200_qset_copy_q(const spsim_b200_qset *qs, float *hkl_host);
+int spsim_b200_qset_destroy(spsim_b200_qset *qs);
+
+/* ---- structure factor ---------------------------------------------------
+ * One pattern: F (complex64, interleaved re/im, npix) and I = |F|^2 (float)
+ * into DEVICE buffers on `stream` (a cudaStream_t, NULL = legacy default).
+ * rot: optional 3x3 row-major FP64 rotation applied to every q (q' = R q,
+ * src/diffraction.c:300-323), NULL = identity.  B: global B factor
+ * (src/diffraction.c:183-193).  Either output may be NULL. */
+int spsim_b200_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot,
+                       float B, int precision, float *F_dev, float *I_dev, void *stream);
+
+/* Many patterns in one persistent launch: pattern i uses mols[i], qsets[i],
+ * rot[9*i] (NULL = identity for all) and writes F_dev[i] / I_dev[i] (device
+ * pointers, entries may be NULL).  Work items (pixel tile x atom range) are
+ * cost-sorted and drained by a persistent kernel; the whole launch sequence
+ * is captured once per plan into a CUDA graph and replayed while the plan's
+ * shapes and pointers stay the same. */
+int spsim_b200_forward_batch(int npatterns, const spsim_b200_molecule *const *mols,
+                             const spsim_b200_qset *const *qsets, const double *rot, float B,
+                             int precision, float *const *F_dev, float *const *I_dev, void *stream);
+
+/* Host-memory convenience: atoms and HKL list from host, F / I back to host
+ * (copies inside).  The reference-shaped compute_pattern_on_list is built on it. */
+int spsim_b200_structure_factor_host(int natoms, const int32_t *Z, const float *pos, const float *occ,
+                                     const float *bfac, float B, int delta_atoms, const float *beam,
+                                     int64_t npix, const float *hkl, int precision, float *F_host,
+                                     float *I_host);
+
+/* ---- adjoint -------------------------------------------------------------
+ * Given G_p = dL/dI_p for every pixel of `npat` patterns (device, float,
+ * npat*npix) and the forward's F (device, complex64, npat*npix), accumulates
+ * dL/dpos (double, 3 per atom, caller's atom order), dL/docc and dL/dB (double
+ * per atom; NULL to skip) on `stream`.  Phases are recomputed, nothing of size
+ * atoms x pixels is stored.  The outputs are overwritten. */
+int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int npat,
+                       const double *rot, float B, int precision, const float *F_dev, const float *G_dev,
+                       double *dpos_dev, double *docc_dev, double *dB_dev, void *stream);
+
+/* ---- detector chain ------------------------------------------------------
+ * The per-pixel chain of src/spsim.c:281-346 after the structure factor:
+ * Thomson (src/diffraction.c:1109-1144), solid angle (:1146-1187), photons
+ * (:1190-1204), Poisson counts (src/noise.c:32-51, counter-based Philox
+ * instead of GSL), electrons (src/amplification.c:54-74), binned real output
+ * with dark current, readout noise and ADC (:77-116), and the noiseless
+ * output (:119-155).  All arrays are DEVICE pointers; any output may be NULL. */
+typedef struct {
+  int nx, ny, nz;                /* detector pixels */
+  int binning_x, binning_y, binning_z;
+  int spherical;
+  int polarization;              /* SPSIM_POL_* */
+  float width, height, distance; /* metres */
+  float center_x, center_y;
+  float pixel_width, pixel_height;
+  float wavelength;              /* metres */
+  float beam_intensity;          /* photons / m^2 */
+  float quantum_efficiency;
+  float electron_hole_production_energy; /* joules; 0 = one electron per photon */
+  float dark_current;            /* electrons / (pixel s) */
+  float exposure_time;           /* s */
+  float readout_noise;           /* electrons rms per binned pixel */
+  float linear_full_well;        /* electrons */
+  float maximum_value;           /* ADC counts */
+  int clamp_to_maximum;          /* extension: clamp the ADC output at maximum_value */
+  uint64_t seed;                 /* Philox key */
+  uint32_t pattern_index;        /* Philox counter word: independent streams per pattern */
+} spsim_b200_chain_params;
+
+typedef struct {
+  float *thomson_correction;   /* [nx*ny*nz] */
+  float *solid_angle;          /* [nx*ny*nz] */
+  float *photons_per_pixel;    /* [nx*ny*nz] */
+  float *photon_count;         /* [nx*ny*nz] */
+  float *electrons_per_pixel;  /* [nx*ny*nz] */
+  float *real_output;          /* [(nx/bx)*(ny/by)*(nz/bz)] */
+  float *noiseless_output;     /* [(nx/bx)*(ny/by)*(nz/bz)] */
+} spsim_b200_chain_outputs;
+
+/* Runs the fused chain on intensities I_dev (|F|^2, device, nx*ny*nz floats). */
+int spsim_b200_detector_chain(const spsim_b200_chain_params *p, const float *I_dev,
+                              const spsim_b200_chain_outputs *out, void *stream);
+/* Individual stages, for the reference-shaped per-stage entry points. */
+int spsim_b200_thomson(const spsim_b200_chain_params *p, float *out_dev, void *stream);
+int spsim_b200_solid_angle(const spsim_b200_chain_params *p, float *out_dev, void *stream);
+/* photon_count_dev[i] = Poisson(lambda_dev[i]) (Gaussian approximation at >= 1000). */
+int spsim_b200_poisson(int64_t n, const float *lambda_dev, uint64_t seed, uint32_t pattern_index,
+                       float *photon_count_dev, void *stream);
+/* photons_dev[i] = T[i] * Omega[i] * I[i] * beam_intensity, in that float order
+ * (src/diffraction.c:1190-1204). */
+int spsim_b200_photons(int64_t n, const float *thomson_dev, const float *solid_angle_dev, const float *I_dev,
+                       float beam_intensity, float *photons_dev, void *stream);
+/* Poisson photon counts of photons_dev[i] * QE (src/noise.c:32-51). */
+int spsim_b200_photon_counts(const spsim_b200_chain_params *p, const float *photons_dev, float *counts_dev,
+                             void *stream);
+/* electrons_dev[i] = counts_dev[i] * electrons-per-photon (src/amplification.c:54-74). */
+int spsim_b200_electrons(const spsim_b200_chain_params *p, const float *counts_dev, float *electrons_dev,
+                         void *stream);
+/* Binned real output from electrons and / or binned noiseless output from
+ * photons (src/amplification.c:77-155); either input/output pair may be NULL. */
+int spsim_b200_binned_outputs(const spsim_b200_chain_params *p, const float *electrons_dev,
+                              const float *photons_dev, float *real_output_dev, float *noiseless_output_dev,
+                              void *stream);
+
+/* ---- Ewald geometry ----------------------------------------------------- */
+/* The reference's HKL list (float, 3 per pixel, row-major) for a flat or
+ * spherical 2-D detector, computed in FP64 on the device and stored as float
+ * (src/diffraction.c:237-297).  out is a DEVICE pointer. */
+int spsim_b200_hkl_for_detector(int nx, int ny, float width, float height, float distance,
+                                float center_x, float center_y, float wavelength, int spherical,
+                                float *hkl_dev, void *stream);
+
+/* ---- completion, errors and timing -------------------------------------
+ * Device-side failures of asynchronous calls (a bounded wait that gave up,
+ * refined positions outside the molecule's bounds) are recorded in device
+ * flags; spsim_b200_synchronize waits for `stream` and reports them. */
+int spsim_b200_synchronize(void *stream);
+
+/* Per-launch timing of the structure-factor kernel with CUDA events recorded
+ * on the launching stream.  While enabled, forwards run as direct launches
+ * (no graph replay) so every launch is bracketed. */
+int spsim_b200_timing_enable(int enable);
+/* Waits for the recorded events and returns up to `cap` kernel durations (ms)
+ * recorded since the last read, oldest first; *n is the number returned. */
+int spsim_b200_timing_read(double *ms, int cap, int *n);
+
+/* Atom-pixel terms evaluated by the last forward on this thread and the
+ * duration (ms) of its last timed kernel launch (0 when timing is off): the
+ * reference's "atoms.pixel/s" self-report (src/diffraction.c:849-851). */
+int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
+
+/* Autotuner: the kernel variant (threads per CTA, pixels per thread) used for
+ * FP32 forwards.  variant < 0 restores automatic choice; autotune times every
+ * compiled variant on the given workload and keeps the fastest for workloads
+ * of that size class. */
+int spsim_b200_set_variant(int threads, int pixels_per_thread);
+int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision, void *stream,
+                        int *best_threads, int *best_pixels_per_thread);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,282 @@
+"""ORACLE — test infrastructure only.
+
+ctypes access to the two CPU checkers built by oracle/Makefile:
+  * oracle/_build/libspsim_oracle.so : the FP64 restatement (sf_oracle.c)
+  * oracle/_ref/libspsim_ref.so      : spsim's own CPU sources compiled unchanged
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module; the product never does.
+"""
+import ctypes
+import os
+from ctypes import POINTER, c_char, c_double, c_float, c_int, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "_build", "libspsim_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libspsim_ref.so")
+
+_oracle = None
+_ref = None
+
+
+def _p(a):
+    return a.ctypes.data_as(c_void_p) if a is not None else None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_LIB):
+            raise ImportError("oracle not built: make -C oracle oracle")
+        _oracle = ctypes.CDLL(ORACLE_LIB)
+        _oracle.oracle_scatt_factor.restype = c_double
+        _oracle.oracle_scatt_factor.argtypes = [c_double, c_int, c_double]
+    return _oracle
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise ImportError("reference library not built: make -C oracle ref (needs the spsim tree)")
+        _ref = ctypes.CDLL(REF_LIB)
+    return _ref
+
+
+# ---------------------------------------------------------------- FP64 oracle
+
+def scatt_factor(q_len, Z, B=0.0):
+    return oracle_lib().oracle_scatt_factor(float(q_len), int(Z), float(B))
+
+
+def hkl_detector(nx, ny, width, height, distance, wavelength, center_x=0.0, center_y=0.0, spherical=False):
+    q = np.empty((nx * ny, 3), np.float64)
+    L = oracle_lib()
+    L.oracle_hkl_detector.argtypes = [c_int, c_int, c_float, c_float, c_float, c_float, c_float, c_float, c_int,
+                                      c_void_p]
+    L.oracle_hkl_detector(nx, ny, width, height, distance, center_x, center_y, wavelength, int(spherical), _p(q))
+    return q
+
+
+def structure_factor(Z, pos, q, occ=None, bfac=None, B=0.0, delta_atoms=False, beam=None, nthreads=None):
+    """FP64 F (complex128) and I = |F|^2 (float64) for atoms (Z, pos [m]) at q [1/m]."""
+    Z = np.ascontiguousarray(Z, np.int32)
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+    q = np.ascontiguousarray(q, np.float64).reshape(-1, 3)
+    occ = np.ascontiguousarray(occ, np.float64) if occ is not None else None
+    bfac = np.ascontiguousarray(bfac, np.float64) if bfac is not None else None
+    n = q.shape[0]
+    fr, fi, I = np.empty(n), np.empty(n), np.empty(n)
+    beam = beam or (0.0, 0.0, 0.0)
+    L = oracle_lib()
+    L.oracle_structure_factor.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double,
+                                          c_double, c_double, ctypes.c_long, c_void_p, c_void_p, c_void_p, c_void_p,
+                                          c_int]
+    L.oracle_structure_factor(len(Z), _p(Z), _p(pos), _p(occ), _p(bfac), float(B), int(delta_atoms), float(beam[0]),
+                              float(beam[1]), float(beam[2]), n, _p(q), _p(fr), _p(fi), _p(I),
+                              int(nthreads or os.cpu_count() or 1))
+    return fr + 1j * fi, I
+
+
+def structure_factor_vjp(Z, pos, q, g, occ=None, bfac=None, nthreads=None):
+    """FP64 dL/dpos (N,3), dL/docc (N,), dL/dB (N,) for dL/dI = g."""
+    Z = np.ascontiguousarray(Z, np.int32)
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+    q = np.ascontiguousarray(q, np.float64).reshape(-1, 3)
+    g = np.ascontiguousarray(g, np.float64).reshape(-1)
+    occ = np.ascontiguousarray(occ, np.float64) if occ is not None else None
+    bfac = np.ascontiguousarray(bfac, np.float64) if bfac is not None else None
+    N = len(Z)
+    dp, do, db = np.empty((N, 3)), np.empty(N), np.empty(N)
+    L = oracle_lib()
+    L.oracle_structure_factor_vjp.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_long, c_void_p,
+                                              c_void_p, c_void_p, c_void_p, c_void_p, c_int]
+    L.oracle_structure_factor_vjp(N, _p(Z), _p(pos), _p(occ), _p(bfac), q.shape[0], _p(q), _p(g), _p(dp), _p(do),
+                                  _p(db), int(nthreads or os.cpu_count() or 1))
+    return dp, do, db
+
+
+def thomson(nx, ny, width, height, distance, polarization=0, center_x=0.0, center_y=0.0, nz=1):
+    out = np.empty(nx * ny * nz)
+    L = oracle_lib()
+    L.oracle_thomson.argtypes = [c_int, c_int, c_int, c_float, c_float, c_float, c_float, c_float, c_int, c_void_p]
+    L.oracle_thomson(nx, ny, nz, width, height, distance, center_x, center_y, polarization, _p(out))
+    return out
+
+
+def solid_angle(nx, ny, width, height, distance, pixel_width, pixel_height, spherical=False, center_x=0.0,
+                center_y=0.0, nz=1):
+    out = np.empty(nx * ny * nz)
+    L = oracle_lib()
+    L.oracle_solid_angle.argtypes = [c_int, c_int, c_int, c_float, c_float, c_float, c_float, c_float, c_float,
+                                     c_float, c_int, c_void_p]
+    L.oracle_solid_angle(nx, ny, nz, width, height, distance, center_x, center_y, pixel_width, pixel_height,
+                         int(spherical), _p(out))
+    return out
+
+
+def noiseless_output(photons, nx, ny, bx, by, qe, wavelength, e_hole, full_well, max_value, nz=1, bz=1):
+    photons = np.ascontiguousarray(photons, np.float64)
+    out = np.empty((nx // bx) * (ny // by) * (nz // bz))
+    L = oracle_lib()
+    L.oracle_noiseless_output.argtypes = [c_int] * 6 + [c_void_p] + [c_double] * 5 + [c_void_p]
+    L.oracle_noiseless_output(nx, ny, nz, bx, by, bz, _p(photons), qe, wavelength, e_hole, full_well, max_value,
+                              _p(out))
+    return out
+
+
+def real_output(electrons, noise, nx, ny, bx, by, dark, exposure, full_well, max_value, clamp=False, nz=1, bz=1):
+    electrons = np.ascontiguousarray(electrons, np.float64)
+    noise = np.ascontiguousarray(noise, np.float64) if noise is not None else None
+    out = np.empty((nx // bx) * (ny // by) * (nz // bz))
+    L = oracle_lib()
+    L.oracle_real_output.argtypes = [c_int] * 6 + [c_void_p, c_double, c_double, c_void_p, c_double, c_double, c_int,
+                                                   c_void_p]
+    L.oracle_real_output(nx, ny, nz, bx, by, bz, _p(electrons), dark, exposure, _p(noise), full_well, max_value,
+                         int(clamp), _p(out))
+    return out
+
+
+def philox(c0, c1, c2, c3, seed):
+    out = np.empty(4, np.uint32)
+    L = oracle_lib()
+    L.oracle_philox.argtypes = [c_uint32] * 4 + [c_uint64, c_void_p]
+    L.oracle_philox(c0, c1, c2, c3, seed, _p(out))
+    return out
+
+
+def poisson(lam, seed, pattern=0):
+    lam = np.ascontiguousarray(lam, np.float32)
+    out = np.empty_like(lam)
+    L = oracle_lib()
+    L.oracle_poisson.argtypes = [ctypes.c_long, c_void_p, c_uint32, c_uint64, c_void_p]
+    L.oracle_poisson(lam.size, _p(lam), pattern, seed, _p(out))
+    return out
+
+
+def readout_noise(n, sigma, seed, pattern=0):
+    out = np.empty(n, np.float32)
+    L = oracle_lib()
+    L.oracle_readout_noise.argtypes = [ctypes.c_long, c_float, c_uint32, c_uint64, c_void_p]
+    L.oracle_readout_noise(n, sigma, pattern, seed, _p(out))
+    return out
+
+
+# ---------------------------------------------------------------- reference (spsim's own C)
+
+class RefComplex(ctypes.Structure):
+    _fields_ = [("re", c_float), ("im", c_float)]
+
+
+class RefMolecule(ctypes.Structure):  # include/config.h:50-58
+    _fields_ = [("natoms", c_int), ("atomic_number", POINTER(c_int)), ("pos", POINTER(c_float)),
+                ("delta_atoms", c_int)]
+
+
+class RefExperiment(ctypes.Structure):  # include/config.h:60-76
+    _fields_ = [(n, c_float) for n in ("wavelength", "bandwidth", "exposure_time", "beam_intensity", "beam_center_x",
+                                       "beam_center_y", "beam_fwhm", "beam_energy", "photon_energy",
+                                       "focal_diameter")] + [("polarization", c_int)]
+
+
+class RefCCD(ctypes.Structure):  # include/config.h:78-128
+    _fields_ = [(n, POINTER(c_float)) for n in ("photons_per_pixel", "thomson_correction", "solid_angle",
+                                                "photon_count", "electrons_per_pixel", "real_output",
+                                                "noiseless_output")] + \
+               [(n, c_float) for n in ("distance", "width", "height", "depth", "pixel_width", "pixel_height",
+                                       "pixel_depth", "quantum_efficiency", "electron_hole_production_energy",
+                                       "readout_noise", "dark_current", "linear_full_well")] + \
+               [(n, c_int) for n in ("binning_x", "binning_y", "binning_z", "nx", "ny", "nz")] + \
+               [("maximum_value", c_float), ("spherical", c_int), ("gaussian_blurring", c_float),
+                ("real_space_blurring", c_float), ("center_x", c_float), ("center_y", c_float),
+                ("center_z", c_float), ("n_patterns", c_int)]
+
+
+class RefChemFormula(ctypes.Structure):
+    _fields_ = [("n_elements", c_int), ("atomic_number", POINTER(c_int)), ("quantity", POINTER(c_int))]
+
+
+class RefOptions(ctypes.Structure):  # include/config.h:131-181
+    _fields_ = [("input_type", c_int), ("chem_formula", POINTER(RefChemFormula)),
+                ("experiment", POINTER(RefExperiment)), ("detector", POINTER(RefCCD)),
+                ("pdb_filename", c_char * 1024), ("sf_filename", c_char * 1024),
+                ("hkl_grid_filename", c_char * 1024), ("box_type", c_int), ("box_dimension", c_float),
+                ("use_fft_for_sf", c_int), ("use_nfft_for_sf", c_int), ("b_factor", c_float),
+                ("origin_to_com", c_int), ("euler_orientation", c_float * 3), ("random_orientation", c_int),
+                ("n_patterns", c_int), ("vectorize", c_int), ("delta_atoms", c_int), ("fast_exit", c_int),
+                ("crystal_size", c_int * 3), ("crystal_cell", c_float * 6)] + \
+               [(n, c_int) for n in ("use_cuda", "wavelength_samples", "random_seed", "output_sf_vtk",
+                                     "output_scatt_int", "output_ewald_vtk", "output_intensities",
+                                     "output_noiseless_photons", "output_photons", "output_electron_pixel_vtk",
+                                     "output_noiseless_count", "output_count", "output_realspace_histogram",
+                                     "output_scattering_factors", "output_solid_angles", "output_real_space",
+                                     "verbosity_level")]
+
+
+class RefPattern(ctypes.Structure):  # include/diffraction.h:46-62
+    _fields_ = [("ints", POINTER(c_float)), ("F", POINTER(RefComplex)), ("N_pix", c_int), ("max_s", c_float * 3),
+                ("d_s", c_float * 3), ("HKL_list", POINTER(c_float)), ("HKL_list_size", c_int),
+                ("rot", c_void_p)]
+
+
+def _ref_setup():
+    L = ref_lib()
+    for name in ("compute_pattern_on_list", "vector_compute_pattern_on_list"):
+        f = getattr(L, name)
+        f.restype = POINTER(RefPattern)
+        f.argtypes = [POINTER(RefMolecule), c_void_p, c_int, c_float, POINTER(RefExperiment), POINTER(RefOptions)]
+    L.set_defaults.restype = POINTER(RefOptions)
+    L.get_HKL_list_for_detector.restype = POINTER(c_float)
+    L.get_HKL_list_for_detector.argtypes = [POINTER(RefCCD), POINTER(RefExperiment), POINTER(c_int)]
+    return L
+
+
+def ref_defaults():
+    L = _ref_setup()
+    return L.set_defaults()
+
+
+def ref_hkl_detector(nx, ny, width, height, distance, wavelength, center_x=0.0, center_y=0.0, spherical=False):
+    L = _ref_setup()
+    det = RefCCD(nx=nx, ny=ny, nz=1, width=width, height=height, distance=distance, center_x=center_x,
+                 center_y=center_y, spherical=int(spherical))
+    exp = RefExperiment(wavelength=wavelength)
+    n = c_int(0)
+    p = L.get_HKL_list_for_detector(ctypes.byref(det), ctypes.byref(exp), ctypes.byref(n))
+    out = np.ctypeslib.as_array(p, shape=(n.value * 3,)).copy().reshape(-1, 3)
+    ctypes.CDLL(None).free(ctypes.cast(p, c_void_p))
+    return out
+
+
+def ref_pattern(Z, pos, hkl, B=0.0, vector=False, delta_atoms=False, beam=None, verbosity=0, slab=None):
+    """spsim's own compute_pattern_on_list / vector_compute_pattern_on_list (float F, ints).
+
+    slab=(start, end) restricts the evaluation to a contiguous pixel range."""
+    L = _ref_setup()
+    Z = np.ascontiguousarray(Z, np.int32)
+    pos = np.ascontiguousarray(pos, np.float32).reshape(-1)
+    hkl = np.ascontiguousarray(hkl, np.float32).reshape(-1, 3)
+    if slab is not None:
+        hkl = np.ascontiguousarray(hkl[slab[0]:slab[1]])
+    mol = RefMolecule(len(Z), Z.ctypes.data_as(POINTER(c_int)), pos.ctypes.data_as(POINTER(c_float)), 0)
+    exp = RefExperiment()
+    if beam is not None:
+        exp.beam_fwhm, exp.beam_center_x, exp.beam_center_y = beam
+    opts = RefOptions()
+    opts.delta_atoms = int(delta_atoms)
+    opts.verbosity_level = verbosity
+    fn = L.vector_compute_pattern_on_list if vector else L.compute_pattern_on_list
+    res = fn(ctypes.byref(mol), _p(hkl), hkl.shape[0], float(B), ctypes.byref(exp), ctypes.byref(opts))
+    n = hkl.shape[0]
+    Fr = np.ctypeslib.as_array(ctypes.cast(res.contents.F, POINTER(c_float)), shape=(2 * n,)).copy()
+    I = np.ctypeslib.as_array(res.contents.ints, shape=(n,)).copy()
+    libc = ctypes.CDLL(None)
+    for ptr in (res.contents.F, res.contents.ints, res.contents.HKL_list):
+        libc.free(ctypes.cast(ptr, c_void_p))
+    libc.free(ctypes.cast(res, c_void_p))
+    return Fr[0::2] + 1j * Fr[1::2], I

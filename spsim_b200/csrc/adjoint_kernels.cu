@@ -1,0 +1,265 @@
+// Adjoint of I = |F|^2 through the structure factor: given g_p = dL/dI_p,
+//   dL/dr_j   = 4 pi w_j     sum_p g_p f_e(p) E_pj q_p Im(conj(A_p) e^{-2 pi i u_pj})
+//   dL/docc_j = 2 wbase_j    sum_p g_p f_e(p) E_pj     Re(conj(A_p) e^{-2 pi i u_pj})
+//   dL/dB_j   = -2 w_j       sum_p g_p f_e(p) E_pj s_p^2 Re(...)
+// with A_p = e^{+2 pi i q_p.c} F_p the centred amplitude, u_pj = q_p.(r_j - c),
+// E_pj = exp(-B_j s_p^2) (1 without per-atom B) and s^2 = (|q| 1e-10)^2 / 4.
+// Phases are recomputed with the forward's compensated arithmetic; nothing of
+// size atoms x pixels is stored.  One CTA owns a block of atoms of one element
+// (registers) and streams a range of pixel records through shared memory.
+#include "adjoint_kernels.cuh"
+
+namespace spsim {
+
+// pixel record: 4 x float4
+//   {qhx, qhy, qhz, qx} {qy, qz, qlx, qly} {qlz, hr, hi, s2} {s2n, 0, 0, 0}
+constexpr int ADJ_PIX_TILE = 256;
+
+template <int MODE>
+__device__ __forceinline__ void adj_sincos(const float4 a0, const float4 a1, const float4 p0, const float4 p1,
+                                           const float4 p2, float &S, float &C) {
+  float u = p0.x * a0.x;
+  u = fmaf(p0.y, a0.y, u);
+  u = fmaf(p0.z, a0.z, u);
+  float c = p0.w * a1.x;
+  c = fmaf(p1.x, a1.y, c);
+  c = fmaf(p1.y, a1.z, c);
+  c = fmaf(p1.z, a0.x, c);
+  c = fmaf(p1.w, a0.y, c);
+  c = fmaf(p2.x, a0.z, c);
+  if (MODE == 0) {
+    const float t = fmaf(u, 4.0f, RINT_MAGIC);
+    const float kf = t - RINT_MAGIC;
+    const float y = fmaf(kf, -0.25f, u) + c;
+    const int ki = __float_as_int(t);
+    float s, co;
+    sincos_quad_poly(y, s, co);
+    const bool odd = (ki & 1) != 0;
+    const float ca = odd ? s : co;
+    const float sa = odd ? co : s;
+    C = __uint_as_float(__float_as_uint(ca) ^ (((unsigned)(ki + 1) << 30) & 0x80000000u));
+    S = __uint_as_float(__float_as_uint(sa) ^ (((unsigned)ki << 30) & 0x80000000u));
+  } else {
+    const float t = u + RINT_MAGIC;
+    const float kf = t - RINT_MAGIC;
+    const float y = (u - kf) + c;
+    __sincosf(y * 6.28318530717958648f, &S, &C);
+  }
+}
+
+template <int MODE, int NT, int A, bool PERB>
+__global__ void __launch_bounds__(NT) adj_kernel(AdjParams prm) {
+  __shared__ __align__(16) float4 pix[ADJ_PIX_TILE * 4];
+  const int tid = threadIdx.x;
+  const AdjItem item = prm.items[blockIdx.x];
+  const AdjBlock blk = prm.blocks[item.block];
+
+  float4 a0[A], a1[A];
+  int aidx[A];
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    aidx[k] = blk.atom_begin + tid + k * NT;
+    if (aidx[k] < blk.atom_end) {
+      a0[k] = prm.atoms[2 * aidx[k]];
+      a1[k] = prm.atoms[2 * aidx[k] + 1];
+    } else {
+      a0[k] = make_float4(0, 0, 0, 0);
+      a1[k] = make_float4(0, 0, 0, 0);
+    }
+  }
+  double gx[A], gy[A], gz[A], go[A], gb[A];
+#pragma unroll
+  for (int k = 0; k < A; ++k) gx[k] = gy[k] = gz[k] = go[k] = gb[k] = 0.0;
+
+  for (long long base = item.pix_begin; base < item.pix_end; base += ADJ_PIX_TILE) {
+    const int n = (int)min((long long)ADJ_PIX_TILE, item.pix_end - base);
+    __syncthreads();
+    for (int i = tid; i < ADJ_PIX_TILE; i += NT) {
+      float4 r0 = make_float4(0, 0, 0, 0), r1 = r0, r2 = r0, r3 = r0;
+      if (i < n) {
+        const long long gp = base + i;
+        const int pat = (int)(gp / prm.npix);
+        const long long p = gp - (long long)pat * prm.npix;
+        double q[3];
+        double a, b, c;
+        if (prm.hkl) {
+          a = prm.hkl[3 * p];
+          b = prm.hkl[3 * p + 1];
+          c = prm.hkl[3 * p + 2];
+        } else {
+          a = prm.q64[3 * p];
+          b = prm.q64[3 * p + 1];
+          c = prm.q64[3 * p + 2];
+        }
+        if (prm.rot) {
+          const double *R = prm.rot + 9 * pat;
+          q[0] = R[0] * a + R[1] * b + R[2] * c;
+          q[1] = R[3] * a + R[4] * b + R[5] * c;
+          q[2] = R[6] * a + R[7] * b + R[8] * c;
+        } else {
+          q[0] = a;
+          q[1] = b;
+          q[2] = c;
+        }
+        const double hx = (double)rintf((float)q[0] * prm.inv_dq) * prm.dq;
+        const double hy = (double)rintf((float)q[1] * prm.inv_dq) * prm.dq;
+        const double hz = (double)rintf((float)q[2] * prm.inv_dq) * prm.dq;
+        // centred amplitude A = e^{+2 pi i q.c} F
+        double t = q[0] * prm.cx + q[1] * prm.cy + q[2] * prm.cz;
+        t -= rint(t);
+        double sn, cs;
+        sincospi(2.0 * t, &sn, &cs);
+        const float2 F = prm.F[gp];
+        const double ar = F.x * cs - F.y * sn;
+        const double ai = F.x * sn + F.y * cs;
+        const double h = (double)prm.G[gp] * prm.ff[(long long)blk.elem * prm.npix + p];
+        const double s2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 0.25;
+        r0 = make_float4((float)hx, (float)hy, (float)hz, (float)q[0]);
+        r1 = make_float4((float)q[1], (float)q[2], (float)(q[0] - hx), (float)(q[1] - hy));
+        r2 = make_float4((float)(q[2] - hz), (float)(h * ar), (float)(h * ai), (float)s2);
+        r3 = make_float4((float)(-s2 * 1.4426950408889634), 0, 0, 0);
+      }
+      pix[4 * i] = r0;
+      pix[4 * i + 1] = r1;
+      pix[4 * i + 2] = r2;
+      pix[4 * i + 3] = r3;
+    }
+    __syncthreads();
+    float fx[A], fy[A], fz[A], fo[A], fb[A];
+#pragma unroll
+    for (int k = 0; k < A; ++k) fx[k] = fy[k] = fz[k] = fo[k] = fb[k] = 0.0f;
+    for (int i = 0; i < n; ++i) {
+      const float4 p0 = pix[4 * i], p1 = pix[4 * i + 1], p2 = pix[4 * i + 2];
+      float s2n = 0.0f;
+      if (PERB) s2n = pix[4 * i + 3].x;
+#pragma unroll
+      for (int k = 0; k < A; ++k) {
+        float S, C;
+        adj_sincos<MODE>(a0[k], a1[k], p0, p1, p2, S, C);
+        // H conj(A) e^{-2 pi i u} = (hr C - hi S) - i (hr S + hi C)
+        float zr = p2.y * C - p2.z * S;
+        float zi = -(p2.y * S + p2.z * C);
+        if (PERB) {
+          const float E = exp2f(a1[k].w * s2n);
+          zr *= E;
+          zi *= E;
+        }
+        fx[k] = fmaf(zi, p0.w, fx[k]);
+        fy[k] = fmaf(zi, p1.x, fy[k]);
+        fz[k] = fmaf(zi, p1.y, fz[k]);
+        fo[k] += zr;
+        fb[k] = fmaf(zr, p2.w, fb[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < A; ++k) {
+      gx[k] += fx[k];
+      gy[k] += fy[k];
+      gz[k] += fz[k];
+      go[k] += fo[k];
+      gb[k] += fb[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    if (aidx[k] >= blk.atom_end) continue;
+    const int src = prm.perm[aidx[k]];
+    if (src < 0) continue;
+    const double w = a0[k].w, wb = prm.wbase[aidx[k]];
+    const double kp = 4.0 * 3.14159265358979323846 * w;
+    atomicAdd(&prm.dpos[3 * src], kp * gx[k]);
+    atomicAdd(&prm.dpos[3 * src + 1], kp * gy[k]);
+    atomicAdd(&prm.dpos[3 * src + 2], kp * gz[k]);
+    if (prm.docc) atomicAdd(&prm.docc[src], 2.0 * wb * go[k]);
+    if (prm.dB) atomicAdd(&prm.dB[src], -2.0 * w * gb[k]);
+  }
+}
+
+// plain FP64 adjoint: same decomposition, FP64 phase and sincos
+template <int NT>
+__global__ void __launch_bounds__(NT) adj_f64_kernel(AdjParams prm) {
+  const int tid = threadIdx.x;
+  const AdjItem item = prm.items[blockIdx.x];
+  const AdjBlock blk = prm.blocks[item.block];
+  const int j = blk.atom_begin + tid;
+  if (j >= blk.atom_end) return;
+  const float4 a0 = prm.atoms[2 * j], a1 = prm.atoms[2 * j + 1];
+  const double rx = (double)a0.x + a1.x, ry = (double)a0.y + a1.y, rz = (double)a0.z + a1.z;
+  double gx = 0, gy = 0, gz = 0, go = 0, gb = 0;
+  for (long long gp = item.pix_begin; gp < item.pix_end; ++gp) {
+    const int pat = (int)(gp / prm.npix);
+    const long long p = gp - (long long)pat * prm.npix;
+    double a, b, c, q[3];
+    if (prm.hkl) {
+      a = prm.hkl[3 * p];
+      b = prm.hkl[3 * p + 1];
+      c = prm.hkl[3 * p + 2];
+    } else {
+      a = prm.q64[3 * p];
+      b = prm.q64[3 * p + 1];
+      c = prm.q64[3 * p + 2];
+    }
+    if (prm.rot) {
+      const double *R = prm.rot + 9 * pat;
+      q[0] = R[0] * a + R[1] * b + R[2] * c;
+      q[1] = R[3] * a + R[4] * b + R[5] * c;
+      q[2] = R[6] * a + R[7] * b + R[8] * c;
+    } else {
+      q[0] = a;
+      q[1] = b;
+      q[2] = c;
+    }
+    double t = q[0] * prm.cx + q[1] * prm.cy + q[2] * prm.cz;
+    t -= rint(t);
+    double sn, cs;
+    sincospi(2.0 * t, &sn, &cs);
+    const float2 F = prm.F[gp];
+    const double ar = F.x * cs - F.y * sn, ai = F.x * sn + F.y * cs;
+    const double h = (double)prm.G[gp] * prm.ff[(long long)blk.elem * prm.npix + p];
+    const double s2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 0.25;
+    double u = q[0] * rx + q[1] * ry + q[2] * rz;
+    u -= rint(u);
+    double S, C;
+    sincospi(2.0 * u, &S, &C);
+    double zr = h * (ar * C - ai * S), zi = -h * (ar * S + ai * C);
+    if (prm.per_atom_b) {
+      const double E = exp(-(double)a1.w * s2);
+      zr *= E;
+      zi *= E;
+    }
+    gx += zi * q[0];
+    gy += zi * q[1];
+    gz += zi * q[2];
+    go += zr;
+    gb += zr * s2;
+  }
+  const int src = prm.perm[j];
+  if (src < 0) return;
+  const double w = a0.w, wb = prm.wbase[j];
+  const double kp = 4.0 * 3.14159265358979323846 * w;
+  atomicAdd(&prm.dpos[3 * src], kp * gx);
+  atomicAdd(&prm.dpos[3 * src + 1], kp * gy);
+  atomicAdd(&prm.dpos[3 * src + 2], kp * gz);
+  if (prm.docc) atomicAdd(&prm.docc[src], 2.0 * wb * go);
+  if (prm.dB) atomicAdd(&prm.dB[src], -2.0 * w * gb);
+}
+
+cudaError_t launch_adjoint(int precision_mode, const AdjParams &prm, int n_items, cudaStream_t st) {
+  if (n_items <= 0) return cudaSuccess;
+  if (precision_mode == 2) {
+    adj_f64_kernel<ADJ_THREADS><<<n_items, ADJ_THREADS, 0, st>>>(prm);
+  } else if (precision_mode == 0) {
+    if (prm.per_atom_b)
+      adj_kernel<0, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, true><<<n_items, ADJ_THREADS, 0, st>>>(prm);
+    else
+      adj_kernel<0, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, false><<<n_items, ADJ_THREADS, 0, st>>>(prm);
+  } else {
+    if (prm.per_atom_b)
+      adj_kernel<1, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, true><<<n_items, ADJ_THREADS, 0, st>>>(prm);
+    else
+      adj_kernel<1, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, false><<<n_items, ADJ_THREADS, 0, st>>>(prm);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace spsim

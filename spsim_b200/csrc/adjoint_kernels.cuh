@@ -1,0 +1,43 @@
+// Adjoint kernels (internal C++ interface).
+#pragma once
+
+#include "sf_device.cuh"
+
+namespace spsim {
+
+constexpr int ADJ_THREADS = 128;
+constexpr int ADJ_ATOMS_PER_THREAD = 2;
+constexpr int ADJ_BLOCK_ATOMS = ADJ_THREADS * ADJ_ATOMS_PER_THREAD;
+
+struct AdjBlock {   // atoms [atom_begin, atom_end) of one element
+  int atom_begin, atom_end, elem, pad;
+};
+
+struct AdjItem {    // one CTA: an atom block x a range of (pattern, pixel) indices
+  int block, pad;
+  long long pix_begin, pix_end;
+};
+
+struct AdjParams {
+  const float4 *atoms;
+  const int *perm;
+  const float *wbase;
+  const AdjBlock *blocks;
+  const AdjItem *items;
+  const float *hkl;
+  const double *q64;
+  const double *rot;   // device, 9 per pattern, or nullptr
+  const double *ff;    // [n_elem][npix]
+  const float2 *F;     // npat * npix
+  const float *G;      // npat * npix
+  long long npix;
+  double cx, cy, cz;
+  float dq, inv_dq;
+  int per_atom_b;
+  double *dpos, *docc, *dB;
+};
+
+// precision_mode: 0 polynomial FP32, 1 MUFU FP32, 2 plain FP64
+cudaError_t launch_adjoint(int precision_mode, const AdjParams &prm, int n_items, cudaStream_t st);
+
+}  // namespace spsim

@@ -1,0 +1,1302 @@
+// C ABI of libspsim_b200.so: handles, planning, scheduling and launches.
+// Declarations and contracts: include/spsim_b200.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/spsim_b200.h"
+#include "atomsf_data.h"
+#include "chain_kernels.cuh"
+#include "adjoint_kernels.cuh"
+#include "sf_kernels.cuh"
+
+using namespace spsim;
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local std::string g_last_error;
+
+static int fail(int status, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+#define CUDA_TRY(expr)                                                                            \
+  do {                                                                                            \
+    cudaError_t _e = (expr);                                                                      \
+    if (_e != cudaSuccess) return fail(SPSIM_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), \
+                                       __FILE__, __LINE__);                                       \
+  } while (0)
+
+extern "C" const char *spsim_b200_status_string(int s) {
+  switch (s) {
+    case SPSIM_OK: return "ok";
+    case SPSIM_ERR_INVALID_ARG: return "invalid argument";
+    case SPSIM_ERR_CUDA: return "CUDA error";
+    case SPSIM_ERR_NO_DEVICE: return "no CUDA device";
+    case SPSIM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case SPSIM_ERR_RANGE: return "phase range outside the compensated FP32 kernel's domain";
+    case SPSIM_ERR_TIMEOUT: return "a bounded device wait gave up";
+    case SPSIM_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char *spsim_b200_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *spsim_b200_version(void) { return "spsim_b200 0.1 (sm_100a)"; }
+
+static std::mutex g_mu;  // serialises planning and workspace use
+
+static int current_device(int *dev) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(SPSIM_ERR_NO_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+  }
+  CUDA_TRY(cudaGetDevice(dev));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_device_count(int *count) {
+  if (!count) return fail(SPSIM_ERR_INVALID_ARG, "count is NULL");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  *count = n;
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_init(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(SPSIM_ERR_NO_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= n) return fail(SPSIM_ERR_INVALID_ARG, "device %d out of range [0,%d)", device, n);
+  CUDA_TRY(cudaSetDevice(device));
+  CUDA_TRY(cudaFree(nullptr));
+  return SPSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// form-factor table, with the reference's ./atomsf.lib override
+// (src/diffraction.c:118-177): read once, on first use, from the working
+// directory; every row gets a1 = -1 and rows present in the file are replaced.
+
+static float g_atomsf[SPSIM_B200_N_ELEMENTS][9];
+static bool g_atomsf_loaded = false;
+
+static void load_atomsf_table() {
+  if (g_atomsf_loaded) return;
+  memcpy(g_atomsf, spsim_b200_atomsf_default, sizeof(g_atomsf));
+  g_atomsf_loaded = true;
+  FILE *f = fopen("atomsf.lib", "r");
+  if (!f) return;
+  for (int i = 0; i < SPSIM_B200_N_ELEMENTS; ++i) g_atomsf[i][0] = -1;
+  char line[1024];
+  auto next = [&](char *buf) -> bool { return fgets(buf, sizeof(line), f) != nullptr; };
+  line[0] = 0;
+  // comment block: lines starting with "AD"
+  while (next(line) && strncmp(line, "AD", 2) == 0) {
+  }
+  // `line` holds the first line of a record (its name line) or is empty
+  while (line[0]) {
+    char zl[1024] = {0}, al[1024] = {0}, bl[1024] = {0}, xl[1024] = {0};
+    if (!next(zl)) break;
+    int z = -1;
+    if (sscanf(zl, "%d", &z) != 1 || z < 0 || z >= SPSIM_B200_N_ELEMENTS) break;
+    next(al);
+    next(bl);
+    next(xl);
+    if (g_atomsf[z][0] == -1) {
+      float v;
+      if (strlen(zl) > 23 && sscanf(zl + 23, "%f", &v) == 1) g_atomsf[z][8] = v;
+      for (int k = 0; k < 4; ++k) {
+        if (strlen(al) > (size_t)(16 * k) && sscanf(al + 16 * k, "%f", &v) == 1) g_atomsf[z][k] = v;
+        if (strlen(bl) > (size_t)(16 * k) && sscanf(bl + 16 * k, "%f", &v) == 1) g_atomsf[z][4 + k] = v;
+      }
+    }
+    line[0] = 0;
+    next(line);
+  }
+  fclose(f);
+}
+
+// ---------------------------------------------------------------------------
+// molecules
+
+static unsigned long long g_next_id = 1;
+
+struct spsim_b200_molecule {
+  unsigned long long id = 0;
+  int device = 0;
+  int natoms_in = 0;
+  int n_kept = 0;
+  int n_padded = 0;
+  int n_elem = 0;
+  int elem_Z[MAX_ELEM];
+  std::vector<float> coeffs;  // n_elem x 9
+  std::vector<int> perm;      // padded index -> caller index (-1 = padding)
+  std::vector<TileDesc> tiles;
+  double center[3] = {0, 0, 0};
+  double rbound = 0;
+  int er = 0, kr = 11;
+  float dr = 1, inv_dr = 1;
+  int per_atom_b = 0, delta_atoms = 0;
+  float4 *d_atoms = nullptr;
+  TileDesc *d_tiles = nullptr;
+  int *d_perm = nullptr;
+  float *d_wbase = nullptr;
+  float *d_coeffs = nullptr;
+  int *d_flags = nullptr;  // [0] range error
+  ~spsim_b200_molecule() {
+    cudaFree(d_atoms);
+    cudaFree(d_tiles);
+    cudaFree(d_perm);
+    cudaFree(d_wbase);
+    cudaFree(d_coeffs);
+    cudaFree(d_flags);
+  }
+};
+
+static int ceil_log2_bound(double x) {
+  // smallest e with x < 2^e
+  if (!(x > 0)) return -80;
+  int e = (int)std::floor(std::log2(x)) + 1;
+  while (std::ldexp(1.0, e) <= x) ++e;
+  while (e > -80 && std::ldexp(1.0, e - 1) > x) --e;
+  return e;
+}
+
+template <typename PosT>
+static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, const float *occ, const float *bfac,
+                                int delta_atoms, const float *beam, spsim_b200_molecule **out) {
+  if (!out) return fail(SPSIM_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (natoms < 0) return fail(SPSIM_ERR_INVALID_ARG, "natoms < 0");
+  if (natoms > 0 && (!Z || !pos)) return fail(SPSIM_ERR_INVALID_ARG, "Z or pos is NULL");
+  for (int j = 0; j < natoms; ++j)
+    if (Z[j] < 0 || Z[j] >= SPSIM_B200_N_ELEMENTS)
+      return fail(SPSIM_ERR_INVALID_ARG, "atom %d: atomic number %d outside [0,%d)", j, Z[j], SPSIM_B200_N_ELEMENTS);
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(g_mu);
+  load_atomsf_table();
+  std::unique_ptr<spsim_b200_molecule> m(new spsim_b200_molecule());
+  m->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
+  m->device = dev;
+  m->natoms_in = natoms;
+  m->per_atom_b = bfac != nullptr;
+  m->delta_atoms = delta_atoms;
+
+  // kept atoms, bounds
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  int count[SPSIM_B200_N_ELEMENTS] = {0};
+  for (int j = 0; j < natoms; ++j) {
+    if (!Z[j]) continue;  // src/diffraction.c:830-832
+    ++count[Z[j]];
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], (double)pos[3 * j + k]);
+      hi[k] = std::max(hi[k], (double)pos[3 * j + k]);
+    }
+    ++m->n_kept;
+  }
+  if (m->n_kept > 0)
+    for (int k = 0; k < 3; ++k) m->center[k] = 0.5 * (lo[k] + hi[k]);
+  double rmax = 0;
+  for (int j = 0; j < natoms; ++j) {
+    if (!Z[j]) continue;
+    double d2 = 0;
+    for (int k = 0; k < 3; ++k) {
+      const double d = (double)pos[3 * j + k] - m->center[k];
+      d2 += d * d;
+    }
+    rmax = std::max(rmax, std::sqrt(d2));
+  }
+  // room for refinement moves: 5% or 0.5 nm, whichever is larger
+  m->rbound = rmax + std::max(0.05 * rmax, 5e-10);
+  m->er = ceil_log2_bound(m->rbound);
+  m->dr = (float)std::ldexp(1.0, m->er - m->kr);
+  m->inv_dr = (float)std::ldexp(1.0, m->kr - m->er);
+
+  // element segments (ascending Z), padded to ATOM_GROUP
+  std::vector<int> seg_begin;
+  int n_pad = 0;
+  for (int z = 1; z < SPSIM_B200_N_ELEMENTS; ++z) {
+    if (!count[z]) continue;
+    if (m->n_elem >= MAX_ELEM) return fail(SPSIM_ERR_INVALID_ARG, "too many elements");
+    m->elem_Z[m->n_elem] = z;
+    for (int k = 0; k < 9; ++k) m->coeffs.push_back(g_atomsf[z][k]);
+    seg_begin.push_back(n_pad);
+    n_pad += (count[z] + ATOM_GROUP - 1) / ATOM_GROUP * ATOM_GROUP;
+    ++m->n_elem;
+  }
+  seg_begin.push_back(n_pad);
+  m->n_padded = n_pad;
+  m->perm.assign(n_pad, -1);
+  std::vector<float4> rec(2 * (size_t)std::max(n_pad, 1), make_float4(0, 0, 0, 0));
+  std::vector<float> wbase(std::max(n_pad, 1), 0.0f);
+  {
+    std::vector<int> fill(m->n_elem, 0);
+    int slot_of_z[SPSIM_B200_N_ELEMENTS];
+    for (int e = 0; e < m->n_elem; ++e) slot_of_z[m->elem_Z[e]] = e;
+    for (int j = 0; j < natoms; ++j) {
+      if (!Z[j]) continue;
+      const int e = slot_of_z[Z[j]];
+      const int idx = seg_begin[e] + fill[e]++;
+      m->perm[idx] = j;
+      // weight: occ * sqrt(illumination) (src/diffraction.c:223-235, :834), float like the reference
+      float w = 1.0f;
+      if (!delta_atoms) {
+        float illum = 1.0f;
+        if (beam && beam[0] != 0.0f) {
+          const double dx = (double)pos[3 * j] - (double)beam[1];
+          const double dy = (double)pos[3 * j + 1] - (double)beam[2];
+          const double sigma = (double)beam[0] / 2.355;
+          illum = (float)std::exp(-(dx * dx + dy * dy) / (2 * sigma * sigma));
+        }
+        w = (float)std::sqrt((double)illum);
+      }
+      wbase[idx] = w;
+      const float o = occ ? occ[j] : 1.0f;
+      double r[3];
+      for (int k = 0; k < 3; ++k) r[k] = (double)pos[3 * j + k] - m->center[k];
+      const double hx = std::rint(r[0] * m->inv_dr) * m->dr;
+      const double hy = std::rint(r[1] * m->inv_dr) * m->dr;
+      const double hz = std::rint(r[2] * m->inv_dr) * m->dr;
+      rec[2 * idx] = make_float4((float)hx, (float)hy, (float)hz, o * w);
+      rec[2 * idx + 1] = make_float4((float)(r[0] - hx), (float)(r[1] - hy), (float)(r[2] - hz), bfac ? bfac[j] : 0.0f);
+    }
+  }
+  // tile table
+  for (int e = 0; e < m->n_elem; ++e) {
+    for (int a = seg_begin[e]; a < seg_begin[e + 1]; a += TILE_ATOMS) {
+      TileDesc t;
+      t.atom_begin = a;
+      t.count = std::min(TILE_ATOMS, seg_begin[e + 1] - a);
+      t.elem = e;
+      t.last = (a + TILE_ATOMS >= seg_begin[e + 1]) ? 1 : 0;
+      m->tiles.push_back(t);
+    }
+  }
+  // upload
+  const size_t na = std::max(n_pad, 1);
+  CUDA_TRY(cudaMalloc(&m->d_atoms, 2 * na * sizeof(float4)));
+  CUDA_TRY(cudaMemcpy(m->d_atoms, rec.data(), 2 * na * sizeof(float4), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&m->d_tiles, std::max<size_t>(m->tiles.size(), 1) * sizeof(TileDesc)));
+  if (!m->tiles.empty())
+    CUDA_TRY(cudaMemcpy(m->d_tiles, m->tiles.data(), m->tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&m->d_perm, na * sizeof(int)));
+  if (n_pad) CUDA_TRY(cudaMemcpy(m->d_perm, m->perm.data(), n_pad * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&m->d_wbase, na * sizeof(float)));
+  CUDA_TRY(cudaMemcpy(m->d_wbase, wbase.data(), na * sizeof(float), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&m->d_coeffs, std::max<size_t>(m->coeffs.size(), 1) * sizeof(float)));
+  if (!m->coeffs.empty())
+    CUDA_TRY(cudaMemcpy(m->d_coeffs, m->coeffs.data(), m->coeffs.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&m->d_flags, 4 * sizeof(int)));
+  CUDA_TRY(cudaMemset(m->d_flags, 0, 4 * sizeof(int)));
+  *out = m.release();
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_molecule_create(int natoms, const int32_t *Z, const float *pos, const float *occ,
+                                          const float *bfac, int delta_atoms, const float *beam,
+                                          spsim_b200_molecule **out) {
+  return molecule_create_impl<float>(natoms, Z, pos, occ, bfac, delta_atoms, beam, out);
+}
+
+extern "C" int spsim_b200_molecule_create_f64(int natoms, const int32_t *Z, const double *pos, const float *occ,
+                                              const float *bfac, int delta_atoms, const float *beam,
+                                              spsim_b200_molecule **out) {
+  return molecule_create_impl<double>(natoms, Z, pos, occ, bfac, delta_atoms, beam, out);
+}
+
+extern "C" int spsim_b200_molecule_update_device(spsim_b200_molecule *m, const void *pos_dev, int pos_is_f64,
+                                                 const float *occ_dev, const float *bfac_dev, void *stream) {
+  if (!m || !pos_dev) return fail(SPSIM_ERR_INVALID_ARG, "molecule or positions NULL");
+  if (bfac_dev && !m->per_atom_b)
+    return fail(SPSIM_ERR_INVALID_ARG, "molecule was created without per-atom B factors");
+  CUDA_TRY(launch_atoms_update(m->d_atoms, m->d_perm, m->n_padded, pos_is_f64 ? nullptr : (const float *)pos_dev,
+                               pos_is_f64 ? (const double *)pos_dev : nullptr, occ_dev, bfac_dev, m->d_wbase,
+                               m->center, m->dr, m->inv_dr, m->rbound, m->d_flags, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_molecule_natoms(const spsim_b200_molecule *m, int *natoms) {
+  if (!m || !natoms) return fail(SPSIM_ERR_INVALID_ARG, "NULL argument");
+  *natoms = m->natoms_in;
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_molecule_destroy(spsim_b200_molecule *m) {
+  delete m;
+  return SPSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// q sets
+
+struct spsim_b200_qset {
+  unsigned long long id = 0;
+  int device = 0;
+  long long npix = 0;
+  float *d_hkl = nullptr;
+  double *d_q64 = nullptr;
+  double qmax = 0;
+  ~spsim_b200_qset() {
+    cudaFree(d_hkl);
+    cudaFree(d_q64);
+  }
+};
+
+extern "C" int spsim_b200_qset_from_list(int64_t npix, const float *hkl, int memory, spsim_b200_qset **out) {
+  if (!out) return fail(SPSIM_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (npix < 0 || (npix > 0 && !hkl)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  std::unique_ptr<spsim_b200_qset> q(new spsim_b200_qset());
+  q->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
+  q->device = dev;
+  q->npix = npix;
+  const size_t bytes = 3 * (size_t)std::max<int64_t>(npix, 1) * sizeof(float);
+  CUDA_TRY(cudaMalloc(&q->d_hkl, bytes));
+  std::vector<float> h;
+  const float *hp = hkl;
+  if (memory == SPSIM_MEM_DEVICE) {
+    if (npix) CUDA_TRY(cudaMemcpy(q->d_hkl, hkl, 3 * npix * sizeof(float), cudaMemcpyDeviceToDevice));
+    h.resize(3 * npix);
+    if (npix) CUDA_TRY(cudaMemcpy(h.data(), hkl, 3 * npix * sizeof(float), cudaMemcpyDeviceToHost));
+    hp = h.data();
+  } else {
+    if (npix) CUDA_TRY(cudaMemcpy(q->d_hkl, hkl, 3 * npix * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  double qm2 = 0;
+  for (long long i = 0; i < npix; ++i) {
+    const double a = hp[3 * i], b = hp[3 * i + 1], c = hp[3 * i + 2];
+    qm2 = std::max(qm2, a * a + b * b + c * c);
+  }
+  q->qmax = std::sqrt(qm2);
+  *out = q.release();
+  return SPSIM_OK;
+}
+
+static double detector_qmax(int nx, int ny, float width, float height, float distance, float cx, float cy,
+                            float wavelength, int spherical) {
+  double m = 0;
+  const int xs[2] = {0, nx - 1}, ys[2] = {0, ny - 1};
+  const double pxs = (double)(width / nx), pys = (double)(height / ny);
+  const double fpx = 2 * std::sin(std::atan(pxs / distance) / 2) / wavelength;
+  const double fpy = 2 * std::sin(std::atan(pys / distance) / 2) / wavelength;
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      const double px = ((xs[a] - (nx - 1.0) / 2.0) / nx) * (double)width - cx;
+      const double py = ((ys[b] - (ny - 1.0) / 2.0) / ny) * (double)height - cy;
+      const double pz = distance;
+      double q0, q1, q2;
+      if (!spherical) {
+        const double p = std::sqrt(px * px + py * py + pz * pz);
+        const double ew = 1.0 / (double)wavelength;
+        q0 = px / p * ew;
+        q1 = py / p * ew;
+        q2 = (pz / p - 1.0) * ew;
+      } else {
+        q0 = fpx * px / pxs;
+        q1 = fpy * py / pys;
+        q2 = 0;
+      }
+      m = std::max(m, std::sqrt(q0 * q0 + q1 * q1 + q2 * q2));
+    }
+  return m * (1 + 1e-12);
+}
+
+static int check_detector(int nx, int ny, float width, float height, float distance, float wavelength) {
+  if (nx <= 0 || ny <= 0) return fail(SPSIM_ERR_INVALID_ARG, "detector has %d x %d pixels", nx, ny);
+  if (!(width > 0) || !(height > 0) || !(distance > 0) || !(wavelength > 0))
+    return fail(SPSIM_ERR_INVALID_ARG, "detector width/height/distance and wavelength must be > 0");
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_qset_from_detector(int nx, int ny, float width, float height, float distance,
+                                             float center_x, float center_y, float wavelength, int spherical,
+                                             spsim_b200_qset **out) {
+  if (!out) return fail(SPSIM_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  int st = check_detector(nx, ny, width, height, distance, wavelength);
+  if (st) return st;
+  int dev;
+  st = current_device(&dev);
+  if (st) return st;
+  std::unique_ptr<spsim_b200_qset> q(new spsim_b200_qset());
+  q->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
+  q->device = dev;
+  q->npix = (long long)nx * ny;
+  CUDA_TRY(cudaMalloc(&q->d_q64, 3 * q->npix * sizeof(double)));
+  CUDA_TRY(launch_ewald(nx, ny, width, height, distance, center_x, center_y, wavelength, spherical, nullptr,
+                        q->d_q64, 0));
+  CUDA_TRY(cudaDeviceSynchronize());
+  q->qmax = detector_qmax(nx, ny, width, height, distance, center_x, center_y, wavelength, spherical);
+  *out = q.release();
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_qset_npix(const spsim_b200_qset *qs, int64_t *npix) {
+  if (!qs || !npix) return fail(SPSIM_ERR_INVALID_ARG, "NULL argument");
+  *npix = qs->npix;
+  return SPSIM_OK;
+}
+
+__global__ static void q64_to_f32_kernel(const double *in, float *out, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (float)in[i];
+}
+
+extern "C" int spsim_b200_qset_copy_q(const spsim_b200_qset *qs, float *hkl_host) {
+  if (!qs || !hkl_host) return fail(SPSIM_ERR_INVALID_ARG, "NULL argument");
+  if (!qs->npix) return SPSIM_OK;
+  if (qs->d_hkl) {
+    CUDA_TRY(cudaMemcpy(hkl_host, qs->d_hkl, 3 * qs->npix * sizeof(float), cudaMemcpyDeviceToHost));
+    return SPSIM_OK;
+  }
+  float *tmp = nullptr;
+  CUDA_TRY(cudaMalloc(&tmp, 3 * qs->npix * sizeof(float)));
+  const long long n = 3 * qs->npix;
+  q64_to_f32_kernel<<<(unsigned)((n + 255) / 256), 256>>>(qs->d_q64, tmp, n);
+  cudaError_t e = cudaMemcpy(hkl_host, tmp, n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(SPSIM_ERR_CUDA, "copy q: %s", cudaGetErrorString(e));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_qset_destroy(spsim_b200_qset *qs) {
+  delete qs;
+  return SPSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// forward planning
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  ~DevBuf() { cudaFree(p); }
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+};
+
+struct Plan {
+  // key
+  std::vector<const void *> key_ptrs;
+  std::vector<double> key_vals;
+  // device state
+  DevBuf pats, items, acc, ff, flags;
+  int n_items = 0, grid = 0, npat = 0;
+  long long max_npix = 0;
+  double terms = 0;
+  int precision = 0, nt = 128, ppt = 4;
+  bool perb = false;
+  std::vector<long long> npix_of;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~Plan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+static std::vector<std::unique_ptr<Plan>> g_plans;  // most recent last
+static const size_t kMaxPlans = 8;
+static int g_force_nt = -1, g_force_p = -1;
+static std::map<long long, std::pair<int, int>> g_tuned;  // size class -> (nt, p)
+static bool g_timing = false;
+static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timing_events;
+static thread_local double g_last_terms = 0, g_last_ms = 0;
+static int g_num_sms = 0;
+
+static int num_sms() {
+  if (!g_num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+static long long size_class(double terms) { return (long long)std::floor(std::log2(std::max(terms, 1.0)) / 2); }
+
+static void choose_variant(double terms, long long min_npix, int precision, int *nt, int *p) {
+  if (g_force_nt > 0 && sf_f32_variant_exists(precision == SPSIM_PREC_F32_FAST ? 1 : 0, g_force_nt, g_force_p)) {
+    *nt = g_force_nt;
+    *p = g_force_p;
+    return;
+  }
+  auto it = g_tuned.find(size_class(terms) * 4 + precision);
+  if (it != g_tuned.end()) {
+    *nt = it->second.first;
+    *p = it->second.second;
+    return;
+  }
+  *nt = 128;
+  *p = (min_npix >= 65536) ? 4 : 2;
+}
+
+static bool is_orthonormal(const double *R) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double d = 0;
+      for (int k = 0; k < 3; ++k) d += R[3 * k + i] * R[3 * k + j];
+      if (std::fabs(d - (i == j ? 1.0 : 0.0)) > 1e-6) return false;
+    }
+  return true;
+}
+
+static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
+                      const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
+                      cudaStream_t stream) {
+  pl.npat = npat;
+  pl.precision = precision;
+  std::vector<SfPattern> pats(npat);
+  // unique (molecule, q set) pairs share one form-factor table
+  std::map<std::pair<const void *, const void *>, size_t> ff_off;
+  size_t ff_total = 0, acc_total = 0;
+  std::vector<size_t> acc_off(npat), ffo(npat);
+  double terms = 0;
+  long long min_npix = -1;
+  bool perb = false;
+  for (int i = 0; i < npat; ++i) {
+    const spsim_b200_molecule *m = mols[i];
+    const spsim_b200_qset *q = qsets[i];
+    if (!m || !q) return fail(SPSIM_ERR_INVALID_ARG, "pattern %d: NULL molecule or q set", i);
+    auto key = std::make_pair((const void *)m, (const void *)q);
+    auto f = ff_off.find(key);
+    if (f == ff_off.end()) {
+      ff_off[key] = ff_total;
+      ffo[i] = ff_total;
+      ff_total += (size_t)m->n_elem * q->npix;
+    } else {
+      ffo[i] = f->second;
+    }
+    acc_off[i] = acc_total;
+    acc_total += q->npix;
+    terms += (double)q->npix * m->n_kept;
+    min_npix = min_npix < 0 ? q->npix : std::min(min_npix, q->npix);
+    perb = perb || m->per_atom_b;
+  }
+  pl.terms = terms;
+  pl.perb = perb;
+  CUDA_TRY(pl.acc.ensure(std::max<size_t>(acc_total, 1) * sizeof(double2)));
+  CUDA_TRY(pl.ff.ensure(std::max<size_t>(ff_total, 1) * sizeof(double)));
+  CUDA_TRY(pl.flags.ensure(64));
+  CUDA_TRY(pl.pats.ensure(std::max(npat, 1) * sizeof(SfPattern)));
+
+  int nt = 128, ppt = 4;
+  if (precision != SPSIM_PREC_FP64) choose_variant(terms, min_npix, precision, &nt, &ppt);
+  pl.nt = nt;
+  pl.ppt = ppt;
+  const long long tile_pix = (long long)nt * ppt;
+
+  pl.max_npix = 0;
+  pl.npix_of.resize(npat);
+  for (int i = 0; i < npat; ++i) {
+    const spsim_b200_molecule *m = mols[i];
+    const spsim_b200_qset *q = qsets[i];
+    SfPattern &pt = pats[i];
+    memset(&pt, 0, sizeof(pt));
+    pt.atoms = m->d_atoms;
+    pt.tiles = m->d_tiles;
+    pt.n_tiles = (int)m->tiles.size();
+    pt.n_elem = m->n_elem;
+    pt.per_atom_b = m->per_atom_b;
+    pt.ff = (double *)pl.ff.p + ffo[i];
+    pt.npix = q->npix;
+    pt.hkl = q->d_hkl;
+    pt.q64 = q->d_q64;
+    double qmax = q->qmax;
+    if (rot) {
+      const double *R = rot + 9 * (size_t)i;
+      memcpy(pt.rot, R, 9 * sizeof(double));
+      pt.has_rot = 1;
+      if (!is_orthonormal(R)) {
+        double fro = 0;
+        for (int k = 0; k < 9; ++k) fro += R[k] * R[k];
+        qmax *= std::sqrt(fro);
+      }
+    } else {
+      pt.has_rot = 0;
+      for (int k = 0; k < 9; ++k) pt.rot[k] = (k % 4 == 0) ? 1.0 : 0.0;
+    }
+    memcpy(pt.center, m->center, sizeof(pt.center));
+    const int eq = ceil_log2_bound(std::max(qmax, 1e-300));
+    const int kq = 22 - m->kr;
+    pt.dq = (float)std::ldexp(1.0, eq - kq);
+    pt.inv_dq = (float)std::ldexp(1.0, kq - eq);
+    pt.acc = (double2 *)pl.acc.p + acc_off[i];
+    pt.F = F_dev ? (float2 *)F_dev[i] : nullptr;
+    pt.I = I_dev ? I_dev[i] : nullptr;
+    pl.max_npix = std::max(pl.max_npix, q->npix);
+    pl.npix_of[i] = q->npix;
+    if (precision != SPSIM_PREC_FP64 && m->n_kept > 0 && q->npix > 0) {
+      // domain checks of the compensated phase
+      const double qr = qmax * m->rbound;
+      if (qr >= std::ldexp(1.0, 19))
+        return fail(SPSIM_ERR_RANGE, "pattern %d: |q|max*|r|max = %.3g cycles exceeds 2^19; use SPSIM_PREC_FP64", i, qr);
+      const double cmax = 0.8660254037844386 * (qmax * m->dr + (double)pt.dq * (m->rbound + m->dr));
+      const double lim = precision == SPSIM_PREC_F32 ? 1.0 / 16 : 0.25;
+      if (cmax > lim)
+        return fail(SPSIM_ERR_RANGE,
+                    "pattern %d: phase cross term %.4f cycles exceeds %.4f (|q|max %.3g 1/m, |r|max %.3g m); use "
+                    "SPSIM_PREC_FP64",
+                    i, cmax, lim, qmax, m->rbound);
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(pl.pats.p, pats.data(), npat * sizeof(SfPattern), cudaMemcpyHostToDevice, stream));
+
+  if (precision != SPSIM_PREC_FP64) {
+    // work items: pixel tile x atom-tile range, cost-sorted (largest first)
+    const int occ = std::max(1, sf_f32_occupancy(precision == SPSIM_PREC_F32_FAST ? 1 : 0, nt, ppt, perb));
+    const long long slots = (long long)num_sms() * occ;
+    long long total_ptiles = 0;
+    for (int i = 0; i < npat; ++i) total_ptiles += (qsets[i]->npix + tile_pix - 1) / tile_pix;
+    // split atoms when pixel tiles alone cannot fill the GPU several times over
+    const long long want = 6 * slots;
+    std::vector<WorkItem> items;
+    std::vector<double> cost;
+    for (int i = 0; i < npat; ++i) {
+      const long long nptile = (qsets[i]->npix + tile_pix - 1) / tile_pix;
+      const int ntile = (int)mols[i]->tiles.size();
+      if (ntile == 0 || qsets[i]->npix == 0) continue;
+      int split = 1;
+      if (total_ptiles < want) split = (int)std::min<long long>((want + total_ptiles - 1) / total_ptiles, ntile);
+      split = std::max(1, std::min(split, std::max(1, ntile / 2)));
+      for (long long t = 0; t < nptile; ++t) {
+        const long long pix_here = std::min(tile_pix, qsets[i]->npix - t * tile_pix);
+        for (int s = 0; s < split; ++s) {
+          WorkItem w;
+          w.pattern = i;
+          w.pixel_tile = (int)t;
+          w.k0 = (int)((long long)ntile * s / split);
+          w.k1 = (int)((long long)ntile * (s + 1) / split);
+          if (w.k1 <= w.k0) continue;
+          items.push_back(w);
+          int atoms_here = 0;
+          for (int k = w.k0; k < w.k1; ++k) atoms_here += mols[i]->tiles[k].count;
+          cost.push_back((double)pix_here * atoms_here);
+        }
+      }
+    }
+    std::vector<size_t> order(items.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+    std::vector<WorkItem> sorted(items.size());
+    for (size_t k = 0; k < order.size(); ++k) sorted[k] = items[order[k]];
+    pl.n_items = (int)sorted.size();
+    pl.grid = (int)std::min<long long>(std::max(pl.n_items, 1), slots);
+    CUDA_TRY(pl.items.ensure(std::max<size_t>(sorted.size(), 1) * sizeof(WorkItem)));
+    if (!sorted.empty())
+      CUDA_TRY(cudaMemcpyAsync(pl.items.p, sorted.data(), sorted.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
+                               stream));
+  }
+  // form-factor tables (per unique molecule / q set pair; fixed for the plan's life)
+  std::map<std::pair<const void *, const void *>, bool> done;
+  for (int i = 0; i < npat; ++i) {
+    auto key = std::make_pair((const void *)mols[i], (const void *)qsets[i]);
+    if (done[key]) continue;
+    done[key] = true;
+    const spsim_b200_qset *q = qsets[i];
+    CUDA_TRY(launch_ff_table(q->d_hkl, q->d_q64, q->npix, mols[i]->n_elem, mols[i]->d_coeffs, (double)B,
+                             mols[i]->delta_atoms, (double *)pl.ff.p + ffo[i], stream));
+  }
+  return SPSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// enqueue, plan cache, forward entry points
+
+static cudaError_t enqueue_plan(Plan &pl, cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1) {
+  cudaError_t e;
+  long long acc_total = 0;
+  for (long long n : pl.npix_of) acc_total += n;
+  if ((e = cudaMemsetAsync(pl.acc.p, 0, std::max<long long>(acc_total, 1) * sizeof(double2), stream))) return e;
+  if ((e = cudaMemsetAsync(pl.flags.p, 0, sizeof(int), stream))) return e;  // work queue head
+  if (ev0 && (e = cudaEventRecord(ev0, stream))) return e;
+  if (pl.precision == SPSIM_PREC_FP64) {
+    for (int i = 0; i < pl.npat; ++i)
+      if ((e = launch_sf_f64((const SfPattern *)pl.pats.p, i, pl.npix_of[i], stream))) return e;
+  } else if (pl.n_items > 0) {
+    const int mode = pl.precision == SPSIM_PREC_F32_FAST ? PREC_MODE_MUFU : PREC_MODE_POLY;
+    int *flags = (int *)pl.flags.p;
+    if ((e = launch_sf_f32(mode, pl.nt, pl.ppt, pl.perb, (const SfPattern *)pl.pats.p, (const WorkItem *)pl.items.p,
+                           pl.n_items, flags, flags + 4, pl.grid, stream)))
+      return e;
+  }
+  if (ev1 && (e = cudaEventRecord(ev1, stream))) return e;
+  return launch_finalize((const SfPattern *)pl.pats.p, 0, pl.npat, pl.max_npix, stream);
+}
+
+static void plan_key(int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
+                     const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
+                     std::vector<const void *> &kp, std::vector<double> &kv) {
+  kv.push_back(npat);
+  kv.push_back(B);
+  kv.push_back(precision);
+  kv.push_back(g_force_nt);
+  kv.push_back(g_force_p);
+  for (int i = 0; i < npat; ++i) {
+    kv.push_back((double)(mols[i] ? mols[i]->id : 0));
+    kv.push_back((double)(qsets[i] ? qsets[i]->id : 0));
+    kp.push_back(F_dev ? (const void *)F_dev[i] : nullptr);
+    kp.push_back(I_dev ? (const void *)I_dev[i] : nullptr);
+  }
+  if (rot)
+    for (long long k = 0; k < 9LL * npat; ++k) kv.push_back(rot[k]);
+  else
+    kv.push_back(-7.0);
+}
+
+static int check_flags(Plan &pl) {
+  int h[8] = {0};
+  CUDA_TRY(cudaMemcpy(h, pl.flags.p, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h[4]) {
+    int z = 0;
+    cudaMemcpy((int *)pl.flags.p + 4, &z, sizeof(int), cudaMemcpyHostToDevice);
+    return fail(SPSIM_ERR_TIMEOUT, "structure-factor kernel: an atom-tile copy did not complete in time");
+  }
+  return SPSIM_OK;
+}
+
+// cache == false: a one-shot plan (host convenience path), synchronised before return
+static int run_forward(int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
+                       const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
+                       cudaStream_t stream, bool cache) {
+  if (npat < 0) return fail(SPSIM_ERR_INVALID_ARG, "npatterns < 0");
+  if (npat == 0) return SPSIM_OK;
+  if (!mols || !qsets) return fail(SPSIM_ERR_INVALID_ARG, "NULL molecule or q-set array");
+  if (precision < SPSIM_PREC_FP64 || precision > SPSIM_PREC_F32_FAST)
+    return fail(SPSIM_ERR_INVALID_ARG, "unknown precision %d", precision);
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  for (int i = 0; i < npat; ++i) {
+    if (!mols[i] || !qsets[i]) return fail(SPSIM_ERR_INVALID_ARG, "pattern %d: NULL handle", i);
+    if (mols[i]->device != dev || qsets[i]->device != dev)
+      return fail(SPSIM_ERR_INVALID_ARG, "pattern %d: handle belongs to another device", i);
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  std::vector<const void *> kp;
+  std::vector<double> kv;
+  plan_key(npat, mols, qsets, rot, B, precision, F_dev, I_dev, kp, kv);
+  Plan *pl = nullptr;
+  std::unique_ptr<Plan> oneshot;
+  if (cache) {
+    for (size_t i = 0; i < g_plans.size(); ++i) {
+      if (g_plans[i]->key_ptrs == kp && g_plans[i]->key_vals == kv) {
+        std::unique_ptr<Plan> p = std::move(g_plans[i]);
+        g_plans.erase(g_plans.begin() + i);
+        g_plans.push_back(std::move(p));
+        pl = g_plans.back().get();
+        break;
+      }
+    }
+  }
+  if (!pl) {
+    std::unique_ptr<Plan> np(new Plan());
+    np->key_ptrs = kp;
+    np->key_vals = kv;
+    st = build_plan(*np, npat, mols, qsets, rot, B, precision, F_dev, I_dev, stream);
+    if (st) return st;
+    if (cache) {
+      if (g_plans.size() >= kMaxPlans) {
+        cudaDeviceSynchronize();  // the evicted plan's buffers may still be in use
+        g_plans.erase(g_plans.begin());
+      }
+      g_plans.push_back(std::move(np));
+      pl = g_plans.back().get();
+    } else {
+      oneshot = std::move(np);
+      pl = oneshot.get();
+    }
+  }
+  g_last_terms = pl->terms;
+  if (g_timing || !cache || stream == nullptr) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (g_timing) {
+      CUDA_TRY(cudaEventCreate(&e0));
+      CUDA_TRY(cudaEventCreate(&e1));
+      g_timing_events.push_back({e0, e1});
+    }
+    CUDA_TRY(enqueue_plan(*pl, stream, e0, e1));
+  } else {
+    if (!pl->exec) {
+      CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      cudaError_t ce = enqueue_plan(*pl, stream, nullptr, nullptr);
+      cudaGraph_t g = nullptr;
+      cudaError_t ee = cudaStreamEndCapture(stream, &g);
+      if (ce != cudaSuccess) return fail(SPSIM_ERR_CUDA, "capture: %s", cudaGetErrorString(ce));
+      if (ee != cudaSuccess) return fail(SPSIM_ERR_CUDA, "end capture: %s", cudaGetErrorString(ee));
+      pl->graph = g;
+      CUDA_TRY(cudaGraphInstantiate(&pl->exec, g, 0));
+    }
+    CUDA_TRY(cudaGraphLaunch(pl->exec, stream));
+  }
+  if (!cache) {
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    return check_flags(*pl);
+  }
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot,
+                                  float B, int precision, float *F_dev, float *I_dev, void *stream) {
+  float *F[1] = {F_dev};
+  float *I[1] = {I_dev};
+  return run_forward(1, &m, &qs, rot, B, precision, F, I, (cudaStream_t)stream, true);
+}
+
+extern "C" int spsim_b200_forward_batch(int npatterns, const spsim_b200_molecule *const *mols,
+                                        const spsim_b200_qset *const *qsets, const double *rot, float B, int precision,
+                                        float *const *F_dev, float *const *I_dev, void *stream) {
+  return run_forward(npatterns, mols, qsets, rot, B, precision, F_dev, I_dev, (cudaStream_t)stream, true);
+}
+
+extern "C" int spsim_b200_structure_factor_host(int natoms, const int32_t *Z, const float *pos, const float *occ,
+                                                const float *bfac, float B, int delta_atoms, const float *beam,
+                                                int64_t npix, const float *hkl, int precision, float *F_host,
+                                                float *I_host) {
+  if (npix < 0 || (npix > 0 && !hkl)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
+  spsim_b200_molecule *m = nullptr;
+  spsim_b200_qset *q = nullptr;
+  int st = spsim_b200_molecule_create(natoms, Z, pos, occ, bfac, delta_atoms, beam, &m);
+  if (st) return st;
+  st = spsim_b200_qset_from_list(npix, hkl, SPSIM_MEM_HOST, &q);
+  if (st) {
+    spsim_b200_molecule_destroy(m);
+    return st;
+  }
+  float *dF = nullptr, *dI = nullptr;
+  cudaError_t e = cudaMalloc(&dF, 2 * std::max<int64_t>(npix, 1) * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dI, std::max<int64_t>(npix, 1) * sizeof(float));
+  if (e != cudaSuccess) {
+    st = fail(SPSIM_ERR_OUT_OF_MEMORY, "device buffers: %s", cudaGetErrorString(e));
+  } else {
+    float *F[1] = {F_host ? dF : nullptr};
+    float *I[1] = {I_host ? dI : nullptr};
+    const spsim_b200_molecule *mm = m;
+    const spsim_b200_qset *qq = q;
+    st = run_forward(1, &mm, &qq, nullptr, B, precision, F, I, nullptr, false);
+    if (!st && F_host && npix)
+      if ((e = cudaMemcpy(F_host, dF, 2 * npix * sizeof(float), cudaMemcpyDeviceToHost)))
+        st = fail(SPSIM_ERR_CUDA, "copy F: %s", cudaGetErrorString(e));
+    if (!st && I_host && npix)
+      if ((e = cudaMemcpy(I_host, dI, npix * sizeof(float), cudaMemcpyDeviceToHost)))
+        st = fail(SPSIM_ERR_CUDA, "copy I: %s", cudaGetErrorString(e));
+  }
+  cudaFree(dF);
+  cudaFree(dI);
+  spsim_b200_qset_destroy(q);
+  spsim_b200_molecule_destroy(m);
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// completion, timing, statistics, variants
+
+extern "C" int spsim_b200_synchronize(void *stream) {
+  CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (auto &p : g_plans) {
+    int st = check_flags(*p);
+    if (st) return st;
+  }
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_timing_enable(int enable) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_timing = enable != 0;
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_timing_read(double *ms, int cap, int *n) {
+  if (!n) return fail(SPSIM_ERR_INVALID_ARG, "n is NULL");
+  std::lock_guard<std::mutex> lk(g_mu);
+  int k = 0;
+  for (auto &pr : g_timing_events) {
+    float t = 0;
+    CUDA_TRY(cudaEventSynchronize(pr.second));
+    CUDA_TRY(cudaEventElapsedTime(&t, pr.first, pr.second));
+    if (ms && k < cap) ms[k] = t;
+    ++k;
+    g_last_ms = t;
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  g_timing_events.clear();
+  *n = std::min(k, cap);
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_last_forward_stats(double *terms, double *kernel_ms) {
+  if (terms) *terms = g_last_terms;
+  if (kernel_ms) *kernel_ms = g_last_ms;
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_set_variant(int threads, int pixels_per_thread) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (threads < 0) {
+    g_force_nt = g_force_p = -1;
+    return SPSIM_OK;
+  }
+  if (!sf_f32_variant_exists(0, threads, pixels_per_thread))
+    return fail(SPSIM_ERR_INVALID_ARG, "no compiled variant with %d threads x %d pixels", threads, pixels_per_thread);
+  g_force_nt = threads;
+  g_force_p = pixels_per_thread;
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision,
+                                   void *stream, int *best_threads, int *best_pixels_per_thread) {
+  if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
+  if (precision == SPSIM_PREC_FP64) return fail(SPSIM_ERR_INVALID_ARG, "the FP64 kernel has a single variant");
+  const int cand[][2] = {{128, 2}, {128, 4}, {256, 2}, {256, 4}};
+  float *dI = nullptr;
+  CUDA_TRY(cudaMalloc(&dI, std::max<long long>(qs->npix, 1) * sizeof(float)));
+  float best = 1e30f;
+  int bt = 128, bp = 4;
+  const int saved_nt = g_force_nt, saved_p = g_force_p;
+  const bool saved_timing = g_timing;
+  int st = SPSIM_OK;
+  for (auto &c : cand) {
+    g_force_nt = c[0];
+    g_force_p = c[1];
+    float *I[1] = {dI};
+    float *F[1] = {nullptr};
+    const spsim_b200_molecule *mm = m;
+    const spsim_b200_qset *qq = qs;
+    // warm-up, then three timed launches
+    st = run_forward(1, &mm, &qq, nullptr, 0.0f, precision, F, I, (cudaStream_t)stream, false);
+    if (st) break;
+    float tot = 0;
+    for (int r = 0; r < 3 && !st; ++r) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, (cudaStream_t)stream);
+      st = run_forward(1, &mm, &qq, nullptr, 0.0f, precision, F, I, (cudaStream_t)stream, false);
+      cudaEventRecord(b, (cudaStream_t)stream);
+      cudaEventSynchronize(b);
+      float t = 0;
+      cudaEventElapsedTime(&t, a, b);
+      tot += t;
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+    if (st) break;
+    if (tot < best) {
+      best = tot;
+      bt = c[0];
+      bp = c[1];
+    }
+  }
+  g_force_nt = saved_nt;
+  g_force_p = saved_p;
+  g_timing = saved_timing;
+  cudaFree(dI);
+  if (st) return st;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_tuned[size_class((double)qs->npix * m->n_kept) * 4 + precision] = {bt, bp};
+  }
+  if (best_threads) *best_threads = bt;
+  if (best_pixels_per_thread) *best_pixels_per_thread = bp;
+  return SPSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// geometry and detector chain
+
+extern "C" int spsim_b200_hkl_for_detector(int nx, int ny, float width, float height, float distance,
+                                           float center_x, float center_y, float wavelength, int spherical,
+                                           float *hkl_dev, void *stream) {
+  int st = check_detector(nx, ny, width, height, distance, wavelength);
+  if (st) return st;
+  if (!hkl_dev) return fail(SPSIM_ERR_INVALID_ARG, "output is NULL");
+  CUDA_TRY(launch_ewald(nx, ny, width, height, distance, center_x, center_y, wavelength, spherical, hkl_dev, nullptr,
+                        (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+static int chain_dev(const spsim_b200_chain_params *p, ChainDev *c) {
+  if (!p) return fail(SPSIM_ERR_INVALID_ARG, "params is NULL");
+  if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0) return fail(SPSIM_ERR_INVALID_ARG, "detector size must be > 0");
+  if (p->binning_x <= 0 || p->binning_y <= 0 || p->binning_z <= 0)
+    return fail(SPSIM_ERR_INVALID_ARG, "binning must be >= 1");
+  memset(c, 0, sizeof(*c));
+  c->nx = p->nx;
+  c->ny = p->ny;
+  c->nz = p->nz;
+  c->bx = p->binning_x;
+  c->by = p->binning_y;
+  c->bz = p->binning_z;
+  c->spherical = p->spherical;
+  c->polarization = p->polarization;
+  c->unbinned = (c->bx == 1 && c->by == 1 && c->bz == 1);
+  c->clamp = p->clamp_to_maximum;
+  c->width = p->width;
+  c->height = p->height;
+  c->distance = p->distance;
+  c->cx = p->center_x;
+  c->cy = p->center_y;
+  c->pw = p->pixel_width;
+  c->ph = p->pixel_height;
+  c->beam_intensity = p->beam_intensity;
+  c->qe = p->quantum_efficiency;
+  // src/amplification.c:56-61 and :121-123
+  const double h_c = 1.98644521e-25;
+  const double photon_energy = h_c / (double)p->wavelength;
+  c->epp = 1.0f;
+  if (p->electron_hole_production_energy) c->epp = (float)(photon_energy / (double)p->electron_hole_production_energy);
+  c->epp_noiseless = (float)(photon_energy / (double)p->electron_hole_production_energy);
+  c->dark_t = p->dark_current * p->exposure_time;
+  c->readout = p->readout_noise;
+  c->adc = 1.0f;
+  if (p->linear_full_well && p->maximum_value) c->adc = p->maximum_value / p->linear_full_well;
+  c->maxv = p->maximum_value;
+  c->seed = p->seed;
+  c->pattern = p->pattern_index;
+  return SPSIM_OK;
+}
+
+static DevBuf g_chain_ph, g_chain_el;
+
+extern "C" int spsim_b200_detector_chain(const spsim_b200_chain_params *p, const float *I_dev,
+                                         const spsim_b200_chain_outputs *out, void *stream) {
+  ChainDev c;
+  int st = chain_dev(p, &c);
+  if (st) return st;
+  if (!out) return fail(SPSIM_ERR_INVALID_ARG, "outputs is NULL");
+  const bool needs_I = out->photons_per_pixel || out->photon_count || out->electrons_per_pixel || out->real_output ||
+                       out->noiseless_output;
+  if (needs_I && !I_dev) return fail(SPSIM_ERR_INVALID_ARG, "intensities are NULL");
+  ChainOut o = {out->thomson_correction, out->solid_angle,  out->photons_per_pixel, out->photon_count,
+                out->electrons_per_pixel, out->real_output, out->noiseless_output};
+  float *sph = nullptr, *sel = nullptr;
+  const size_t n = (size_t)p->nx * p->ny * p->nz;
+  if (!c.unbinned) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    CUDA_TRY(g_chain_ph.ensure(n * sizeof(float)));
+    CUDA_TRY(g_chain_el.ensure(n * sizeof(float)));
+    sph = (float *)g_chain_ph.p;
+    sel = (float *)g_chain_el.p;
+  }
+  CUDA_TRY(launch_chain(c, I_dev, o, sph, sel, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_thomson(const spsim_b200_chain_params *p, float *out_dev, void *stream) {
+  spsim_b200_chain_outputs o;
+  memset(&o, 0, sizeof(o));
+  o.thomson_correction = out_dev;
+  return spsim_b200_detector_chain(p, nullptr, &o, stream);
+}
+
+extern "C" int spsim_b200_solid_angle(const spsim_b200_chain_params *p, float *out_dev, void *stream) {
+  spsim_b200_chain_outputs o;
+  memset(&o, 0, sizeof(o));
+  o.solid_angle = out_dev;
+  return spsim_b200_detector_chain(p, nullptr, &o, stream);
+}
+
+extern "C" int spsim_b200_poisson(int64_t n, const float *lambda_dev, uint64_t seed, uint32_t pattern_index,
+                                  float *photon_count_dev, void *stream) {
+  if (n < 0 || (n > 0 && (!lambda_dev || !photon_count_dev))) return fail(SPSIM_ERR_INVALID_ARG, "bad arrays");
+  CUDA_TRY(launch_poisson(n, lambda_dev, seed, pattern_index, photon_count_dev, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_photons(int64_t n, const float *thomson_dev, const float *solid_angle_dev,
+                                  const float *I_dev, float beam_intensity, float *photons_dev, void *stream) {
+  if (n < 0 || (n > 0 && (!thomson_dev || !solid_angle_dev || !I_dev || !photons_dev)))
+    return fail(SPSIM_ERR_INVALID_ARG, "bad arrays");
+  CUDA_TRY(launch_photons(n, thomson_dev, solid_angle_dev, I_dev, beam_intensity, photons_dev, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_photon_counts(const spsim_b200_chain_params *p, const float *photons_dev,
+                                        float *counts_dev, void *stream) {
+  ChainDev c;
+  int st = chain_dev(p, &c);
+  if (st) return st;
+  if (!photons_dev || !counts_dev) return fail(SPSIM_ERR_INVALID_ARG, "bad arrays");
+  CUDA_TRY(launch_counts(c, photons_dev, counts_dev, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_electrons(const spsim_b200_chain_params *p, const float *counts_dev, float *electrons_dev,
+                                    void *stream) {
+  ChainDev c;
+  int st = chain_dev(p, &c);
+  if (st) return st;
+  if (!counts_dev || !electrons_dev) return fail(SPSIM_ERR_INVALID_ARG, "bad arrays");
+  CUDA_TRY(launch_electrons(c, counts_dev, electrons_dev, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_binned_outputs(const spsim_b200_chain_params *p, const float *electrons_dev,
+                                         const float *photons_dev, float *real_output_dev,
+                                         float *noiseless_output_dev, void *stream) {
+  ChainDev c;
+  int st = chain_dev(p, &c);
+  if (st) return st;
+  if ((real_output_dev && !electrons_dev) || (noiseless_output_dev && !photons_dev))
+    return fail(SPSIM_ERR_INVALID_ARG, "an output needs its input array");
+  CUDA_TRY(launch_binned(c, electrons_dev, photons_dev, real_output_dev, noiseless_output_dev, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// adjoint
+
+extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int npat,
+                                  const double *rot, float B, int precision, const float *F_dev, const float *G_dev,
+                                  double *dpos_dev, double *docc_dev, double *dB_dev, void *stream) {
+  if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
+  if (npat <= 0) return fail(SPSIM_ERR_INVALID_ARG, "npat must be > 0");
+  if (!F_dev || !G_dev || !dpos_dev) return fail(SPSIM_ERR_INVALID_ARG, "F, G and dpos are required");
+  if (precision < SPSIM_PREC_FP64 || precision > SPSIM_PREC_F32_FAST)
+    return fail(SPSIM_ERR_INVALID_ARG, "unknown precision %d", precision);
+  if (dB_dev && !m->per_atom_b) return fail(SPSIM_ERR_INVALID_ARG, "dB needs a molecule with per-atom B factors");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long npix = qs->npix;
+  const long long total = npix * npat;
+  double qmax = qs->qmax;
+  if (rot) {
+    for (int i = 0; i < npat; ++i)
+      if (!is_orthonormal(rot + 9 * (size_t)i)) {
+        double fro = 0;
+        for (int k = 0; k < 9; ++k) fro += rot[9 * (size_t)i + k] * rot[9 * (size_t)i + k];
+        qmax = std::max(qmax, qs->qmax * std::sqrt(fro));
+      }
+  }
+  const int eq = ceil_log2_bound(std::max(qmax, 1e-300));
+  const int kq = 22 - m->kr;
+  const float dq = (float)std::ldexp(1.0, eq - kq);
+  if (precision != SPSIM_PREC_FP64 && m->n_kept > 0) {
+    const double cmax = 0.8660254037844386 * (qmax * m->dr + (double)dq * (m->rbound + m->dr));
+    const double lim = precision == SPSIM_PREC_F32 ? 1.0 / 16 : 0.25;
+    if (qmax * m->rbound >= std::ldexp(1.0, 19) || cmax > lim)
+      return fail(SPSIM_ERR_RANGE, "adjoint: phase range outside the FP32 kernel's domain; use SPSIM_PREC_FP64");
+  }
+  CUDA_TRY(cudaMemsetAsync(dpos_dev, 0, 3 * (size_t)m->natoms_in * sizeof(double), st));
+  if (docc_dev) CUDA_TRY(cudaMemsetAsync(docc_dev, 0, (size_t)m->natoms_in * sizeof(double), st));
+  if (dB_dev) CUDA_TRY(cudaMemsetAsync(dB_dev, 0, (size_t)m->natoms_in * sizeof(double), st));
+  if (m->n_kept == 0 || total == 0) return SPSIM_OK;
+
+  // atom blocks (single element each) x pixel chunks
+  const int block_atoms = precision == SPSIM_PREC_FP64 ? ADJ_THREADS : ADJ_BLOCK_ATOMS;
+  std::vector<AdjBlock> blocks;
+  {
+    int e = -1, seg0 = 0;
+    for (size_t k = 0; k <= m->tiles.size(); ++k) {
+      const bool end = k == m->tiles.size();
+      if (end || m->tiles[k].elem != e) {
+        if (e >= 0) {
+          const int seg1 = m->tiles[k - 1].atom_begin + m->tiles[k - 1].count;
+          for (int a = seg0; a < seg1; a += block_atoms) blocks.push_back({a, std::min(a + block_atoms, seg1), e, 0});
+        }
+        if (!end) {
+          e = m->tiles[k].elem;
+          seg0 = m->tiles[k].atom_begin;
+        }
+      }
+    }
+  }
+  const long long want = 8LL * num_sms();
+  long long nchunk = std::max<long long>(1, (want + (long long)blocks.size() - 1) / (long long)blocks.size());
+  long long chunk = (total + nchunk - 1) / nchunk;
+  chunk = (chunk + 255) / 256 * 256;
+  std::vector<AdjItem> items;
+  for (size_t b = 0; b < blocks.size(); ++b)
+    for (long long p0 = 0; p0 < total; p0 += chunk) items.push_back({(int)b, 0, p0, std::min(total, p0 + chunk)});
+
+  void *d_ff = nullptr, *d_blocks = nullptr, *d_items = nullptr, *d_rot = nullptr;
+  CUDA_TRY(cudaMallocAsync(&d_ff, std::max<size_t>((size_t)m->n_elem * npix, 1) * sizeof(double), st));
+  CUDA_TRY(cudaMallocAsync(&d_blocks, blocks.size() * sizeof(AdjBlock), st));
+  CUDA_TRY(cudaMallocAsync(&d_items, items.size() * sizeof(AdjItem), st));
+  CUDA_TRY(cudaMemcpyAsync(d_blocks, blocks.data(), blocks.size() * sizeof(AdjBlock), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(AdjItem), cudaMemcpyHostToDevice, st));
+  if (rot) {
+    CUDA_TRY(cudaMallocAsync(&d_rot, 9 * (size_t)npat * sizeof(double), st));
+    CUDA_TRY(cudaMemcpyAsync(d_rot, rot, 9 * (size_t)npat * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  CUDA_TRY(launch_ff_table(qs->d_hkl, qs->d_q64, npix, m->n_elem, m->d_coeffs, (double)B, m->delta_atoms,
+                           (double *)d_ff, st));
+  AdjParams prm;
+  memset(&prm, 0, sizeof(prm));
+  prm.atoms = m->d_atoms;
+  prm.perm = m->d_perm;
+  prm.wbase = m->d_wbase;
+  prm.blocks = (const AdjBlock *)d_blocks;
+  prm.items = (const AdjItem *)d_items;
+  prm.hkl = qs->d_hkl;
+  prm.q64 = qs->d_q64;
+  prm.rot = (const double *)d_rot;
+  prm.ff = (const double *)d_ff;
+  prm.F = (const float2 *)F_dev;
+  prm.G = G_dev;
+  prm.npix = npix;
+  prm.cx = m->center[0];
+  prm.cy = m->center[1];
+  prm.cz = m->center[2];
+  prm.dq = dq;
+  prm.inv_dq = (float)std::ldexp(1.0, kq - eq);
+  prm.per_atom_b = m->per_atom_b;
+  prm.dpos = dpos_dev;
+  prm.docc = docc_dev;
+  prm.dB = dB_dev;
+  const int mode = precision == SPSIM_PREC_FP64 ? 2 : (precision == SPSIM_PREC_F32_FAST ? 1 : 0);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (g_timing) {
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    CUDA_TRY(cudaEventRecord(e0, st));
+  }
+  CUDA_TRY(launch_adjoint(mode, prm, (int)items.size(), st));
+  if (g_timing) {
+    CUDA_TRY(cudaEventRecord(e1, st));
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_timing_events.push_back({e0, e1});
+  }
+  cudaFreeAsync(d_ff, st);
+  cudaFreeAsync(d_blocks, st);
+  cudaFreeAsync(d_items, st);
+  if (d_rot) cudaFreeAsync(d_rot, st);
+  return SPSIM_OK;
+}

@@ -1,0 +1,474 @@
+/*
+ * Reference-shaped entry points (include/spsim.h) on top of the native ABI.
+ * Each function keeps the reference's signature, allocation and ownership
+ * rules; the arithmetic runs on the GPU.  Failures print the reason and
+ * abort(), as the reference's sp_error_fatal paths do: there is no CPU fallback.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <cuda_runtime.h>
+
+#include "../../../include/spsim.h"
+#include "../../../include/spsim_b200.h"
+
+static int g_precision = SPSIM_PREC_F32;
+static unsigned long long g_seed = 0x5eed5eedULL;
+static uint32_t g_pattern_counter = 0;
+
+void spsim_b200_set_legacy_precision(int precision) { g_precision = precision; }
+int spsim_b200_get_legacy_precision(void) { return g_precision; }
+void spsim_b200_set_noise_seed(unsigned long long seed) { g_seed = seed; }
+
+static void die(const char *where, int st) {
+  fprintf(stderr, "spsim_b200: %s failed: %s (%s)\n", where, spsim_b200_status_string(st), spsim_b200_last_error());
+  abort();
+}
+
+static void cuda_die(const char *where, cudaError_t e) {
+  fprintf(stderr, "spsim_b200: %s failed: %s\n", where, cudaGetErrorString(e));
+  abort();
+}
+
+static void *dev_alloc(size_t bytes) {
+  void *p = NULL;
+  cudaError_t e = cudaMalloc(&p, bytes ? bytes : 4);
+  if (e != cudaSuccess) cuda_die("cudaMalloc", e);
+  return p;
+}
+
+static void h2d(void *d, const void *h, size_t bytes) {
+  cudaError_t e = cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) cuda_die("cudaMemcpy H2D", e);
+}
+
+static void d2h(void *h, const void *d, size_t bytes) {
+  cudaError_t e = cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) cuda_die("cudaMemcpy D2H", e);
+}
+
+static double now_us(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return t.tv_sec * 1e6 + t.tv_nsec * 1e-3;
+}
+
+/* ------------------------------------------------------------ geometry */
+
+/* src/diffraction.c:237-297, computed on the GPU in FP64, stored as float */
+float *get_HKL_list_for_detector(CCD *det, Experiment *exp, int *HKL_list_size) {
+  const long long n = (long long)det->nx * det->ny;
+  float *out = (float *)malloc(sizeof(float) * 3 * (n > 0 ? n : 1));
+  float *d = (float *)dev_alloc(sizeof(float) * 3 * n);
+  int st = spsim_b200_hkl_for_detector(det->nx, det->ny, det->width, det->height, det->distance, det->center_x,
+                                       det->center_y, exp->wavelength, det->spherical, d, NULL);
+  if (st) die("get_HKL_list_for_detector", st);
+  d2h(out, d, sizeof(float) * 3 * n);
+  cudaFree(d);
+  *HKL_list_size = (int)n;
+  return out;
+}
+
+/* src/diffraction.c:325-369: the 3-D (volume) detector is not implemented. */
+float *get_HKL_list_for_3d_detector(CCD *det, Experiment *exp, int *HKL_list_size) {
+  (void)det;
+  (void)exp;
+  (void)HKL_list_size;
+  fprintf(stderr, "spsim_b200: 3-D detectors (nz > 1) are not supported\n");
+  abort();
+}
+
+/* src/spsim.c:98-108 */
+float *get_HKL_list(Options *opts, int *HKL_list_size) {
+  if (opts->detector->nz > 1) return get_HKL_list_for_3d_detector(opts->detector, opts->experiment, HKL_list_size);
+  return get_HKL_list_for_detector(opts->detector, opts->experiment, HKL_list_size);
+}
+
+/* Rotation R = Rz(a1) Ry(a2) Rz(a3) (intrinsic z-y-z Euler angles) or a
+ * Haar-uniform rotation from Shoemake's quaternion construction, drawn from
+ * a splitmix64 stream keyed by the noise seed and a call counter. */
+static uint64_t g_rot_state = 0;
+static uint64_t splitmix64(void) {
+  uint64_t z = (g_rot_state += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+static double u01(void) { return ((splitmix64() >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
+
+static void rotation_matrix(Options *opts, double m[9]) {
+  if (opts->random_orientation) {
+    if (!g_rot_state) g_rot_state = g_seed ^ 0xA5A5A5A5DEADBEEFULL;
+    double u1 = u01(), u2 = u01(), u3 = u01();
+    double a = sqrt(1 - u1), b = sqrt(u1);
+    double w = a * sin(2 * M_PI * u2), x = a * cos(2 * M_PI * u2);
+    double y = b * sin(2 * M_PI * u3), z = b * cos(2 * M_PI * u3);
+    double r[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w),
+                   2 * (x * y + z * w),     1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                   2 * (x * z - y * w),     2 * (y * z + x * w), 1 - 2 * (x * x + y * y)};
+    memcpy(m, r, sizeof(r));
+  } else {
+    double a1 = opts->euler_orientation[0], a2 = opts->euler_orientation[1], a3 = opts->euler_orientation[2];
+    double c1 = cos(a1), s1 = sin(a1), c2 = cos(a2), s2 = sin(a2), c3 = cos(a3), s3 = sin(a3);
+    double r[9] = {c1 * c2 * c3 - s1 * s3, -c1 * c2 * s3 - s1 * c3, c1 * s2,
+                   s1 * c2 * c3 + c1 * s3, -s1 * c2 * s3 + c1 * c3, s1 * s2,
+                   -s2 * c3,               s2 * s3,                 c2};
+    memcpy(m, r, sizeof(r));
+  }
+}
+
+/* src/diffraction.c:300-323: q <- R q in float, like sp_matrix_vector_prod.
+ * The returned rotation owns its data in the same allocation, so free() on it
+ * (src/spsim.c:357-359) releases everything. */
+SpRotation *apply_orientation_to_HKL_list(float **HKL_list, int *HKL_list_size, Options *opts) {
+  double m[9];
+  rotation_matrix(opts, m);
+  SpRotation *rot = (SpRotation *)malloc(sizeof(SpRotation) + 9 * sizeof(float));
+  rot->rows = 3;
+  rot->cols = 3;
+  rot->data = (float *)(rot + 1);
+  for (int k = 0; k < 9; k++) rot->data[k] = (float)m[k];
+  float *q = *HKL_list;
+  for (long long i = 0; i < *HKL_list_size; i++) {
+    float v[3] = {q[3 * i], q[3 * i + 1], q[3 * i + 2]};
+    for (int r = 0; r < 3; r++) {
+      float acc = 0;
+      for (int c = 0; c < 3; c++) acc += rot->data[3 * r + c] * v[c];
+      q[3 * i + r] = acc;
+    }
+  }
+  return rot;
+}
+
+/* ------------------------------------------------------------ structure factor */
+
+static Diffraction_Pattern *pattern_on_list(Molecule *mol, float *HKL_list, int n, float B, Experiment *exp,
+                                            Options *opts) {
+  double t0 = now_us();
+  Diffraction_Pattern *res = (Diffraction_Pattern *)calloc(1, sizeof(Diffraction_Pattern));
+  res->F = (Complex *)malloc(sizeof(Complex) * (n > 0 ? n : 1));
+  res->ints = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  res->HKL_list = (float *)malloc(sizeof(float) * 3 * (n > 0 ? n : 1));
+  if (n > 0) memcpy(res->HKL_list, HKL_list, sizeof(float) * 3 * n);
+  res->HKL_list_size = n;
+  res->N_pix = n;
+  float beam[3] = {exp ? exp->beam_fwhm : 0.0f, exp ? exp->beam_center_x : 0.0f, exp ? exp->beam_center_y : 0.0f};
+  int st = spsim_b200_structure_factor_host(mol->natoms, mol->atomic_number, mol->pos, NULL, NULL, B,
+                                            opts ? opts->delta_atoms : 0, beam, n, HKL_list, g_precision,
+                                            (float *)res->F, res->ints);
+  if (st) die("compute_pattern_on_list", st);
+  if (opts && opts->verbosity_level > 0) /* src/diffraction.c:849-851 */
+    printf("%g atoms.pixel/s\n", 1.0e6 * n * mol->natoms / (now_us() - t0));
+  return res;
+}
+
+/* src/diffraction.c:770 */
+Diffraction_Pattern *compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
+                                             Experiment *exp, Options *opts) {
+  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts);
+}
+
+/* src/diffraction.c:856 (the SSE path): same GPU evaluation */
+Diffraction_Pattern *vector_compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
+                                                    Experiment *exp, Options *opts) {
+  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts);
+}
+
+/* src/diffraction.cu:135 */
+Diffraction_Pattern *cuda_compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
+                                                  Experiment *exp, Options *opts) {
+  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts);
+}
+
+/* src/diffraction.cu:235 */
+Diffraction_Pattern *cuda_compute_pattern_on_list2(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
+                                                   Experiment *exp, Options *opts) {
+  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts);
+}
+
+/* src/spsim.c:110-144: the FFT / NFFT structure factors are other algorithms,
+ * not provided; every direct-summation path runs on the GPU. */
+Diffraction_Pattern *compute_sf(Molecule *mol, float *HKL_list, int HKL_list_size, Options *opts) {
+  if (opts->use_fft_for_sf || opts->use_nfft_for_sf) {
+    fprintf(stderr, "spsim_b200: the FFT/NFFT structure factors are not supported\n");
+    abort();
+  }
+  Diffraction_Pattern *p = pattern_on_list(mol, HKL_list, HKL_list_size, opts->b_factor, opts->experiment, opts);
+  p->rot = NULL;
+  return p;
+}
+
+/* ------------------------------------------------------------ detector chain */
+
+static spsim_b200_chain_params chain_params(const CCD *det, const Experiment *exp) {
+  spsim_b200_chain_params p;
+  memset(&p, 0, sizeof(p));
+  p.nx = det->nx;
+  p.ny = det->ny;
+  p.nz = det->nz > 0 ? det->nz : 1;
+  p.binning_x = det->binning_x;
+  p.binning_y = det->binning_y;
+  p.binning_z = det->binning_z;
+  p.spherical = det->spherical;
+  p.polarization = exp ? exp->polarization : 0;
+  p.width = det->width;
+  p.height = det->height;
+  p.distance = det->distance;
+  p.center_x = det->center_x;
+  p.center_y = det->center_y;
+  p.pixel_width = det->pixel_width;
+  p.pixel_height = det->pixel_height;
+  p.wavelength = exp ? exp->wavelength : 0.0f;
+  p.beam_intensity = exp ? exp->beam_intensity : 0.0f;
+  p.quantum_efficiency = det->quantum_efficiency;
+  p.electron_hole_production_energy = det->electron_hole_production_energy;
+  p.dark_current = det->dark_current;
+  p.exposure_time = exp ? exp->exposure_time : 0.0f;
+  p.readout_noise = det->readout_noise;
+  p.linear_full_well = det->linear_full_well;
+  p.maximum_value = det->maximum_value;
+  p.clamp_to_maximum = 0;
+  p.seed = g_seed;
+  p.pattern_index = g_pattern_counter;
+  return p;
+}
+
+static long long npix_of(const CCD *det) { return (long long)det->nx * det->ny * (det->nz > 0 ? det->nz : 1); }
+static long long nbin_of(const CCD *det) {
+  return (long long)(det->nx / det->binning_x) * (det->ny / det->binning_y) *
+         ((det->nz > 0 ? det->nz : 1) / det->binning_z);
+}
+
+/* src/diffraction.c:1109 */
+void calculate_thomson_correction(CCD *det, Experiment *exp) {
+  const long long n = npix_of(det);
+  spsim_b200_chain_params p = chain_params(det, exp);
+  float *d = (float *)dev_alloc(sizeof(float) * n);
+  int st = spsim_b200_thomson(&p, d, NULL);
+  if (st) die("calculate_thomson_correction", st);
+  det->thomson_correction = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  d2h(det->thomson_correction, d, sizeof(float) * n);
+  cudaFree(d);
+}
+
+/* src/diffraction.c:1146 */
+void calculate_pixel_solid_angle(CCD *det) {
+  const long long n = npix_of(det);
+  spsim_b200_chain_params p = chain_params(det, NULL);
+  float *d = (float *)dev_alloc(sizeof(float) * n);
+  int st = spsim_b200_solid_angle(&p, d, NULL);
+  if (st) die("calculate_pixel_solid_angle", st);
+  det->solid_angle = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  d2h(det->solid_angle, d, sizeof(float) * n);
+  cudaFree(d);
+}
+
+/* src/diffraction.c:1190 */
+void calculate_photons_per_pixel(Diffraction_Pattern *pattern, Options *opts) {
+  CCD *det = opts->detector;
+  Experiment *exp = opts->experiment;
+  if (!det->thomson_correction) calculate_thomson_correction(det, exp);
+  if (!det->solid_angle) calculate_pixel_solid_angle(det);
+  const long long n = npix_of(det);
+  float *dT = (float *)dev_alloc(sizeof(float) * n), *dO = (float *)dev_alloc(sizeof(float) * n);
+  float *dI = (float *)dev_alloc(sizeof(float) * n), *dP = (float *)dev_alloc(sizeof(float) * n);
+  h2d(dT, det->thomson_correction, sizeof(float) * n);
+  h2d(dO, det->solid_angle, sizeof(float) * n);
+  h2d(dI, pattern->ints, sizeof(float) * n);
+  int st = spsim_b200_photons(n, dT, dO, dI, exp->beam_intensity, dP, NULL);
+  if (st) die("calculate_photons_per_pixel", st);
+  det->photons_per_pixel = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  d2h(det->photons_per_pixel, dP, sizeof(float) * n);
+  cudaFree(dT);
+  cudaFree(dO);
+  cudaFree(dI);
+  cudaFree(dP);
+}
+
+/* src/noise.c:32 */
+void generate_poisson_noise(CCD *det) {
+  if (!det->photons_per_pixel) {
+    fprintf(stderr, "Please calculate photons per pixel first\n");
+    return;
+  }
+  const long long n = npix_of(det);
+  spsim_b200_chain_params p = chain_params(det, NULL);
+  float *dP = (float *)dev_alloc(sizeof(float) * n), *dC = (float *)dev_alloc(sizeof(float) * n);
+  h2d(dP, det->photons_per_pixel, sizeof(float) * n);
+  int st = spsim_b200_photon_counts(&p, dP, dC, NULL);
+  if (st) die("generate_poisson_noise", st);
+  det->photon_count = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  d2h(det->photon_count, dC, sizeof(float) * n);
+  cudaFree(dP);
+  cudaFree(dC);
+}
+
+/* src/amplification.c:54 */
+void calculate_electrons_per_pixel(CCD *det, Experiment *experiment) {
+  if (!det->photon_count) {
+    fprintf(stderr, "Calculate photon_count first\n");
+    return;
+  }
+  const long long n = npix_of(det);
+  spsim_b200_chain_params p = chain_params(det, experiment);
+  float *dC = (float *)dev_alloc(sizeof(float) * n), *dE = (float *)dev_alloc(sizeof(float) * n);
+  h2d(dC, det->photon_count, sizeof(float) * n);
+  int st = spsim_b200_electrons(&p, dC, dE, NULL);
+  if (st) die("calculate_electrons_per_pixel", st);
+  det->electrons_per_pixel = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  d2h(det->electrons_per_pixel, dE, sizeof(float) * n);
+  cudaFree(dC);
+  cudaFree(dE);
+}
+
+/* src/amplification.c:77 */
+void calculate_real_detector_output(CCD *det, Experiment *experiment) {
+  if (!det->electrons_per_pixel) {
+    fprintf(stderr, "Calculate electrons_per_pixel first\n");
+    return;
+  }
+  const long long n = npix_of(det), nb = nbin_of(det);
+  spsim_b200_chain_params p = chain_params(det, experiment);
+  float *dE = (float *)dev_alloc(sizeof(float) * n), *dR = (float *)dev_alloc(sizeof(float) * nb);
+  h2d(dE, det->electrons_per_pixel, sizeof(float) * n);
+  int st = spsim_b200_binned_outputs(&p, dE, NULL, dR, NULL, NULL);
+  if (st) die("calculate_real_detector_output", st);
+  det->real_output = (float *)malloc(sizeof(float) * (nb > 0 ? nb : 1));
+  d2h(det->real_output, dR, sizeof(float) * nb);
+  cudaFree(dE);
+  cudaFree(dR);
+}
+
+/* src/amplification.c:119 */
+void calculate_noiseless_detector_output(CCD *det, Experiment *experiment) {
+  if (!det->photons_per_pixel) {
+    fprintf(stderr, "Calculate photons_per_pixel first\n");
+    return;
+  }
+  const long long n = npix_of(det), nb = nbin_of(det);
+  spsim_b200_chain_params p = chain_params(det, experiment);
+  float *dP = (float *)dev_alloc(sizeof(float) * n), *dN = (float *)dev_alloc(sizeof(float) * nb);
+  h2d(dP, det->photons_per_pixel, sizeof(float) * n);
+  int st = spsim_b200_binned_outputs(&p, NULL, dP, NULL, dN, NULL);
+  if (st) die("calculate_noiseless_detector_output", st);
+  det->noiseless_output = (float *)malloc(sizeof(float) * (nb > 0 ? nb : 1));
+  d2h(det->noiseless_output, dN, sizeof(float) * nb);
+  cudaFree(dP);
+  cudaFree(dN);
+}
+
+/* ------------------------------------------------------------ orchestration */
+
+/* src/spsim.c:281-346, with the detector chain fused into one GPU pass. */
+Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
+  CCD *det = opts->detector;
+  Experiment *exp = opts->experiment;
+  if (opts->sf_filename[0]) {
+    fprintf(stderr, "spsim_b200: precalculated_sf patterns are not supported\n");
+    abort();
+  }
+  if (det->gaussian_blurring != 0.0f) {
+    fprintf(stderr, "spsim_b200: detector_gaussian_blurring is not supported\n");
+    abort();
+  }
+  if (opts->random_seed >= 0) spsim_b200_set_noise_seed((unsigned long long)opts->random_seed);
+  int n = 0;
+  float *HKL_list = get_HKL_list(opts, &n);
+  SpRotation *rot = apply_orientation_to_HKL_list(&HKL_list, &n, opts);
+  Diffraction_Pattern *pattern = compute_sf(mol, HKL_list, n, opts);
+  pattern->rot = rot;
+
+  const long long np = npix_of(det), nb = nbin_of(det);
+  spsim_b200_chain_params p = chain_params(det, exp);
+  float *dI = (float *)dev_alloc(sizeof(float) * np);
+  float *bufs[7];
+  for (int k = 0; k < 5; k++) bufs[k] = (float *)dev_alloc(sizeof(float) * np);
+  bufs[5] = (float *)dev_alloc(sizeof(float) * nb);
+  bufs[6] = (float *)dev_alloc(sizeof(float) * nb);
+  h2d(dI, pattern->ints, sizeof(float) * np);
+  spsim_b200_chain_outputs o = {bufs[0], bufs[1], bufs[2], bufs[3], bufs[4], bufs[5], bufs[6]};
+  int st = spsim_b200_detector_chain(&p, dI, &o, NULL);
+  if (st) die("simulate_shot detector chain", st);
+  float **dst[7] = {&det->thomson_correction, &det->solid_angle, &det->photons_per_pixel, &det->photon_count,
+                    &det->electrons_per_pixel, &det->real_output, &det->noiseless_output};
+  for (int k = 0; k < 7; k++) {
+    const long long m = k < 5 ? np : nb;
+    *dst[k] = (float *)malloc(sizeof(float) * (m > 0 ? m : 1));
+    d2h(*dst[k], bufs[k], sizeof(float) * m);
+    cudaFree(bufs[k]);
+  }
+  cudaFree(dI);
+  g_pattern_counter++;
+  free(HKL_list);
+  return pattern;
+}
+
+/* src/spsim.c:348-371 */
+void free_diffraction_pattern(Diffraction_Pattern *pattern) {
+  free(pattern->F);
+  free(pattern->ints);
+  free(pattern->HKL_list);
+  if (pattern->rot) free(pattern->rot);
+  free(pattern);
+}
+
+void free_output_in_options(Options *opts) {
+  CCD *d = opts->detector;
+  free(d->photons_per_pixel);
+  free(d->thomson_correction);
+  free(d->solid_angle);
+  free(d->photon_count);
+  free(d->electrons_per_pixel);
+  free(d->real_output);
+  free(d->noiseless_output);
+  d->photons_per_pixel = d->thomson_correction = d->solid_angle = d->photon_count = NULL;
+  d->electrons_per_pixel = d->real_output = d->noiseless_output = NULL;
+}
+
+void free_stuff(Diffraction_Pattern *pattern, Options *opts) {
+  free_diffraction_pattern(pattern);
+  free_output_in_options(opts);
+}
+
+/* ------------------------------------------------------------ molecules */
+
+/* src/molecule.c:394-417 */
+Molecule *alloc_mol(void) {
+  Molecule *mol = (Molecule *)malloc(sizeof(Molecule));
+  mol->natoms = 0;
+  mol->atomic_number = NULL;
+  mol->pos = NULL;
+  mol->delta_atoms = 0;
+  return mol;
+}
+
+void add_atom_to_mol(Molecule *mol, int atomic_number, float x, float y, float z) {
+  int i = mol->natoms++;
+  mol->atomic_number = (int *)realloc(mol->atomic_number, sizeof(int) * mol->natoms);
+  mol->pos = (float *)realloc(mol->pos, sizeof(float) * 3 * mol->natoms);
+  mol->atomic_number[i] = atomic_number;
+  mol->pos[3 * i] = x;
+  mol->pos[3 * i + 1] = y;
+  mol->pos[3 * i + 2] = z;
+}
+
+void free_mol(Molecule *mol) {
+  free(mol->atomic_number);
+  free(mol->pos);
+  free(mol);
+}
+
+/* ------------------------------------------------------------ distribution */
+
+/* src/mpi.c:30-48 without MPI: the whole range */
+void get_my_loop_start_and_end(int size, int *start, int *end) {
+  *start = 0;
+  *end = size;
+}
+
+void syncronize_patterns(Diffraction_Pattern *pat) { (void)pat; }
+void sum_patterns(Diffraction_Pattern *pat) { (void)pat; }

@@ -1,0 +1,141 @@
+// Device-side data layout and helpers for the structure-factor kernels.
+//
+// Atom record (two float4 per atom, element-sorted, each element segment
+// padded with zero-weight atoms to a multiple of ATOM_GROUP):
+//   a0 = {hx, hy, hz, w}   coarse part R_hi of (r - centre), on the molecule's
+//                          power-of-two grid dr; w = occ * sqrt(illumination)
+//   a1 = {lx, ly, lz, b}   remainder R_lo = (r - centre) - R_hi; b = per-atom B (A^2)
+// Pixel q is split the same way on the q set's grid dq, so that Q_hi . R_hi
+// is exact in FP32 (<= 22 significant bits per product, dq*dr a power of two)
+// and the phase u = q.(r - c) in cycles is
+//   u = Q_hi.R_hi (exact)  +  [Q.R_lo + Q_lo.R_hi]  (small cross term, FP32)
+// reduced modulo a quarter (or whole) cycle before sin/cos.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sincos_poly.h"
+
+namespace spsim {
+
+constexpr int ATOM_GROUP = 8;        // segment padding and inner unroll
+constexpr int TILE_ATOMS = 128;      // atoms per shared-memory tile (4 KiB)
+constexpr int RING_STAGES = 3;       // bulk-copy ring depth
+constexpr int MAX_ELEM = 100;
+
+// Magic constant 1.5 * 2^23: x + MAGIC rounds x to the nearest integer for
+// |x| < 2^22 and leaves that integer in the low mantissa bits.
+constexpr float RINT_MAGIC = 12582912.0f;
+
+// Work-item / pattern descriptors (host-built, device-read).
+struct TileDesc {      // one shared-memory tile of a molecule
+  int atom_begin;      // padded atom index
+  int count;           // atoms in tile, multiple of ATOM_GROUP
+  int elem;            // element slot (row of the form-factor table)
+  int last;            // 1 if the tile ends its element segment
+};
+
+struct SfPattern {
+  const float4 *atoms;     // 2 float4 per padded atom
+  const TileDesc *tiles;   // molecule tile table
+  int n_tiles;
+  int n_elem;
+  int per_atom_b;
+  int has_rot;
+  const double *ff;        // [n_elem][npix] FP64 form factors for this pattern
+  long long npix;
+  const float *hkl;        // AoS float3 q (1/m), or nullptr
+  const double *q64;       // AoS double3 q (1/m), or nullptr
+  double rot[9];           // row-major, applied as q' = R q
+  double center[3];        // molecule centre (m)
+  float dq, inv_dq;        // pixel grid step (power of two) and its inverse
+  double2 *acc;            // FP64 accumulator [npix] (zeroed before the forward)
+  float2 *F;               // complex64 output [npix] or nullptr
+  float *I;                // intensity output [npix] or nullptr
+  long long tile0;         // first pixel-tile index of this pattern in a grid-mapped launch
+};
+
+struct WorkItem {      // one CTA's unit of work
+  int pattern;
+  int pixel_tile;
+  int k0, k1;          // tile range [k0, k1) of the molecule
+};
+
+// ---------------------------------------------------------------------------
+// shared-memory barriers and bulk copies (inline PTX, sm_90+ forms)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: gives up after ~`limit_cycles` SM clocks and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit_cycles) {
+  if (mbar_try_wait(bar, parity)) return true;
+  long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > limit_cycles) return false;
+  }
+  return true;
+}
+
+// 1-D bulk copy global -> shared completing on an mbarrier (no multicast).
+__device__ __forceinline__ void bulk_copy_g2s(void *smem_dst, const void *gmem_src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(smem_dst)),
+      "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// per-term arithmetic
+
+// sin(2 pi y), cos(2 pi y) for |y| <= 3/16 cycle: minimax polynomials on the
+// FMA pipe (coefficients from gen_sincos_poly.py).
+__device__ __forceinline__ void sincos_quad_poly(float y, float &s, float &c) {
+  const float z = y * y;
+  float ps = fmaf(z, SPSIM_QUAD_S4, SPSIM_QUAD_S3);
+  ps = fmaf(z, ps, SPSIM_QUAD_S2);
+  ps = fmaf(z, ps, SPSIM_QUAD_S1);
+  ps = fmaf(z, ps, SPSIM_QUAD_S0);
+  float pc = fmaf(z, SPSIM_QUAD_C4, SPSIM_QUAD_C3);
+  pc = fmaf(z, pc, SPSIM_QUAD_C2);
+  pc = fmaf(z, pc, SPSIM_QUAD_C1);
+  pc = fmaf(z, pc, SPSIM_QUAD_C0);
+  s = y * ps;
+  c = pc;
+}
+
+// Fast2Sum-style float-float accumulation of a block sum b into (hi, lo).
+__device__ __forceinline__ void ff_accumulate(float &hi, float &lo, float b) {
+  const float s = hi + b;
+  const float z = s - hi;
+  lo += b - z;
+  hi = s;
+}
+
+}  // namespace spsim

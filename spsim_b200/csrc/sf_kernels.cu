@@ -1,0 +1,502 @@
+// Structure-factor kernels for sm_100a.
+//
+//   ff_table_kernel      f_e(|q|) per pixel per element, FP64 (src/diffraction.c:183-193)
+//   sf_f32_kernel        compensated-FP32 forward, persistent over cost-sorted work items;
+//                        atom tiles staged in shared memory by 1-D bulk copies on an
+//                        mbarrier ring and read as warp-broadcasts
+//   sf_f64_kernel        plain FP64 per-pixel forward (the precision/speed baseline)
+//   sf_finalize_kernel   centre phase, complex64 F and |F|^2
+//   ewald_kernel         HKL list of a flat/spherical detector (src/diffraction.c:237-297)
+//   atoms_update_kernel  refinement: device positions -> atom records
+#include "sf_kernels.cuh"
+
+#include <cstdio>
+
+namespace spsim {
+
+// ---------------------------------------------------------------------------
+// form factors
+
+__global__ void ff_table_kernel(const float *__restrict__ hkl, const double *__restrict__ q64, long long npix,
+                                int n_elem, const float *__restrict__ coeffs, double B, int delta_atoms,
+                                double *__restrict__ ff) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = blockIdx.y;
+  if (p >= npix || e >= n_elem) return;
+  double qx, qy, qz;
+  if (hkl) {
+    qx = hkl[3 * p];
+    qy = hkl[3 * p + 1];
+    qz = hkl[3 * p + 2];
+  } else {
+    qx = q64[3 * p];
+    qy = q64[3 * p + 1];
+    qz = q64[3 * p + 2];
+  }
+  double f = 1.0;
+  if (!delta_atoms) {
+    const double qlen = sqrt(qx * qx + qy * qy + qz * qz);
+    const double d = qlen * 1e-10;
+    const double s2 = d * d * 0.25;
+    const float *c = coeffs + 9 * e;
+    f = 0.0;
+    for (int i = 0; i < 4; ++i) f += (double)c[i] * exp(-((double)c[i + 4] + B) * s2);
+    f += (double)c[8] * exp(-B * s2);
+  }
+  ff[(long long)e * npix + p] = f;
+}
+
+// ---------------------------------------------------------------------------
+// pixel set-up shared by the kernels: q (FP64) of pixel p, rotated
+
+__device__ __forceinline__ void load_q(const SfPattern &pt, long long p, double q[3]) {
+  double a, b, c;
+  if (pt.hkl) {
+    a = pt.hkl[3 * p];
+    b = pt.hkl[3 * p + 1];
+    c = pt.hkl[3 * p + 2];
+  } else {
+    a = pt.q64[3 * p];
+    b = pt.q64[3 * p + 1];
+    c = pt.q64[3 * p + 2];
+  }
+  if (pt.has_rot) {
+    q[0] = pt.rot[0] * a + pt.rot[1] * b + pt.rot[2] * c;
+    q[1] = pt.rot[3] * a + pt.rot[4] * b + pt.rot[5] * c;
+    q[2] = pt.rot[6] * a + pt.rot[7] * b + pt.rot[8] * c;
+  } else {
+    q[0] = a;
+    q[1] = b;
+    q[2] = c;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// compensated FP32 forward
+
+template <int MODE>
+__device__ __forceinline__ void sf_term(const float4 a0, const float4 a1, float w, float qhx, float qhy, float qhz,
+                                        float qx, float qy, float qz, float qlx, float qly, float qlz, float &bc,
+                                        float &bs) {
+  // u = Q_hi . R_hi : exact on the dq*dr grid
+  float u = qhx * a0.x;
+  u = fmaf(qhy, a0.y, u);
+  u = fmaf(qhz, a0.z, u);
+  // cross term Q . R_lo + Q_lo . R_hi (|c| <= 1/16 cycle, checked on the host)
+  float c = qx * a1.x;
+  c = fmaf(qy, a1.y, c);
+  c = fmaf(qz, a1.z, c);
+  c = fmaf(qlx, a0.x, c);
+  c = fmaf(qly, a0.y, c);
+  c = fmaf(qlz, a0.z, c);
+  if (MODE == PREC_MODE_POLY) {
+    // quarter-cycle reduction: u = k/4 + y0 exactly, |y0| <= 1/8
+    const float t = fmaf(u, 4.0f, RINT_MAGIC);
+    const float kf = t - RINT_MAGIC;
+    const float y = fmaf(kf, -0.25f, u) + c;
+    const int ki = __float_as_int(t);
+    float s, co;
+    sincos_quad_poly(y, s, co);
+    // e^{+2 pi i (k/4 + y)}: rotate (co, s) by k quarter turns
+    const bool odd = (ki & 1) != 0;
+    const float ca = odd ? s : co;
+    const float sa = odd ? co : s;
+    const unsigned wb = __float_as_uint(w);
+    const float wc = __uint_as_float(wb ^ (((unsigned)(ki + 1) << 30) & 0x80000000u));
+    const float ws = __uint_as_float(wb ^ (((unsigned)ki << 30) & 0x80000000u));
+    bc = fmaf(wc, ca, bc);  // sum w cos(2 pi u)
+    bs = fmaf(ws, sa, bs);  // sum w sin(2 pi u)
+  } else {
+    // whole-cycle reduction, MUFU sin/cos on |x| <= pi (1 + 1/8)
+    const float t = u + RINT_MAGIC;
+    const float kf = t - RINT_MAGIC;
+    const float y = (u - kf) + c;
+    float s, co;
+    __sincosf(y * 6.28318530717958648f, &s, &co);
+    bc = fmaf(w, co, bc);
+    bs = fmaf(w, s, bs);
+  }
+}
+
+template <int MODE, int NT, int P, bool PERB>
+__global__ void __launch_bounds__(NT) sf_f32_kernel(const SfPattern *__restrict__ pats,
+                                                    const WorkItem *__restrict__ items, int n_items,
+                                                    int *__restrict__ queue, int *__restrict__ err) {
+  __shared__ __align__(128) float4 ring[RING_STAGES][2 * TILE_ATOMS];
+  __shared__ __align__(8) uint64_t full_bar[RING_STAGES];
+  __shared__ int s_item;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < RING_STAGES; ++s) mbar_init(&full_bar[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  uint32_t g_issue = 0;  // tiles issued by this CTA (meaningful in thread 0)
+  uint32_t g_cons = 0;   // tiles consumed by this CTA (uniform)
+  const long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const WorkItem wi = items[it];
+    const SfPattern &pt = pats[wi.pattern];
+    const long long npix = pt.npix;
+    const float dq = pt.dq, inv_dq = pt.inv_dq;
+    const float4 *__restrict__ atoms = pt.atoms;
+    const TileDesc *__restrict__ tiles = pt.tiles;
+
+    // ---- per-thread pixels
+    float qhx[P], qhy[P], qhz[P], qx[P], qy[P], qz[P], qlx[P], qly[P], qlz[P], s2n[P];
+    long long pix[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      pix[i] = (long long)wi.pixel_tile * (NT * P) + i * NT + tid;
+      double q[3] = {0.0, 0.0, 0.0};
+      if (pix[i] < npix) load_q(pt, pix[i], q);
+      const double hx = (double)rintf((float)q[0] * inv_dq) * dq;
+      const double hy = (double)rintf((float)q[1] * inv_dq) * dq;
+      const double hz = (double)rintf((float)q[2] * inv_dq) * dq;
+      qhx[i] = (float)hx;
+      qhy[i] = (float)hy;
+      qhz[i] = (float)hz;
+      qx[i] = (float)q[0];
+      qy[i] = (float)q[1];
+      qz[i] = (float)q[2];
+      qlx[i] = (float)(q[0] - hx);
+      qly[i] = (float)(q[1] - hy);
+      qlz[i] = (float)(q[2] - hz);
+      // -(|q| 1e-10)^2 / 4 * log2(e): per-atom B factor exponent in base 2
+      const double d2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20;
+      s2n[i] = (float)(-0.25 * d2 * 1.4426950408889634);
+    }
+    double fre[P], fim[P];
+    float shc[P], slc[P], shs[P], sls[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      fre[i] = fim[i] = 0.0;
+      shc[i] = slc[i] = shs[i] = sls[i] = 0.0f;
+    }
+
+    const int k0 = wi.k0, k1 = wi.k1;
+    if (tid == 0) {
+      for (int k = k0; k < k1 && k < k0 + RING_STAGES; ++k) {
+        const TileDesc td = tiles[k];
+        const uint32_t st = g_issue % RING_STAGES;
+        const uint32_t bytes = (uint32_t)td.count * 32u;
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atoms + 2 * (long long)td.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+    }
+
+    for (int k = k0; k < k1; ++k) {
+      const uint32_t st = g_cons % RING_STAGES;
+      const uint32_t par = (g_cons / RING_STAGES) & 1u;
+      const bool ok = mbar_wait_bounded(&full_bar[st], par, kWaitCycles);
+      if (__syncthreads_or(!ok)) {
+        // a copy never landed: report, wait (bounded) for copies still in flight, leave
+        if (tid == 0) {
+          atomicOr(err, 1);
+          for (uint32_t g = g_cons; g < g_issue; ++g)
+            mbar_wait_bounded(&full_bar[g % RING_STAGES], (g / RING_STAGES) & 1u, kWaitCycles);
+        }
+        return;
+      }
+      const TileDesc td = tiles[k];
+      const float4 *__restrict__ ta = ring[st];
+      for (int a = 0; a < td.count; a += ATOM_GROUP) {
+        float bc[P], bs[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) bc[i] = bs[i] = 0.0f;
+#pragma unroll
+        for (int g = 0; g < ATOM_GROUP; ++g) {
+          const float4 a0 = ta[2 * (a + g)];
+          const float4 a1 = ta[2 * (a + g) + 1];
+#pragma unroll
+          for (int i = 0; i < P; ++i) {
+            const float w = PERB ? a0.w * exp2f(a1.w * s2n[i]) : a0.w;
+            sf_term<MODE>(a0, a1, w, qhx[i], qhy[i], qhz[i], qx[i], qy[i], qz[i], qlx[i], qly[i], qlz[i], bc[i],
+                          bs[i]);
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+          ff_accumulate(shc[i], slc[i], bc[i]);
+          ff_accumulate(shs[i], sls[i], bs[i]);
+        }
+      }
+      if (td.last || k == k1 - 1) {
+        const double *__restrict__ ffe = pt.ff + (long long)td.elem * npix;
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+          const double f = pix[i] < npix ? ffe[pix[i]] : 0.0;
+          fre[i] += f * ((double)shc[i] + (double)slc[i]);
+          fim[i] -= f * ((double)shs[i] + (double)sls[i]);
+          shc[i] = slc[i] = shs[i] = sls[i] = 0.0f;
+        }
+      }
+      __syncthreads();  // every thread is done with stage st
+      if (tid == 0 && k + RING_STAGES < k1) {
+        const TileDesc tn = tiles[k + RING_STAGES];
+        const uint32_t bytes = (uint32_t)tn.count * 32u;
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atoms + 2 * (long long)tn.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+      ++g_cons;
+    }
+
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      if (pix[i] < npix) {
+        atomicAdd(&pt.acc[pix[i]].x, fre[i]);
+        atomicAdd(&pt.acc[pix[i]].y, fim[i]);
+      }
+    }
+    __syncthreads();  // s_item is rewritten next round
+  }
+}
+
+// ---------------------------------------------------------------------------
+// plain FP64 forward: one thread per pixel, atoms read as warp-uniform loads
+
+__global__ void __launch_bounds__(256) sf_f64_kernel(const SfPattern *__restrict__ pats, int pattern) {
+  const SfPattern &pt = pats[pattern];
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= pt.npix) return;
+  double q[3];
+  load_q(pt, p, q);
+  const double s2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 0.25;
+  double fr = 0.0, fi = 0.0, ar = 0.0, ai = 0.0;
+  for (int k = 0; k < pt.n_tiles; ++k) {
+    const TileDesc td = pt.tiles[k];
+    for (int j = td.atom_begin; j < td.atom_begin + td.count; ++j) {
+      const float4 a0 = __ldg(&pt.atoms[2 * j]);
+      const float4 a1 = __ldg(&pt.atoms[2 * j + 1]);
+      const double rx = (double)a0.x + (double)a1.x;
+      const double ry = (double)a0.y + (double)a1.y;
+      const double rz = (double)a0.z + (double)a1.z;
+      double t = q[0] * rx + q[1] * ry + q[2] * rz;
+      t -= rint(t);
+      double s, c;
+      sincospi(2.0 * t, &s, &c);
+      double w = a0.w;
+      if (pt.per_atom_b) w *= exp(-(double)a1.w * s2);
+      ar += w * c;
+      ai -= w * s;
+    }
+    if (td.last) {
+      const double f = pt.ff[(long long)td.elem * pt.npix + p];
+      fr += f * ar;
+      fi += f * ai;
+      ar = ai = 0.0;
+    }
+  }
+  pt.acc[p] = make_double2(fr, fi);
+}
+
+// ---------------------------------------------------------------------------
+// finalize: F = e^{-2 pi i q.c} acc, I = |acc|^2
+
+__global__ void sf_finalize_kernel(const SfPattern *__restrict__ pats, int pattern0) {
+  const SfPattern &pt = pats[pattern0 + blockIdx.y];
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= pt.npix) return;
+  const double2 a = pt.acc[p];
+  if (pt.I) pt.I[p] = (float)(a.x * a.x + a.y * a.y);
+  if (pt.F) {
+    double q[3];
+    load_q(pt, p, q);
+    double t = q[0] * pt.center[0] + q[1] * pt.center[1] + q[2] * pt.center[2];
+    t -= rint(t);
+    double s, c;
+    sincospi(2.0 * t, &s, &c);
+    pt.F[p] = make_float2((float)(a.x * c + a.y * s), (float)(a.y * c - a.x * s));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ewald geometry: the reference's operation order, FP64 without contraction
+
+__global__ void ewald_kernel(int nx, int ny, double width, double height, double distance, double cx, double cy,
+                             double ewald, int spherical, double fpx, double fpy, double px_size, double py_size,
+                             float *__restrict__ out32, double *__restrict__ out64) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nx * ny) return;
+  const int x = (int)(i % nx), y = (int)(i / nx);
+  const double px = __dsub_rn(__dmul_rn(__ddiv_rn(__dsub_rn((double)x, (nx - 1.0) / 2.0), (double)nx), width), cx);
+  const double py = __dsub_rn(__dmul_rn(__ddiv_rn(__dsub_rn((double)y, (ny - 1.0) / 2.0), (double)ny), height), cy);
+  const double pz = distance;
+  double q0, q1, q2;
+  if (!spherical) {
+    const double p = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz)));
+    q0 = __dmul_rn(__ddiv_rn(px, p), ewald);
+    q1 = __dmul_rn(__ddiv_rn(py, p), ewald);
+    q2 = __dmul_rn(__dsub_rn(__ddiv_rn(pz, p), 1.0), ewald);
+  } else {
+    q0 = __ddiv_rn(__dmul_rn(fpx, px), px_size);
+    q1 = __ddiv_rn(__dmul_rn(fpy, py), py_size);
+    q2 = 0.0;
+  }
+  if (out32) {
+    out32[3 * i] = (float)q0;
+    out32[3 * i + 1] = (float)q1;
+    out32[3 * i + 2] = (float)q2;
+  }
+  if (out64) {
+    out64[3 * i] = q0;
+    out64[3 * i + 1] = q1;
+    out64[3 * i + 2] = q2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// refinement: rewrite atom records from device positions (caller order)
+
+__global__ void atoms_update_kernel(float4 *__restrict__ atoms, const int *__restrict__ perm, int n_padded,
+                                    const float *__restrict__ pos32, const double *__restrict__ pos64,
+                                    const float *__restrict__ occ, const float *__restrict__ bfac,
+                                    const float *__restrict__ wbase, double cx, double cy, double cz, float dr,
+                                    float inv_dr, double rbound, int *__restrict__ range_err) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_padded) return;
+  const int src = perm[j];
+  if (src < 0) return;
+  double r[3];
+  if (pos64) {
+    r[0] = pos64[3 * src] - cx;
+    r[1] = pos64[3 * src + 1] - cy;
+    r[2] = pos64[3 * src + 2] - cz;
+  } else {
+    r[0] = (double)pos32[3 * src] - cx;
+    r[1] = (double)pos32[3 * src + 1] - cy;
+    r[2] = (double)pos32[3 * src + 2] - cz;
+  }
+  if (r[0] * r[0] + r[1] * r[1] + r[2] * r[2] > rbound * rbound) atomicOr(range_err, 1);
+  float4 a0 = atoms[2 * j], a1 = atoms[2 * j + 1];
+  const double hx = (double)rintf((float)r[0] * inv_dr) * dr;
+  const double hy = (double)rintf((float)r[1] * inv_dr) * dr;
+  const double hz = (double)rintf((float)r[2] * inv_dr) * dr;
+  a0.x = (float)hx;
+  a0.y = (float)hy;
+  a0.z = (float)hz;
+  a1.x = (float)(r[0] - hx);
+  a1.y = (float)(r[1] - hy);
+  a1.z = (float)(r[2] - hz);
+  if (occ) a0.w = occ[src] * wbase[j];
+  if (bfac) a1.w = bfac[src];
+  atoms[2 * j] = a0;
+  atoms[2 * j + 1] = a1;
+}
+
+// ---------------------------------------------------------------------------
+// launch wrappers
+
+cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix, int n_elem, const float *coeffs,
+                            double B, int delta_atoms, double *ff, cudaStream_t st) {
+  if (npix <= 0 || n_elem <= 0) return cudaSuccess;
+  dim3 grid((unsigned)((npix + 255) / 256), (unsigned)n_elem);
+  ff_table_kernel<<<grid, 256, 0, st>>>(hkl, q64, npix, n_elem, coeffs, B, delta_atoms, ff);
+  return cudaGetLastError();
+}
+
+template <int MODE, int NT, int P, bool PERB>
+static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, int n_items, int *queue, int *err,
+                                int grid, cudaStream_t st) {
+  sf_f32_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err);
+  return cudaGetLastError();
+}
+
+template <int MODE, int NT, int P, bool PERB>
+static int occupancy_t() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_f32_kernel<MODE, NT, P, PERB>, NT, 0);
+  return n;
+}
+
+#define SPSIM_F32_VARIANTS(X) \
+  X(0, 128, 2)                \
+  X(0, 128, 4)                \
+  X(0, 256, 2)                \
+  X(0, 256, 4)                \
+  X(1, 128, 2)                \
+  X(1, 128, 4)                \
+  X(1, 256, 2)                \
+  X(1, 256, 4)
+
+cudaError_t launch_sf_f32(int mode, int nt, int p, bool perb, const SfPattern *pats, const WorkItem *items,
+                          int n_items, int *queue, int *err, int grid, cudaStream_t st) {
+#define X(M, N, PP)                                                                          \
+  if (mode == M && nt == N && p == PP) {                                                     \
+    return perb ? launch_f32_t<M, N, PP, true>(pats, items, n_items, queue, err, grid, st)   \
+                : launch_f32_t<M, N, PP, false>(pats, items, n_items, queue, err, grid, st); \
+  }
+  SPSIM_F32_VARIANTS(X)
+#undef X
+  return cudaErrorInvalidConfiguration;
+}
+
+int sf_f32_occupancy(int mode, int nt, int p, bool perb) {
+#define X(M, N, PP) \
+  if (mode == M && nt == N && p == PP) return perb ? occupancy_t<M, N, PP, true>() : occupancy_t<M, N, PP, false>();
+  SPSIM_F32_VARIANTS(X)
+#undef X
+  return 0;
+}
+
+bool sf_f32_variant_exists(int mode, int nt, int p) {
+#define X(M, N, PP) \
+  if (mode == M && nt == N && p == PP) return true;
+  SPSIM_F32_VARIANTS(X)
+#undef X
+  return false;
+}
+
+cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cudaStream_t st) {
+  if (npix <= 0) return cudaSuccess;
+  sf_f64_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(pats, pattern);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st) {
+  if (max_npix <= 0 || npat <= 0) return cudaSuccess;
+  for (int p0 = 0; p0 < npat; p0 += 65535) {
+    const int n = npat - p0 < 65535 ? npat - p0 : 65535;
+    dim3 grid((unsigned)((max_npix + 255) / 256), (unsigned)n);
+    sf_finalize_kernel<<<grid, 256, 0, st>>>(pats, pattern0 + p0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_ewald(int nx, int ny, double width, double height, double distance, double cx, double cy,
+                         double wavelength, int spherical, float *out32, double *out64, cudaStream_t st) {
+  const long long n = (long long)nx * ny;
+  if (n <= 0) return cudaSuccess;
+  const double ewald = 1.0 / wavelength;
+  // the reference forms the pixel pitch as a float quotient (src/diffraction.c:259-260)
+  const double px_size = (double)((float)width / nx);
+  const double py_size = (double)((float)height / ny);
+  const double fpx = 2 * sin(atan(px_size / distance) / 2) / wavelength;
+  const double fpy = 2 * sin(atan(py_size / distance) / 2) / wavelength;
+  ewald_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nx, ny, width, height, distance, cx, cy, ewald, spherical,
+                                                           fpx, fpy, px_size, py_size, out32, out64);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_atoms_update(float4 *atoms, const int *perm, int n_padded, const float *pos32,
+                                const double *pos64, const float *occ, const float *bfac, const float *wbase,
+                                const double c[3], float dr, float inv_dr, double rbound, int *range_err,
+                                cudaStream_t st) {
+  if (n_padded <= 0) return cudaSuccess;
+  atoms_update_kernel<<<(n_padded + 255) / 256, 256, 0, st>>>(atoms, perm, n_padded, pos32, pos64, occ, bfac, wbase,
+                                                             c[0], c[1], c[2], dr, inv_dr, rbound, range_err);
+  return cudaGetLastError();
+}
+
+}  // namespace spsim

@@ -1,0 +1,182 @@
+"""Structure factor on the GPU against the FP64 oracle and spsim's own outputs.
+
+Tolerances (relative |F|^2 error against FP64, floored at 1e-3 of the mean
+intensity, and L2 over the pattern):
+  fp64      1e-10 / 1e-12
+  f32       1e-5  / 1e-6     compensated phase, FMA-pipe sin/cos
+  f32_fast  2e-4  / 1e-5     compensated phase, MUFU sin/cos
+and against the reference's float results, its own error band (2e-5 / 2e-6).
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, intensity_errors
+from oracle import oracle as O
+from spsim_b200 import core, synth
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": (1e-10, 1e-12), "f32": (1e-5, 1e-6), "f32_fast": (2e-4, 1e-5)}
+PRECS = ["fp64", "f32", "f32_fast"]
+
+
+def _run(Z, pos, hkl, precision, **kw):
+    B = kw.pop("B", 0.0)
+    mol = core.Molecule(Z, pos, **kw)
+    qs = core.QSet.from_list(hkl)
+    F, I = core.forward(mol, qs, B=B, precision=precision)
+    torch.cuda.synchronize()
+    core.synchronize()
+    return F.cpu().numpy().astype(np.complex128), I.cpu().numpy().astype(np.float64)
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_small_molecule_against_fp64_and_reference(cuda, precision):
+    g = golden("sf_small.npz")
+    F64, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64))
+    F, I = _run(g["Z"], g["pos"], g["hkl"], precision)
+    e_max, e_l2 = intensity_errors(I, I64)
+    print(precision, "vs FP64: floored max %.3g  L2 %.3g" % (e_max, e_l2))
+    assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1]
+    assert np.abs(F - F64).max() < 10 * TOL[precision][0] * np.abs(F64).max()
+    r_max, r_l2 = intensity_errors(g["I"], I)  # the reference, measured against ours
+    assert r_max < 2e-5 + TOL[precision][0] and r_l2 < 2e-6 + TOL[precision][1]
+
+
+@pytest.mark.parametrize("precision", PRECS)
+@pytest.mark.parametrize("variant,kw", [("_B20", {"B": 20.0}), ("_delta", {"delta_atoms": True})])
+def test_b_factor_and_delta_atoms(cuda, precision, variant, kw):
+    g = golden("sf_small.npz")
+    F64, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64), **kw)
+    F, I = _run(g["Z"], g["pos"], g["hkl"], precision, **kw)
+    e_max, e_l2 = intensity_errors(I, I64)
+    assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1], (e_max, e_l2)
+    r_max, _ = intensity_errors(g["I" + variant], I)
+    assert r_max < 2e-5 + TOL[precision][0]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "f32"])
+def test_gaussian_beam_illumination(cuda, precision):
+    g = golden("sf_small.npz")
+    beam = tuple(float(b) for b in g["beam"])
+    F64, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64), beam=beam)
+    F, I = _run(g["Z"], g["pos"], g["hkl"], precision, beam=beam)
+    e_max, e_l2 = intensity_errors(I, I64)
+    assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1], (e_max, e_l2)
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_plain_1k_workload_rows(cuda, precision):
+    g = golden("sf_plain1k.npz")
+    F64, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64))
+    F, I = _run(g["Z"], g["pos"], g["hkl"], precision)
+    e_max, e_l2 = intensity_errors(I, I64)
+    print(precision, "plain_1k vs FP64: floored max %.3g  L2 %.3g" % (e_max, e_l2))
+    assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1]
+    r_max, r_l2 = intensity_errors(g["I"], I)
+    assert r_max < 2e-5 + TOL[precision][0] and r_l2 < 2e-6 + TOL[precision][1]
+
+
+@pytest.mark.parametrize("precision", ["f32", "f32_fast"])
+def test_precision_stress_50k_subset(cuda, precision):
+    # the 50,000-atom / 1024^2 workload on every 64th detector row: phases up to ~39 cycles
+    w = synth.WORKLOADS["precision_50k"]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    d = w["det"]
+    q64 = O.hkl_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+    rows = np.arange(0, d["ny"], 64)
+    sel = (rows[:, None] * d["nx"] + np.arange(d["nx"])[None, :]).reshape(-1)
+    hkl = q64[sel].astype(np.float32)
+    F64, I64 = O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64))
+    F, I = _run(Z, pos, hkl, precision)
+    e_max, e_l2 = intensity_errors(I, I64)
+    print(precision, "precision_50k rows vs FP64: floored max %.3g  L2 %.3g" % (e_max, e_l2))
+    assert e_max < TOL[precision][0] * 3 and e_l2 < TOL[precision][1]
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_edge_shapes(cuda, precision):
+    rng = np.random.Generator(np.random.PCG64(9))
+    for natoms, npix in [(1, 1), (7, 3), (9, 517), (130, 1), (257, 1031)]:
+        Z = rng.choice([1, 6, 7, 8, 16, 26, 79], natoms).astype(np.int32)
+        pos = (rng.normal(size=(natoms, 3)) * 1e-9).astype(np.float32)
+        hkl = (rng.normal(size=(npix, 3)) * 3e8).astype(np.float32)
+        F64, I64 = O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64))
+        F, I = _run(Z, pos, hkl, precision)
+        assert np.abs(F - F64).max() <= 1e-5 * max(1.0, np.abs(F64).max()), (natoms, npix)
+
+
+def test_empty_and_skipped_atoms(cuda):
+    hkl = np.random.default_rng(1).normal(size=(100, 3)).astype(np.float32) * 1e8
+    for Z in (np.zeros(0, np.int32), np.zeros(5, np.int32)):
+        pos = np.zeros((len(Z), 3), np.float32)
+        F, I = _run(Z, pos, hkl, "f32")
+        assert np.all(F == 0) and np.all(I == 0)
+
+
+def test_off_centre_molecule_phase(cuda):
+    # a molecule 200 nm from the origin: F carries the exp(-2 pi i q.c) phase
+    g = golden("sf_small.npz")
+    pos = g["pos"].astype(np.float64) + np.array([2e-7, -1.5e-7, 0.7e-7])
+    F64, I64 = O.structure_factor(g["Z"], pos, g["hkl"].astype(np.float64))
+    F, I = _run(g["Z"], pos.astype(np.float32), g["hkl"], "f32")
+    F64b, _ = O.structure_factor(g["Z"], pos.astype(np.float32).astype(np.float64), g["hkl"].astype(np.float64))
+    e_max, e_l2 = intensity_errors(I, np.abs(F64b) ** 2)
+    assert e_max < 1e-5 and e_l2 < 1e-6
+    assert np.abs(F - F64b).max() < 1e-4 * np.abs(F64b).max()
+
+
+@pytest.mark.parametrize("precision", ["f32", "fp64"])
+def test_rotation_and_detector_qset(cuda, precision):
+    w = synth.WORKLOADS["orientations_20k"]
+    Z, pos = synth.random_molecule(2000, 3e-9, 77)
+    d = w["det"]
+    R = synth.haar_rotations(3, 5)
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(64, 64, d["width"] / 4, d["height"] / 4, d["distance"], d["wavelength"])
+    q0 = O.hkl_detector(64, 64, d["width"] / 4, d["height"] / 4, d["distance"], d["wavelength"])
+    for r in R:
+        F, I = core.forward(mol, qs, rot=r, precision=precision)
+        F64, I64 = O.structure_factor(Z, pos.astype(np.float64), q0 @ r.T)
+        e_max, e_l2 = intensity_errors(I.cpu().numpy(), I64)
+        assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1], (e_max, e_l2)
+
+
+def test_batch_equals_single_patterns(cuda):
+    rng = np.random.Generator(np.random.PCG64(3))
+    mols, qsets, ref = [], [], []
+    for i, (n, nx) in enumerate([(300, 24), (1500, 40), (64, 16), (4000, 8)]):
+        Z, pos = synth.random_molecule(n, (n / 50e27 * 3 / 4 / np.pi) ** (1 / 3), 40 + i)
+        m = core.Molecule(Z, pos)
+        q = core.QSet.from_detector(nx, nx, nx * 150e-6, nx * 150e-6, 0.1, 0.2e-9)
+        mols.append(m)
+        qsets.append(q)
+        ref.append(core.forward(m, q, precision="f32")[1].clone())
+    R = np.stack([np.eye(3)] * 4)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):  # a non-default stream: captured once, then graph-replayed
+        F, I = core.forward_batch(mols, qsets, rots=R, precision="f32")
+        F2, I2 = core.forward_batch(mols, qsets, rots=R, precision="f32")
+    s.synchronize()
+    core.synchronize(s)
+    for a, b, c in zip(I, I2, ref):
+        torch.testing.assert_close(a, c, rtol=1e-6, atol=1e-6 * float(c.abs().max()))
+        torch.testing.assert_close(b, c, rtol=1e-6, atol=1e-6 * float(c.abs().max()))
+
+
+def test_range_error_is_reported(cuda):
+    # a 2 um object at 3e9 1/m is outside the compensated kernel's phase domain
+    Z = np.array([6, 6], np.int32)
+    pos = np.array([[-1e-6, 0, 0], [1e-6, 0, 0]], np.float32)
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_list(np.array([[3e9, 0, 0]], np.float32))
+    from spsim_b200._native import SpsimError, SPSIM_ERR_RANGE
+
+    with pytest.raises(SpsimError) as e:
+        core.forward(mol, qs, precision="f32")
+    assert e.value.status == SPSIM_ERR_RANGE
+    F, I = core.forward(mol, qs, precision="fp64")
+    F64, I64 = O.structure_factor(Z, pos.astype(np.float64), np.array([[3e9, 0, 0]]))
+    assert np.abs(I.cpu().numpy() - I64).max() < 1e-9 * I64.max()
