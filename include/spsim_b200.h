@@ -230,13 +230,14 @@ int spsim_b200_timing_read(double *ms, int cap, int *n);
  * reference's "atoms.pixel/s" self-report (src/diffraction.c:849-851). */
 int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
 
-/* Autotuner: the kernel variant (threads per CTA, pixels per thread) used for
- * FP32 forwards.  variant < 0 restores automatic choice; autotune times every
+/* Autotuner: the kernel variant used for FP32 forwards: threads per CTA,
+ * pixels per thread and packed (1: pixel pairs in f32x2 instructions, 0:
+ * scalar FP32).  threads < 0 restores automatic choice; autotune times every
  * compiled variant on the given workload and keeps the fastest for workloads
  * of that size class. */
-int spsim_b200_set_variant(int threads, int pixels_per_thread);
+int spsim_b200_set_variant(int threads, int pixels_per_thread, int packed);
 int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision, void *stream,
-                        int *best_threads, int *best_pixels_per_thread);
+                        int *best_threads, int *best_pixels_per_thread, int *best_packed);
 
 #ifdef __cplusplus
 }

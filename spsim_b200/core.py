@@ -314,17 +314,18 @@ def last_forward_stats():
     return t.value, ms.value
 
 
-def set_variant(threads=-1, pixels_per_thread=-1):
-    check(lib().spsim_b200_set_variant(int(threads), int(pixels_per_thread)))
+def set_variant(threads=-1, pixels_per_thread=-1, packed=1):
+    """Force an FP32 kernel variant (threads per CTA, pixels per thread, packed pixel pairs); threads < 0 = auto."""
+    check(lib().spsim_b200_set_variant(int(threads), int(pixels_per_thread), int(packed)))
 
 
 def autotune(mol, qs, precision="f32", stream=None):
-    """Time every compiled FP32 kernel variant on this workload; returns (threads, pixels_per_thread)."""
+    """Time every compiled FP32 kernel variant on this workload; returns (threads, pixels_per_thread, packed)."""
     _native.use_device(mol.device)
-    bt, bp = c_int(0), c_int(0)
+    bt, bp, bk = c_int(0), c_int(0), c_int(0)
     check(lib().spsim_b200_autotune(mol.handle, qs.handle, _prec(precision), _stream_ptr(stream), byref(bt),
-                                    byref(bp)))
-    return bt.value, bp.value
+                                    byref(bp), byref(bk)))
+    return bt.value, bp.value, bk.value
 
 
 def npix_of(qs):

@@ -161,6 +161,7 @@ struct spsim_b200_molecule {
   float dr = 1, inv_dr = 1;
   int per_atom_b = 0, delta_atoms = 0;
   float4 *d_atoms = nullptr;
+  float4 *d_atoms2 = nullptr;  // pixel-pair layout of the same records
   TileDesc *d_tiles = nullptr;
   int *d_perm = nullptr;
   float *d_wbase = nullptr;
@@ -168,6 +169,7 @@ struct spsim_b200_molecule {
   int *d_flags = nullptr;  // [0] range error
   ~spsim_b200_molecule() {
     cudaFree(d_atoms);
+    cudaFree(d_atoms2);
     cudaFree(d_tiles);
     cudaFree(d_perm);
     cudaFree(d_wbase);
@@ -301,6 +303,18 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
   const size_t na = std::max(n_pad, 1);
   CUDA_TRY(cudaMalloc(&m->d_atoms, 2 * na * sizeof(float4)));
   CUDA_TRY(cudaMemcpy(m->d_atoms, rec.data(), 2 * na * sizeof(float4), cudaMemcpyHostToDevice));
+  {
+    std::vector<float4> dup(4 * na);
+    for (size_t j = 0; j < na; ++j) {
+      const float4 a0 = rec[2 * j], a1 = rec[2 * j + 1];
+      dup[4 * j] = make_float4(a0.x, a0.x, a0.y, a0.y);
+      dup[4 * j + 1] = make_float4(a0.z, a0.z, a0.w, a0.w);
+      dup[4 * j + 2] = make_float4(a1.x, a1.x, a1.y, a1.y);
+      dup[4 * j + 3] = make_float4(a1.z, a1.z, a1.w, a1.w);
+    }
+    CUDA_TRY(cudaMalloc(&m->d_atoms2, 4 * na * sizeof(float4)));
+    CUDA_TRY(cudaMemcpy(m->d_atoms2, dup.data(), 4 * na * sizeof(float4), cudaMemcpyHostToDevice));
+  }
   CUDA_TRY(cudaMalloc(&m->d_tiles, std::max<size_t>(m->tiles.size(), 1) * sizeof(TileDesc)));
   if (!m->tiles.empty())
     CUDA_TRY(cudaMemcpy(m->d_tiles, m->tiles.data(), m->tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice));
@@ -334,7 +348,7 @@ extern "C" int spsim_b200_molecule_update_device(spsim_b200_molecule *m, const v
   if (!m || !pos_dev) return fail(SPSIM_ERR_INVALID_ARG, "molecule or positions NULL");
   if (bfac_dev && !m->per_atom_b)
     return fail(SPSIM_ERR_INVALID_ARG, "molecule was created without per-atom B factors");
-  CUDA_TRY(launch_atoms_update(m->d_atoms, m->d_perm, m->n_padded, pos_is_f64 ? nullptr : (const float *)pos_dev,
+  CUDA_TRY(launch_atoms_update(m->d_atoms, m->d_atoms2, m->d_perm, m->n_padded, pos_is_f64 ? nullptr : (const float *)pos_dev,
                                pos_is_f64 ? (const double *)pos_dev : nullptr, occ_dev, bfac_dev, m->d_wbase,
                                m->center, m->dr, m->inv_dr, m->rbound, m->d_flags, (cudaStream_t)stream));
   return SPSIM_OK;
@@ -519,7 +533,7 @@ struct Plan {
   int n_items = 0, grid = 0, npat = 0;
   long long max_npix = 0;
   double terms = 0;
-  int precision = 0, nt = 128, ppt = 4;
+  int precision = 0, nt = 128, ppt = 4, packed = 1;
   bool perb = false;
   std::vector<long long> npix_of;
   cudaGraph_t graph = nullptr;
@@ -532,8 +546,11 @@ struct Plan {
 
 static std::vector<std::unique_ptr<Plan>> g_plans;  // most recent last
 static const size_t kMaxPlans = 8;
-static int g_force_nt = -1, g_force_p = -1;
-static std::map<long long, std::pair<int, int>> g_tuned;  // size class -> (nt, p)
+static int g_force_nt = -1, g_force_p = -1, g_force_pk = 1;
+struct Variant {
+  int nt, p, packed;
+};
+static std::map<long long, Variant> g_tuned;  // size class -> kernel variant
 static bool g_timing = false;
 static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timing_events;
 static thread_local double g_last_terms = 0, g_last_ms = 0;
@@ -551,20 +568,13 @@ static int num_sms() {
 
 static long long size_class(double terms) { return (long long)std::floor(std::log2(std::max(terms, 1.0)) / 2); }
 
-static void choose_variant(double terms, long long min_npix, int precision, int *nt, int *p) {
-  if (g_force_nt > 0 && sf_f32_variant_exists(precision == SPSIM_PREC_F32_FAST ? 1 : 0, g_force_nt, g_force_p)) {
-    *nt = g_force_nt;
-    *p = g_force_p;
-    return;
-  }
+static Variant choose_variant(double terms, long long min_npix, int precision) {
+  const int mode = precision == SPSIM_PREC_F32_FAST ? 1 : 0;
+  if (g_force_nt > 0 && sf_f32_variant_exists(mode, g_force_nt, g_force_p, g_force_pk))
+    return {g_force_nt, g_force_p, g_force_pk};
   auto it = g_tuned.find(size_class(terms) * 4 + precision);
-  if (it != g_tuned.end()) {
-    *nt = it->second.first;
-    *p = it->second.second;
-    return;
-  }
-  *nt = 128;
-  *p = (min_npix >= 65536) ? 4 : 2;
+  if (it != g_tuned.end()) return it->second;
+  return {128, (min_npix >= 65536) ? 4 : 2, 1};
 }
 
 static bool is_orthonormal(const double *R) {
@@ -614,12 +624,15 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
   CUDA_TRY(pl.acc.ensure(std::max<size_t>(acc_total, 1) * sizeof(double2)));
   CUDA_TRY(pl.ff.ensure(std::max<size_t>(ff_total, 1) * sizeof(double)));
   CUDA_TRY(pl.flags.ensure(64));
+  CUDA_TRY(cudaMemsetAsync(pl.flags.p, 0, 64, stream));  // queue head and the sticky error word
   CUDA_TRY(pl.pats.ensure(std::max(npat, 1) * sizeof(SfPattern)));
 
-  int nt = 128, ppt = 4;
-  if (precision != SPSIM_PREC_FP64) choose_variant(terms, min_npix, precision, &nt, &ppt);
-  pl.nt = nt;
-  pl.ppt = ppt;
+  Variant var = {128, 4, 1};
+  if (precision != SPSIM_PREC_FP64) var = choose_variant(terms, min_npix, precision);
+  const int nt = var.nt, ppt = var.p;
+  pl.nt = var.nt;
+  pl.ppt = var.p;
+  pl.packed = var.packed;
   const long long tile_pix = (long long)nt * ppt;
 
   pl.max_npix = 0;
@@ -630,6 +643,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     SfPattern &pt = pats[i];
     memset(&pt, 0, sizeof(pt));
     pt.atoms = m->d_atoms;
+    pt.atoms2 = m->d_atoms2;
     pt.tiles = m->d_tiles;
     pt.n_tiles = (int)m->tiles.size();
     pt.n_elem = m->n_elem;
@@ -680,7 +694,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
 
   if (precision != SPSIM_PREC_FP64) {
     // work items: pixel tile x atom-tile range, cost-sorted (largest first)
-    const int occ = std::max(1, sf_f32_occupancy(precision == SPSIM_PREC_F32_FAST ? 1 : 0, nt, ppt, perb));
+    const int occ = std::max(1, sf_f32_occupancy(precision == SPSIM_PREC_F32_FAST ? 1 : 0, nt, ppt, pl.packed, perb));
     const long long slots = (long long)num_sms() * occ;
     long long total_ptiles = 0;
     for (int i = 0; i < npat; ++i) total_ptiles += (qsets[i]->npix + tile_pix - 1) / tile_pix;
@@ -752,7 +766,7 @@ static cudaError_t enqueue_plan(Plan &pl, cudaStream_t stream, cudaEvent_t ev0, 
   } else if (pl.n_items > 0) {
     const int mode = pl.precision == SPSIM_PREC_F32_FAST ? PREC_MODE_MUFU : PREC_MODE_POLY;
     int *flags = (int *)pl.flags.p;
-    if ((e = launch_sf_f32(mode, pl.nt, pl.ppt, pl.perb, (const SfPattern *)pl.pats.p, (const WorkItem *)pl.items.p,
+    if ((e = launch_sf_f32(mode, pl.nt, pl.ppt, pl.packed, pl.perb, (const SfPattern *)pl.pats.p, (const WorkItem *)pl.items.p,
                            pl.n_items, flags, flags + 4, pl.grid, stream)))
       return e;
   }
@@ -768,6 +782,7 @@ static void plan_key(int npat, const spsim_b200_molecule *const *mols, const sps
   kv.push_back(precision);
   kv.push_back(g_force_nt);
   kv.push_back(g_force_p);
+  kv.push_back(g_force_pk);
   for (int i = 0; i < npat; ++i) {
     kv.push_back((double)(mols[i] ? mols[i]->id : 0));
     kv.push_back((double)(qsets[i] ? qsets[i]->id : 0));
@@ -968,34 +983,39 @@ extern "C" int spsim_b200_last_forward_stats(double *terms, double *kernel_ms) {
   return SPSIM_OK;
 }
 
-extern "C" int spsim_b200_set_variant(int threads, int pixels_per_thread) {
+extern "C" int spsim_b200_set_variant(int threads, int pixels_per_thread, int packed) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (threads < 0) {
     g_force_nt = g_force_p = -1;
+    g_force_pk = 1;
     return SPSIM_OK;
   }
-  if (!sf_f32_variant_exists(0, threads, pixels_per_thread))
-    return fail(SPSIM_ERR_INVALID_ARG, "no compiled variant with %d threads x %d pixels", threads, pixels_per_thread);
+  if (!sf_f32_variant_exists(0, threads, pixels_per_thread, packed) ||
+      !sf_f32_variant_exists(1, threads, pixels_per_thread, packed))
+    return fail(SPSIM_ERR_INVALID_ARG, "no compiled variant with %d threads x %d pixels (packed %d)", threads,
+                pixels_per_thread, packed);
   g_force_nt = threads;
   g_force_p = pixels_per_thread;
+  g_force_pk = packed;
   return SPSIM_OK;
 }
 
 extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision,
-                                   void *stream, int *best_threads, int *best_pixels_per_thread) {
+                                   void *stream, int *best_threads, int *best_pixels_per_thread, int *best_packed) {
   if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
   if (precision == SPSIM_PREC_FP64) return fail(SPSIM_ERR_INVALID_ARG, "the FP64 kernel has a single variant");
-  const int cand[][2] = {{128, 2}, {128, 4}, {256, 2}, {256, 4}};
+  const int cand[][3] = {{128, 2, 0}, {128, 4, 0}, {256, 4, 0}, {128, 2, 1}, {128, 4, 1}, {256, 4, 1}, {128, 6, 1}};
   float *dI = nullptr;
   CUDA_TRY(cudaMalloc(&dI, std::max<long long>(qs->npix, 1) * sizeof(float)));
   float best = 1e30f;
-  int bt = 128, bp = 4;
-  const int saved_nt = g_force_nt, saved_p = g_force_p;
+  int bt = 128, bp = 4, bk = 1;
+  const int saved_nt = g_force_nt, saved_p = g_force_p, saved_pk = g_force_pk;
   const bool saved_timing = g_timing;
   int st = SPSIM_OK;
   for (auto &c : cand) {
     g_force_nt = c[0];
     g_force_p = c[1];
+    g_force_pk = c[2];
     float *I[1] = {dI};
     float *F[1] = {nullptr};
     const spsim_b200_molecule *mm = m;
@@ -1023,19 +1043,22 @@ extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b20
       best = tot;
       bt = c[0];
       bp = c[1];
+      bk = c[2];
     }
   }
   g_force_nt = saved_nt;
   g_force_p = saved_p;
+  g_force_pk = saved_pk;
   g_timing = saved_timing;
   cudaFree(dI);
   if (st) return st;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    g_tuned[size_class((double)qs->npix * m->n_kept) * 4 + precision] = {bt, bp};
+    g_tuned[size_class((double)qs->npix * m->n_kept) * 4 + precision] = {bt, bp, bk};
   }
   if (best_threads) *best_threads = bt;
   if (best_pixels_per_thread) *best_pixels_per_thread = bp;
+  if (best_packed) *best_packed = bk;
   return SPSIM_OK;
 }
 

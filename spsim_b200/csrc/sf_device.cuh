@@ -38,6 +38,8 @@ struct TileDesc {      // one shared-memory tile of a molecule
 
 struct SfPattern {
   const float4 *atoms;     // 2 float4 per padded atom
+  const float4 *atoms2;    // the same records duplicated for pixel pairs: 4 float4 per atom,
+                           // {hx,hx,hy,hy} {hz,hz,w,w} {lx,lx,ly,ly} {lz,lz,b,b}
   const TileDesc *tiles;   // molecule tile table
   int n_tiles;
   int n_elem;

@@ -262,6 +262,227 @@ __global__ void __launch_bounds__(NT) sf_f32_kernel(const SfPattern *__restrict_
 }
 
 // ---------------------------------------------------------------------------
+// compensated FP32 forward on pixel pairs: every FP32 operation of the term is
+// a packed f32x2 instruction (two pixels, one issue slot).  Atom records are
+// stored duplicated (4 float4 per atom, see SfPattern::atoms2) so each shared
+// load yields ready operand pairs.  Element sums are flushed straight into the
+// FP64 accumulator with atomics, which keeps the per-pixel register set small.
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+__device__ __forceinline__ void quadrant_select(float t, float s, float c, float w, float &wc, float &ca, float &ws,
+                                                float &sa) {
+  const int ki = __float_as_int(t);
+  const bool odd = (ki & 1) != 0;
+  ca = odd ? s : c;
+  sa = odd ? c : s;
+  const unsigned wb = __float_as_uint(w);
+  wc = __uint_as_float(wb ^ (((unsigned)(ki + 1) << 30) & 0x80000000u));
+  ws = __uint_as_float(wb ^ (((unsigned)ki << 30) & 0x80000000u));
+}
+
+template <int MODE, int NT, int P, bool PERB>
+__global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restrict__ pats,
+                                                      const WorkItem *__restrict__ items, int n_items,
+                                                      int *__restrict__ queue, int *__restrict__ err) {
+  static_assert(P % 2 == 0, "pixels per thread must be even");
+  constexpr int NP = P / 2;
+  __shared__ __align__(128) float4 ring[RING_STAGES][4 * TILE_ATOMS];
+  __shared__ __align__(8) uint64_t full_bar[RING_STAGES];
+  __shared__ int s_item;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < RING_STAGES; ++s) mbar_init(&full_bar[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  uint32_t g_issue = 0, g_cons = 0;
+  const long long kWaitCycles = 4000000000LL;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const WorkItem wi = items[it];
+    const SfPattern &pt = pats[wi.pattern];
+    const long long npix = pt.npix;
+    const float dq = pt.dq, inv_dq = pt.inv_dq;
+    const float4 *__restrict__ atoms2 = pt.atoms2;
+    const TileDesc *__restrict__ tiles = pt.tiles;
+
+    float2 qhx[NP], qhy[NP], qhz[NP], qx[NP], qy[NP], qz[NP], qlx[NP], qly[NP], qlz[NP], s2n[NP];
+    long long pix[P];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      float v[10][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long long p = (long long)wi.pixel_tile * (NT * P) + (2 * j + h) * NT + tid;
+        pix[2 * j + h] = p;
+        double q[3] = {0.0, 0.0, 0.0};
+        if (p < npix) load_q(pt, p, q);
+        const double hx = (double)rintf((float)q[0] * inv_dq) * dq;
+        const double hy = (double)rintf((float)q[1] * inv_dq) * dq;
+        const double hz = (double)rintf((float)q[2] * inv_dq) * dq;
+        v[0][h] = (float)hx;
+        v[1][h] = (float)hy;
+        v[2][h] = (float)hz;
+        v[3][h] = (float)q[0];
+        v[4][h] = (float)q[1];
+        v[5][h] = (float)q[2];
+        v[6][h] = (float)(q[0] - hx);
+        v[7][h] = (float)(q[1] - hy);
+        v[8][h] = (float)(q[2] - hz);
+        v[9][h] = (float)(-0.25 * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 1.4426950408889634);
+      }
+      qhx[j] = make_float2(v[0][0], v[0][1]);
+      qhy[j] = make_float2(v[1][0], v[1][1]);
+      qhz[j] = make_float2(v[2][0], v[2][1]);
+      qx[j] = make_float2(v[3][0], v[3][1]);
+      qy[j] = make_float2(v[4][0], v[4][1]);
+      qz[j] = make_float2(v[5][0], v[5][1]);
+      qlx[j] = make_float2(v[6][0], v[6][1]);
+      qly[j] = make_float2(v[7][0], v[7][1]);
+      qlz[j] = make_float2(v[8][0], v[8][1]);
+      s2n[j] = make_float2(v[9][0], v[9][1]);
+    }
+    float2 shc[NP], slc[NP], shs[NP], sls[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) shc[j] = slc[j] = shs[j] = sls[j] = make_float2(0.f, 0.f);
+
+    const int k0 = wi.k0, k1 = wi.k1;
+    if (tid == 0) {
+      for (int k = k0; k < k1 && k < k0 + RING_STAGES; ++k) {
+        const TileDesc td = tiles[k];
+        const uint32_t st = g_issue % RING_STAGES;
+        const uint32_t bytes = (uint32_t)td.count * 64u;
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atoms2 + 4 * (long long)td.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+    }
+
+    for (int k = k0; k < k1; ++k) {
+      const uint32_t st = g_cons % RING_STAGES;
+      const uint32_t par = (g_cons / RING_STAGES) & 1u;
+      const bool ok = mbar_wait_bounded(&full_bar[st], par, kWaitCycles);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicOr(err, 1);
+          for (uint32_t g = g_cons; g < g_issue; ++g)
+            mbar_wait_bounded(&full_bar[g % RING_STAGES], (g / RING_STAGES) & 1u, kWaitCycles);
+        }
+        return;
+      }
+      const TileDesc td = tiles[k];
+      const float4 *__restrict__ ta = ring[st];
+      for (int a = 0; a < td.count; a += ATOM_GROUP) {
+        float2 bc[NP], bs[NP];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) bc[j] = bs[j] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int g = 0; g < ATOM_GROUP; ++g) {
+          const float4 d0 = ta[4 * (a + g)], d1 = ta[4 * (a + g) + 1];
+          const float4 d2 = ta[4 * (a + g) + 2], d3 = ta[4 * (a + g) + 3];
+          const float2 Hx = make_float2(d0.x, d0.y), Hy = make_float2(d0.z, d0.w);
+          const float2 Hz = make_float2(d1.x, d1.y), W = make_float2(d1.z, d1.w);
+          const float2 Lx = make_float2(d2.x, d2.y), Ly = make_float2(d2.z, d2.w);
+          const float2 Lz = make_float2(d3.x, d3.y);
+#pragma unroll
+          for (int j = 0; j < NP; ++j) {
+            float2 w = W;
+            if (PERB) w = make_float2(W.x * exp2f(d3.z * s2n[j].x), W.y * exp2f(d3.w * s2n[j].y));
+            float2 u = mul2(qhx[j], Hx);
+            u = fma2(qhy[j], Hy, u);
+            u = fma2(qhz[j], Hz, u);
+            float2 c = mul2(qx[j], Lx);
+            c = fma2(qy[j], Ly, c);
+            c = fma2(qz[j], Lz, c);
+            c = fma2(qlx[j], Hx, c);
+            c = fma2(qly[j], Hy, c);
+            c = fma2(qlz[j], Hz, c);
+            if (MODE == PREC_MODE_POLY) {
+              const float2 t = fma2(u, f2(4.0f), f2(RINT_MAGIC));
+              const float2 kf = add2(t, f2(-RINT_MAGIC));
+              const float2 y = add2(fma2(kf, f2(-0.25f), u), c);
+              const float2 z = mul2(y, y);
+              float2 ps = fma2(z, f2(SPSIM_QUAD_S4), f2(SPSIM_QUAD_S3));
+              ps = fma2(z, ps, f2(SPSIM_QUAD_S2));
+              ps = fma2(z, ps, f2(SPSIM_QUAD_S1));
+              ps = fma2(z, ps, f2(SPSIM_QUAD_S0));
+              float2 pc = fma2(z, f2(SPSIM_QUAD_C4), f2(SPSIM_QUAD_C3));
+              pc = fma2(z, pc, f2(SPSIM_QUAD_C2));
+              pc = fma2(z, pc, f2(SPSIM_QUAD_C1));
+              pc = fma2(z, pc, f2(SPSIM_QUAD_C0));
+              const float2 S = mul2(y, ps);
+              float2 wc, ca, ws, sa;
+              quadrant_select(t.x, S.x, pc.x, w.x, wc.x, ca.x, ws.x, sa.x);
+              quadrant_select(t.y, S.y, pc.y, w.y, wc.y, ca.y, ws.y, sa.y);
+              bc[j] = fma2(wc, ca, bc[j]);
+              bs[j] = fma2(ws, sa, bs[j]);
+            } else {
+              const float2 t = add2(u, f2(RINT_MAGIC));
+              const float2 kf = add2(t, f2(-RINT_MAGIC));
+              const float2 y = add2(add2(u, make_float2(-kf.x, -kf.y)), c);
+              const float2 x = mul2(y, f2(6.28318530717958648f));
+              float2 sn, cs;
+              __sincosf(x.x, &sn.x, &cs.x);
+              __sincosf(x.y, &sn.y, &cs.y);
+              bc[j] = fma2(w, cs, bc[j]);
+              bs[j] = fma2(w, sn, bs[j]);
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          // Fast2Sum of the group sums into the float-float element sums
+          float2 s1 = add2(shc[j], bc[j]);
+          slc[j] = add2(slc[j], add2(bc[j], make_float2(-(s1.x - shc[j].x), -(s1.y - shc[j].y))));
+          shc[j] = s1;
+          float2 s2 = add2(shs[j], bs[j]);
+          sls[j] = add2(sls[j], add2(bs[j], make_float2(-(s2.x - shs[j].x), -(s2.y - shs[j].y))));
+          shs[j] = s2;
+        }
+      }
+      if (td.last || k == k1 - 1) {
+        const double *__restrict__ ffe = pt.ff + (long long)td.elem * npix;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const long long p = pix[2 * j + h];
+            if (p < npix) {
+              const double f = ffe[p];
+              const double re = h ? (double)shc[j].y + (double)slc[j].y : (double)shc[j].x + (double)slc[j].x;
+              const double sm = h ? (double)shs[j].y + (double)sls[j].y : (double)shs[j].x + (double)sls[j].x;
+              atomicAdd(&pt.acc[p].x, f * re);
+              atomicAdd(&pt.acc[p].y, -f * sm);
+            }
+          }
+          shc[j] = slc[j] = shs[j] = sls[j] = make_float2(0.f, 0.f);
+        }
+      }
+      __syncthreads();
+      if (tid == 0 && k + RING_STAGES < k1) {
+        const TileDesc tn = tiles[k + RING_STAGES];
+        const uint32_t bytes = (uint32_t)tn.count * 64u;
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atoms2 + 4 * (long long)tn.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+      ++g_cons;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // plain FP64 forward: one thread per pixel, atoms read as warp-uniform loads
 
 __global__ void __launch_bounds__(256) sf_f64_kernel(const SfPattern *__restrict__ pats, int pattern) {
@@ -357,7 +578,8 @@ __global__ void ewald_kernel(int nx, int ny, double width, double height, double
 // ---------------------------------------------------------------------------
 // refinement: rewrite atom records from device positions (caller order)
 
-__global__ void atoms_update_kernel(float4 *__restrict__ atoms, const int *__restrict__ perm, int n_padded,
+__global__ void atoms_update_kernel(float4 *__restrict__ atoms, float4 *__restrict__ atoms2,
+                                    const int *__restrict__ perm, int n_padded,
                                     const float *__restrict__ pos32, const double *__restrict__ pos64,
                                     const float *__restrict__ occ, const float *__restrict__ bfac,
                                     const float *__restrict__ wbase, double cx, double cy, double cz, float dr,
@@ -391,6 +613,10 @@ __global__ void atoms_update_kernel(float4 *__restrict__ atoms, const int *__res
   if (bfac) a1.w = bfac[src];
   atoms[2 * j] = a0;
   atoms[2 * j + 1] = a1;
+  atoms2[4 * j] = make_float4(a0.x, a0.x, a0.y, a0.y);
+  atoms2[4 * j + 1] = make_float4(a0.z, a0.z, a0.w, a0.w);
+  atoms2[4 * j + 2] = make_float4(a1.x, a1.x, a1.y, a1.y);
+  atoms2[4 * j + 3] = make_float4(a1.z, a1.z, a1.w, a1.w);
 }
 
 // ---------------------------------------------------------------------------
@@ -404,53 +630,68 @@ cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix,
   return cudaGetLastError();
 }
 
-template <int MODE, int NT, int P, bool PERB>
+// Variants: (mode, threads, pixels per thread, packed).  packed == 1 selects
+// the pixel-pair kernel (sf_f32x2_kernel), 0 the scalar one (sf_f32_kernel).
+template <int MODE, int NT, int P, bool PERB, int PK>
 static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, int n_items, int *queue, int *err,
                                 int grid, cudaStream_t st) {
-  sf_f32_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err);
+  if (PK)
+    sf_f32x2_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err);
+  else
+    sf_f32_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err);
   return cudaGetLastError();
 }
 
-template <int MODE, int NT, int P, bool PERB>
+template <int MODE, int NT, int P, bool PERB, int PK>
 static int occupancy_t() {
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_f32_kernel<MODE, NT, P, PERB>, NT, 0);
+  if (PK)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_f32x2_kernel<MODE, NT, P, PERB>, NT, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_f32_kernel<MODE, NT, P, PERB>, NT, 0);
   return n;
 }
 
 #define SPSIM_F32_VARIANTS(X) \
-  X(0, 128, 2)                \
-  X(0, 128, 4)                \
-  X(0, 256, 2)                \
-  X(0, 256, 4)                \
-  X(1, 128, 2)                \
-  X(1, 128, 4)                \
-  X(1, 256, 2)                \
-  X(1, 256, 4)
+  X(0, 128, 2, 0)             \
+  X(0, 128, 4, 0)             \
+  X(0, 256, 4, 0)             \
+  X(1, 128, 2, 0)             \
+  X(1, 128, 4, 0)             \
+  X(1, 256, 4, 0)             \
+  X(0, 128, 2, 1)             \
+  X(0, 128, 4, 1)             \
+  X(0, 256, 4, 1)             \
+  X(0, 128, 6, 1)             \
+  X(1, 128, 2, 1)             \
+  X(1, 128, 4, 1)             \
+  X(1, 256, 4, 1)             \
+  X(1, 128, 6, 1)
 
-cudaError_t launch_sf_f32(int mode, int nt, int p, bool perb, const SfPattern *pats, const WorkItem *items,
-                          int n_items, int *queue, int *err, int grid, cudaStream_t st) {
-#define X(M, N, PP)                                                                          \
-  if (mode == M && nt == N && p == PP) {                                                     \
-    return perb ? launch_f32_t<M, N, PP, true>(pats, items, n_items, queue, err, grid, st)   \
-                : launch_f32_t<M, N, PP, false>(pats, items, n_items, queue, err, grid, st); \
+cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
+                          const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st) {
+#define X(M, N, PP, PK)                                                                               \
+  if (mode == M && nt == N && p == PP && packed == PK) {                                              \
+    return perb ? launch_f32_t<M, N, PP, true, PK>(pats, items, n_items, queue, err, grid, st)        \
+                : launch_f32_t<M, N, PP, false, PK>(pats, items, n_items, queue, err, grid, st);      \
   }
   SPSIM_F32_VARIANTS(X)
 #undef X
   return cudaErrorInvalidConfiguration;
 }
 
-int sf_f32_occupancy(int mode, int nt, int p, bool perb) {
-#define X(M, N, PP) \
-  if (mode == M && nt == N && p == PP) return perb ? occupancy_t<M, N, PP, true>() : occupancy_t<M, N, PP, false>();
+int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb) {
+#define X(M, N, PP, PK)                                 \
+  if (mode == M && nt == N && p == PP && packed == PK) \
+    return perb ? occupancy_t<M, N, PP, true, PK>() : occupancy_t<M, N, PP, false, PK>();
   SPSIM_F32_VARIANTS(X)
 #undef X
   return 0;
 }
 
-bool sf_f32_variant_exists(int mode, int nt, int p) {
-#define X(M, N, PP) \
-  if (mode == M && nt == N && p == PP) return true;
+bool sf_f32_variant_exists(int mode, int nt, int p, int packed) {
+#define X(M, N, PP, PK) \
+  if (mode == M && nt == N && p == PP && packed == PK) return true;
   SPSIM_F32_VARIANTS(X)
 #undef X
   return false;
@@ -489,12 +730,12 @@ cudaError_t launch_ewald(int nx, int ny, double width, double height, double dis
   return cudaGetLastError();
 }
 
-cudaError_t launch_atoms_update(float4 *atoms, const int *perm, int n_padded, const float *pos32,
+cudaError_t launch_atoms_update(float4 *atoms, float4 *atoms2, const int *perm, int n_padded, const float *pos32,
                                 const double *pos64, const float *occ, const float *bfac, const float *wbase,
                                 const double c[3], float dr, float inv_dr, double rbound, int *range_err,
                                 cudaStream_t st) {
   if (n_padded <= 0) return cudaSuccess;
-  atoms_update_kernel<<<(n_padded + 255) / 256, 256, 0, st>>>(atoms, perm, n_padded, pos32, pos64, occ, bfac, wbase,
+  atoms_update_kernel<<<(n_padded + 255) / 256, 256, 0, st>>>(atoms, atoms2, perm, n_padded, pos32, pos64, occ, bfac, wbase,
                                                              c[0], c[1], c[2], dr, inv_dr, rbound, range_err);
   return cudaGetLastError();
 }

@@ -10,15 +10,15 @@ constexpr int PREC_MODE_MUFU = 1;  // MUFU sin/cos (SPSIM_PREC_F32_FAST)
 
 cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix, int n_elem, const float *coeffs,
                             double B, int delta_atoms, double *ff, cudaStream_t st);
-cudaError_t launch_sf_f32(int mode, int nt, int p, bool perb, const SfPattern *pats, const WorkItem *items,
-                          int n_items, int *queue, int *err, int grid, cudaStream_t st);
-int sf_f32_occupancy(int mode, int nt, int p, bool perb);
-bool sf_f32_variant_exists(int mode, int nt, int p);
+cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
+                          const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st);
+int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb);
+bool sf_f32_variant_exists(int mode, int nt, int p, int packed);
 cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cudaStream_t st);
 cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st);
 cudaError_t launch_ewald(int nx, int ny, double width, double height, double distance, double cx, double cy,
                          double wavelength, int spherical, float *out32, double *out64, cudaStream_t st);
-cudaError_t launch_atoms_update(float4 *atoms, const int *perm, int n_padded, const float *pos32,
+cudaError_t launch_atoms_update(float4 *atoms, float4 *atoms2, const int *perm, int n_padded, const float *pos32,
                                 const double *pos64, const float *occ, const float *bfac, const float *wbase,
                                 const double c[3], float dr, float inv_dr, double rbound, int *range_err,
                                 cudaStream_t st);

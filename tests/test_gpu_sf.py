@@ -1,8 +1,9 @@
 """Structure factor on the GPU against the FP64 oracle and spsim's own outputs.
 
 Tolerances (relative |F|^2 error against FP64, floored at 1e-3 of the mean
-intensity, and L2 over the pattern):
-  fp64      1e-10 / 1e-12
+intensity, and L2 over the pattern; every path stores F and I as float32, so
+one float ulp, ~6e-8, is the floor):
+  fp64      2e-7  / 1e-7
   f32       1e-5  / 1e-6     compensated phase, FMA-pipe sin/cos
   f32_fast  2e-4  / 1e-5     compensated phase, MUFU sin/cos
 and against the reference's float results, its own error band (2e-5 / 2e-6).
@@ -17,7 +18,7 @@ from spsim_b200 import core, synth
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": (1e-10, 1e-12), "f32": (1e-5, 1e-6), "f32_fast": (2e-4, 1e-5)}
+TOL = {"fp64": (2e-7, 1e-7), "f32": (1e-5, 1e-6), "f32_fast": (2e-4, 1e-5)}
 PRECS = ["fp64", "f32", "f32_fast"]
 
 
@@ -179,4 +180,4 @@ def test_range_error_is_reported(cuda):
     assert e.value.status == SPSIM_ERR_RANGE
     F, I = core.forward(mol, qs, precision="fp64")
     F64, I64 = O.structure_factor(Z, pos.astype(np.float64), np.array([[3e9, 0, 0]]))
-    assert np.abs(I.cpu().numpy() - I64).max() < 1e-9 * I64.max()
+    assert np.abs(I.cpu().numpy() - I64).max() < 2e-7 * I64.max()
