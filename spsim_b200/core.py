@@ -251,8 +251,8 @@ def detector_chain(params, I, outputs=CHAIN_OUTPUTS, stream=None):
         t = torch.empty(nb if name in ("real_output", "noiseless_output") else n, dtype=torch.float32, device=dev)
         res[name] = t
         setattr(o, name, t.data_ptr())
-    check(lib().spsim_b200_detector_chain(byref(params), _dev(I.contiguous()) if I is not None else None, byref(o),
-                                          _stream_ptr(stream)))
+    Ic = I.contiguous() if I is not None else None  # held until the launch is enqueued
+    check(lib().spsim_b200_detector_chain(byref(params), _dev(Ic), byref(o), _stream_ptr(stream)))
     return res
 
 

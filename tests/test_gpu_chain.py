@@ -58,8 +58,8 @@ def test_photons_electrons_and_binned_outputs_match_reference(cuda):
     np.testing.assert_array_equal(el.cpu().numpy(), g["electrons"])
     nb = (p.nx // p.binning_x) * (p.ny // p.binning_y)
     ro, nl = torch.empty(nb, device="cuda"), torch.empty(nb, device="cuda")
-    _native.check(L.spsim_b200_binned_outputs(p, _dev(_t(g["electrons"])), _dev(_t(g["photons"])), _dev(ro),
-                                              _dev(nl), _stream_ptr()))
+    el_in, ph_in = _t(g["electrons"]), _t(g["photons"])  # keep the inputs alive across the launch
+    _native.check(L.spsim_b200_binned_outputs(p, _dev(el_in), _dev(ph_in), _dev(ro), _dev(nl), _stream_ptr()))
     np.testing.assert_allclose(ro.cpu().numpy(), g["real_output"], rtol=1e-6)
     np.testing.assert_allclose(nl.cpu().numpy(), g["noiseless_output"], rtol=1e-6)
 
@@ -69,7 +69,8 @@ def test_fused_chain_agrees_with_stages(cuda):
     p = _params(g, pol=3, readout=0.0, seed=11)
     out = core.detector_chain(p, _t(g["ints"]))
     ph = out["photons_per_pixel"].cpu().numpy()
-    np.testing.assert_allclose(ph, g["photons"], rtol=1.2e-7)
+    # T and Omega are recomputed in the fused kernel (each within an ulp of the reference's)
+    np.testing.assert_allclose(ph, g["photons"], rtol=4e-7)
     counts = O.poisson(ph * np.float32(p.quantum_efficiency), seed=11)
     k = out["photon_count"].cpu().numpy()
     assert np.mean(k == counts) > 0.999
@@ -120,17 +121,17 @@ def test_readout_noise_stream_and_clamp(cuda):
     p = core.chain_params(nx=nx, ny=ny, width=nx * 1e-4, height=ny * 1e-4, distance=0.1, pixel_width=1e-4,
                           pixel_height=1e-4, wavelength=1e-10, beam_intensity=0.0, quantum_efficiency=1.0,
                           electron_hole_production_energy=5.8e-19, dark_current=1e6, exposure_time=1.0,
-                          readout_noise=10.0, linear_full_well=2e5, maximum_value=65535.0, clamp_to_maximum=1,
+                          readout_noise=10.0, linear_full_well=2e7, maximum_value=65535.0, clamp_to_maximum=1,
                           seed=99)
     out = core.detector_chain(p, torch.zeros(nx * ny, device="cuda"), outputs=["real_output"])
     ro = out["real_output"].cpu().numpy().astype(np.float64)
     noise = O.readout_noise(nx * ny, 10.0, seed=99)
-    adc = np.float32(65535.0) / np.float32(2e5)
+    adc = np.float32(65535.0) / np.float32(2e7)
     expect = np.minimum(np.maximum(0, np.float32(1e6) + noise) * adc, 65535.0)
     assert np.mean(np.abs(ro - expect) <= 1e-6 * expect) > 0.999
     assert abs(np.std(ro / adc) - 10.0) < 0.5
     # clamp: a huge dark current saturates every pixel at maximum_value
-    p.dark_current = 1e9
+    p.dark_current = 1e12
     out = core.detector_chain(p, torch.zeros(nx * ny, device="cuda"), outputs=["real_output"])
     assert float(out["real_output"].max()) == 65535.0
 
