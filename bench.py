@@ -257,40 +257,42 @@ def run_b200(args):
     outs = ["photon_count", "real_output", "noiseless_output"]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
-    def step(pattern):
+    def step(pattern, prec=prec):
         chain.pattern_index = pattern
         core.forward(mol, qs, rot=rot, precision=prec, F=F, I=I)
         return core.detector_chain(chain, I, outputs=outs)
 
-    for i in range(args.warmup):
-        step(i)
-    torch.cuda.synchronize()
-    core.synchronize()
-
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with core.timing() as kt, ClockSampler(local) as clocks:
-        for i, (a, b) in enumerate(evs):
-            flush.zero_()  # L2 flush between timed steps, outside the events
-            a.record()
-            step(args.warmup + i)
-            b.record()
+    def timed(prec, steps, warmup):
+        for i in range(warmup):
+            step(i, prec)
         torch.cuda.synchronize()
-        kt.read()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    core.synchronize()
-    elapsed_ms = sum(a.elapsed_time(b) for a, b in evs)
-    if dist:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+        core.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with core.timing() as kt, ClockSampler(local) as clocks:
+            for i, (a, b) in enumerate(evs):
+                flush.zero_()  # L2 flush between timed steps, outside the events
+                a.record()
+                step(warmup + i, prec)
+                b.record()
+            torch.cuda.synchronize()
+            kt.read()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        core.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        if dist:
+            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        sf = kt.ms[-steps:] if kt.ms else []
+        return ms, (statistics.mean(sf) if sf else None), clocks
+
+    elapsed_ms, sf_avg, clocks = timed(prec, args.steps, args.warmup)
     value = world * args.steps * terms / (elapsed_ms * 1e-3)
-    sf_ms = kt.ms[-args.steps:] if kt.ms else []
-    sf_avg = statistics.mean(sf_ms) if sf_ms else None
 
     line = None
     if rank == 0:
@@ -317,6 +319,10 @@ def run_b200(args):
             "clocks": clocks.summary(),
             "gpu_launches": 3 * args.steps,
         }
+    # the other precisions on the same workload, and accuracy against the FP64 GPU kernel
+    extra = _modes(args, core, mol, qs, rot, terms, timed, prec) if rank == 0 and not args.no_modes else None
+    if rank == 0 and extra:
+        line.update(extra)
     # end to end through the reference-facing simulate_shot (host buffers)
     if rank == 0 and not args.no_e2e:
         line["e2e"] = _e2e(args, w, Z, pos, terms, world)
@@ -325,12 +331,59 @@ def run_b200(args):
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nproc, "kind": _ref_kind(), "sample": desc}
         pool.close()
     if rank == 0:
+        if line.get("fp64_plain"):
+            f = line["fp64_plain"]
+            f["f32_speedup"] = line["roofline"]["achieved"] / f["kernel_terms_per_s"] if line["roofline"]["achieved"] else None
+            if line.get("f32_fast", {}).get("kernel_terms_per_s"):
+                f["f32_fast_speedup"] = line["f32_fast"]["kernel_terms_per_s"] / f["kernel_terms_per_s"]
         line["backward_forward_ratio"] = _adjoint_ratio(prec) if not args.no_adjoint else None
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _modes(args, core, mol, qs, rot, terms, timed, prec):
+    """f32_fast throughput, the plain FP64 kernel on every 8th pixel, and the
+    relative |F|^2 errors of both FP32 modes against that FP64 kernel (itself
+    within 2e-7 of the FP64 oracle: tests/test_gpu_sf.py) on every 64th row."""
+    import torch
+
+    out = {}
+    R = None
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    R = _peaks(props)[0]
+    if prec != "f32_fast":
+        ms, sf_ms, _ = timed("f32_fast", max(2, args.steps // 2), 1)
+        out["f32_fast"] = {"value": terms * max(2, args.steps // 2) / (ms * 1e-3), "unit": UNIT,
+                           "kernel_terms_per_s": terms / (sf_ms * 1e-3) if sf_ms else None,
+                           "frac_of_R": terms / (sf_ms * 1e-3) / R if sf_ms else None}
+    q = qs.q()
+    sub_rows = core.QSet.from_list(q.reshape(1024, 1024, 3)[::64].reshape(-1, 3))
+    sub8 = core.QSet.from_list(q[::8])
+    with core.timing() as t:
+        for _ in range(3):
+            core.forward(mol, sub8, rot=rot, precision="fp64")
+        torch.cuda.synchronize()
+    fp64_ms = statistics.median(t.ms[1:])
+    fp64_rate = terms / 8 / (fp64_ms * 1e-3)
+    _, I64 = core.forward(mol, sub_rows, rot=rot, precision="fp64")
+    I64 = I64.double().cpu().numpy()
+    acc = {}
+    for p in ("f32", "f32_fast"):
+        _, Ip = core.forward(mol, sub_rows, rot=rot, precision=p)
+        Ip = Ip.double().cpu().numpy()
+        den = np.maximum(I64, 1e-3 * I64.mean())
+        acc[p] = {"floored_max_rel": float(np.max(np.abs(Ip - I64) / den)),
+                  "l2_rel": float(np.linalg.norm(Ip - I64) / np.linalg.norm(I64)),
+                  "p99_rel": float(np.percentile(np.abs(Ip - I64) / np.maximum(I64, 1e-30), 99))}
+    torch.cuda.synchronize()
+    out["accuracy"] = {"reference": "plain FP64 GPU kernel", "pixels": "every 64th detector row (16,384)",
+                       "floor": "1e-3 x mean intensity", **acc}
+    out["fp64_plain"] = {"kernel_terms_per_s": fp64_rate, "sample": "every 8th pixel",
+                         "f32_speedup": None, "f32_fast_speedup": None}
+    return out
 
 
 def _e2e(args, w, Z, pos, terms, world):
@@ -402,6 +455,59 @@ def _adjoint_ratio(prec):
     return statistics.median(tb) / statistics.median(ta)
 
 
+def profile_case(precisions):
+    """One forward per precision on the 20,000-atom / 256^2 case (~1.3e9 terms):
+    a short, small-memory command for ncu captures."""
+    import torch
+
+    from spsim_b200 import core, synth
+
+    w = synth.WORKLOADS["orientations_20k"]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    d = w["det"]
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+    core.set_variant(128, 4, 1)
+    for p in precisions:
+        core.forward(mol, qs, precision=p)
+    torch.cuda.synchronize()
+    core.synchronize()
+    print("profile case ok")
+    return 0
+
+
+def sweep():
+    """Kernel-variant sweep on the benchmark workload (structure-factor kernel time)."""
+    import torch
+
+    from spsim_b200 import core, synth
+
+    w, Z, pos = _make_workload()
+    d = w["det"]
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+    terms = float(len(Z)) * d["nx"] * d["ny"]
+    R = _peaks(torch.cuda.get_device_properties(0))[0]
+    F = torch.empty(qs.npix, dtype=torch.complex64, device="cuda")
+    I = torch.empty(qs.npix, device="cuda")
+    for prec in ("f32", "f32_fast"):
+        for v in [(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1)]:
+            core.set_variant(*v)
+            for _ in range(2):
+                core.forward(mol, qs, precision=prec, F=F, I=I)
+            torch.cuda.synchronize()
+            with core.timing() as t:
+                for _ in range(4):
+                    core.forward(mol, qs, precision=prec, F=F, I=I)
+                torch.cuda.synchronize()
+            ms = statistics.median(t.ms)
+            print(json.dumps({"precision": prec, "threads": v[0], "pixels_per_thread": v[1], "packed": v[2],
+                              "ms": ms, "terms_per_s": terms / ms * 1e3, "frac_of_R": terms / ms * 1e3 / R}),
+                  flush=True)
+    core.set_variant(-1)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -412,7 +518,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-modes", action="store_true", help="skip the f32_fast / fp64 / accuracy extras")
+    ap.add_argument("--profile-case", default=None,
+                    help="comma-separated precisions: one forward each on the 20,000-atom x 256^2 case (for ncu)")
+    ap.add_argument("--sweep", action="store_true", help="time every compiled FP32 kernel variant")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args.profile_case.split(","))
+    if args.sweep:
+        return sweep()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
