@@ -129,6 +129,26 @@ int spsim_b200_structure_factor_host(int natoms, const int32_t *Z, const float *
                                      int64_t npix, const float *hkl, int precision, float *F_host,
                                      float *I_host);
 
+/* ---- allocation-free variant (no counterpart in the reference) ------------
+ * The same computation, arguments and results as
+ * spsim_b200_structure_factor_host, for callers that may not allocate device
+ * memory while they run: applications that hand out all device memory from
+ * their own fixed budget or pool, and services that cannot afford a
+ * cudaMalloc / cudaFree (which synchronise the whole device) on every call.
+ * It calls no cudaMalloc, cudaFree or other allocating routine: its device
+ * scratch is one static 64 MiB array per GPU (held by every GPU that loads
+ * the library, until the process exits) and its host staging a static
+ * 48 MiB array.  A call needs about 96 bytes per atom plus (40 + 8 x number of
+ * elements) bytes per pixel of scratch; larger calls return
+ * SPSIM_ERR_INVALID_ARG and print the sizes.  The first call on a device looks
+ * up that device's address of the array, so make it before any stream capture.
+ * Calls share the array: they are serialised and synchronised before
+ * returning; calls that overlapped on the GPU would race. */
+int spsim_b200_structure_factor_host_noalloc(int natoms, const int32_t *Z, const float *pos, const float *occ,
+                                             const float *bfac, float B, int delta_atoms, const float *beam,
+                                             int64_t npix, const float *hkl, int precision, float *F_host,
+                                             float *I_host);
+
 /* ---- adjoint -------------------------------------------------------------
  * Given G_p = dL/dI_p for every pixel of `npat` patterns (device, float,
  * npat*npix) and the forward's F (device, complex64, npat*npix), accumulates

@@ -139,6 +139,14 @@ static void load_atomsf_table() {
   fclose(f);
 }
 
+// Row Z of the coefficient table in use (the ./atomsf.lib override applied);
+// internal, shared with the allocation-free entry point in noalloc.cu.
+void spsim_internal_atomsf_row(int Z, float out[9]) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  load_atomsf_table();
+  memcpy(out, g_atomsf[Z], 9 * sizeof(float));
+}
+
 // ---------------------------------------------------------------------------
 // molecules
 
