@@ -1,0 +1,120 @@
+"""Multi-GPU work distribution over torch.distributed (one process per GPU).
+
+The forward path shards: orientations, molecules and pixel slabs are
+independent, so ranks split the units and compute with no collective on the
+data path (weak or strong scaling).  The only exchange is the adjoint's sum of
+per-rank gradients (one all-reduce), plus an optional gather of patterns to
+one rank, the analogue of spsim's MPI gather to the master
+(src/mpi.c:50-60, :96-117).
+
+Unit assignment:
+  slab_range          contiguous equal slabs, spsim's own split (src/mpi.c:30-48)
+  balanced_assignment cost-balanced (longest-processing-time first) for
+                      uneven units such as molecules of different sizes
+"""
+import heapq
+
+import torch
+import torch.distributed as dist
+
+__all__ = ["slab_range", "balanced_assignment", "rank_world", "forward_sharded", "gather_to", "allreduce_",
+           "sharded_intensity"]
+
+
+def rank_world(group=None):
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(group), dist.get_world_size(group)
+    return 0, 1
+
+
+def slab_range(size, rank, world):
+    """[start, end) of `rank`'s contiguous slab; the last rank takes the remainder (src/mpi.c:30-48)."""
+    start = rank * size // world
+    end = size if rank == world - 1 else (rank + 1) * size // world
+    return start, end
+
+
+def balanced_assignment(costs, world):
+    """Unit indices per rank: each unit, largest first, goes to the least-loaded rank.
+    Deterministic, so every rank computes the same assignment without communicating."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    heap = [(0.0, r) for r in range(world)]
+    out = [[] for _ in range(world)]
+    for i in order:
+        load, r = heapq.heappop(heap)
+        out[r].append(i)
+        heapq.heappush(heap, (load + float(costs[i]), r))
+    return [sorted(v) for v in out]
+
+
+def forward_sharded(units, compute, costs=None, group=None):
+    """Run compute(unit_index) for this rank's units; returns {index: result}.
+
+    With costs, units are cost-balanced across ranks, else split in contiguous
+    slabs.  No collective is issued."""
+    rank, world = rank_world(group)
+    n = len(units) if hasattr(units, "__len__") else int(units)
+    if costs is not None:
+        mine = balanced_assignment(costs, world)[rank]
+    else:
+        s, e = slab_range(n, rank, world)
+        mine = range(s, e)
+    return {i: compute(i) for i in mine}
+
+
+def gather_to(local, n_units, shape, dtype, dst=0, group=None, device=None):
+    """Gather {index: tensor} from all ranks into one (n_units, *shape) tensor on rank dst.
+
+    Every rank contributes a full-size buffer holding its own units (zeros
+    elsewhere) to a sum-reduce, so ranks need not agree on sizes beforehand."""
+    rank, world = rank_world(group)
+    dev = device or (next(iter(local.values())).device if local else torch.device("cpu"))
+    buf = torch.zeros((n_units,) + tuple(shape), dtype=dtype, device=dev)
+    for i, t in local.items():
+        buf[i] = t
+    if world > 1:
+        dist.reduce(buf, dst=dst, op=dist.ReduceOp.SUM, group=group)
+    return buf if rank == dst else None
+
+
+def allreduce_(*tensors, group=None):
+    """Sum tensors over ranks in place (the adjoint's gradient exchange)."""
+    _, world = rank_world(group)
+    if world > 1:
+        for t in tensors:
+            if t is not None:
+                dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return tensors
+
+
+class _AllReduceGrad(torch.autograd.Function):
+    """Identity in the forward; sums the incoming gradient over ranks in the backward."""
+
+    @staticmethod
+    def forward(ctx, x, group):
+        ctx.group = group
+        return x.view_as(x)
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous().clone()
+        allreduce_(g, group=ctx.group)
+        return g, None
+
+
+def sharded_intensity(mol, qs, pos, occ, bfac, rots, precision="f32", group=None):
+    """Differentiable intensities of this rank's slab of orientations.
+
+    Returns (I_local (n_local, npix), (start, end)).  Losses summed over the
+    local patterns and backpropagated give every rank the gradient of the
+    global loss (sum over ranks), through one all-reduce per parameter."""
+    from .autograd import intensity
+
+    rank, world = rank_world(group)
+    if len(rots) < world:
+        raise ValueError("every rank needs at least one orientation (%d orientations, %d ranks)" % (len(rots), world))
+    s, e = slab_range(len(rots), rank, world)
+    p = _AllReduceGrad.apply(pos, group)
+    o = _AllReduceGrad.apply(occ, group) if occ is not None else None
+    b = _AllReduceGrad.apply(bfac, group) if bfac is not None else None
+    return intensity(mol, qs, p, o, b, rots=rots[s:e], precision=precision), (s, e)
