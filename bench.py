@@ -187,7 +187,32 @@ class ClockSampler:
                 "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
 
 
+_PROBE = {}
+
+
+def measured_pipe_peaks():
+    """FP32-FMA lane-ops/s and MUFU ops/s measured on this GPU by the pipe probe
+    (spsim_b200/csrc/tools/pipe_probe.cu), or None when it is not built."""
+    if "v" not in _PROBE:
+        _PROBE["v"] = None
+        exe = os.path.join(ROOT, "spsim_b200", "_lib", "pipe_probe")
+        if os.path.exists(exe):
+            try:
+                out = subprocess.run([exe], capture_output=True, text=True, timeout=120).stdout
+                for line in out.splitlines():
+                    if line.startswith("{"):
+                        _PROBE["v"] = json.loads(line)
+            except (OSError, subprocess.TimeoutExpired, ValueError):
+                pass
+    return _PROBE["v"]
+
+
 def _peaks(props):
+    probe = measured_pipe_peaks()
+    if probe and probe.get("fma_lane_ops_per_s") and probe.get("mufu_ops_per_s"):
+        p_fma, p_mufu = probe["fma_lane_ops_per_s"], probe["mufu_ops_per_s"]
+        src = "measured by spsim_b200/_lib/pipe_probe at %s MHz (%d SMs)" % (probe.get("clock_mhz"), probe.get("sms"))
+        return min(p_fma / OPS_PER_TERM_FMA, p_mufu / OPS_PER_TERM_MUFU), p_mufu, p_fma, probe.get("clock_mhz"), src
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     src = "nominal"
     sm_max = 1965.0
@@ -312,9 +337,9 @@ def run_b200(args):
                 "frac": achieved / R if achieved else None, "traffic": _traffic_per_launch(),
                 "kernel": "sf_f32_kernel" if prec != "fp64" else "sf_f64_kernel",
                 "kernel_ms": sf_avg,
-                "peak_source": "min(P_FMA/5, P_MUFU/2) terms/s with %d SMs x %d MUFU and %d FMA lanes per clock at "
-                               "%.0f MHz (%s); MEASURED_PEAKS.json has no FMA/MUFU figure" %
-                               (props.multi_processor_count, MUFU_PER_SM_CLK, FMA_PER_SM_CLK, sm_max, src),
+                "peak_source": "R = min(P_FMA/5, P_MUFU/2) terms/s; P_FMA = %.4g FMA lane-ops/s, P_MUFU = %.4g "
+                               "ops/s, %s (MEASURED_PEAKS.json has no FP32-FMA or MUFU figure)" % (p_fma, p_mufu, src),
+                "peak_nominal": props.multi_processor_count * MUFU_PER_SM_CLK * 1965e6 / OPS_PER_TERM_MUFU,
             },
             "clocks": clocks.summary(),
             "gpu_launches": 3 * args.steps,
@@ -491,7 +516,8 @@ def sweep():
     F = torch.empty(qs.npix, dtype=torch.complex64, device="cuda")
     I = torch.empty(qs.npix, device="cuda")
     for prec in ("f32", "f32_fast"):
-        for v in [(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1)]:
+        for v in [(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1),
+                  (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2)]:
             core.set_variant(*v)
             for _ in range(2):
                 core.forward(mol, qs, precision=prec, F=F, I=I)
@@ -501,10 +527,95 @@ def sweep():
                     core.forward(mol, qs, precision=prec, F=F, I=I)
                 torch.cuda.synchronize()
             ms = statistics.median(t.ms)
-            print(json.dumps({"precision": prec, "threads": v[0], "pixels_per_thread": v[1], "packed": v[2],
+            print(json.dumps({"precision": prec, "threads": v[0], "pixels_per_thread": v[1], "form": v[2],
                               "ms": ms, "terms_per_s": terms / ms * 1e3, "frac_of_R": terms / ms * 1e3 / R}),
                   flush=True)
     core.set_variant(-1)
+    return 0
+
+
+def workloads(prec, n_orient=512):
+    """The batched workloads, each timed with CUDA events (one JSON line each):
+    orientations_20k  20,000 atoms, 256^2 pixels, n_orient Haar rotations in one
+                      persistent launch (graph-replayed) vs a loop of single-pattern calls
+    uneven_64         64 molecules of 500..100,000 atoms on 128^2..1024^2 detectors
+    adjoint_5k        5,000 atoms, 512^2 pixels, 256 orientations: adjoint / forward"""
+    import torch
+
+    from spsim_b200 import core, synth
+
+    R0 = _peaks(torch.cuda.get_device_properties(0))[0]
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+
+    def ev_time(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    # orientations
+    w = synth.WORKLOADS["orientations_20k"]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    d = w["det"]
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+    R = synth.haar_rotations(n_orient, w["rot_seed"])
+    terms = float(len(Z)) * qs.npix * n_orient
+    with torch.cuda.stream(stream):
+        F, I = core.forward_batch([mol] * n_orient, [qs] * n_orient, rots=R, precision=prec, want_F=False)
+        t_batch = ev_time(lambda: core.forward_batch([mol] * n_orient, [qs] * n_orient, rots=R, precision=prec,
+                                                     I=I, want_F=False))
+        nloop = min(n_orient, 64)
+        Iloop = torch.empty(qs.npix, device="cuda")
+        t_loop = ev_time(lambda: [core.forward(mol, qs, rot=R[i], precision=prec, I=Iloop, want_F=False)
+                                  for i in range(nloop)], reps=2) * n_orient / nloop
+    print(json.dumps({"workload": "orientations_20k", "precision": prec, "orientations": n_orient,
+                      "batch_ms": t_batch, "terms_per_s": terms / t_batch * 1e3, "frac_of_R": terms / t_batch * 1e3 / R0,
+                      "loop_of_single_calls_ms": t_loop, "batch_speedup": t_loop / t_batch}), flush=True)
+    del F, I
+
+    # uneven molecules
+    mols, qsets, cost = [], [], 0.0
+    for m in synth.uneven_batch():
+        Zm, pm = synth.random_molecule(m["natoms"], m["radius"], m["seed"])
+        dm = m["det"]
+        mols.append(core.Molecule(Zm, pm))
+        qsets.append(core.QSet.from_detector(dm["nx"], dm["ny"], dm["width"], dm["height"], dm["distance"],
+                                             dm["wavelength"]))
+        cost += float(len(Zm)) * qsets[-1].npix
+    with torch.cuda.stream(stream):
+        F, I = core.forward_batch(mols, qsets, precision=prec, want_F=False)
+        t_u = ev_time(lambda: core.forward_batch(mols, qsets, precision=prec, I=I, want_F=False))
+    print(json.dumps({"workload": "uneven_64", "precision": prec, "terms": cost, "batch_ms": t_u,
+                      "terms_per_s": cost / t_u * 1e3, "frac_of_R": cost / t_u * 1e3 / R0}), flush=True)
+    del mols, qsets, F, I
+
+    # adjoint
+    w = synth.WORKLOADS["adjoint_5k"]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    d = w["det"]
+    mol = core.Molecule(Z, pos, occ=np.ones(len(Z), np.float32), bfac=np.zeros(len(Z), np.float32))
+    qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+    R = synth.haar_rotations(w["n_orient"], w["rot_seed"])
+    terms = float(len(Z)) * qs.npix * len(R)
+    with torch.cuda.stream(stream):
+        F, I = core.forward_batch([mol] * len(R), [qs] * len(R), rots=R, precision=prec)
+        Fc = torch.cat(F)
+        G = torch.rand(Fc.numel(), device="cuda")
+        t_f = ev_time(lambda: core.forward_batch([mol] * len(R), [qs] * len(R), rots=R, precision=prec, F=F, I=I))
+        t_b = ev_time(lambda: core.adjoint(mol, qs, Fc, G, rots=R, precision=prec, stream=stream))
+    print(json.dumps({"workload": "adjoint_5k", "precision": prec, "orientations": len(R), "forward_ms": t_f,
+                      "adjoint_ms": t_b, "backward_forward_ratio": t_b / t_f,
+                      "forward_terms_per_s": terms / t_f * 1e3, "adjoint_terms_per_s": terms / t_b * 1e3}),
+          flush=True)
     return 0
 
 
@@ -522,7 +633,11 @@ def main():
     ap.add_argument("--profile-case", default=None,
                     help="comma-separated precisions: one forward each on the 20,000-atom x 256^2 case (for ncu)")
     ap.add_argument("--sweep", action="store_true", help="time every compiled FP32 kernel variant")
+    ap.add_argument("--workloads", action="store_true", help="time the batched workloads (orientations, uneven, "
+                                                              "adjoint)")
     args = ap.parse_args()
+    if args.workloads:
+        return workloads(args.precision)
     if args.profile_case:
         return profile_case(args.profile_case.split(","))
     if args.sweep:

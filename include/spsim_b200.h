@@ -251,13 +251,18 @@ int spsim_b200_timing_read(double *ms, int cap, int *n);
 int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
 
 /* Autotuner: the kernel variant used for FP32 forwards: threads per CTA,
- * pixels per thread and packed (1: pixel pairs in f32x2 instructions, 0:
- * scalar FP32).  threads < 0 restores automatic choice; autotune times every
- * compiled variant on the given workload and keeps the fastest for workloads
- * of that size class. */
-int spsim_b200_set_variant(int threads, int pixels_per_thread, int packed);
+ * pixels per thread and form:
+ *   0  compensated FP32 phase (hi/lo split), one pixel per lane
+ *   1  compensated FP32 phase, pixel pairs in f32x2 instructions
+ *   2  FP64 phase and half-cycle reduction, FP32 sin/cos and sums on pixel
+ *      pairs (f32x2); the default, and free of the compensated forms' phase
+ *      range limit (SPSIM_ERR_RANGE)
+ * threads < 0 restores automatic choice; autotune times every compiled
+ * variant on the given workload and keeps the fastest for workloads of that
+ * size class. */
+int spsim_b200_set_variant(int threads, int pixels_per_thread, int form);
 int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision, void *stream,
-                        int *best_threads, int *best_pixels_per_thread, int *best_packed);
+                        int *best_threads, int *best_pixels_per_thread, int *best_form);
 
 #ifdef __cplusplus
 }

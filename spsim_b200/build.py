@@ -7,6 +7,9 @@ statically and every symbol except the functions declared in include/*.h is
 hidden by a linker version script, so the library neither exports nor binds
 to another CUDA runtime loaded in the same process (PyTorch's, for example).
 
+Also builds spsim_b200/_lib/pipe_probe, the pipe-throughput probe bench.py
+runs for the measured FMA / MUFU peaks.
+
 Usage: python -m spsim_b200.build [--force] [--verbose]
 """
 import os
@@ -104,6 +107,10 @@ def build(force=False, verbose=False):
              ["-Xlinker", "--version-script=" + vmap, "-Xlinker", "-Bsymbolic", "-lrt", "-ldl", "-lpthread"],
              verbose)
         shutil.move(tmp, out)
+    probe = os.path.join(LIBDIR, "pipe_probe")
+    psrc = os.path.join(CSRC, "tools", "pipe_probe.cu")
+    if force or _newer(probe, [psrc]):
+        _run([NVCC] + ARCH + ["-O3", "-o", probe, psrc], verbose)
     return out
 
 

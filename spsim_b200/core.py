@@ -314,13 +314,18 @@ def last_forward_stats():
     return t.value, ms.value
 
 
-def set_variant(threads=-1, pixels_per_thread=-1, packed=1):
-    """Force an FP32 kernel variant (threads per CTA, pixels per thread, packed pixel pairs); threads < 0 = auto."""
-    check(lib().spsim_b200_set_variant(int(threads), int(pixels_per_thread), int(packed)))
+FORMS = {0: "compensated FP32, one pixel per lane", 1: "compensated FP32, pixel pairs (f32x2)",
+         2: "FP64 phase, FP32 sin/cos on pixel pairs (f32x2)"}
+
+
+def set_variant(threads=-1, pixels_per_thread=-1, form=2):
+    """Force an FP32 kernel variant: threads per CTA, pixels per thread and the
+    kernel form (FORMS); threads < 0 returns to automatic choice."""
+    check(lib().spsim_b200_set_variant(int(threads), int(pixels_per_thread), int(form)))
 
 
 def autotune(mol, qs, precision="f32", stream=None):
-    """Time every compiled FP32 kernel variant on this workload; returns (threads, pixels_per_thread, packed)."""
+    """Time every compiled FP32 kernel variant on this workload; returns (threads, pixels_per_thread, form)."""
     _native.use_device(mol.device)
     bt, bp, bk = c_int(0), c_int(0), c_int(0)
     check(lib().spsim_b200_autotune(mol.handle, qs.handle, _prec(precision), _stream_ptr(stream), byref(bt),

@@ -170,6 +170,7 @@ struct spsim_b200_molecule {
   int per_atom_b = 0, delta_atoms = 0;
   float4 *d_atoms = nullptr;
   float4 *d_atoms2 = nullptr;  // pixel-pair layout of the same records
+  AtomD *d_atomsd = nullptr;   // FP64-phase records
   TileDesc *d_tiles = nullptr;
   int *d_perm = nullptr;
   float *d_wbase = nullptr;
@@ -178,6 +179,7 @@ struct spsim_b200_molecule {
   ~spsim_b200_molecule() {
     cudaFree(d_atoms);
     cudaFree(d_atoms2);
+    cudaFree(d_atomsd);
     cudaFree(d_tiles);
     cudaFree(d_perm);
     cudaFree(d_wbase);
@@ -263,6 +265,7 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
   m->n_padded = n_pad;
   m->perm.assign(n_pad, -1);
   std::vector<float4> rec(2 * (size_t)std::max(n_pad, 1), make_float4(0, 0, 0, 0));
+  std::vector<AtomD> recd((size_t)std::max(n_pad, 1), AtomD{0.0, 0.0, 0.0, 0.0f, 0.0f});
   std::vector<float> wbase(std::max(n_pad, 1), 0.0f);
   {
     std::vector<int> fill(m->n_elem, 0);
@@ -294,6 +297,7 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
       const double hz = std::rint(r[2] * m->inv_dr) * m->dr;
       rec[2 * idx] = make_float4((float)hx, (float)hy, (float)hz, o * w);
       rec[2 * idx + 1] = make_float4((float)(r[0] - hx), (float)(r[1] - hy), (float)(r[2] - hz), bfac ? bfac[j] : 0.0f);
+      recd[idx] = AtomD{r[0], r[1], r[2], o * w, bfac ? bfac[j] : 0.0f};
     }
   }
   // tile table
@@ -323,6 +327,8 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
     CUDA_TRY(cudaMalloc(&m->d_atoms2, 4 * na * sizeof(float4)));
     CUDA_TRY(cudaMemcpy(m->d_atoms2, dup.data(), 4 * na * sizeof(float4), cudaMemcpyHostToDevice));
   }
+  CUDA_TRY(cudaMalloc(&m->d_atomsd, na * sizeof(AtomD)));
+  CUDA_TRY(cudaMemcpy(m->d_atomsd, recd.data(), na * sizeof(AtomD), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMalloc(&m->d_tiles, std::max<size_t>(m->tiles.size(), 1) * sizeof(TileDesc)));
   if (!m->tiles.empty())
     CUDA_TRY(cudaMemcpy(m->d_tiles, m->tiles.data(), m->tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice));
@@ -356,7 +362,7 @@ extern "C" int spsim_b200_molecule_update_device(spsim_b200_molecule *m, const v
   if (!m || !pos_dev) return fail(SPSIM_ERR_INVALID_ARG, "molecule or positions NULL");
   if (bfac_dev && !m->per_atom_b)
     return fail(SPSIM_ERR_INVALID_ARG, "molecule was created without per-atom B factors");
-  CUDA_TRY(launch_atoms_update(m->d_atoms, m->d_atoms2, m->d_perm, m->n_padded, pos_is_f64 ? nullptr : (const float *)pos_dev,
+  CUDA_TRY(launch_atoms_update(m->d_atoms, m->d_atoms2, m->d_atomsd, m->d_perm, m->n_padded, pos_is_f64 ? nullptr : (const float *)pos_dev,
                                pos_is_f64 ? (const double *)pos_dev : nullptr, occ_dev, bfac_dev, m->d_wbase,
                                m->center, m->dr, m->inv_dr, m->rbound, m->d_flags, (cudaStream_t)stream));
   return SPSIM_OK;
@@ -544,6 +550,7 @@ struct Plan {
   int precision = 0, nt = 128, ppt = 4, packed = 1;
   bool perb = false;
   std::vector<long long> npix_of;
+  std::vector<SfPattern> host_pats;  // descriptors as last uploaded (rotations change per call)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   ~Plan() {
@@ -554,7 +561,7 @@ struct Plan {
 
 static std::vector<std::unique_ptr<Plan>> g_plans;  // most recent last
 static const size_t kMaxPlans = 8;
-static int g_force_nt = -1, g_force_p = -1, g_force_pk = 1;
+static int g_force_nt = -1, g_force_p = -1, g_force_pk = 2;
 struct Variant {
   int nt, p, packed;
 };
@@ -576,13 +583,17 @@ static int num_sms() {
 
 static long long size_class(double terms) { return (long long)std::floor(std::log2(std::max(terms, 1.0)) / 2); }
 
-static Variant choose_variant(double terms, long long min_npix, int precision) {
+static Variant choose_variant(double terms, long long total_npix, int precision) {
   const int mode = precision == SPSIM_PREC_F32_FAST ? 1 : 0;
   if (g_force_nt > 0 && sf_f32_variant_exists(mode, g_force_nt, g_force_p, g_force_pk))
     return {g_force_nt, g_force_p, g_force_pk};
   auto it = g_tuned.find(size_class(terms) * 4 + precision);
   if (it != g_tuned.end()) return it->second;
-  return {128, (min_npix >= 65536) ? 4 : 2, 1};
+  // untuned defaults, from sweeps on B200: the FP64-phase form for FP32, the
+  // compensated pixel-pair form for FP32_FAST (MUFU sin/cos); more pixels per
+  // thread once there are enough pixel tiles to fill every SM several times
+  if (precision == SPSIM_PREC_F32_FAST) return {128, total_npix >= (1LL << 20) ? 6 : total_npix >= 65536 ? 4 : 2, 1};
+  return {128, total_npix >= (1LL << 20) ? 8 : total_npix >= 65536 ? 4 : 2, 2};
 }
 
 static bool is_orthonormal(const double *R) {
@@ -606,7 +617,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
   size_t ff_total = 0, acc_total = 0;
   std::vector<size_t> acc_off(npat), ffo(npat);
   double terms = 0;
-  long long min_npix = -1;
+  long long total_npix = 0;
   bool perb = false;
   for (int i = 0; i < npat; ++i) {
     const spsim_b200_molecule *m = mols[i];
@@ -624,7 +635,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     acc_off[i] = acc_total;
     acc_total += q->npix;
     terms += (double)q->npix * m->n_kept;
-    min_npix = min_npix < 0 ? q->npix : std::min(min_npix, q->npix);
+    total_npix += q->npix;
     perb = perb || m->per_atom_b;
   }
   pl.terms = terms;
@@ -636,7 +647,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
   CUDA_TRY(pl.pats.ensure(std::max(npat, 1) * sizeof(SfPattern)));
 
   Variant var = {128, 4, 1};
-  if (precision != SPSIM_PREC_FP64) var = choose_variant(terms, min_npix, precision);
+  if (precision != SPSIM_PREC_FP64) var = choose_variant(terms, total_npix, precision);
   const int nt = var.nt, ppt = var.p;
   pl.nt = var.nt;
   pl.ppt = var.p;
@@ -652,6 +663,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     memset(&pt, 0, sizeof(pt));
     pt.atoms = m->d_atoms;
     pt.atoms2 = m->d_atoms2;
+    pt.atomsd = m->d_atomsd;
     pt.tiles = m->d_tiles;
     pt.n_tiles = (int)m->tiles.size();
     pt.n_elem = m->n_elem;
@@ -684,7 +696,12 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     pt.I = I_dev ? I_dev[i] : nullptr;
     pl.max_npix = std::max(pl.max_npix, q->npix);
     pl.npix_of[i] = q->npix;
-    if (precision != SPSIM_PREC_FP64 && m->n_kept > 0 && q->npix > 0) {
+    if (precision != SPSIM_PREC_FP64 && pl.packed == 2 && m->n_kept > 0 && q->npix > 0) {
+      // FP64 phase: the half-cycle rounding needs |2 q.r| < 2^51
+      const double qr = qmax * m->rbound;
+      if (qr >= std::ldexp(1.0, 48))
+        return fail(SPSIM_ERR_RANGE, "pattern %d: |q|max*|r|max = %.3g cycles exceeds 2^48", i, qr);
+    } else if (precision != SPSIM_PREC_FP64 && m->n_kept > 0 && q->npix > 0) {
       // domain checks of the compensated phase
       const double qr = qmax * m->rbound;
       if (qr >= std::ldexp(1.0, 19))
@@ -699,6 +716,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     }
   }
   CUDA_TRY(cudaMemcpyAsync(pl.pats.p, pats.data(), npat * sizeof(SfPattern), cudaMemcpyHostToDevice, stream));
+  pl.host_pats = pats;
 
   if (precision != SPSIM_PREC_FP64) {
     // work items: pixel tile x atom-tile range, cost-sorted (largest first)
@@ -797,10 +815,27 @@ static void plan_key(int npat, const spsim_b200_molecule *const *mols, const sps
     kp.push_back(F_dev ? (const void *)F_dev[i] : nullptr);
     kp.push_back(I_dev ? (const void *)I_dev[i] : nullptr);
   }
+  // Orthonormal rotations only change the descriptors, which are re-uploaded
+  // per call; any other matrix changes the phase grid, so it keys the plan.
+  bool ortho = true;
   if (rot)
+    for (int i = 0; i < npat && ortho; ++i) ortho = is_orthonormal(rot + 9 * (size_t)i);
+  kv.push_back(rot ? (ortho ? 1.0 : 2.0) : 0.0);
+  if (rot && !ortho)
     for (long long k = 0; k < 9LL * npat; ++k) kv.push_back(rot[k]);
-  else
-    kv.push_back(-7.0);
+}
+
+// Write this call's rotations into the plan's descriptors (device copy ordered on `stream`).
+static cudaError_t refresh_rotations(Plan &pl, const double *rot, cudaStream_t stream) {
+  if (!rot) return cudaSuccess;
+  bool changed = false;
+  for (int i = 0; i < pl.npat; ++i)
+    if (memcmp(pl.host_pats[i].rot, rot + 9 * (size_t)i, 9 * sizeof(double)) != 0) {
+      memcpy(pl.host_pats[i].rot, rot + 9 * (size_t)i, 9 * sizeof(double));
+      changed = true;
+    }
+  if (!changed) return cudaSuccess;
+  return cudaMemcpyAsync(pl.pats.p, pl.host_pats.data(), pl.npat * sizeof(SfPattern), cudaMemcpyHostToDevice, stream);
 }
 
 static int check_flags(Plan &pl) {
@@ -867,6 +902,7 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
     }
   }
   g_last_terms = pl->terms;
+  CUDA_TRY(refresh_rotations(*pl, rot, stream));
   if (g_timing || !cache || stream == nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (g_timing) {
@@ -995,7 +1031,7 @@ extern "C" int spsim_b200_set_variant(int threads, int pixels_per_thread, int pa
   std::lock_guard<std::mutex> lk(g_mu);
   if (threads < 0) {
     g_force_nt = g_force_p = -1;
-    g_force_pk = 1;
+    g_force_pk = 2;
     return SPSIM_OK;
   }
   if (!sf_f32_variant_exists(0, threads, pixels_per_thread, packed) ||
@@ -1012,11 +1048,12 @@ extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b20
                                    void *stream, int *best_threads, int *best_pixels_per_thread, int *best_packed) {
   if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
   if (precision == SPSIM_PREC_FP64) return fail(SPSIM_ERR_INVALID_ARG, "the FP64 kernel has a single variant");
-  const int cand[][3] = {{128, 2, 0}, {128, 4, 0}, {256, 4, 0}, {128, 2, 1}, {128, 4, 1}, {256, 4, 1}, {128, 6, 1}};
+  const int cand[][3] = {{128, 2, 0}, {128, 4, 0}, {256, 4, 0}, {128, 2, 1}, {128, 4, 1}, {256, 4, 1},
+                         {128, 6, 1}, {128, 2, 2}, {128, 4, 2}, {256, 4, 2}, {128, 6, 2}, {128, 8, 2}};
   float *dI = nullptr;
   CUDA_TRY(cudaMalloc(&dI, std::max<long long>(qs->npix, 1) * sizeof(float)));
   float best = 1e30f;
-  int bt = 128, bp = 4, bk = 1;
+  int bt = 128, bp = 4, bk = 2;
   const int saved_nt = g_force_nt, saved_p = g_force_p, saved_pk = g_force_pk;
   const bool saved_timing = g_timing;
   int st = SPSIM_OK;

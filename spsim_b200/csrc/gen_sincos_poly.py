@@ -10,9 +10,12 @@ float32 Horner evaluation (with fused multiply-add, as the kernel does it) is
 measured and printed into the header.  No library sin/cos internals are used:
 the reference values come from numpy's float64 sin/cos.
 
-Two domains are generated:
-  HALF: |y| <= 1/4 + 1/16  (half-cycle reduction plus the phase cross-term)
-  QUAD: |y| <= 1/8 + 1/16  (quarter-cycle reduction plus the cross-term)
+Three domains are generated:
+  HALF:  |y| <= 1/4 + 1/16  (half-cycle reduction plus the phase cross-term)
+  QUAD:  |y| <= 1/8 + 1/16  (quarter-cycle reduction plus the cross-term)
+  DHALF: |y| <= 1/4         (half-cycle reduction of an FP64 phase, no cross-term)
+Degrees are the smallest whose float32 evaluation stays near the float32
+rounding floor (a higher sine degree on HALF only adds rounding error).
 
 Usage: python gen_sincos_poly.py > sincos_poly.h
 """
@@ -70,14 +73,21 @@ def f32_horner(coeffs32, z32):
 
 
 def fit(Y, sdeg, cdeg):
+    """Constant terms pinned: S_0 = float32(2 pi) and C_0 = 1, so phases near
+    zero (the bright forward-scattering pixels, where every atom's phase is
+    small) keep float32 relative accuracy; Remez fits the remaining
+    coefficients for the absolute error of sin and cos."""
     z_hi = Y * Y
-    # sin: P(z) ~ sin(2 pi sqrt z)/sqrt z, weight sqrt(z)
-    fs = lambda z: np.where(z > 0, np.sin(2 * np.pi * np.sqrt(z)) / np.sqrt(np.maximum(z, 1e-300)), 2 * np.pi)
-    ws = lambda z: np.sqrt(np.maximum(z, 1e-12))
-    fc = lambda z: np.cos(2 * np.pi * np.sqrt(z))
-    wc = lambda z: np.ones_like(z)
-    ps = remez(fs, ws, 0.0, z_hi, sdeg)
-    pc = remez(fc, wc, 0.0, z_hi, cdeg)
+    z_lo = z_hi * 1e-7  # keeps the vanishing weights below off zero
+    s0 = np.float64(np.float32(2 * np.pi))
+    # sin: P(z) = s0 + z P1(z) ~ sin(2 pi sqrt z)/sqrt z; the error of sin is sqrt(z) z (P1 - g)
+    gs = lambda z: (np.sin(2 * np.pi * np.sqrt(z)) / np.sqrt(z) - s0) / z
+    ws = lambda z: z ** 1.5
+    # cos: Q(z) = 1 + z Q1(z); the error of cos is z (Q1 - g)
+    gc = lambda z: (np.cos(2 * np.pi * np.sqrt(z)) - 1.0) / z
+    wc = lambda z: z
+    ps = np.concatenate([[s0], remez(gs, ws, z_lo, z_hi, sdeg - 1)])
+    pc = np.concatenate([[1.0], remez(gc, wc, z_lo, z_hi, cdeg - 1)])
     ps32 = ps.astype(np.float32)
     pc32 = pc.astype(np.float32)
     y = np.linspace(-Y, Y, 400001).astype(np.float32)
@@ -111,8 +121,9 @@ def main():
         "#ifndef SPSIM_B200_SINCOS_POLY_H",
         "#define SPSIM_B200_SINCOS_POLY_H",
     ]
-    emit("HALF", 0.25 + 1.0 / 16, 5, 5, out)
+    emit("HALF", 0.25 + 1.0 / 16, 4, 5, out)
     emit("QUAD", 0.125 + 1.0 / 16, 4, 4, out)
+    emit("DHALF", 0.25, 4, 4, out)
     out += ["#endif", ""]
     print("\n".join(out))
 

@@ -36,10 +36,18 @@ struct TileDesc {      // one shared-memory tile of a molecule
   int last;            // 1 if the tile ends its element segment
 };
 
+// FP64-phase record of one padded atom (32 bytes): r - centre in FP64, the
+// weight w = occ * sqrt(illumination) and the per-atom B factor.
+struct __align__(16) AtomD {
+  double x, y, z;
+  float w, b;
+};
+
 struct SfPattern {
   const float4 *atoms;     // 2 float4 per padded atom
   const float4 *atoms2;    // the same records duplicated for pixel pairs: 4 float4 per atom,
                            // {hx,hx,hy,hy} {hz,hz,w,w} {lx,lx,ly,ly} {lz,lz,b,b}
+  const AtomD *atomsd;     // FP64-phase records, one per padded atom
   const TileDesc *tiles;   // molecule tile table
   int n_tiles;
   int n_elem;
@@ -130,6 +138,34 @@ __device__ __forceinline__ void sincos_quad_poly(float y, float &s, float &c) {
   pc = fmaf(z, pc, SPSIM_QUAD_C0);
   s = y * ps;
   c = pc;
+}
+
+// sin(2 pi y), cos(2 pi y) for |y| <= 5/16 cycle (half-cycle reduction plus
+// the phase cross term): the wider-range pair from gen_sincos_poly.py.
+__device__ __forceinline__ void sincos_half_poly(float y, float &s, float &c) {
+  const float z = y * y;
+  float ps = fmaf(z, SPSIM_HALF_S4, SPSIM_HALF_S3);
+  ps = fmaf(z, ps, SPSIM_HALF_S2);
+  ps = fmaf(z, ps, SPSIM_HALF_S1);
+  ps = fmaf(z, ps, SPSIM_HALF_S0);
+  float pc = fmaf(z, SPSIM_HALF_C5, SPSIM_HALF_C4);
+  pc = fmaf(z, pc, SPSIM_HALF_C3);
+  pc = fmaf(z, pc, SPSIM_HALF_C2);
+  pc = fmaf(z, pc, SPSIM_HALF_C1);
+  pc = fmaf(z, pc, SPSIM_HALF_C0);
+  s = y * ps;
+  c = pc;
+}
+
+// (-1)^k w for an integer k whose bit 0 sits in bit 0 of kbits: one integer
+// multiply-add, w_bits + kbits * 2^31 (adding 2^31 flips the sign bit).  The
+// multiplier comes in as a register (m31 = 2^31, a kernel argument) so the
+// operation stays a single multiply-add on the FMA pipe instead of a shift and
+// a logic op.
+__device__ __forceinline__ float sign_by_parity(float w, uint32_t kbits, uint32_t m31) {
+  uint32_t r;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(kbits), "r"(m31), "r"(__float_as_uint(w)));
+  return __uint_as_float(r);
 }
 
 // Fast2Sum-style float-float accumulation of a block sum b into (hi, lo).

@@ -90,22 +90,15 @@ __device__ __forceinline__ void sf_term(const float4 a0, const float4 a1, float 
   c = fmaf(qly, a0.y, c);
   c = fmaf(qlz, a0.z, c);
   if (MODE == PREC_MODE_POLY) {
-    // quarter-cycle reduction: u = k/4 + y0 exactly, |y0| <= 1/8
-    const float t = fmaf(u, 4.0f, RINT_MAGIC);
+    // half-cycle reduction: u = k/2 + y0 exactly, |y0| <= 1/4; e^{2 pi i u} = (-1)^k e^{2 pi i y}
+    const float t = fmaf(u, 2.0f, RINT_MAGIC);
     const float kf = t - RINT_MAGIC;
-    const float y = fmaf(kf, -0.25f, u) + c;
-    const int ki = __float_as_int(t);
+    const float y = fmaf(kf, -0.5f, u) + c;
     float s, co;
-    sincos_quad_poly(y, s, co);
-    // e^{+2 pi i (k/4 + y)}: rotate (co, s) by k quarter turns
-    const bool odd = (ki & 1) != 0;
-    const float ca = odd ? s : co;
-    const float sa = odd ? co : s;
-    const unsigned wb = __float_as_uint(w);
-    const float wc = __uint_as_float(wb ^ (((unsigned)(ki + 1) << 30) & 0x80000000u));
-    const float ws = __uint_as_float(wb ^ (((unsigned)ki << 30) & 0x80000000u));
-    bc = fmaf(wc, ca, bc);  // sum w cos(2 pi u)
-    bs = fmaf(ws, sa, bs);  // sum w sin(2 pi u)
+    sincos_half_poly(y, s, co);
+    const float ws = __uint_as_float(__float_as_uint(w) ^ (__float_as_uint(t) << 31));
+    bc = fmaf(ws, co, bc);  // sum w cos(2 pi u)
+    bs = fmaf(ws, s, bs);   // sum w sin(2 pi u)
   } else {
     // whole-cycle reduction, MUFU sin/cos on |x| <= pi (1 + 1/8)
     const float t = u + RINT_MAGIC;
@@ -273,17 +266,6 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
-__device__ __forceinline__ void quadrant_select(float t, float s, float c, float w, float &wc, float &ca, float &ws,
-                                                float &sa) {
-  const int ki = __float_as_int(t);
-  const bool odd = (ki & 1) != 0;
-  ca = odd ? s : c;
-  sa = odd ? c : s;
-  const unsigned wb = __float_as_uint(w);
-  wc = __uint_as_float(wb ^ (((unsigned)(ki + 1) << 30) & 0x80000000u));
-  ws = __uint_as_float(wb ^ (((unsigned)ki << 30) & 0x80000000u));
-}
-
 template <int MODE, int NT, int P, bool PERB>
 __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restrict__ pats,
                                                       const WorkItem *__restrict__ items, int n_items,
@@ -408,24 +390,25 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
             c = fma2(qly[j], Hy, c);
             c = fma2(qlz[j], Hz, c);
             if (MODE == PREC_MODE_POLY) {
-              const float2 t = fma2(u, f2(4.0f), f2(RINT_MAGIC));
+              // half-cycle reduction, one sign per term: e^{2 pi i (k/2 + y)} = (-1)^k e^{2 pi i y}
+              const float2 t = fma2(u, f2(2.0f), f2(RINT_MAGIC));
               const float2 kf = add2(t, f2(-RINT_MAGIC));
-              const float2 y = add2(fma2(kf, f2(-0.25f), u), c);
+              const float2 y = add2(fma2(kf, f2(-0.5f), u), c);
               const float2 z = mul2(y, y);
-              float2 ps = fma2(z, f2(SPSIM_QUAD_S4), f2(SPSIM_QUAD_S3));
-              ps = fma2(z, ps, f2(SPSIM_QUAD_S2));
-              ps = fma2(z, ps, f2(SPSIM_QUAD_S1));
-              ps = fma2(z, ps, f2(SPSIM_QUAD_S0));
-              float2 pc = fma2(z, f2(SPSIM_QUAD_C4), f2(SPSIM_QUAD_C3));
-              pc = fma2(z, pc, f2(SPSIM_QUAD_C2));
-              pc = fma2(z, pc, f2(SPSIM_QUAD_C1));
-              pc = fma2(z, pc, f2(SPSIM_QUAD_C0));
+              float2 ps = fma2(z, f2(SPSIM_HALF_S4), f2(SPSIM_HALF_S3));
+              ps = fma2(z, ps, f2(SPSIM_HALF_S2));
+              ps = fma2(z, ps, f2(SPSIM_HALF_S1));
+              ps = fma2(z, ps, f2(SPSIM_HALF_S0));
+              float2 pc = fma2(z, f2(SPSIM_HALF_C5), f2(SPSIM_HALF_C4));
+              pc = fma2(z, pc, f2(SPSIM_HALF_C3));
+              pc = fma2(z, pc, f2(SPSIM_HALF_C2));
+              pc = fma2(z, pc, f2(SPSIM_HALF_C1));
+              pc = fma2(z, pc, f2(SPSIM_HALF_C0));
               const float2 S = mul2(y, ps);
-              float2 wc, ca, ws, sa;
-              quadrant_select(t.x, S.x, pc.x, w.x, wc.x, ca.x, ws.x, sa.x);
-              quadrant_select(t.y, S.y, pc.y, w.y, wc.y, ca.y, ws.y, sa.y);
-              bc[j] = fma2(wc, ca, bc[j]);
-              bs[j] = fma2(ws, sa, bs[j]);
+              const float2 ws = make_float2(__uint_as_float(__float_as_uint(w.x) ^ (__float_as_uint(t.x) << 31)),
+                                            __uint_as_float(__float_as_uint(w.y) ^ (__float_as_uint(t.y) << 31)));
+              bc[j] = fma2(ws, pc, bc[j]);
+              bs[j] = fma2(ws, S, bs[j]);
             } else {
               const float2 t = add2(u, f2(RINT_MAGIC));
               const float2 kf = add2(t, f2(-RINT_MAGIC));
@@ -474,6 +457,194 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
         const uint32_t bytes = (uint32_t)tn.count * 64u;
         mbar_arrive_expect_tx(&full_bar[st], bytes);
         bulk_copy_g2s(&ring[st][0], atoms2 + 4 * (long long)tn.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+      ++g_cons;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64-phase forward on pixel pairs.  B200 runs FP64 FMA at half the FP32 rate
+// and largely beside the FP32 pipe, so the phase q.(r - c) and its half-cycle
+// reduction are FP64 (3 + 3 DFMA per term, the reduction exact) and only the
+// sin/cos polynomial and the accumulation stay FP32, as packed f32x2
+// instructions.  The reduced phase |y| <= 1/4 carries no cross term, so the
+// polynomial pair is the shorter DHALF one and the only phase-range limit is
+// |q.r| < 2^50 cycles.  Atom records are AtomD (32 bytes), staged by the same
+// bulk-copy ring as the compensated kernels.
+
+template <int MODE, int NT, int P, bool PERB>
+__global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restrict__ pats,
+                                                       const WorkItem *__restrict__ items, int n_items,
+                                                       int *__restrict__ queue, int *__restrict__ err, uint32_t m31) {
+  static_assert(P % 2 == 0, "pixels per thread must be even");
+  constexpr int NP = P / 2;
+  __shared__ __align__(128) float4 ring[RING_STAGES][2 * TILE_ATOMS];
+  __shared__ __align__(8) uint64_t full_bar[RING_STAGES];
+  __shared__ int s_item;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < RING_STAGES; ++s) mbar_init(&full_bar[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  uint32_t g_issue = 0, g_cons = 0;
+  const long long kWaitCycles = 4000000000LL;
+  const double M52 = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const WorkItem wi = items[it];
+    const SfPattern &pt = pats[wi.pattern];
+    const long long npix = pt.npix;
+    const AtomD *__restrict__ atomsd = pt.atomsd;
+    const TileDesc *__restrict__ tiles = pt.tiles;
+
+    double qx[P], qy[P], qz[P];
+    float s2n[P];
+    long long pix[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      const long long p = (long long)wi.pixel_tile * (NT * P) + i * NT + tid;
+      pix[i] = p;
+      double q[3] = {0.0, 0.0, 0.0};
+      if (p < npix) load_q(pt, p, q);
+      qx[i] = q[0];
+      qy[i] = q[1];
+      qz[i] = q[2];
+      s2n[i] = (float)(-0.25 * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 1.4426950408889634);
+    }
+    float2 shc[NP], slc[NP], shs[NP], sls[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) shc[j] = slc[j] = shs[j] = sls[j] = make_float2(0.f, 0.f);
+
+    const int k0 = wi.k0, k1 = wi.k1;
+    if (tid == 0) {
+      for (int k = k0; k < k1 && k < k0 + RING_STAGES; ++k) {
+        const TileDesc td = tiles[k];
+        const uint32_t st = g_issue % RING_STAGES;
+        const uint32_t bytes = (uint32_t)td.count * (uint32_t)sizeof(AtomD);
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atomsd + td.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+    }
+
+    for (int k = k0; k < k1; ++k) {
+      const uint32_t st = g_cons % RING_STAGES;
+      const uint32_t par = (g_cons / RING_STAGES) & 1u;
+      const bool ok = mbar_wait_bounded(&full_bar[st], par, kWaitCycles);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicOr(err, 1);
+          for (uint32_t g = g_cons; g < g_issue; ++g)
+            mbar_wait_bounded(&full_bar[g % RING_STAGES], (g / RING_STAGES) & 1u, kWaitCycles);
+        }
+        return;
+      }
+      const TileDesc td = tiles[k];
+      const float4 *__restrict__ ta = ring[st];
+      for (int a = 0; a < td.count; a += ATOM_GROUP) {
+        float2 bc[NP], bs[NP];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) bc[j] = bs[j] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int g = 0; g < ATOM_GROUP; ++g) {
+          const float4 d0 = ta[2 * (a + g)], d1 = ta[2 * (a + g) + 1];
+          const double rx = __hiloint2double(__float_as_int(d0.y), __float_as_int(d0.x));
+          const double ry = __hiloint2double(__float_as_int(d0.w), __float_as_int(d0.z));
+          const double rz = __hiloint2double(__float_as_int(d1.y), __float_as_int(d1.x));
+          const float W = d1.z;
+#pragma unroll
+          for (int j = 0; j < NP; ++j) {
+            float y[2], w[2];
+            uint32_t kb[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int i = 2 * j + h;
+              double u = qx[i] * rx;
+              u = fma(qy[i], ry, u);
+              u = fma(qz[i], rz, u);
+              if (MODE == PREC_MODE_POLY) {
+                const double t = fma(u, 2.0, M52);  // rint(2u) in the low bits
+                y[h] = __double2float_rn(fma(t - M52, -0.5, u));  // u - k/2, exact before the rounding
+                kb[h] = (uint32_t)__double2loint(t);
+              } else {
+                const double t = u + M52;
+                y[h] = __double2float_rn(u - (t - M52));
+                kb[h] = 0;
+              }
+              w[h] = PERB ? W * exp2f(d1.w * s2n[i]) : W;
+            }
+            const float2 yy = make_float2(y[0], y[1]);
+            if (MODE == PREC_MODE_POLY) {
+              // e^{2 pi i (k/2 + y)} = (-1)^k e^{2 pi i y}, |y| <= 1/4
+              const float2 z = mul2(yy, yy);
+              float2 ps = fma2(z, f2(SPSIM_DHALF_S4), f2(SPSIM_DHALF_S3));
+              ps = fma2(z, ps, f2(SPSIM_DHALF_S2));
+              ps = fma2(z, ps, f2(SPSIM_DHALF_S1));
+              ps = fma2(z, ps, f2(SPSIM_DHALF_S0));
+              float2 pc = fma2(z, f2(SPSIM_DHALF_C4), f2(SPSIM_DHALF_C3));
+              pc = fma2(z, pc, f2(SPSIM_DHALF_C2));
+              pc = fma2(z, pc, f2(SPSIM_DHALF_C1));
+              pc = fma2(z, pc, f2(SPSIM_DHALF_C0));
+              const float2 S = mul2(yy, ps);
+              const float2 ws = make_float2(sign_by_parity(w[0], kb[0], m31), sign_by_parity(w[1], kb[1], m31));
+              bc[j] = fma2(ws, pc, bc[j]);
+              bs[j] = fma2(ws, S, bs[j]);
+            } else {
+              const float2 x = mul2(yy, f2(6.28318530717958648f));
+              float2 sn, cs;
+              __sincosf(x.x, &sn.x, &cs.x);
+              __sincosf(x.y, &sn.y, &cs.y);
+              const float2 ww = make_float2(w[0], w[1]);
+              bc[j] = fma2(ww, cs, bc[j]);
+              bs[j] = fma2(ww, sn, bs[j]);
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          // Fast2Sum of the group sums into the float-float element sums
+          float2 s1 = add2(shc[j], bc[j]);
+          slc[j] = add2(slc[j], add2(bc[j], make_float2(-(s1.x - shc[j].x), -(s1.y - shc[j].y))));
+          shc[j] = s1;
+          float2 s2 = add2(shs[j], bs[j]);
+          sls[j] = add2(sls[j], add2(bs[j], make_float2(-(s2.x - shs[j].x), -(s2.y - shs[j].y))));
+          shs[j] = s2;
+        }
+      }
+      if (td.last || k == k1 - 1) {
+        const double *__restrict__ ffe = pt.ff + (long long)td.elem * npix;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const long long p = pix[2 * j + h];
+            if (p < npix) {
+              const double f = ffe[p];
+              const double re = h ? (double)shc[j].y + (double)slc[j].y : (double)shc[j].x + (double)slc[j].x;
+              const double sm = h ? (double)shs[j].y + (double)sls[j].y : (double)shs[j].x + (double)sls[j].x;
+              atomicAdd(&pt.acc[p].x, f * re);
+              atomicAdd(&pt.acc[p].y, -f * sm);
+            }
+          }
+          shc[j] = slc[j] = shs[j] = sls[j] = make_float2(0.f, 0.f);
+        }
+      }
+      __syncthreads();
+      if (tid == 0 && k + RING_STAGES < k1) {
+        const TileDesc tn = tiles[k + RING_STAGES];
+        const uint32_t bytes = (uint32_t)tn.count * (uint32_t)sizeof(AtomD);
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atomsd + tn.atom_begin, bytes, &full_bar[st]);
         ++g_issue;
       }
       ++g_cons;
@@ -578,7 +749,7 @@ __global__ void ewald_kernel(int nx, int ny, double width, double height, double
 // ---------------------------------------------------------------------------
 // refinement: rewrite atom records from device positions (caller order)
 
-__global__ void atoms_update_kernel(float4 *__restrict__ atoms, float4 *__restrict__ atoms2,
+__global__ void atoms_update_kernel(float4 *__restrict__ atoms, float4 *__restrict__ atoms2, AtomD *__restrict__ atomsd,
                                     const int *__restrict__ perm, int n_padded,
                                     const float *__restrict__ pos32, const double *__restrict__ pos64,
                                     const float *__restrict__ occ, const float *__restrict__ bfac,
@@ -617,6 +788,7 @@ __global__ void atoms_update_kernel(float4 *__restrict__ atoms, float4 *__restri
   atoms2[4 * j + 1] = make_float4(a0.z, a0.z, a0.w, a0.w);
   atoms2[4 * j + 2] = make_float4(a1.x, a1.x, a1.y, a1.y);
   atoms2[4 * j + 3] = make_float4(a1.z, a1.z, a1.w, a1.w);
+  atomsd[j] = AtomD{r[0], r[1], r[2], a0.w, a1.w};
 }
 
 // ---------------------------------------------------------------------------
@@ -630,12 +802,15 @@ cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix,
   return cudaGetLastError();
 }
 
-// Variants: (mode, threads, pixels per thread, packed).  packed == 1 selects
-// the pixel-pair kernel (sf_f32x2_kernel), 0 the scalar one (sf_f32_kernel).
+// Variants: (mode, threads, pixels per thread, form).  form 0 selects the
+// scalar compensated kernel (sf_f32_kernel), 1 the pixel-pair compensated one
+// (sf_f32x2_kernel), 2 the pixel-pair FP64-phase one (sf_dphase_kernel).
 template <int MODE, int NT, int P, bool PERB, int PK>
 static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, int n_items, int *queue, int *err,
                                 int grid, cudaStream_t st) {
-  if (PK)
+  if constexpr (PK == 2)
+    sf_dphase_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
+  else if constexpr (PK == 1)
     sf_f32x2_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err);
   else
     sf_f32_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err);
@@ -645,7 +820,9 @@ static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, in
 template <int MODE, int NT, int P, bool PERB, int PK>
 static int occupancy_t() {
   int n = 0;
-  if (PK)
+  if constexpr (PK == 2)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dphase_kernel<MODE, NT, P, PERB>, NT, 0);
+  else if constexpr (PK == 1)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_f32x2_kernel<MODE, NT, P, PERB>, NT, 0);
   else
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_f32_kernel<MODE, NT, P, PERB>, NT, 0);
@@ -666,7 +843,17 @@ static int occupancy_t() {
   X(1, 128, 2, 1)             \
   X(1, 128, 4, 1)             \
   X(1, 256, 4, 1)             \
-  X(1, 128, 6, 1)
+  X(1, 128, 6, 1)             \
+  X(0, 128, 2, 2)             \
+  X(0, 128, 4, 2)             \
+  X(0, 256, 4, 2)             \
+  X(0, 128, 6, 2)             \
+  X(0, 128, 8, 2)             \
+  X(1, 128, 2, 2)             \
+  X(1, 128, 4, 2)             \
+  X(1, 256, 4, 2)             \
+  X(1, 128, 6, 2)             \
+  X(1, 128, 8, 2)
 
 cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
                           const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st) {
@@ -730,12 +917,12 @@ cudaError_t launch_ewald(int nx, int ny, double width, double height, double dis
   return cudaGetLastError();
 }
 
-cudaError_t launch_atoms_update(float4 *atoms, float4 *atoms2, const int *perm, int n_padded, const float *pos32,
+cudaError_t launch_atoms_update(float4 *atoms, float4 *atoms2, AtomD *atomsd, const int *perm, int n_padded, const float *pos32,
                                 const double *pos64, const float *occ, const float *bfac, const float *wbase,
                                 const double c[3], float dr, float inv_dr, double rbound, int *range_err,
                                 cudaStream_t st) {
   if (n_padded <= 0) return cudaSuccess;
-  atoms_update_kernel<<<(n_padded + 255) / 256, 256, 0, st>>>(atoms, atoms2, perm, n_padded, pos32, pos64, occ, bfac, wbase,
+  atoms_update_kernel<<<(n_padded + 255) / 256, 256, 0, st>>>(atoms, atoms2, atomsd, perm, n_padded, pos32, pos64, occ, bfac, wbase,
                                                              c[0], c[1], c[2], dr, inv_dr, rbound, range_err);
   return cudaGetLastError();
 }

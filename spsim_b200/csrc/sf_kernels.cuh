@@ -18,7 +18,7 @@ cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cu
 cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st);
 cudaError_t launch_ewald(int nx, int ny, double width, double height, double distance, double cx, double cy,
                          double wavelength, int spherical, float *out32, double *out64, cudaStream_t st);
-cudaError_t launch_atoms_update(float4 *atoms, float4 *atoms2, const int *perm, int n_padded, const float *pos32,
+cudaError_t launch_atoms_update(float4 *atoms, float4 *atoms2, AtomD *atomsd, const int *perm, int n_padded, const float *pos32,
                                 const double *pos64, const float *occ, const float *bfac, const float *wbase,
                                 const double c[3], float dr, float inv_dr, double rbound, int *range_err,
                                 cudaStream_t st);

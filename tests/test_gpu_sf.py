@@ -168,16 +168,49 @@ def test_batch_equals_single_patterns(cuda):
 
 
 def test_range_error_is_reported(cuda):
-    # a 2 um object at 3e9 1/m is outside the compensated kernel's phase domain
+    # a 2 um object at 3e9 1/m (6000 cycles) is outside the compensated kernels'
+    # phase domain; the FP64-phase form (the default) has no such limit
     Z = np.array([6, 6], np.int32)
     pos = np.array([[-1e-6, 0, 0], [1e-6, 0, 0]], np.float32)
     mol = core.Molecule(Z, pos)
-    qs = core.QSet.from_list(np.array([[3e9, 0, 0]], np.float32))
+    hkl = np.array([[3e9, 0, 0], [2.9e9, 1e8, 3e7]], np.float32)
+    qs = core.QSet.from_list(hkl)
     from spsim_b200._native import SpsimError, SPSIM_ERR_RANGE
 
-    with pytest.raises(SpsimError) as e:
-        core.forward(mol, qs, precision="f32")
-    assert e.value.status == SPSIM_ERR_RANGE
+    F64, I64 = O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64))
+    try:
+        for form in (0, 1):
+            core.set_variant(128, 4, form)
+            with pytest.raises(SpsimError) as e:
+                core.forward(mol, qs, precision="f32")
+            assert e.value.status == SPSIM_ERR_RANGE
+        core.set_variant(128, 4, 2)
+        F, I = core.forward(mol, qs, precision="f32")
+        assert np.abs(I.cpu().numpy() - I64).max() < 1e-5 * I64.max()
+    finally:
+        core.set_variant(-1)
     F, I = core.forward(mol, qs, precision="fp64")
-    F64, I64 = O.structure_factor(Z, pos.astype(np.float64), np.array([[3e9, 0, 0]]))
     assert np.abs(I.cpu().numpy() - I64).max() < 2e-7 * I64.max()
+
+
+VARIANTS = [(128, 2, 0), (256, 4, 0), (128, 4, 1), (128, 6, 1), (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 8, 2)]
+
+
+@pytest.mark.parametrize("precision", ["f32", "f32_fast"])
+@pytest.mark.parametrize("variant", VARIANTS, ids=["%dx%d_form%d" % v for v in VARIANTS])
+def test_every_kernel_form_meets_tolerance(cuda, precision, variant):
+    # each compiled variant, forced, on the plain 1k workload and with per-atom B factors
+    g = golden("sf_plain1k.npz")
+    F64, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64))
+    rng = np.random.Generator(np.random.PCG64(17))
+    bfac = rng.uniform(0, 40, len(g["Z"])).astype(np.float32)
+    F64b, I64b = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64), bfac=bfac)
+    try:
+        core.set_variant(*variant)
+        F, I = _run(g["Z"], g["pos"], g["hkl"], precision)
+        Fb, Ib = _run(g["Z"], g["pos"], g["hkl"], precision, bfac=bfac)
+    finally:
+        core.set_variant(-1)
+    for got, want in ((I, I64), (Ib, I64b)):
+        e_max, e_l2 = intensity_errors(got, want)
+        assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1], (variant, e_max, e_l2)
