@@ -480,9 +480,13 @@ def _adjoint_ratio(prec):
     return statistics.median(tb) / statistics.median(ta)
 
 
+PROFILE_VARIANTS = {"f32": (128, 8, 2), "f32_fast": (128, 6, 1)}  # the untuned defaults on the 1024^2 workload
+
+
 def profile_case(precisions):
-    """One forward per precision on the 20,000-atom / 256^2 case (~1.3e9 terms):
-    a short, small-memory command for ncu captures."""
+    """One forward per precision on the 20,000-atom / 256^2 case (~1.3e9 terms),
+    each with the kernel variant the benchmark workload runs by default: a
+    short, small-memory command for ncu captures."""
     import torch
 
     from spsim_b200 import core, synth
@@ -492,9 +496,10 @@ def profile_case(precisions):
     d = w["det"]
     mol = core.Molecule(Z, pos)
     qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
-    core.set_variant(128, 4, 1)
     for p in precisions:
+        core.set_variant(*PROFILE_VARIANTS[p])
         core.forward(mol, qs, precision=p)
+    core.set_variant(-1)
     torch.cuda.synchronize()
     core.synchronize()
     print("profile case ok")

@@ -4,8 +4,8 @@
 //   dL/dB_j   = -2 w_j       sum_p g_p f_e(p) E_pj s_p^2 Re(...)
 // with A_p = e^{+2 pi i q_p.c} F_p the centred amplitude, u_pj = q_p.(r_j - c),
 // E_pj = exp(-B_j s_p^2) (1 without per-atom B) and s^2 = (|q| 1e-10)^2 / 4.
-// Phases are recomputed with the forward's compensated arithmetic; nothing of
-// size atoms x pixels is stored.  One CTA owns a block of atoms of one element
+// Phases are recomputed with the forward's arithmetic (compensated FP32 or the
+// FP64-phase form); nothing of size atoms x pixels is stored.  One CTA owns a block of atoms of one element
 // (registers) and streams a range of pixel records through shared memory.
 #include "adjoint_kernels.cuh"
 
@@ -14,6 +14,46 @@ namespace spsim {
 // pixel record: 4 x float4
 //   {qhx, qhy, qhz, qx} {qy, qz, qlx, qly} {qlz, hr, hi, s2} {s2n, 0, 0, 0}
 constexpr int ADJ_PIX_TILE = 256;
+
+// One pixel of the adjoint: q (rotated, FP64), (hr, hi) = g_p f_e(p) A_p with
+// the centred amplitude A_p = e^{+2 pi i q.c} F_p, and s^2 = (|q| 1e-10)^2 / 4.
+__device__ __forceinline__ void adj_pixel(const AdjParams &prm, int elem, long long gp, double q[3], double &hr,
+                                          double &hi, double &s2) {
+  const int pat = (int)(gp / prm.npix);
+  const long long p = gp - (long long)pat * prm.npix;
+  double a, b, c;
+  if (prm.hkl) {
+    a = prm.hkl[3 * p];
+    b = prm.hkl[3 * p + 1];
+    c = prm.hkl[3 * p + 2];
+  } else {
+    a = prm.q64[3 * p];
+    b = prm.q64[3 * p + 1];
+    c = prm.q64[3 * p + 2];
+  }
+  if (prm.rot) {
+    const double *R = prm.rot + 9 * pat;
+    q[0] = R[0] * a + R[1] * b + R[2] * c;
+    q[1] = R[3] * a + R[4] * b + R[5] * c;
+    q[2] = R[6] * a + R[7] * b + R[8] * c;
+  } else {
+    q[0] = a;
+    q[1] = b;
+    q[2] = c;
+  }
+  // centred amplitude A = e^{+2 pi i q.c} F
+  double t = q[0] * prm.cx + q[1] * prm.cy + q[2] * prm.cz;
+  t -= rint(t);
+  double sn, cs;
+  sincospi(2.0 * t, &sn, &cs);
+  const float2 F = prm.F[gp];
+  const double ar = F.x * cs - F.y * sn;
+  const double ai = F.x * sn + F.y * cs;
+  const double h = (double)prm.G[gp] * prm.ff[(long long)elem * prm.npix + p];
+  hr = h * ar;
+  hi = h * ai;
+  s2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 0.25;
+}
 
 template <int MODE>
 __device__ __forceinline__ void adj_sincos(const float4 a0, const float4 a1, const float4 p0, const float4 p1,
@@ -78,45 +118,14 @@ __global__ void __launch_bounds__(NT) adj_kernel(AdjParams prm) {
       float4 r0 = make_float4(0, 0, 0, 0), r1 = r0, r2 = r0, r3 = r0;
       if (i < n) {
         const long long gp = base + i;
-        const int pat = (int)(gp / prm.npix);
-        const long long p = gp - (long long)pat * prm.npix;
-        double q[3];
-        double a, b, c;
-        if (prm.hkl) {
-          a = prm.hkl[3 * p];
-          b = prm.hkl[3 * p + 1];
-          c = prm.hkl[3 * p + 2];
-        } else {
-          a = prm.q64[3 * p];
-          b = prm.q64[3 * p + 1];
-          c = prm.q64[3 * p + 2];
-        }
-        if (prm.rot) {
-          const double *R = prm.rot + 9 * pat;
-          q[0] = R[0] * a + R[1] * b + R[2] * c;
-          q[1] = R[3] * a + R[4] * b + R[5] * c;
-          q[2] = R[6] * a + R[7] * b + R[8] * c;
-        } else {
-          q[0] = a;
-          q[1] = b;
-          q[2] = c;
-        }
+        double q[3], hr, hi, s2;
+        adj_pixel(prm, blk.elem, gp, q, hr, hi, s2);
         const double hx = (double)rintf((float)q[0] * prm.inv_dq) * prm.dq;
         const double hy = (double)rintf((float)q[1] * prm.inv_dq) * prm.dq;
         const double hz = (double)rintf((float)q[2] * prm.inv_dq) * prm.dq;
-        // centred amplitude A = e^{+2 pi i q.c} F
-        double t = q[0] * prm.cx + q[1] * prm.cy + q[2] * prm.cz;
-        t -= rint(t);
-        double sn, cs;
-        sincospi(2.0 * t, &sn, &cs);
-        const float2 F = prm.F[gp];
-        const double ar = F.x * cs - F.y * sn;
-        const double ai = F.x * sn + F.y * cs;
-        const double h = (double)prm.G[gp] * prm.ff[(long long)blk.elem * prm.npix + p];
-        const double s2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 0.25;
         r0 = make_float4((float)hx, (float)hy, (float)hz, (float)q[0]);
         r1 = make_float4((float)q[1], (float)q[2], (float)(q[0] - hx), (float)(q[1] - hy));
-        r2 = make_float4((float)(q[2] - hz), (float)(h * ar), (float)(h * ai), (float)s2);
+        r2 = make_float4((float)(q[2] - hz), (float)hr, (float)hi, (float)s2);
         r3 = make_float4((float)(-s2 * 1.4426950408889634), 0, 0, 0);
       }
       pix[4 * i] = r0;
@@ -166,6 +175,127 @@ __global__ void __launch_bounds__(NT) adj_kernel(AdjParams prm) {
     const int src = prm.perm[aidx[k]];
     if (src < 0) continue;
     const double w = a0[k].w, wb = prm.wbase[aidx[k]];
+    const double kp = 4.0 * 3.14159265358979323846 * w;
+    atomicAdd(&prm.dpos[3 * src], kp * gx[k]);
+    atomicAdd(&prm.dpos[3 * src + 1], kp * gy[k]);
+    atomicAdd(&prm.dpos[3 * src + 2], kp * gz[k]);
+    if (prm.docc) atomicAdd(&prm.docc[src], 2.0 * wb * go[k]);
+    if (prm.dB) atomicAdd(&prm.dB[src], -2.0 * w * gb[k]);
+  }
+}
+
+// FP64-phase adjoint: the phase u = q.(r - c) and its half-cycle reduction in
+// FP64 (as in the FP64-phase forward), sin/cos and the five gradient sums in
+// packed f32x2 over pairs of atoms.  Each thread holds A atoms (A/2 pairs) in
+// registers; a CTA streams pixel records through shared memory:
+//   pq[2i]   = {qx, qy}  pq[2i+1] = {qz, 0}          (FP64)
+//   pf[2i]   = {qx, qy, qz, hr}  pf[2i+1] = {hi, s2, s2n, 0}   (FP32)
+// Per term the sign (-1)^k of the half-cycle reduction is applied to the two
+// products z = H conj(A) e^{-2 pi i u} with one integer multiply-add each.
+template <int NT, int A, bool PERB>
+__global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t m31) {
+  static_assert(A % 2 == 0, "atoms per thread must be even");
+  constexpr int NP = A / 2;
+  __shared__ __align__(16) double2 pq[ADJ_PIX_TILE * 2];
+  __shared__ __align__(16) float4 pf[ADJ_PIX_TILE * 2];
+  const int tid = threadIdx.x;
+  const AdjItem item = prm.items[blockIdx.x];
+  const AdjBlock blk = prm.blocks[item.block];
+  const double M52 = 6755399441055744.0;  // 1.5 * 2^52
+
+  double rx[A], ry[A], rz[A];
+  float bfac[A];
+  int aidx[A];
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    aidx[k] = blk.atom_begin + tid + k * NT;
+    rx[k] = ry[k] = rz[k] = 0.0;
+    bfac[k] = 0.0f;
+    if (aidx[k] < blk.atom_end) {
+      const AtomD a = prm.atomsd[aidx[k]];
+      rx[k] = a.x;
+      ry[k] = a.y;
+      rz[k] = a.z;
+      bfac[k] = a.b;
+    }
+  }
+  double gx[A], gy[A], gz[A], go[A], gb[A];
+#pragma unroll
+  for (int k = 0; k < A; ++k) gx[k] = gy[k] = gz[k] = go[k] = gb[k] = 0.0;
+
+  for (long long base = item.pix_begin; base < item.pix_end; base += ADJ_PIX_TILE) {
+    const int n = (int)min((long long)ADJ_PIX_TILE, item.pix_end - base);
+    __syncthreads();
+    for (int i = tid; i < ADJ_PIX_TILE; i += NT) {
+      double q[3] = {0.0, 0.0, 0.0}, hr = 0.0, hi = 0.0, s2 = 0.0;
+      if (i < n) adj_pixel(prm, blk.elem, base + i, q, hr, hi, s2);
+      pq[2 * i] = make_double2(q[0], q[1]);
+      pq[2 * i + 1] = make_double2(q[2], 0.0);
+      pf[2 * i] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)hr);
+      pf[2 * i + 1] = make_float4((float)hi, (float)s2, (float)(-s2 * 1.4426950408889634), 0.0f);
+    }
+    __syncthreads();
+    // sums of z_i = -Im part (so that dL/dr = -4 pi w sum z_i q) and z_r
+    float2 fx[NP], fy[NP], fz[NP], fo[NP], fb[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) fx[j] = fy[j] = fz[j] = fo[j] = fb[j] = make_float2(0.f, 0.f);
+    for (int i = 0; i < n; ++i) {
+      const double2 qa = pq[2 * i], qb = pq[2 * i + 1];
+      const float4 f0 = pf[2 * i], f1 = pf[2 * i + 1];
+      const float2 hr = f2(f0.w), nhi = f2(-f1.x), hi = f2(f1.x);
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        float y[2];
+        uint32_t kb[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int k = 2 * j + h;
+          double u = qa.x * rx[k];
+          u = fma(qa.y, ry[k], u);
+          u = fma(qb.x, rz[k], u);
+          const double t = fma(u, 2.0, M52);
+          y[h] = __double2float_rn(fma(t - M52, -0.5, u));
+          kb[h] = (uint32_t)__double2loint(t);
+        }
+        float2 S, C;
+        sincos_dhalf_poly2(make_float2(y[0], y[1]), S, C);
+        // H conj(A) e^{-2 pi i u} = (hr C - hi S) - i (hr S + hi C), times (-1)^k
+        float2 zr = fma2(nhi, S, mul2(hr, C));
+        float2 zn = fma2(hi, C, mul2(hr, S));  // = -Im
+        zr = make_float2(sign_by_parity(zr.x, kb[0], m31), sign_by_parity(zr.y, kb[1], m31));
+        zn = make_float2(sign_by_parity(zn.x, kb[0], m31), sign_by_parity(zn.y, kb[1], m31));
+        if (PERB) {
+          const float2 E = make_float2(exp2f(bfac[2 * j] * f1.z), exp2f(bfac[2 * j + 1] * f1.z));
+          zr = mul2(zr, E);
+          zn = mul2(zn, E);
+        }
+        fx[j] = fma2(zn, f2(f0.x), fx[j]);
+        fy[j] = fma2(zn, f2(f0.y), fy[j]);
+        fz[j] = fma2(zn, f2(f0.z), fz[j]);
+        fo[j] = add2(fo[j], zr);
+        fb[j] = fma2(zr, f2(f1.y), fb[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      gx[2 * j] -= fx[j].x;
+      gx[2 * j + 1] -= fx[j].y;
+      gy[2 * j] -= fy[j].x;
+      gy[2 * j + 1] -= fy[j].y;
+      gz[2 * j] -= fz[j].x;
+      gz[2 * j + 1] -= fz[j].y;
+      go[2 * j] += fo[j].x;
+      go[2 * j + 1] += fo[j].y;
+      gb[2 * j] += fb[j].x;
+      gb[2 * j + 1] += fb[j].y;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    if (aidx[k] >= blk.atom_end) continue;
+    const int src = prm.perm[aidx[k]];
+    if (src < 0) continue;
+    const double w = prm.atomsd[aidx[k]].w, wb = prm.wbase[aidx[k]];
     const double kp = 4.0 * 3.14159265358979323846 * w;
     atomicAdd(&prm.dpos[3 * src], kp * gx[k]);
     atomicAdd(&prm.dpos[3 * src + 1], kp * gy[k]);
@@ -248,6 +378,12 @@ cudaError_t launch_adjoint(int precision_mode, const AdjParams &prm, int n_items
   if (n_items <= 0) return cudaSuccess;
   if (precision_mode == 2) {
     adj_f64_kernel<ADJ_THREADS><<<n_items, ADJ_THREADS, 0, st>>>(prm);
+  } else if (precision_mode == 3) {
+    if (prm.per_atom_b)
+      adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, true><<<n_items, ADJ_THREADS, 0, st>>>(prm, 0x80000000u);
+    else
+      adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, false><<<n_items, ADJ_THREADS, 0, st>>>(prm,
+                                                                                                      0x80000000u);
   } else if (precision_mode == 0) {
     if (prm.per_atom_b)
       adj_kernel<0, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, true><<<n_items, ADJ_THREADS, 0, st>>>(prm);

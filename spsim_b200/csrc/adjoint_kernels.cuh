@@ -8,6 +8,8 @@ namespace spsim {
 constexpr int ADJ_THREADS = 128;
 constexpr int ADJ_ATOMS_PER_THREAD = 2;
 constexpr int ADJ_BLOCK_ATOMS = ADJ_THREADS * ADJ_ATOMS_PER_THREAD;
+constexpr int ADJ_DPHASE_ATOMS_PER_THREAD = 4;
+constexpr int ADJ_DPHASE_BLOCK_ATOMS = ADJ_THREADS * ADJ_DPHASE_ATOMS_PER_THREAD;
 
 struct AdjBlock {   // atoms [atom_begin, atom_end) of one element
   int atom_begin, atom_end, elem, pad;
@@ -20,6 +22,7 @@ struct AdjItem {    // one CTA: an atom block x a range of (pattern, pixel) indi
 
 struct AdjParams {
   const float4 *atoms;
+  const AtomD *atomsd;
   const int *perm;
   const float *wbase;
   const AdjBlock *blocks;
@@ -37,7 +40,8 @@ struct AdjParams {
   double *dpos, *docc, *dB;
 };
 
-// precision_mode: 0 polynomial FP32, 1 MUFU FP32, 2 plain FP64
+// precision_mode: 0 compensated FP32 polynomial, 1 compensated FP32 MUFU,
+// 2 plain FP64, 3 FP64 phase with FP32 polynomial (packed over atom pairs)
 cudaError_t launch_adjoint(int precision_mode, const AdjParams &prm, int n_items, cudaStream_t st);
 
 }  // namespace spsim

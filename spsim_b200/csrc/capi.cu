@@ -1276,7 +1276,12 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   const int eq = ceil_log2_bound(std::max(qmax, 1e-300));
   const int kq = 22 - m->kr;
   const float dq = (float)std::ldexp(1.0, eq - kq);
-  if (precision != SPSIM_PREC_FP64 && m->n_kept > 0) {
+  // FP32 adjoints follow the forward's kernel form: the FP64-phase one unless
+  // a compensated form is forced with spsim_b200_set_variant
+  const bool dphase = precision == SPSIM_PREC_F32 && !(g_force_nt > 0 && g_force_pk != 2);
+  if (dphase && qmax * m->rbound >= std::ldexp(1.0, 48))
+    return fail(SPSIM_ERR_RANGE, "adjoint: |q|max*|r|max exceeds 2^48 cycles");
+  if (precision != SPSIM_PREC_FP64 && !dphase && m->n_kept > 0) {
     const double cmax = 0.8660254037844386 * (qmax * m->dr + (double)dq * (m->rbound + m->dr));
     const double lim = precision == SPSIM_PREC_F32 ? 1.0 / 16 : 0.25;
     if (qmax * m->rbound >= std::ldexp(1.0, 19) || cmax > lim)
@@ -1288,7 +1293,8 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   if (m->n_kept == 0 || total == 0) return SPSIM_OK;
 
   // atom blocks (single element each) x pixel chunks
-  const int block_atoms = precision == SPSIM_PREC_FP64 ? ADJ_THREADS : ADJ_BLOCK_ATOMS;
+  const int block_atoms =
+      precision == SPSIM_PREC_FP64 ? ADJ_THREADS : (dphase ? ADJ_DPHASE_BLOCK_ATOMS : ADJ_BLOCK_ATOMS);
   std::vector<AdjBlock> blocks;
   {
     int e = -1, seg0 = 0;
@@ -1329,6 +1335,7 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   AdjParams prm;
   memset(&prm, 0, sizeof(prm));
   prm.atoms = m->d_atoms;
+  prm.atomsd = m->d_atomsd;
   prm.perm = m->d_perm;
   prm.wbase = m->d_wbase;
   prm.blocks = (const AdjBlock *)d_blocks;
@@ -1349,7 +1356,7 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   prm.dpos = dpos_dev;
   prm.docc = docc_dev;
   prm.dB = dB_dev;
-  const int mode = precision == SPSIM_PREC_FP64 ? 2 : (precision == SPSIM_PREC_F32_FAST ? 1 : 0);
+  const int mode = precision == SPSIM_PREC_FP64 ? 2 : (precision == SPSIM_PREC_F32_FAST ? 1 : (dphase ? 3 : 0));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (g_timing) {
     CUDA_TRY(cudaEventCreate(&e0));

@@ -157,6 +157,27 @@ __device__ __forceinline__ void sincos_half_poly(float y, float &s, float &c) {
   c = pc;
 }
 
+// packed f32x2 arithmetic (sm_100): two lanes' worth of FP32 per instruction
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// sin(2 pi y), cos(2 pi y) of two phases |y| <= 1/4 cycle (the DHALF pair)
+__device__ __forceinline__ void sincos_dhalf_poly2(float2 y, float2 &S, float2 &C) {
+  const float2 z = mul2(y, y);
+  float2 ps = fma2(z, f2(SPSIM_DHALF_S4), f2(SPSIM_DHALF_S3));
+  ps = fma2(z, ps, f2(SPSIM_DHALF_S2));
+  ps = fma2(z, ps, f2(SPSIM_DHALF_S1));
+  ps = fma2(z, ps, f2(SPSIM_DHALF_S0));
+  float2 pc = fma2(z, f2(SPSIM_DHALF_C4), f2(SPSIM_DHALF_C3));
+  pc = fma2(z, pc, f2(SPSIM_DHALF_C2));
+  pc = fma2(z, pc, f2(SPSIM_DHALF_C1));
+  pc = fma2(z, pc, f2(SPSIM_DHALF_C0));
+  S = mul2(y, ps);
+  C = pc;
+}
+
 // (-1)^k w for an integer k whose bit 0 sits in bit 0 of kbits: one integer
 // multiply-add, w_bits + kbits * 2^31 (adding 2^31 flips the sign bit).  The
 // multiplier comes in as a register (m31 = 2^31, a kernel argument) so the

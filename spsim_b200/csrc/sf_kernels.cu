@@ -259,12 +259,8 @@ __global__ void __launch_bounds__(NT) sf_f32_kernel(const SfPattern *__restrict_
 // a packed f32x2 instruction (two pixels, one issue slot).  Atom records are
 // stored duplicated (4 float4 per atom, see SfPattern::atoms2) so each shared
 // load yields ready operand pairs.  Element sums are flushed straight into the
-// FP64 accumulator with atomics, which keeps the per-pixel register set small.
+// per-thread FP64 slots in shared memory, written once per work item.
 
-__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
 template <int MODE, int NT, int P, bool PERB>
 __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restrict__ pats,
@@ -273,6 +269,7 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
   static_assert(P % 2 == 0, "pixels per thread must be even");
   constexpr int NP = P / 2;
   __shared__ __align__(128) float4 ring[RING_STAGES][4 * TILE_ATOMS];
+  __shared__ __align__(16) double2 sacc[P * NT];  // per-thread FP64 pixel sums of the current work item
   __shared__ __align__(8) uint64_t full_bar[RING_STAGES];
   __shared__ int s_item;
 
@@ -337,6 +334,8 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
     float2 shc[NP], slc[NP], shs[NP], sls[NP];
 #pragma unroll
     for (int j = 0; j < NP; ++j) shc[j] = slc[j] = shs[j] = sls[j] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < P; ++i) sacc[i * NT + tid] = make_double2(0.0, 0.0);
 
     const int k0 = wi.k0, k1 = wi.k1;
     if (tid == 0) {
@@ -434,6 +433,7 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
         }
       }
       if (td.last || k == k1 - 1) {
+        // element done: f_e times its float-float sums into this thread's FP64 slots
         const double *__restrict__ ffe = pt.ff + (long long)td.elem * npix;
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
@@ -444,8 +444,10 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
               const double f = ffe[p];
               const double re = h ? (double)shc[j].y + (double)slc[j].y : (double)shc[j].x + (double)slc[j].x;
               const double sm = h ? (double)shs[j].y + (double)sls[j].y : (double)shs[j].x + (double)sls[j].x;
-              atomicAdd(&pt.acc[p].x, f * re);
-              atomicAdd(&pt.acc[p].y, -f * sm);
+              double2 v = sacc[(2 * j + h) * NT + tid];
+              v.x = fma(f, re, v.x);
+              v.y = fma(-f, sm, v.y);
+              sacc[(2 * j + h) * NT + tid] = v;
             }
           }
           shc[j] = slc[j] = shs[j] = sls[j] = make_float2(0.f, 0.f);
@@ -460,6 +462,21 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
         ++g_issue;
       }
       ++g_cons;
+    }
+    // work item done: one write per pixel, a plain store when the item covers
+    // every atom tile of the molecule (no other item touches these pixels)
+    const bool whole = k0 == 0 && k1 == pt.n_tiles;
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      if (pix[i] < npix) {
+        const double2 v = sacc[i * NT + tid];
+        if (whole) {
+          pt.acc[pix[i]] = v;
+        } else {
+          atomicAdd(&pt.acc[pix[i]].x, v.x);
+          atomicAdd(&pt.acc[pix[i]].y, v.y);
+        }
+      }
     }
     __syncthreads();
   }
@@ -482,6 +499,7 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
   static_assert(P % 2 == 0, "pixels per thread must be even");
   constexpr int NP = P / 2;
   __shared__ __align__(128) float4 ring[RING_STAGES][2 * TILE_ATOMS];
+  __shared__ __align__(16) double2 sacc[P * NT];  // per-thread FP64 pixel sums of the current work item
   __shared__ __align__(8) uint64_t full_bar[RING_STAGES];
   __shared__ int s_item;
 
@@ -509,11 +527,10 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
 
     double qx[P], qy[P], qz[P];
     float s2n[P];
-    long long pix[P];
+    const long long pix0 = (long long)wi.pixel_tile * (NT * P) + tid;  // pixel i of this thread: pix0 + i * NT
 #pragma unroll
     for (int i = 0; i < P; ++i) {
-      const long long p = (long long)wi.pixel_tile * (NT * P) + i * NT + tid;
-      pix[i] = p;
+      const long long p = pix0 + i * NT;
       double q[3] = {0.0, 0.0, 0.0};
       if (p < npix) load_q(pt, p, q);
       qx[i] = q[0];
@@ -524,6 +541,8 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
     float2 shc[NP], slc[NP], shs[NP], sls[NP];
 #pragma unroll
     for (int j = 0; j < NP; ++j) shc[j] = slc[j] = shs[j] = sls[j] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < P; ++i) sacc[i * NT + tid] = make_double2(0.0, 0.0);
 
     const int k0 = wi.k0, k1 = wi.k1;
     if (tid == 0) {
@@ -586,16 +605,8 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
             const float2 yy = make_float2(y[0], y[1]);
             if (MODE == PREC_MODE_POLY) {
               // e^{2 pi i (k/2 + y)} = (-1)^k e^{2 pi i y}, |y| <= 1/4
-              const float2 z = mul2(yy, yy);
-              float2 ps = fma2(z, f2(SPSIM_DHALF_S4), f2(SPSIM_DHALF_S3));
-              ps = fma2(z, ps, f2(SPSIM_DHALF_S2));
-              ps = fma2(z, ps, f2(SPSIM_DHALF_S1));
-              ps = fma2(z, ps, f2(SPSIM_DHALF_S0));
-              float2 pc = fma2(z, f2(SPSIM_DHALF_C4), f2(SPSIM_DHALF_C3));
-              pc = fma2(z, pc, f2(SPSIM_DHALF_C2));
-              pc = fma2(z, pc, f2(SPSIM_DHALF_C1));
-              pc = fma2(z, pc, f2(SPSIM_DHALF_C0));
-              const float2 S = mul2(yy, ps);
+              float2 S, pc;
+              sincos_dhalf_poly2(yy, S, pc);
               const float2 ws = make_float2(sign_by_parity(w[0], kb[0], m31), sign_by_parity(w[1], kb[1], m31));
               bc[j] = fma2(ws, pc, bc[j]);
               bs[j] = fma2(ws, S, bs[j]);
@@ -622,18 +633,21 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
         }
       }
       if (td.last || k == k1 - 1) {
+        // element done: f_e times its float-float sums into this thread's FP64 slots
         const double *__restrict__ ffe = pt.ff + (long long)td.elem * npix;
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const long long p = pix[2 * j + h];
+            const long long p = pix0 + (2 * j + h) * NT;
             if (p < npix) {
               const double f = ffe[p];
               const double re = h ? (double)shc[j].y + (double)slc[j].y : (double)shc[j].x + (double)slc[j].x;
               const double sm = h ? (double)shs[j].y + (double)sls[j].y : (double)shs[j].x + (double)sls[j].x;
-              atomicAdd(&pt.acc[p].x, f * re);
-              atomicAdd(&pt.acc[p].y, -f * sm);
+              double2 v = sacc[(2 * j + h) * NT + tid];
+              v.x = fma(f, re, v.x);
+              v.y = fma(-f, sm, v.y);
+              sacc[(2 * j + h) * NT + tid] = v;
             }
           }
           shc[j] = slc[j] = shs[j] = sls[j] = make_float2(0.f, 0.f);
@@ -648,6 +662,22 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
         ++g_issue;
       }
       ++g_cons;
+    }
+    // work item done: one write per pixel, a plain store when the item covers
+    // every atom tile of the molecule (no other item touches these pixels)
+    const bool whole = k0 == 0 && k1 == pt.n_tiles;
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      const long long p = pix0 + i * NT;
+      if (p < npix) {
+        const double2 v = sacc[i * NT + tid];
+        if (whole) {
+          pt.acc[p] = v;
+        } else {
+          atomicAdd(&pt.acc[p].x, v.x);
+          atomicAdd(&pt.acc[p].y, v.y);
+        }
+      }
     }
     __syncthreads();
   }

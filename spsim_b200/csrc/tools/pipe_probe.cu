@@ -107,6 +107,66 @@ __global__ void k_f2f(float *out, double b) {
   out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// FP64 -> int32 (round to nearest) -> FP64 conversions: two conversions per op
+__global__ void k_cvt(double *out, double b) {
+  double a[8];
+  for (int i = 0; i < 8; ++i) a[i] = threadIdx.x * 1e-3 + i;
+  for (int it = 0; it < N_IT / 4; ++it)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = (double)__double2int_rn(a[i] * b);
+  double s = 0; for (int i = 0; i < 8; ++i) s += a[i];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// FP64 tensor-core MMA (m8n8k4): 8 independent accumulator tiles per warp;
+// 8 x 8 x 4 = 256 FMA per MMA per warp, i.e. 8 FP64 FMA lane-ops per thread
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+__global__ void k_dmma(double *out, double a, double b) {
+  double d[8][2];
+  for (int i = 0; i < 8; ++i) d[i][0] = d[i][1] = threadIdx.x * 1e-3 + i;
+  const double aa = a + threadIdx.x * 1e-9, bb = b - threadIdx.x * 1e-9;
+  for (int it = 0; it < N_IT / 8; ++it)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dmma(d[i][0], d[i][1], aa, bb);
+  double s = 0; for (int i = 0; i < 8; ++i) s += d[i][0] + d[i][1];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+// packed FP32 chains with FP64 MMAs riding along: counts FMA lane-ops; 2 MMAs
+// (16 FP64 FMA lane-ops per thread) per 16 FP32 FMA lane-ops
+__global__ void k_ffma2_dmma(float2 *out, float b, float c, double ad, double bd) {
+  float2 a[8]; double d[2][2];
+  for (int i = 0; i < 8; ++i) a[i] = make_float2(threadIdx.x * 1e-3f + i, i);
+  for (int i = 0; i < 2; ++i) d[i][0] = d[i][1] = threadIdx.x * 1e-3 + i;
+  const float2 bb = make_float2(b, b), cc = make_float2(c, c);
+  for (int it = 0; it < N_IT; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = __ffma2_rn(a[i], bb, cc);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) dmma(d[i][0], d[i][1], ad, bd);
+  }
+  float s = 0; double t = 0; for (int i = 0; i < 8; ++i) s += a[i].x + a[i].y;
+  for (int i = 0; i < 2; ++i) t += d[i][0] + d[i][1];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = make_float2(s, (float)t);
+}
+// FP64 vector FMA chains with FP64 MMAs riding along: counts DFMA lane-ops; 1 MMA per 4 DFMA
+__global__ void k_dfma_dmma(double *out, double b, double c, double ad, double bd) {
+  double a[4]; double d[2][2];
+  for (int i = 0; i < 4; ++i) a[i] = threadIdx.x * 1e-3 + i;
+  for (int i = 0; i < 2; ++i) d[i][0] = d[i][1] = threadIdx.x * 1e-3 + i;
+  for (int it = 0; it < N_IT / 2; ++it) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = fma(a[i], b, c);
+    dmma(d[it & 1][0], d[it & 1][1], ad, bd);
+  }
+  double s = 0; for (int i = 0; i < 4; ++i) s += a[i];
+  for (int i = 0; i < 2; ++i) s += d[i][0] + d[i][1];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 // ---- the structure-factor inner loop in isolation: 256 atoms in shared
 // memory, PP pixel pairs per thread, every term of the half-cycle polynomial
 // form.  term32: compensated FP32 phase (Q_hi.R_hi + cross term);
@@ -196,7 +256,10 @@ __global__ void __launch_bounds__(256) k_term32(float4 *out, int reps, unsigned 
   for (int j = 0; j < PP; ++j) { o.x += bc[j].x; o.y += bc[j].y; o.z += bs[j].x; o.w += bs[j].y; }
   out[blockIdx.x * blockDim.x + threadIdx.x] = o;
 }
-template <int SIGN>
+// term64 with the rounding of 2u done by conversions (XU pipe): k = rint(2u)
+// as an integer, back to FP64, one DFMA for u - k/2.  RED 0: the magic-number
+// rounding (two more FP64 operations, no conversions).
+template <int SIGN, int RED = 0>
 __global__ void __launch_bounds__(256) k_term64(float4 *out, int reps, unsigned m31) {
   __shared__ double4 at[N_ATOMS];
   for (int i = threadIdx.x; i < N_ATOMS; i += blockDim.x)
@@ -221,10 +284,16 @@ __global__ void __launch_bounds__(256) k_term64(float4 *out, int reps, unsigned 
           double u = q[2 * j + h][0] * A.x;
           u = fma(q[2 * j + h][1], A.y, u);
           u = fma(q[2 * j + h][2], A.z, u);
-          const double t = fma(u, 2.0, M);
-          const double kf = t - M;
-          yv[h] = __double2float_rn(fma(kf, -0.5, u));
-          t2[h] = t;
+          if (RED == 0) {
+            const double t = fma(u, 2.0, M);
+            const double kf = t - M;
+            yv[h] = __double2float_rn(fma(kf, -0.5, u));
+            t2[h] = t;
+          } else {
+            const int k = __double2int_rn(2.0 * u);
+            yv[h] = __double2float_rn(fma((double)k, -0.5, u));
+            t2[h] = __hiloint2double(0, k);
+          }
         }
         float2 S, C;
         dhalf_poly2(make_float2(yv[0], yv[1]), S, C);
@@ -270,12 +339,23 @@ int main() {
       16.0 * N_IT);
   printf("(ffma2+dfma counts only FMA lane-ops; 4 DFMA per 16 FMA lane-ops ride along)\n");
   run("f2f_dmul", [&] { k_f2f<<<blocks, threads>>>((float *)buf, 0.999); }, 8.0 * (N_IT / 4));
+  run("cvt_d2i2d", [&] { k_cvt<<<blocks, threads>>>((double *)buf, 1.001); }, 8.0 * (N_IT / 4));
+  printf("(cvt_d2i2d counts round trips: DMUL + F2I.F64 + I2F.F64 each)\n");
+  run("dmma", [&] { k_dmma<<<blocks, threads>>>((double *)buf, 0.999, 1e-3); }, 8.0 * 8 * (N_IT / 8));
+  printf("(dmma counts FP64 FMA lane-ops: 8 per thread per m8n8k4)\n");
+  run("ffma2+dmma", [&] { k_ffma2_dmma<<<blocks, threads>>>((float2 *)buf, 0.999f, 1e-3f, 0.999, 1e-3); },
+      16.0 * N_IT);
+  printf("(ffma2+dmma counts only FP32 FMA lane-ops; 16 FP64 MMA lane-ops per 16 ride along)\n");
+  run("dfma+dmma", [&] { k_dfma_dmma<<<blocks, threads>>>((double *)buf, 0.999, 1e-3, 0.999, 1e-3); },
+      4.0 * (N_IT / 2));
+  printf("(dfma+dmma counts only DFMA lane-ops; 8 FP64 MMA lane-ops per 4 ride along)\n");
   const int reps = 16;
   const unsigned m31 = 0x80000000u;
   run("term32", [&] { k_term32<0><<<blocks, threads>>>((float4 *)buf, reps, m31); }, 2.0 * PP * N_ATOMS * reps);
   run("term32_imad", [&] { k_term32<1><<<blocks, threads>>>((float4 *)buf, reps, m31); }, 2.0 * PP * N_ATOMS * reps);
   run("term64", [&] { k_term64<0><<<blocks, threads>>>((float4 *)buf, reps, m31); }, 2.0 * PP * N_ATOMS * reps);
   run("term64_imad", [&] { k_term64<1><<<blocks, threads>>>((float4 *)buf, reps, m31); }, 2.0 * PP * N_ATOMS * reps);
+  run("term64_cvt", [&] { k_term64<1, 1><<<blocks, threads>>>((float4 *)buf, reps, m31); }, 2.0 * PP * N_ATOMS * reps);
   printf("(term32 / term64 count structure-factor terms)\n");
   printf("{\"fma_lane_ops_per_s\": %.6e, \"mufu_ops_per_s\": %.6e, \"sms\": %d, \"clock_mhz\": %.0f}\n", g_fma, g_mufu,
          sms, clk / 1e3);

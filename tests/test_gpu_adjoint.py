@@ -47,6 +47,34 @@ def test_adjoint_kernel_matches_oracle_vjp(cuda, precision, tol, bfac):
         assert _rel(dB.cpu().numpy(), db) < tol
 
 
+@pytest.mark.parametrize("form", [1, 2])
+def test_adjoint_forms_on_several_atom_blocks(cuda, form):
+    # 1,500 atoms (several atom blocks per element, ragged last blocks) through
+    # the compensated (form 1) and the FP64-phase (form 2) adjoint kernels
+    Z, pos = synth.random_molecule(1500, 2.2e-9, 12)
+    rng = np.random.Generator(np.random.PCG64(12))
+    occ = rng.uniform(0.5, 1.0, len(Z)).astype(np.float32)
+    b = rng.uniform(0.0, 30.0, len(Z)).astype(np.float32)
+    R = synth.haar_rotations(2, 13)
+    d = dict(nx=36, ny=30, width=36 * 300e-6, height=30 * 300e-6, distance=0.1, wavelength=0.2e-9)
+    q0 = O.hkl_detector(**d)
+    q = np.concatenate([q0 @ r.T for r in R])
+    g = rng.normal(size=q.shape[0]).astype(np.float32)
+    mol = core.Molecule(Z, pos, occ=occ, bfac=b)
+    qs = core.QSet.from_detector(**d)
+    try:
+        core.set_variant(128, 4, form)
+        F, I = core.forward_batch([mol] * len(R), [qs] * len(R), rots=R, precision="f32")
+        dpos, docc, dB = core.adjoint(mol, qs, torch.cat(F), torch.from_numpy(g).cuda(), rots=R, precision="f32")
+        torch.cuda.synchronize()
+    finally:
+        core.set_variant(-1)
+    dp, do, db = O.structure_factor_vjp(Z, pos.astype(np.float64), q, g.astype(np.float64), occ=occ, bfac=b)
+    assert _rel(dpos.cpu().numpy(), dp) < 1e-4
+    assert _rel(docc.cpu().numpy(), do) < 1e-4
+    assert _rel(dB.cpu().numpy(), db) < 1e-4
+
+
 def test_autograd_poisson_refinement_gradient(cuda):
     Z, pos, occ, b, R, d, q, g = _case(n=60, nx=24, npat=3, seed=8, bfac=True)
     mol = core.Molecule(Z, pos, occ=occ, bfac=b)
