@@ -207,6 +207,42 @@ def measured_pipe_peaks():
     return _PROBE["v"]
 
 
+# Per-term instruction mix of each kernel form (lane operations per atom.pixel
+# term, counted from the kernel source): FP32 = FP32 FMA/MUL/ADD, DFMA = FP64
+# FMA/ADD, IMAD = integer multiply-add, XU = MUFU / conversions.
+MIX = {
+    "sf_dphase_kernel": {"fp32": 12, "dfma": 6, "imad": 1, "xu": 1},   # FP64 phase + reduction, DHALF poly
+    "sf_f32x2_kernel/f32": {"fp32": 27, "alu": 2},                   # compensated phase, HALF poly
+    "sf_f32x2_kernel/f32_fast": {"fp32": 16, "xu": 2},               # compensated phase, MUFU sin/cos
+}
+
+
+def balanced_bound(kernel, prec, probe):
+    """Terms/s the kernel's own instruction mix allows on the measured pipe
+    rates.  FP32, FP64 and integer multiply-add issue through pipes that the
+    probe shows to be additive (packed FP32 beside FP64 FMA or FP64 MMA runs at
+    the sum of their times), so their times add; the XU pipe (MUFU,
+    conversions) runs beside them, so the bound is the larger of the two."""
+    if not probe or not probe.get("fma_lane_ops_per_s"):
+        return None
+    mix = MIX.get(kernel) or MIX.get("%s/%s" % (kernel, prec))
+    if not mix:
+        return None
+    rate = {"fp32": probe["fma_lane_ops_per_s"], "dfma": probe.get("dfma_lane_ops_per_s"),
+            "imad": probe.get("imad_lane_ops_per_s"), "alu": probe.get("alu_lane_ops_per_s"),
+            "xu": probe.get("mufu_ops_per_s")}
+    t_issue = 0.0
+    for k in ("fp32", "dfma", "imad", "alu"):
+        if mix.get(k):
+            if not rate[k]:
+                return None
+            t_issue += mix[k] / rate[k]
+    t_xu = mix.get("xu", 0) / rate["xu"] if mix.get("xu") else 0.0
+    return {"terms_per_s": 1.0 / max(t_issue, t_xu), "mix_per_term": mix,
+            "model": "1 / max(sum_p ops_p / rate_p over FP32, FP64, IMAD, ALU; XU ops / XU rate), rates from "
+                     "spsim_b200/_lib/pipe_probe"}
+
+
 def _peaks(props):
     probe = measured_pipe_peaks()
     if probe and probe.get("fma_lane_ops_per_s") and probe.get("mufu_ops_per_s"):
@@ -229,13 +265,18 @@ def _peaks(props):
     return min(p_fma / OPS_PER_TERM_FMA, p_mufu / OPS_PER_TERM_MUFU), p_mufu, p_fma, sm_max, src
 
 
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "sf_dphase_precision50k_traffic.md")
+
+
 def _traffic_per_launch():
-    p = os.path.join(ROOT, "profiles", "sf_f32_precision50k_traffic.json")
-    if os.path.exists(p):
-        try:
-            return json.load(open(p)).get("dram_bytes_per_launch")
-        except (ValueError, OSError):
-            return None
+    """DRAM bytes (read + write) of one structure-factor launch on this workload,
+    from the committed ncu summary (its "dram bytes per launch:" line)."""
+    try:
+        for line in open(TRAFFIC_PROFILE):
+            if line.lower().startswith("dram bytes per launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except (OSError, ValueError, IndexError):
+        return None
     return None
 
 
@@ -318,12 +359,16 @@ def run_b200(args):
 
     elapsed_ms, sf_avg, clocks = timed(prec, args.steps, args.warmup)
     value = world * args.steps * terms / (elapsed_ms * 1e-3)
+    kname = core.kernel_name()
 
     line = None
     if rank == 0:
         props = torch.cuda.get_device_properties(local)
         R, p_mufu, p_fma, sm_max, src = _peaks(props)
         achieved = terms / (sf_avg * 1e-3) if sf_avg else None
+        balanced = balanced_bound(kname, prec, measured_pipe_peaks())
+        if balanced and achieved:
+            balanced["frac"] = achieved / balanced["terms_per_s"]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
@@ -335,8 +380,9 @@ def run_b200(args):
             "roofline": {
                 "bound": "sfu", "achieved": achieved, "peak": R, "unit": UNIT,
                 "frac": achieved / R if achieved else None, "traffic": _traffic_per_launch(),
-                "kernel": "sf_f32_kernel" if prec != "fp64" else "sf_f64_kernel",
+                "kernel": kname,
                 "kernel_ms": sf_avg,
+                "balanced": balanced,
                 "peak_source": "R = min(P_FMA/5, P_MUFU/2) terms/s; P_FMA = %.4g FMA lane-ops/s, P_MUFU = %.4g "
                                "ops/s, %s (MEASURED_PEAKS.json has no FP32-FMA or MUFU figure)" % (p_fma, p_mufu, src),
                 "peak_nominal": props.multi_processor_count * MUFU_PER_SM_CLK * 1965e6 / OPS_PER_TERM_MUFU,

@@ -250,6 +250,13 @@ int spsim_b200_timing_read(double *ms, int cap, int *n);
  * reference's "atoms.pixel/s" self-report (src/diffraction.c:849-851). */
 int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
 
+/* The reference-shaped calls (include/spsim.h) and
+ * spsim_b200_structure_factor_host keep device scratch between calls on the
+ * calling thread (grow-only buffers, the last molecule while its atom arrays
+ * stay byte-identical, a reusable plan); this frees it for the current device.
+ * No reference counterpart: spsim allocates and frees per call. */
+void spsim_b200_release_scratch(void);
+
 /* Autotuner: the kernel variant used for FP32 forwards: threads per CTA,
  * pixels per thread and form:
  *   0  compensated FP32 phase (hi/lo split), one pixel per lane
@@ -261,6 +268,9 @@ int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
  * variant on the given workload and keeps the fastest for workloads of that
  * size class. */
 int spsim_b200_set_variant(int threads, int pixels_per_thread, int form);
+/* The kernel variant the last forward on this thread ran: threads per CTA,
+ * pixels per thread and form (-1 for the plain FP64 kernel). */
+int spsim_b200_last_variant(int *threads, int *pixels_per_thread, int *form);
 int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision, void *stream,
                         int *best_threads, int *best_pixels_per_thread, int *best_form);
 

@@ -111,6 +111,8 @@ _SIGNATURES = {
     "spsim_b200_timing_read": (c_int, [POINTER(c_double), c_int, POINTER(c_int)]),
     "spsim_b200_last_forward_stats": (c_int, [POINTER(c_double), POINTER(c_double)]),
     "spsim_b200_set_variant": (c_int, [c_int, c_int, c_int]),
+    "spsim_b200_last_variant": (c_int, [POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "spsim_b200_release_scratch": (None, []),
     "spsim_b200_autotune": (c_int, [_P, _P, c_int, _P, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "spsim_b200_set_legacy_precision": (None, [c_int]),
     "spsim_b200_get_legacy_precision": (c_int, []),

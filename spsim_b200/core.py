@@ -21,6 +21,7 @@ from ._native import PRECISIONS, ChainOutputs, ChainParams, check, lib
 __all__ = [
     "Molecule", "QSet", "forward", "forward_batch", "adjoint", "detector_chain", "chain_params",
     "hkl_for_detector", "synchronize", "timing", "autotune", "set_variant", "last_forward_stats",
+    "last_variant", "kernel_name",
 ]
 
 
@@ -316,6 +317,19 @@ def last_forward_stats():
 
 FORMS = {0: "compensated FP32, one pixel per lane", 1: "compensated FP32, pixel pairs (f32x2)",
          2: "FP64 phase, FP32 sin/cos on pixel pairs (f32x2)"}
+KERNELS = {-1: "sf_f64_kernel", 0: "sf_f32_kernel", 1: "sf_f32x2_kernel", 2: "sf_dphase_kernel"}
+
+
+def last_variant():
+    """(threads, pixels_per_thread, form) of the last forward on this thread; form -1 = plain FP64."""
+    t, p, f = c_int(0), c_int(0), c_int(0)
+    check(lib().spsim_b200_last_variant(byref(t), byref(p), byref(f)))
+    return t.value, p.value, f.value
+
+
+def kernel_name():
+    """Name of the structure-factor kernel the last forward on this thread ran."""
+    return KERNELS[last_variant()[2]]
 
 
 def set_variant(threads=-1, pixels_per_thread=-1, form=2):

@@ -386,6 +386,7 @@ struct spsim_b200_qset {
   unsigned long long id = 0;
   int device = 0;
   long long npix = 0;
+  size_t cap_bytes = 0;  // allocated bytes of d_hkl (reused q sets only)
   float *d_hkl = nullptr;
   double *d_q64 = nullptr;
   double qmax = 0;
@@ -560,6 +561,11 @@ struct Plan {
 };
 
 static std::vector<std::unique_ptr<Plan>> g_plans;  // most recent last
+struct OneShot {  // per-thread scratch plan of uncached calls; lives until the process ends
+  Plan *plan = nullptr;
+  int device = -1;
+};
+static thread_local OneShot g_oneshot;
 static const size_t kMaxPlans = 8;
 static int g_force_nt = -1, g_force_p = -1, g_force_pk = 2;
 struct Variant {
@@ -569,6 +575,7 @@ static std::map<long long, Variant> g_tuned;  // size class -> kernel variant
 static bool g_timing = false;
 static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timing_events;
 static thread_local double g_last_terms = 0, g_last_ms = 0;
+static thread_local int g_last_variant[3] = {0, 0, -1};  // threads, pixels per thread, form (-1: FP64 kernel)
 static int g_num_sms = 0;
 
 static int num_sms() {
@@ -871,7 +878,6 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
   std::vector<double> kv;
   plan_key(npat, mols, qsets, rot, B, precision, F_dev, I_dev, kp, kv);
   Plan *pl = nullptr;
-  std::unique_ptr<Plan> oneshot;
   if (cache) {
     for (size_t i = 0; i < g_plans.size(); ++i) {
       if (g_plans[i]->key_ptrs == kp && g_plans[i]->key_vals == kv) {
@@ -883,25 +889,36 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
       }
     }
   }
-  if (!pl) {
+  if (!pl && cache) {
     std::unique_ptr<Plan> np(new Plan());
     np->key_ptrs = kp;
     np->key_vals = kv;
     st = build_plan(*np, npat, mols, qsets, rot, B, precision, F_dev, I_dev, stream);
     if (st) return st;
-    if (cache) {
-      if (g_plans.size() >= kMaxPlans) {
-        cudaDeviceSynchronize();  // the evicted plan's buffers may still be in use
-        g_plans.erase(g_plans.begin());
-      }
-      g_plans.push_back(std::move(np));
-      pl = g_plans.back().get();
-    } else {
-      oneshot = std::move(np);
-      pl = oneshot.get();
+    if (g_plans.size() >= kMaxPlans) {
+      cudaDeviceSynchronize();  // the evicted plan's buffers may still be in use
+      g_plans.erase(g_plans.begin());
     }
+    g_plans.push_back(std::move(np));
+    pl = g_plans.back().get();
+  } else if (!pl) {
+    // one-shot calls rebuild the descriptors of this thread's scratch plan,
+    // whose device buffers only grow (no cudaMalloc / cudaFree per call)
+    OneShot &os = g_oneshot;
+    if (!os.plan || os.device != dev) {
+      os.plan = new Plan();  // a plan left on another device is kept, not freed, while its context may be busy
+      os.device = dev;
+    }
+    pl = os.plan;
+    pl->key_ptrs = kp;
+    pl->key_vals = kv;
+    st = build_plan(*pl, npat, mols, qsets, rot, B, precision, F_dev, I_dev, stream);
+    if (st) return st;
   }
   g_last_terms = pl->terms;
+  g_last_variant[0] = pl->precision == SPSIM_PREC_FP64 ? 256 : pl->nt;
+  g_last_variant[1] = pl->precision == SPSIM_PREC_FP64 ? 1 : pl->ppt;
+  g_last_variant[2] = pl->precision == SPSIM_PREC_FP64 ? -1 : pl->packed;
   CUDA_TRY(refresh_rotations(*pl, rot, stream));
   if (g_timing || !cache || stream == nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -944,43 +961,135 @@ extern "C" int spsim_b200_forward_batch(int npatterns, const spsim_b200_molecule
   return run_forward(npatterns, mols, qsets, rot, B, precision, F_dev, I_dev, (cudaStream_t)stream, true);
 }
 
+// Reusable state of the host-buffer entry point, one per thread: the last
+// molecule (reused while the caller's atom arrays are byte-identical to the
+// copies kept here), a q set whose device buffer grows and is rewritten per
+// call, and device F / I buffers.  Nothing is freed per call; a device change
+// starts a fresh session (the old one is dropped without freeing, as its
+// context may still be in use).
+struct HostSession {
+  int device = -1;
+  spsim_b200_molecule *mol = nullptr;
+  std::vector<unsigned char> mol_inputs;  // natoms, Z, pos, occ, bfac, delta_atoms, beam, as passed
+  spsim_b200_qset *qs = nullptr;
+  DevBuf *F = nullptr, *I = nullptr;
+};
+static thread_local HostSession g_host;
+
+static void append_bytes(std::vector<unsigned char> &v, const void *p, size_t n) {
+  const unsigned char *b = (const unsigned char *)p;
+  v.insert(v.end(), b, b + n);
+}
+
+static int host_session_molecule(int natoms, const int32_t *Z, const float *pos, const float *occ, const float *bfac,
+                                 int delta_atoms, const float *beam, spsim_b200_molecule **out) {
+  std::vector<unsigned char> key;
+  const size_t n = natoms > 0 ? (size_t)natoms : 0;
+  append_bytes(key, &natoms, sizeof(natoms));
+  append_bytes(key, &delta_atoms, sizeof(delta_atoms));
+  const int flags = (Z ? 1 : 0) | (pos ? 2 : 0) | (occ ? 4 : 0) | (bfac ? 8 : 0) | (beam ? 16 : 0);
+  append_bytes(key, &flags, sizeof(flags));
+  if (Z) append_bytes(key, Z, n * sizeof(int32_t));
+  if (pos) append_bytes(key, pos, 3 * n * sizeof(float));
+  if (occ) append_bytes(key, occ, n * sizeof(float));
+  if (bfac) append_bytes(key, bfac, n * sizeof(float));
+  if (beam) append_bytes(key, beam, 3 * sizeof(float));
+  if (g_host.mol && key == g_host.mol_inputs) {
+    *out = g_host.mol;
+    return SPSIM_OK;
+  }
+  spsim_b200_molecule *m = nullptr;
+  int st = spsim_b200_molecule_create(natoms, Z, pos, occ, bfac, delta_atoms, beam, &m);
+  if (st) return st;
+  if (g_host.mol) {
+    cudaDeviceSynchronize();  // its records may still be read by queued work
+    spsim_b200_molecule_destroy(g_host.mol);
+  }
+  g_host.mol = m;
+  g_host.mol_inputs.swap(key);
+  *out = m;
+  return SPSIM_OK;
+}
+
+// Rewrite the session's q set with a host HKL list (new id: cached plans keyed
+// on the old contents are never matched again).
+static int host_session_qset(int64_t npix, const float *hkl, spsim_b200_qset **out) {
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (!g_host.qs) {
+    g_host.qs = new spsim_b200_qset();
+    g_host.qs->device = dev;
+  }
+  spsim_b200_qset *q = g_host.qs;
+  const size_t need = 3 * (size_t)std::max<int64_t>(npix, 1) * sizeof(float);
+  if (!q->d_hkl || q->cap_bytes < need) {
+    cudaFree(q->d_hkl);
+    q->d_hkl = nullptr;
+    q->cap_bytes = 0;
+    CUDA_TRY(cudaMalloc(&q->d_hkl, need));
+    q->cap_bytes = need;
+  }
+  q->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
+  q->npix = npix;
+  if (npix) CUDA_TRY(cudaMemcpy(q->d_hkl, hkl, 3 * npix * sizeof(float), cudaMemcpyHostToDevice));
+  double qm2 = 0;
+  for (long long i = 0; i < npix; ++i) {
+    const double a = hkl[3 * i], b = hkl[3 * i + 1], c = hkl[3 * i + 2];
+    qm2 = std::max(qm2, a * a + b * b + c * c);
+  }
+  q->qmax = std::sqrt(qm2);
+  *out = q;
+  return SPSIM_OK;
+}
+
+// Frees this thread's host-call session and scratch plan (called by
+// spsim_b200_release_scratch after a device synchronisation).
+extern "C" void spsim_internal_release_host_session(void) {
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (g_host.device == dev) {
+    if (g_host.mol) spsim_b200_molecule_destroy(g_host.mol);
+    if (g_host.qs) spsim_b200_qset_destroy(g_host.qs);
+    delete g_host.F;
+    delete g_host.I;
+  }
+  g_host = HostSession();
+  if (g_oneshot.plan && g_oneshot.device == dev) delete g_oneshot.plan;
+  g_oneshot = OneShot();
+}
+
 extern "C" int spsim_b200_structure_factor_host(int natoms, const int32_t *Z, const float *pos, const float *occ,
                                                 const float *bfac, float B, int delta_atoms, const float *beam,
                                                 int64_t npix, const float *hkl, int precision, float *F_host,
                                                 float *I_host) {
   if (npix < 0 || (npix > 0 && !hkl)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (g_host.device != dev) {
+    g_host = HostSession();
+    g_host.device = dev;
+  }
   spsim_b200_molecule *m = nullptr;
   spsim_b200_qset *q = nullptr;
-  int st = spsim_b200_molecule_create(natoms, Z, pos, occ, bfac, delta_atoms, beam, &m);
+  st = host_session_molecule(natoms, Z, pos, occ, bfac, delta_atoms, beam, &m);
   if (st) return st;
-  st = spsim_b200_qset_from_list(npix, hkl, SPSIM_MEM_HOST, &q);
-  if (st) {
-    spsim_b200_molecule_destroy(m);
-    return st;
-  }
-  float *dF = nullptr, *dI = nullptr;
-  cudaError_t e = cudaMalloc(&dF, 2 * std::max<int64_t>(npix, 1) * sizeof(float));
-  if (e == cudaSuccess) e = cudaMalloc(&dI, std::max<int64_t>(npix, 1) * sizeof(float));
-  if (e != cudaSuccess) {
-    st = fail(SPSIM_ERR_OUT_OF_MEMORY, "device buffers: %s", cudaGetErrorString(e));
-  } else {
-    float *F[1] = {F_host ? dF : nullptr};
-    float *I[1] = {I_host ? dI : nullptr};
-    const spsim_b200_molecule *mm = m;
-    const spsim_b200_qset *qq = q;
-    st = run_forward(1, &mm, &qq, nullptr, B, precision, F, I, nullptr, false);
-    if (!st && F_host && npix)
-      if ((e = cudaMemcpy(F_host, dF, 2 * npix * sizeof(float), cudaMemcpyDeviceToHost)))
-        st = fail(SPSIM_ERR_CUDA, "copy F: %s", cudaGetErrorString(e));
-    if (!st && I_host && npix)
-      if ((e = cudaMemcpy(I_host, dI, npix * sizeof(float), cudaMemcpyDeviceToHost)))
-        st = fail(SPSIM_ERR_CUDA, "copy I: %s", cudaGetErrorString(e));
-  }
-  cudaFree(dF);
-  cudaFree(dI);
-  spsim_b200_qset_destroy(q);
-  spsim_b200_molecule_destroy(m);
-  return st;
+  st = host_session_qset(npix, hkl, &q);
+  if (st) return st;
+  if (!g_host.F) g_host.F = new DevBuf();
+  if (!g_host.I) g_host.I = new DevBuf();
+  CUDA_TRY(g_host.F->ensure(2 * std::max<int64_t>(npix, 1) * sizeof(float)));
+  CUDA_TRY(g_host.I->ensure(std::max<int64_t>(npix, 1) * sizeof(float)));
+  float *F[1] = {F_host ? (float *)g_host.F->p : nullptr};
+  float *I[1] = {I_host ? (float *)g_host.I->p : nullptr};
+  const spsim_b200_molecule *mm = m;
+  const spsim_b200_qset *qq = q;
+  st = run_forward(1, &mm, &qq, nullptr, B, precision, F, I, nullptr, false);
+  if (st) return st;
+  if (F_host && npix) CUDA_TRY(cudaMemcpy(F_host, F[0], 2 * npix * sizeof(float), cudaMemcpyDeviceToHost));
+  if (I_host && npix) CUDA_TRY(cudaMemcpy(I_host, I[0], npix * sizeof(float), cudaMemcpyDeviceToHost));
+  return SPSIM_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1024,6 +1133,13 @@ extern "C" int spsim_b200_timing_read(double *ms, int cap, int *n) {
 extern "C" int spsim_b200_last_forward_stats(double *terms, double *kernel_ms) {
   if (terms) *terms = g_last_terms;
   if (kernel_ms) *kernel_ms = g_last_ms;
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_last_variant(int *threads, int *pixels_per_thread, int *form) {
+  if (threads) *threads = g_last_variant[0];
+  if (pixels_per_thread) *pixels_per_thread = g_last_variant[1];
+  if (form) *form = g_last_variant[2];
   return SPSIM_OK;
 }
 

@@ -34,11 +34,55 @@ static void cuda_die(const char *where, cudaError_t e) {
   abort();
 }
 
-static void *dev_alloc(size_t bytes) {
-  void *p = NULL;
-  cudaError_t e = cudaMalloc(&p, bytes ? bytes : 4);
+/* Device scratch of the reference-shaped calls: one grow-only buffer per
+ * slot, kept between calls (no cudaMalloc / cudaFree per call) and released by
+ * spsim_b200_release_scratch.  Each call site owns its slots, so nested calls
+ * (calculate_photons_per_pixel computing the Thomson factor first) never share
+ * one.  Like the reference's own static state, this makes the calls
+ * non-reentrant. */
+enum {
+  SLOT_HKL,
+  SLOT_THOMSON,
+  SLOT_SOLID,
+  SLOT_PH_T, SLOT_PH_O, SLOT_PH_I, SLOT_PH_P,
+  SLOT_PO_P, SLOT_PO_C,
+  SLOT_EL_C, SLOT_EL_E,
+  SLOT_RO_E, SLOT_RO_R,
+  SLOT_NL_P, SLOT_NL_N,
+  SLOT_SHOT_I, SLOT_SHOT_0,
+  N_SLOTS = SLOT_SHOT_0 + 7
+};
+static void *g_slot[N_SLOTS];
+static size_t g_slot_bytes[N_SLOTS];
+static int g_slot_device[N_SLOTS];
+
+static void *dev_alloc(int slot, size_t bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!bytes) bytes = 4;
+  if (g_slot[slot] && g_slot_bytes[slot] >= bytes && g_slot_device[slot] == dev) return g_slot[slot];
+  if (g_slot[slot] && g_slot_device[slot] == dev) cudaFree(g_slot[slot]);
+  g_slot[slot] = NULL; /* a buffer left on another device is dropped, not freed */
+  g_slot_bytes[slot] = 0;
+  cudaError_t e = cudaMalloc(&g_slot[slot], bytes);
   if (e != cudaSuccess) cuda_die("cudaMalloc", e);
-  return p;
+  g_slot_bytes[slot] = bytes;
+  g_slot_device[slot] = dev;
+  return g_slot[slot];
+}
+
+void spsim_internal_release_host_session(void);
+
+void spsim_b200_release_scratch(void) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceSynchronize();
+  for (int k = 0; k < N_SLOTS; k++) {
+    if (g_slot[k] && g_slot_device[k] == dev) cudaFree(g_slot[k]);
+    g_slot[k] = NULL;
+    g_slot_bytes[k] = 0;
+  }
+  spsim_internal_release_host_session();
 }
 
 static void h2d(void *d, const void *h, size_t bytes) {
@@ -63,12 +107,11 @@ static double now_us(void) {
 float *get_HKL_list_for_detector(CCD *det, Experiment *exp, int *HKL_list_size) {
   const long long n = (long long)det->nx * det->ny;
   float *out = (float *)malloc(sizeof(float) * 3 * (n > 0 ? n : 1));
-  float *d = (float *)dev_alloc(sizeof(float) * 3 * n);
+  float *d = (float *)dev_alloc(SLOT_HKL, sizeof(float) * 3 * n);
   int st = spsim_b200_hkl_for_detector(det->nx, det->ny, det->width, det->height, det->distance, det->center_x,
                                        det->center_y, exp->wavelength, det->spherical, d, NULL);
   if (st) die("get_HKL_list_for_detector", st);
   d2h(out, d, sizeof(float) * 3 * n);
-  cudaFree(d);
   *HKL_list_size = (int)n;
   return out;
 }
@@ -247,24 +290,22 @@ static long long nbin_of(const CCD *det) {
 void calculate_thomson_correction(CCD *det, Experiment *exp) {
   const long long n = npix_of(det);
   spsim_b200_chain_params p = chain_params(det, exp);
-  float *d = (float *)dev_alloc(sizeof(float) * n);
+  float *d = (float *)dev_alloc(SLOT_THOMSON, sizeof(float) * n);
   int st = spsim_b200_thomson(&p, d, NULL);
   if (st) die("calculate_thomson_correction", st);
   det->thomson_correction = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->thomson_correction, d, sizeof(float) * n);
-  cudaFree(d);
 }
 
 /* src/diffraction.c:1146 */
 void calculate_pixel_solid_angle(CCD *det) {
   const long long n = npix_of(det);
   spsim_b200_chain_params p = chain_params(det, NULL);
-  float *d = (float *)dev_alloc(sizeof(float) * n);
+  float *d = (float *)dev_alloc(SLOT_SOLID, sizeof(float) * n);
   int st = spsim_b200_solid_angle(&p, d, NULL);
   if (st) die("calculate_pixel_solid_angle", st);
   det->solid_angle = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->solid_angle, d, sizeof(float) * n);
-  cudaFree(d);
 }
 
 /* src/diffraction.c:1190 */
@@ -274,8 +315,8 @@ void calculate_photons_per_pixel(Diffraction_Pattern *pattern, Options *opts) {
   if (!det->thomson_correction) calculate_thomson_correction(det, exp);
   if (!det->solid_angle) calculate_pixel_solid_angle(det);
   const long long n = npix_of(det);
-  float *dT = (float *)dev_alloc(sizeof(float) * n), *dO = (float *)dev_alloc(sizeof(float) * n);
-  float *dI = (float *)dev_alloc(sizeof(float) * n), *dP = (float *)dev_alloc(sizeof(float) * n);
+  float *dT = (float *)dev_alloc(SLOT_PH_T, sizeof(float) * n), *dO = (float *)dev_alloc(SLOT_PH_O, sizeof(float) * n);
+  float *dI = (float *)dev_alloc(SLOT_PH_I, sizeof(float) * n), *dP = (float *)dev_alloc(SLOT_PH_P, sizeof(float) * n);
   h2d(dT, det->thomson_correction, sizeof(float) * n);
   h2d(dO, det->solid_angle, sizeof(float) * n);
   h2d(dI, pattern->ints, sizeof(float) * n);
@@ -283,10 +324,6 @@ void calculate_photons_per_pixel(Diffraction_Pattern *pattern, Options *opts) {
   if (st) die("calculate_photons_per_pixel", st);
   det->photons_per_pixel = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->photons_per_pixel, dP, sizeof(float) * n);
-  cudaFree(dT);
-  cudaFree(dO);
-  cudaFree(dI);
-  cudaFree(dP);
 }
 
 /* src/noise.c:32 */
@@ -297,14 +334,12 @@ void generate_poisson_noise(CCD *det) {
   }
   const long long n = npix_of(det);
   spsim_b200_chain_params p = chain_params(det, NULL);
-  float *dP = (float *)dev_alloc(sizeof(float) * n), *dC = (float *)dev_alloc(sizeof(float) * n);
+  float *dP = (float *)dev_alloc(SLOT_PO_P, sizeof(float) * n), *dC = (float *)dev_alloc(SLOT_PO_C, sizeof(float) * n);
   h2d(dP, det->photons_per_pixel, sizeof(float) * n);
   int st = spsim_b200_photon_counts(&p, dP, dC, NULL);
   if (st) die("generate_poisson_noise", st);
   det->photon_count = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->photon_count, dC, sizeof(float) * n);
-  cudaFree(dP);
-  cudaFree(dC);
 }
 
 /* src/amplification.c:54 */
@@ -315,14 +350,12 @@ void calculate_electrons_per_pixel(CCD *det, Experiment *experiment) {
   }
   const long long n = npix_of(det);
   spsim_b200_chain_params p = chain_params(det, experiment);
-  float *dC = (float *)dev_alloc(sizeof(float) * n), *dE = (float *)dev_alloc(sizeof(float) * n);
+  float *dC = (float *)dev_alloc(SLOT_EL_C, sizeof(float) * n), *dE = (float *)dev_alloc(SLOT_EL_E, sizeof(float) * n);
   h2d(dC, det->photon_count, sizeof(float) * n);
   int st = spsim_b200_electrons(&p, dC, dE, NULL);
   if (st) die("calculate_electrons_per_pixel", st);
   det->electrons_per_pixel = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->electrons_per_pixel, dE, sizeof(float) * n);
-  cudaFree(dC);
-  cudaFree(dE);
 }
 
 /* src/amplification.c:77 */
@@ -333,14 +366,12 @@ void calculate_real_detector_output(CCD *det, Experiment *experiment) {
   }
   const long long n = npix_of(det), nb = nbin_of(det);
   spsim_b200_chain_params p = chain_params(det, experiment);
-  float *dE = (float *)dev_alloc(sizeof(float) * n), *dR = (float *)dev_alloc(sizeof(float) * nb);
+  float *dE = (float *)dev_alloc(SLOT_RO_E, sizeof(float) * n), *dR = (float *)dev_alloc(SLOT_RO_R, sizeof(float) * nb);
   h2d(dE, det->electrons_per_pixel, sizeof(float) * n);
   int st = spsim_b200_binned_outputs(&p, dE, NULL, dR, NULL, NULL);
   if (st) die("calculate_real_detector_output", st);
   det->real_output = (float *)malloc(sizeof(float) * (nb > 0 ? nb : 1));
   d2h(det->real_output, dR, sizeof(float) * nb);
-  cudaFree(dE);
-  cudaFree(dR);
 }
 
 /* src/amplification.c:119 */
@@ -351,14 +382,12 @@ void calculate_noiseless_detector_output(CCD *det, Experiment *experiment) {
   }
   const long long n = npix_of(det), nb = nbin_of(det);
   spsim_b200_chain_params p = chain_params(det, experiment);
-  float *dP = (float *)dev_alloc(sizeof(float) * n), *dN = (float *)dev_alloc(sizeof(float) * nb);
+  float *dP = (float *)dev_alloc(SLOT_NL_P, sizeof(float) * n), *dN = (float *)dev_alloc(SLOT_NL_N, sizeof(float) * nb);
   h2d(dP, det->photons_per_pixel, sizeof(float) * n);
   int st = spsim_b200_binned_outputs(&p, NULL, dP, NULL, dN, NULL);
   if (st) die("calculate_noiseless_detector_output", st);
   det->noiseless_output = (float *)malloc(sizeof(float) * (nb > 0 ? nb : 1));
   d2h(det->noiseless_output, dN, sizeof(float) * nb);
-  cudaFree(dP);
-  cudaFree(dN);
 }
 
 /* ------------------------------------------------------------ orchestration */
@@ -384,11 +413,11 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
 
   const long long np = npix_of(det), nb = nbin_of(det);
   spsim_b200_chain_params p = chain_params(det, exp);
-  float *dI = (float *)dev_alloc(sizeof(float) * np);
+  float *dI = (float *)dev_alloc(SLOT_SHOT_I, sizeof(float) * np);
   float *bufs[7];
-  for (int k = 0; k < 5; k++) bufs[k] = (float *)dev_alloc(sizeof(float) * np);
-  bufs[5] = (float *)dev_alloc(sizeof(float) * nb);
-  bufs[6] = (float *)dev_alloc(sizeof(float) * nb);
+  for (int k = 0; k < 5; k++) bufs[k] = (float *)dev_alloc(SLOT_SHOT_0 + k, sizeof(float) * np);
+  bufs[5] = (float *)dev_alloc(SLOT_SHOT_0 + 5, sizeof(float) * nb);
+  bufs[6] = (float *)dev_alloc(SLOT_SHOT_0 + 6, sizeof(float) * nb);
   h2d(dI, pattern->ints, sizeof(float) * np);
   spsim_b200_chain_outputs o = {bufs[0], bufs[1], bufs[2], bufs[3], bufs[4], bufs[5], bufs[6]};
   int st = spsim_b200_detector_chain(&p, dI, &o, NULL);
@@ -399,9 +428,7 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
     const long long m = k < 5 ? np : nb;
     *dst[k] = (float *)malloc(sizeof(float) * (m > 0 ? m : 1));
     d2h(*dst[k], bufs[k], sizeof(float) * m);
-    cudaFree(bufs[k]);
   }
-  cudaFree(dI);
   g_pattern_counter++;
   free(HKL_list);
   return pattern;

@@ -7,6 +7,7 @@
 // and a JSON line with the measured FP32-FMA and MUFU rates (ops/s) that
 // bench.py uses as the measured peak of R = min(P_FMA/5, P_MUFU/2).
 #include <cstdio>
+#include <cstring>
 #include <cuda_runtime.h>
 #include "../sincos_poly.h"
 #define N_IT 4096
@@ -104,6 +105,17 @@ __global__ void k_f2f(float *out, double b) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) { a[i] = a[i] * b + 1e-3; f[i] += __double2float_rn(a[i]); }
   float s = 0; for (int i = 0; i < 8; ++i) s += f[i];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// 32-bit integer multiply-add chains, multiplier in a register (kernel argument)
+__global__ void k_imad(unsigned *out, unsigned m) {
+  unsigned a[16];
+  for (int i = 0; i < 16; ++i) a[i] = threadIdx.x + i;
+  for (int it = 0; it < N_IT; ++it)
+#pragma unroll
+    for (int i = 0; i < 16; ++i) asm("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[i]) : "r"(m), "r"((unsigned)i));
+  unsigned s = 0; for (int i = 0; i < 16; ++i) s ^= a[i];
   out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
@@ -308,7 +320,7 @@ __global__ void __launch_bounds__(256) k_term64(float4 *out, int reps, unsigned 
   out[blockIdx.x * blockDim.x + threadIdx.x] = o;
 }
 
-static double g_fma = 0, g_mufu = 0;
+static double g_fma = 0, g_mufu = 0, g_dfma = 0, g_imad = 0, g_alu = 0;
 
 int main() {
   int sms; cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
@@ -326,6 +338,9 @@ int main() {
            per_s / sms / (clk * 1e3), clk / 1e3);
     if (name[0] == 'f' && name[1] == 'f' && name[4] == 0) g_fma = per_s > g_fma ? per_s : g_fma;
     if (name[0] == 'm') g_mufu = per_s;
+    if (!strcmp(name, "dfma")) g_dfma = per_s;
+    if (!strcmp(name, "imad")) g_imad = per_s;
+    if (!strcmp(name, "alu_lop3")) g_alu = per_s;
   };
   run("ffma", [&] { k_ffma<<<blocks, threads>>>((float *)buf, 0.999f, 1e-3f); }, 16.0 * N_IT);
   run("ffma2", [&] { k_ffma2<<<blocks, threads>>>((float2 *)buf, 0.999f, 1e-3f); }, 16.0 * N_IT);
@@ -335,6 +350,7 @@ int main() {
   run("ffma2+alu", [&] { k_ffma2_alu<<<blocks, threads>>>((float2 *)buf, 0.999f, 1e-3f, 0x55u); }, 16.0 * N_IT);
   printf("(ffma2+alu counts only FMA lane-ops; 8 ALU ops per 16 FMA lane-ops ride along)\n");
   run("dfma", [&] { k_dfma<<<blocks, threads>>>((double *)buf, 0.999, 1e-3); }, 8.0 * (N_IT / 2));
+  run("imad", [&] { k_imad<<<blocks, threads>>>((unsigned *)buf, 0x9e3779b9u); }, 16.0 * N_IT);
   run("ffma2+dfma", [&] { k_ffma2_dfma<<<blocks, threads>>>((float2 *)buf, 0.999f, 1e-3f, 0.999, 1e-3); },
       16.0 * N_IT);
   printf("(ffma2+dfma counts only FMA lane-ops; 4 DFMA per 16 FMA lane-ops ride along)\n");
@@ -357,8 +373,9 @@ int main() {
   run("term64_imad", [&] { k_term64<1><<<blocks, threads>>>((float4 *)buf, reps, m31); }, 2.0 * PP * N_ATOMS * reps);
   run("term64_cvt", [&] { k_term64<1, 1><<<blocks, threads>>>((float4 *)buf, reps, m31); }, 2.0 * PP * N_ATOMS * reps);
   printf("(term32 / term64 count structure-factor terms)\n");
-  printf("{\"fma_lane_ops_per_s\": %.6e, \"mufu_ops_per_s\": %.6e, \"sms\": %d, \"clock_mhz\": %.0f}\n", g_fma, g_mufu,
-         sms, clk / 1e3);
+  printf("{\"fma_lane_ops_per_s\": %.6e, \"mufu_ops_per_s\": %.6e, \"dfma_lane_ops_per_s\": %.6e, "
+         "\"imad_lane_ops_per_s\": %.6e, \"alu_lane_ops_per_s\": %.6e, \"sms\": %d, \"clock_mhz\": %.0f}\n",
+         g_fma, g_mufu, g_dfma, g_imad, g_alu, sms, clk / 1e3);
   cudaError_t e = cudaGetLastError(); printf("status %s\n", cudaGetErrorString(e));
   return e != cudaSuccess;
 }

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN, golden, intensity_errors
+from oracle import oracle as O
 from spsim_b200 import spsim as S
 
 pytestmark = pytest.mark.gpu
@@ -83,3 +84,40 @@ def test_simulate_shot_chain_arrays(cuda, tmp_path):
         S.free_mol(mol)
     finally:
         os.chdir(cwd)
+
+
+def test_host_entry_point_reuses_scratch_safely(cuda):
+    # repeated host-buffer calls: the same molecule with new HKL lists (the
+    # molecule is reused), an edited copy of it (rebuilt), after a release
+    from spsim_b200 import _native
+
+    L = _native.lib()
+    g = golden("sf_small.npz")
+    Z = np.ascontiguousarray(g["Z"], np.int32)
+    pos = np.ascontiguousarray(g["pos"], np.float32)
+    hkl = np.ascontiguousarray(g["hkl"], np.float32)
+    p = ctypes.c_void_p
+
+    def call(Z, pos, hkl):
+        n = hkl.shape[0]
+        F = np.empty(2 * n, np.float32)
+        I = np.empty(n, np.float32)
+        st = L.spsim_b200_structure_factor_host(len(Z), Z.ctypes.data_as(p), pos.ctypes.data_as(p), None, None,
+                                                ctypes.c_float(0), 0, None, ctypes.c_int64(n), hkl.ctypes.data_as(p),
+                                                _native.PREC_F32, F.ctypes.data_as(p), I.ctypes.data_as(p))
+        assert st == 0
+        return I
+
+    def want(Z, pos, hkl):
+        return O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64))[1]
+
+    cases = [(Z, pos, hkl), (Z, pos, hkl[::2].copy()), (Z, pos, (hkl * 0.7).astype(np.float32))]
+    pos2 = pos.copy()
+    pos2[3] += 1e-10  # one atom moved: the kept molecule must not be reused
+    cases.append((Z, pos2, hkl))
+    for Zc, pc, hc in cases:
+        e_max, e_l2 = intensity_errors(call(Zc, pc, hc), want(Zc, pc, hc))
+        assert e_max < 1e-5 and e_l2 < 1e-6, (e_max, e_l2)
+    L.spsim_b200_release_scratch()
+    e_max, _ = intensity_errors(call(Z, pos, hkl), want(Z, pos, hkl))
+    assert e_max < 1e-5
