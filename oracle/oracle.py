@@ -1,8 +1,10 @@
 """ORACLE — test infrastructure only.
 
-ctypes access to the two CPU checkers built by oracle/Makefile:
+ctypes access to the checkers built by oracle/Makefile:
   * oracle/_build/libspsim_oracle.so : the FP64 restatement (sf_oracle.c)
   * oracle/_ref/libspsim_ref.so      : spsim's own CPU sources compiled unchanged
+  * oracle/_ref/libspsim_refgpu.so   : spsim's own CUDA source compiled unchanged
+                                       (GPU comparison point, GPU tests only)
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module; the product never does.
 """
@@ -15,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "libspsim_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libspsim_ref.so")
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libspsim_refgpu.so")
 
 _oracle = None
 _ref = None
@@ -272,6 +275,51 @@ def ref_pattern(Z, pos, hkl, B=0.0, vector=False, delta_atoms=False, beam=None, 
     opts.verbosity_level = verbosity
     fn = L.vector_compute_pattern_on_list if vector else L.compute_pattern_on_list
     res = fn(ctypes.byref(mol), _p(hkl), hkl.shape[0], float(B), ctypes.byref(exp), ctypes.byref(opts))
+    n = hkl.shape[0]
+    Fr = np.ctypeslib.as_array(ctypes.cast(res.contents.F, POINTER(c_float)), shape=(2 * n,)).copy()
+    I = np.ctypeslib.as_array(res.contents.ints, shape=(n,)).copy()
+    libc = ctypes.CDLL(None)
+    for ptr in (res.contents.F, res.contents.ints, res.contents.HKL_list):
+        libc.free(ctypes.cast(ptr, c_void_p))
+    libc.free(ctypes.cast(res, c_void_p))
+    return Fr[0::2] + 1j * Fr[1::2], I
+
+
+_refgpu = None
+
+
+def ref_gpu_lib():
+    """spsim's CUDA path (src/diffraction.cu) built for sm_100a, or None when absent."""
+    global _refgpu
+    if _refgpu is None and os.path.exists(REF_GPU_LIB):
+        L = ctypes.CDLL(REF_GPU_LIB)
+        for name in ("cuda_compute_pattern_on_list", "cuda_compute_pattern_on_list2"):
+            f = getattr(L, name)
+            f.restype = POINTER(RefPattern)
+            f.argtypes = [POINTER(RefMolecule), c_void_p, c_int, c_float, POINTER(RefExperiment),
+                          POINTER(RefOptions)]
+        _refgpu = L
+    return _refgpu
+
+
+def ref_gpu_pattern(Z, pos, hkl, B=0.0, wavelength_samples=1, bandwidth=0.0, wavelength=0.0):
+    """spsim's cuda_compute_pattern_on_list2 (src/diffraction.cu:235-339): float F and
+    ints from CUDA_scattering_from_all_atoms (or the spectrum kernel when
+    wavelength_samples > 1 and bandwidth > 0), 100 atoms per launch."""
+    L = ref_gpu_lib()
+    if L is None:
+        raise FileNotFoundError(REF_GPU_LIB)
+    Z = np.ascontiguousarray(Z, np.int32)
+    pos = np.ascontiguousarray(pos, np.float32).reshape(-1)
+    hkl = np.ascontiguousarray(hkl, np.float32).reshape(-1, 3)
+    mol = RefMolecule(len(Z), Z.ctypes.data_as(POINTER(c_int)), pos.ctypes.data_as(POINTER(c_float)), 0)
+    exp = RefExperiment()
+    exp.wavelength = wavelength
+    exp.bandwidth = bandwidth
+    opts = RefOptions()
+    opts.wavelength_samples = int(wavelength_samples)
+    res = L.cuda_compute_pattern_on_list2(ctypes.byref(mol), _p(hkl), hkl.shape[0], float(B), ctypes.byref(exp),
+                                          ctypes.byref(opts))
     n = hkl.shape[0]
     Fr = np.ctypeslib.as_array(ctypes.cast(res.contents.F, POINTER(c_float)), shape=(2 * n,)).copy()
     I = np.ctypeslib.as_array(res.contents.ints, shape=(n,)).copy()

@@ -20,6 +20,22 @@
 #include <stdio.h>
 #include <stdlib.h>
 
+/* the CUDA build of src/diffraction.cu: libspimage's CUDA helpers, as checks
+ * that print and abort; cufftComplex comes from the toolkit header */
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#include <cufft.h>
+#define cutilSafeCall(call)                                                            \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      fprintf(stderr, "reference CUDA call failed: %s\n", cudaGetErrorString(e_));     \
+      abort();                                                                         \
+    }                                                                                  \
+  } while (0)
+#define sp_cuda_check_errors() cutilSafeCall(cudaGetLastError())
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
