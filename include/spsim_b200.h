@@ -68,7 +68,8 @@ int spsim_b200_device_count(int *count);
  * (src/diffraction.c:223-235, :834), or 1 under delta_atoms.
  * pos: xyz per atom (metres), host memory.  occ / bfac may be NULL (1 / 0).
  * beam: {fwhm, centre_x, centre_y} in metres, or NULL for a plane wave.
- * bfac != NULL selects per-atom Debye-Waller factors exp(-B_j |q|^2/4). */
+ * bfac != NULL selects per-atom Debye-Waller factors exp(-B_j |q|^2/4), on top
+ * of the global B of the forward call (the total is exp(-(B + B_j) |q|^2/4)). */
 typedef struct spsim_b200_molecule spsim_b200_molecule;
 int spsim_b200_molecule_create(int natoms, const int32_t *Z, const float *pos, const float *occ,
                                const float *bfac, int delta_atoms, const float *beam,
@@ -122,12 +123,35 @@ int spsim_b200_forward_batch(int npatterns, const spsim_b200_molecule *const *mo
                              const spsim_b200_qset *const *qsets, const double *rot, float B,
                              int precision, float *const *F_dev, float *const *I_dev, void *stream);
 
+/* Polychromatic forward, the semantics of spsim's spectrum kernel
+ * (src/diffraction.cu:415-476, CUDA_spectrum_scattering_from_all_atoms, which
+ * its default CUDA path runs when experiment_bandwidth != 0): with S samples
+ * (an even S > 1 is raised by one, src/diffraction.cu:305-307),
+ *   lambda_j = lambda (1 - bw/2) + j/(S-1) lambda bw,
+ *   F(q) = sum_j w_j sum_atoms f_e(|q|) w_a exp(-2 pi i (lambda/lambda_j) q.r),
+ * w_j proportional to exp(-z_j^2/2), z_j = (lambda_j - lambda)/(lambda bw/4),
+ * summing to one; form factors stay at the unscaled |q| as in the reference.
+ * All S samples run as one batched launch (a captured graph on non-default
+ * streams), combined in FP64.  bandwidth == 0 or samples == 1 is the plain
+ * forward.  samples < 1 is SPSIM_ERR_INVALID_ARG. */
+int spsim_b200_forward_spectrum(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot,
+                                float B, int precision, float wavelength, float bandwidth, int samples,
+                                float *F_dev, float *I_dev, void *stream);
+
 /* Host-memory convenience: atoms and HKL list from host, F / I back to host
  * (copies inside).  The reference-shaped compute_pattern_on_list is built on it. */
 int spsim_b200_structure_factor_host(int natoms, const int32_t *Z, const float *pos, const float *occ,
                                      const float *bfac, float B, int delta_atoms, const float *beam,
                                      int64_t npix, const float *hkl, int precision, float *F_host,
                                      float *I_host);
+
+/* spsim_b200_structure_factor_host with a bandwidth-broadened beam
+ * (spsim_b200_forward_spectrum's semantics); cuda_compute_pattern_on_list2
+ * and compute_sf (use_cuda = 1) are built on it. */
+int spsim_b200_structure_factor_host_spectrum(int natoms, const int32_t *Z, const float *pos, const float *occ,
+                                              const float *bfac, float B, int delta_atoms, const float *beam,
+                                              float wavelength, float bandwidth, int samples, int64_t npix,
+                                              const float *hkl, int precision, float *F_host, float *I_host);
 
 /* ---- allocation-free variant (no counterpart in the reference) ------------
  * The same computation, arguments and results as

@@ -86,6 +86,29 @@ def structure_factor(Z, pos, q, occ=None, bfac=None, B=0.0, delta_atoms=False, b
     return fr + 1j * fi, I
 
 
+def structure_factor_spectrum(Z, pos, q, wavelength, bandwidth, samples, occ=None, bfac=None, B=0.0,
+                              delta_atoms=False, beam=None, nthreads=None):
+    """FP64 polychromatic structure factor (spsim's spectrum kernel semantics,
+    src/diffraction.cu:415-476): (F complex128, I float64)."""
+    L = oracle_lib()
+    Z = np.ascontiguousarray(Z, np.int32)
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+    q = np.ascontiguousarray(q, np.float64).reshape(-1, 3)
+    occ = np.ascontiguousarray(occ, np.float64) if occ is not None else None
+    bfac = np.ascontiguousarray(bfac, np.float64) if bfac is not None else None
+    beam = beam or (0.0, 0.0, 0.0)
+    n = q.shape[0]
+    Fr, Fi, I = np.zeros(n), np.zeros(n), np.zeros(n)
+    L.oracle_structure_factor_spectrum.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int,
+                                                   c_double, c_double, c_double, c_double, c_double, c_int,
+                                                   ctypes.c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_int]
+    L.oracle_structure_factor_spectrum(len(Z), _p(Z), _p(pos), _p(occ), _p(bfac), float(B), int(delta_atoms),
+                                       float(beam[0]), float(beam[1]), float(beam[2]), float(wavelength),
+                                       float(bandwidth), int(samples), n, _p(q), _p(Fr), _p(Fi), _p(I),
+                                       nthreads or os.cpu_count() or 1)
+    return Fr + 1j * Fi, I
+
+
 def structure_factor_vjp(Z, pos, q, g, occ=None, bfac=None, nthreads=None):
     """FP64 dL/dpos (N,3), dL/docc (N,), dL/dB (N,) for dL/dI = g."""
     Z = np.ascontiguousarray(Z, np.int32)

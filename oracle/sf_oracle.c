@@ -102,7 +102,7 @@ void oracle_hkl_detector(int nx, int ny, float width, float height, float distan
  *   F(q) = sum_j f_Zj(|q|, B_j) * occ_j * sqrt(illum_j) * exp(-2 pi i q.r_j),  I = |F|^2
  * Atoms with Z == 0 are skipped (:830-832); delta_atoms replaces f*sqrt(illum)
  * by 1 (:837-843).  Extensions beyond the reference: per-atom occupancy (occ,
- * NULL = 1) and per-atom B (bj, NULL = the global B for every atom).
+ * NULL = 1) and per-atom B (bj, NULL = none), added to the global B.
  */
 typedef struct {
   int natoms;
@@ -113,6 +113,7 @@ typedef struct {
   long p0, p1;
   const double *q;
   double *F_re, *F_im, *I;
+  double qscale; /* the phase uses qscale * q; form factors stay at |q| */
 } sf_job_t;
 
 static void *sf_worker(void *arg) {
@@ -131,7 +132,7 @@ static void *sf_worker(void *arg) {
       if (jb->delta_atoms) {
         f = 1.0;
       } else if (jb->bj) {
-        f = oracle_scatt_factor(qlen, z, jb->bj[j]);
+        f = oracle_scatt_factor(qlen, z, jb->B + jb->bj[j]);  /* the global B adds to the atom's own */
       } else {
         if (!have[z]) {
           cache[z] = oracle_scatt_factor(qlen, z, jb->B);
@@ -140,7 +141,7 @@ static void *sf_worker(void *arg) {
         f = cache[z];
       }
       const double *r = jb->pos + 3 * j;
-      double t = qx * r[0] + qy * r[1] + qz * r[2];
+      double t = jb->qscale * (qx * r[0] + qy * r[1] + qz * r[2]);
       t -= rint(t);
       double s, c;
       sincos(-2.0 * M_PI * t, &s, &c);
@@ -187,10 +188,70 @@ void oracle_structure_factor(int natoms, const int *Z, const double *pos, const 
   sf_job_t jobs[256];
   for (int t = 0; t < nthreads; t++) {
     sf_job_t j = {natoms, Z, pos, occ, bj, w, B, delta_atoms,
-                  npix * t / nthreads, npix * (t + 1) / nthreads, q, F_re, F_im, I};
+                  npix * t / nthreads, npix * (t + 1) / nthreads, q, F_re, F_im, I, 1.0};
     jobs[t] = j;
   }
   run_slabs(nthreads, jobs, sizeof(sf_job_t), sf_worker);
+  free(w);
+}
+
+/*
+ * src/diffraction.cu:415-476 (CUDA_spectrum_scattering_from_all_atoms) in FP64,
+ * with the sample count rule of :305-307 (an even count above one is raised by
+ * one).  lambda_j = lambda (1 - bw/2) + j/(S-1) lambda bw, the phase of sample
+ * j uses q lambda/lambda_j, the form factor the unscaled |q| (:440-447), the
+ * weight exp(-z^2/2) with z = (lambda_j - lambda) / ((lambda - lambda (1 -
+ * bw/2)) / 2) (:431, :454-456); the amplitude is the weighted mean over the
+ * samples (:465-466).  bandwidth == 0 or S == 1: the monochromatic sum.
+ */
+void oracle_structure_factor_spectrum(int natoms, const int *Z, const double *pos, const double *occ,
+                                      const double *bj, double B, int delta_atoms, double beam_fwhm,
+                                      double beam_cx, double beam_cy, double wavelength, double bandwidth,
+                                      int samples, long npix, const double *q, double *F_re, double *F_im,
+                                      double *I, int nthreads) {
+  if (samples > 1 && (samples & 1) == 0) samples++;
+  if (bandwidth == 0.0 || samples <= 1) {
+    oracle_structure_factor(natoms, Z, pos, occ, bj, B, delta_atoms, beam_fwhm, beam_cx, beam_cy, npix, q, F_re,
+                            F_im, I, nthreads);
+    return;
+  }
+  ensure_table();
+  double *w = (double *)malloc(sizeof(double) * (natoms > 0 ? natoms : 1));
+  for (int j = 0; j < natoms; j++) {
+    double o = occ ? occ[j] : 1.0;
+    w[j] = delta_atoms ? 1.0 : o * sqrt(illumination(beam_fwhm, beam_cx, beam_cy, pos[3 * j], pos[3 * j + 1]));
+  }
+  double *re = (double *)malloc(sizeof(double) * (npix > 0 ? npix : 1));
+  double *im = (double *)malloc(sizeof(double) * (npix > 0 ? npix : 1));
+  for (long i = 0; i < npix; i++) F_re[i] = F_im[i] = 0.0;
+  const double sigma = (wavelength - wavelength * (1.0 - bandwidth / 2.0)) / 2.0;
+  double total = 0.0;
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  for (int s = 0; s < samples; s++) {
+    const double lj = wavelength * (1.0 - bandwidth / 2.0) + ((double)s / (samples - 1)) * wavelength * bandwidth;
+    const double z = (lj - wavelength) / sigma;
+    const double ws = exp(-z * z / 2.0);
+    total += ws;
+    sf_job_t jobs[256];
+    for (int t = 0; t < nthreads; t++) {
+      sf_job_t jb = {natoms, Z, pos, occ, bj, w, B, delta_atoms,
+                     npix * t / nthreads, npix * (t + 1) / nthreads, q, re, im, NULL, wavelength / lj};
+      jobs[t] = jb;
+    }
+    run_slabs(nthreads, jobs, sizeof(sf_job_t), sf_worker);
+    for (long i = 0; i < npix; i++) {
+      F_re[i] += ws * re[i];
+      F_im[i] += ws * im[i];
+    }
+  }
+  for (long i = 0; i < npix; i++) {
+    F_re[i] /= total;
+    F_im[i] /= total;
+    if (I) I[i] = F_re[i] * F_re[i] + F_im[i] * F_im[i];
+  }
+  free(re);
+  free(im);
   free(w);
 }
 

@@ -20,7 +20,7 @@ from ._native import PRECISIONS, ChainOutputs, ChainParams, check, lib
 
 __all__ = [
     "Molecule", "QSet", "forward", "forward_batch", "adjoint", "detector_chain", "chain_params",
-    "hkl_for_detector", "synchronize", "timing", "autotune", "set_variant", "last_forward_stats",
+    "hkl_for_detector", "synchronize", "forward_spectrum", "timing", "autotune", "set_variant", "last_forward_stats",
     "last_variant", "kernel_name",
 ]
 
@@ -163,6 +163,27 @@ def forward(mol, qs, rot=None, B=0.0, precision="f32", F=None, I=None, want_F=Tr
     check(lib().spsim_b200_forward(mol.handle, qs.handle, r.ctypes.data_as(c_void_p) if r is not None else None,
                                    float(B), _prec(precision), _dev(F) if want_F else None,
                                    _dev(I) if want_I else None, _stream_ptr(stream)))
+    return (F if want_F else None), (I if want_I else None)
+
+
+def forward_spectrum(mol, qs, wavelength, bandwidth, samples=5, rot=None, B=0.0, precision="f32", F=None, I=None,
+                     want_F=True, want_I=True, stream=None):
+    """Polychromatic pattern with spsim's spectrum-kernel semantics
+    (src/diffraction.cu:415-476): the amplitude averaged over `samples`
+    wavelengths across the relative bandwidth, Gaussian-weighted, all samples
+    in one batched launch.  Returns (F, I) like forward()."""
+    _native.use_device(mol.device)
+    dev = torch.device("cuda", mol.device)
+    if want_F and F is None:
+        F = torch.empty(qs.npix, dtype=torch.complex64, device=dev)
+    if want_I and I is None:
+        I = torch.empty(qs.npix, dtype=torch.float32, device=dev)
+    r = _rot_array(rot, 1)
+    check(lib().spsim_b200_forward_spectrum(mol.handle, qs.handle,
+                                            r.ctypes.data_as(c_void_p) if r is not None else None, float(B),
+                                            _prec(precision), float(wavelength), float(bandwidth), int(samples),
+                                            _dev(F) if want_F else None, _dev(I) if want_I else None,
+                                            _stream_ptr(stream)))
     return (F if want_F else None), (I if want_I else None)
 
 

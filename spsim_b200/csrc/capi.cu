@@ -539,6 +539,17 @@ struct DevBuf {
   }
 };
 
+// A polychromatic forward: the plan's npat patterns are the wavelength
+// samples of one detector (phase-space scales qscale[j]); their amplitudes are
+// combined with weight[j] into one F / I instead of being finalized one by one.
+struct Spectrum {
+  int samples = 0;
+  const double *qscale = nullptr;
+  const double *weight = nullptr;
+  float *F = nullptr;
+  float *I = nullptr;
+};
+
 struct Plan {
   // key
   std::vector<const void *> key_ptrs;
@@ -552,6 +563,9 @@ struct Plan {
   bool perb = false;
   std::vector<long long> npix_of;
   std::vector<SfPattern> host_pats;  // descriptors as last uploaded (rotations change per call)
+  int spectrum = 0;                  // > 0: combine this many patterns into spec_F / spec_I
+  DevBuf spec_w;
+  float *spec_F = nullptr, *spec_I = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   ~Plan() {
@@ -615,7 +629,7 @@ static bool is_orthonormal(const double *R) {
 
 static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
                       const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, const Spectrum *spec) {
   pl.npat = npat;
   pl.precision = precision;
   std::vector<SfPattern> pats(npat);
@@ -693,6 +707,9 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
       pt.has_rot = 0;
       for (int k = 0; k < 9; ++k) pt.rot[k] = (k % 4 == 0) ? 1.0 : 0.0;
     }
+    pt.qscale = spec ? spec->qscale[i] : 1.0;
+    pt.s2scale = 1.0 / (pt.qscale * pt.qscale);
+    qmax *= std::fabs(pt.qscale);
     memcpy(pt.center, m->center, sizeof(pt.center));
     const int eq = ceil_log2_bound(std::max(qmax, 1e-300));
     const int kq = 22 - m->kr;
@@ -724,6 +741,13 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
   }
   CUDA_TRY(cudaMemcpyAsync(pl.pats.p, pats.data(), npat * sizeof(SfPattern), cudaMemcpyHostToDevice, stream));
   pl.host_pats = pats;
+  pl.spectrum = spec ? spec->samples : 0;
+  pl.spec_F = spec ? spec->F : nullptr;
+  pl.spec_I = spec ? spec->I : nullptr;
+  if (spec) {
+    CUDA_TRY(pl.spec_w.ensure(npat * sizeof(double)));
+    CUDA_TRY(cudaMemcpyAsync(pl.spec_w.p, spec->weight, npat * sizeof(double), cudaMemcpyHostToDevice, stream));
+  }
 
   if (precision != SPSIM_PREC_FP64) {
     // work items: pixel tile x atom-tile range, cost-sorted (largest first)
@@ -804,13 +828,25 @@ static cudaError_t enqueue_plan(Plan &pl, cudaStream_t stream, cudaEvent_t ev0, 
       return e;
   }
   if (ev1 && (e = cudaEventRecord(ev1, stream))) return e;
+  if (pl.spectrum > 0)
+    return launch_spectrum_combine((const SfPattern *)pl.pats.p, 0, pl.spectrum, (const double *)pl.spec_w.p, pl.spec_F,
+                                   pl.spec_I, pl.npix_of.empty() ? 0 : pl.npix_of[0], stream);
   return launch_finalize((const SfPattern *)pl.pats.p, 0, pl.npat, pl.max_npix, stream);
 }
 
 static void plan_key(int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
                      const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
-                     std::vector<const void *> &kp, std::vector<double> &kv) {
+                     const Spectrum *spec, std::vector<const void *> &kp, std::vector<double> &kv) {
   kv.push_back(npat);
+  kv.push_back(spec ? spec->samples : 0);
+  if (spec) {
+    for (int i = 0; i < npat; ++i) {
+      kv.push_back(spec->qscale[i]);
+      kv.push_back(spec->weight[i]);
+    }
+    kp.push_back(spec->F);
+    kp.push_back(spec->I);
+  }
   kv.push_back(B);
   kv.push_back(precision);
   kv.push_back(g_force_nt);
@@ -859,7 +895,7 @@ static int check_flags(Plan &pl) {
 // cache == false: a one-shot plan (host convenience path), synchronised before return
 static int run_forward(int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
                        const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
-                       cudaStream_t stream, bool cache) {
+                       cudaStream_t stream, bool cache, const Spectrum *spec = nullptr) {
   if (npat < 0) return fail(SPSIM_ERR_INVALID_ARG, "npatterns < 0");
   if (npat == 0) return SPSIM_OK;
   if (!mols || !qsets) return fail(SPSIM_ERR_INVALID_ARG, "NULL molecule or q-set array");
@@ -876,7 +912,7 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
   std::lock_guard<std::mutex> lk(g_mu);
   std::vector<const void *> kp;
   std::vector<double> kv;
-  plan_key(npat, mols, qsets, rot, B, precision, F_dev, I_dev, kp, kv);
+  plan_key(npat, mols, qsets, rot, B, precision, F_dev, I_dev, spec, kp, kv);
   Plan *pl = nullptr;
   if (cache) {
     for (size_t i = 0; i < g_plans.size(); ++i) {
@@ -893,7 +929,7 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
     std::unique_ptr<Plan> np(new Plan());
     np->key_ptrs = kp;
     np->key_vals = kv;
-    st = build_plan(*np, npat, mols, qsets, rot, B, precision, F_dev, I_dev, stream);
+    st = build_plan(*np, npat, mols, qsets, rot, B, precision, F_dev, I_dev, stream, spec);
     if (st) return st;
     if (g_plans.size() >= kMaxPlans) {
       cudaDeviceSynchronize();  // the evicted plan's buffers may still be in use
@@ -912,7 +948,7 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
     pl = os.plan;
     pl->key_ptrs = kp;
     pl->key_vals = kv;
-    st = build_plan(*pl, npat, mols, qsets, rot, B, precision, F_dev, I_dev, stream);
+    st = build_plan(*pl, npat, mols, qsets, rot, B, precision, F_dev, I_dev, stream, spec);
     if (st) return st;
   }
   g_last_terms = pl->terms;
@@ -953,6 +989,73 @@ extern "C" int spsim_b200_forward(const spsim_b200_molecule *m, const spsim_b200
   float *F[1] = {F_dev};
   float *I[1] = {I_dev};
   return run_forward(1, &m, &qs, rot, B, precision, F, I, (cudaStream_t)stream, true);
+}
+
+// Wavelength samples of a bandwidth-broadened beam, as spsim's spectrum kernel
+// takes them (src/diffraction.cu:305-307, :415-476): an even sample count
+// above one is raised by one; lambda_j = lambda (1 - bw/2) + j/(S-1) lambda bw;
+// the phase uses q lambda / lambda_j (form factors stay at |q|); weights are
+// exp(-z_j^2 / 2) with z_j = (lambda_j - lambda) / (lambda bw / 4), normalised
+// to sum to one.  Returns the sample count used (1: monochromatic).
+static int spectrum_samples(float wavelength, float bandwidth, int samples, std::vector<double> &qscale,
+                            std::vector<double> &weight) {
+  if (samples > 1 && (samples & 1) == 0) ++samples;
+  qscale.clear();
+  weight.clear();
+  if (bandwidth == 0.0f || samples <= 1) {
+    qscale.push_back(1.0);
+    weight.push_back(1.0);
+    return 1;
+  }
+  const double lam = wavelength, bw = bandwidth;
+  const double sigma = (lam - lam * (1.0 - bw / 2.0)) / 2.0;
+  double tot = 0.0;
+  for (int j = 0; j < samples; ++j) {
+    const double lj = lam * (1.0 - bw / 2.0) + ((double)j / (samples - 1)) * lam * bw;
+    const double z = (lj - lam) / sigma;
+    qscale.push_back(lam / lj);
+    weight.push_back(std::exp(-z * z / 2.0));
+    tot += weight.back();
+  }
+  for (double &w : weight) w /= tot;
+  return samples;
+}
+
+static int forward_spectrum(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot, float B,
+                            int precision, float wavelength, float bandwidth, int samples, float *F_dev, float *I_dev,
+                            cudaStream_t stream, bool cache) {
+  if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
+  if (samples < 1) return fail(SPSIM_ERR_INVALID_ARG, "wavelength samples must be >= 1 (got %d)", samples);
+  if (bandwidth != 0.0f && !(wavelength > 0.0f))
+    return fail(SPSIM_ERR_INVALID_ARG, "a bandwidth needs a wavelength > 0");
+  std::vector<double> qscale, weight;
+  const int S = spectrum_samples(wavelength, bandwidth, samples, qscale, weight);
+  if (S == 1) {
+    float *F[1] = {F_dev};
+    float *I[1] = {I_dev};
+    return run_forward(1, &m, &qs, rot, B, precision, F, I, stream, cache);
+  }
+  std::vector<const spsim_b200_molecule *> mols(S, m);
+  std::vector<const spsim_b200_qset *> qsets(S, qs);
+  std::vector<double> rots;
+  if (rot)
+    for (int j = 0; j < S; ++j) rots.insert(rots.end(), rot, rot + 9);
+  std::vector<float *> none(S, nullptr);
+  Spectrum spec;
+  spec.samples = S;
+  spec.qscale = qscale.data();
+  spec.weight = weight.data();
+  spec.F = F_dev;
+  spec.I = I_dev;
+  return run_forward(S, mols.data(), qsets.data(), rot ? rots.data() : nullptr, B, precision, none.data(), none.data(),
+                     stream, cache, &spec);
+}
+
+extern "C" int spsim_b200_forward_spectrum(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot,
+                                           float B, int precision, float wavelength, float bandwidth, int samples,
+                                           float *F_dev, float *I_dev, void *stream) {
+  return forward_spectrum(m, qs, rot, B, precision, wavelength, bandwidth, samples, F_dev, I_dev,
+                          (cudaStream_t)stream, true);
 }
 
 extern "C" int spsim_b200_forward_batch(int npatterns, const spsim_b200_molecule *const *mols,
@@ -1059,10 +1162,10 @@ extern "C" void spsim_internal_release_host_session(void) {
   g_oneshot = OneShot();
 }
 
-extern "C" int spsim_b200_structure_factor_host(int natoms, const int32_t *Z, const float *pos, const float *occ,
-                                                const float *bfac, float B, int delta_atoms, const float *beam,
-                                                int64_t npix, const float *hkl, int precision, float *F_host,
-                                                float *I_host) {
+static int structure_factor_host(int natoms, const int32_t *Z, const float *pos, const float *occ, const float *bfac,
+                                 float B, int delta_atoms, const float *beam, float wavelength, float bandwidth,
+                                 int samples, int64_t npix, const float *hkl, int precision, float *F_host,
+                                 float *I_host) {
   if (npix < 0 || (npix > 0 && !hkl)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
   int dev;
   int st = current_device(&dev);
@@ -1085,11 +1188,28 @@ extern "C" int spsim_b200_structure_factor_host(int natoms, const int32_t *Z, co
   float *I[1] = {I_host ? (float *)g_host.I->p : nullptr};
   const spsim_b200_molecule *mm = m;
   const spsim_b200_qset *qq = q;
-  st = run_forward(1, &mm, &qq, nullptr, B, precision, F, I, nullptr, false);
+  st = forward_spectrum(mm, qq, nullptr, B, precision, wavelength, bandwidth, samples, F[0], I[0], nullptr, false);
   if (st) return st;
   if (F_host && npix) CUDA_TRY(cudaMemcpy(F_host, F[0], 2 * npix * sizeof(float), cudaMemcpyDeviceToHost));
   if (I_host && npix) CUDA_TRY(cudaMemcpy(I_host, I[0], npix * sizeof(float), cudaMemcpyDeviceToHost));
   return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_structure_factor_host(int natoms, const int32_t *Z, const float *pos, const float *occ,
+                                                const float *bfac, float B, int delta_atoms, const float *beam,
+                                                int64_t npix, const float *hkl, int precision, float *F_host,
+                                                float *I_host) {
+  return structure_factor_host(natoms, Z, pos, occ, bfac, B, delta_atoms, beam, 0.0f, 0.0f, 1, npix, hkl, precision,
+                               F_host, I_host);
+}
+
+extern "C" int spsim_b200_structure_factor_host_spectrum(int natoms, const int32_t *Z, const float *pos,
+                                                         const float *occ, const float *bfac, float B, int delta_atoms,
+                                                         const float *beam, float wavelength, float bandwidth,
+                                                         int samples, int64_t npix, const float *hkl, int precision,
+                                                         float *F_host, float *I_host) {
+  return structure_factor_host(natoms, Z, pos, occ, bfac, B, delta_atoms, beam, wavelength, bandwidth, samples, npix,
+                               hkl, precision, F_host, I_host);
 }
 
 // ---------------------------------------------------------------------------

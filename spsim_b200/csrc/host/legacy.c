@@ -189,8 +189,12 @@ SpRotation *apply_orientation_to_HKL_list(float **HKL_list, int *HKL_list_size, 
 
 /* ------------------------------------------------------------ structure factor */
 
+/* spectrum != 0: the semantics of spsim's default CUDA path
+ * (cuda_compute_pattern_on_list2, src/diffraction.cu:235-339): an even
+ * wavelength_samples above one is raised by one in opts (as the reference
+ * does), and a non-zero bandwidth samples the spectrum. */
 static Diffraction_Pattern *pattern_on_list(Molecule *mol, float *HKL_list, int n, float B, Experiment *exp,
-                                            Options *opts) {
+                                            Options *opts, int spectrum) {
   double t0 = now_us();
   Diffraction_Pattern *res = (Diffraction_Pattern *)calloc(1, sizeof(Diffraction_Pattern));
   res->F = (Complex *)malloc(sizeof(Complex) * (n > 0 ? n : 1));
@@ -200,9 +204,25 @@ static Diffraction_Pattern *pattern_on_list(Molecule *mol, float *HKL_list, int 
   res->HKL_list_size = n;
   res->N_pix = n;
   float beam[3] = {exp ? exp->beam_fwhm : 0.0f, exp ? exp->beam_center_x : 0.0f, exp ? exp->beam_center_y : 0.0f};
-  int st = spsim_b200_structure_factor_host(mol->natoms, mol->atomic_number, mol->pos, NULL, NULL, B,
-                                            opts ? opts->delta_atoms : 0, beam, n, HKL_list, g_precision,
-                                            (float *)res->F, res->ints);
+  int samples = 1;
+  if (spectrum && opts) {
+    if (opts->wavelength_samples > 1 && (opts->wavelength_samples & 1) == 0) opts->wavelength_samples++;
+    samples = opts->wavelength_samples;
+  }
+  int st;
+  if (spectrum && exp && exp->bandwidth != 0.0f && samples != 1) {
+    if (samples < 1) {
+      fprintf(stderr, "spsim_b200: wavelength_samples must be >= 1 with a bandwidth (got %d)\n", samples);
+      abort();
+    }
+    st = spsim_b200_structure_factor_host_spectrum(mol->natoms, mol->atomic_number, mol->pos, NULL, NULL, B,
+                                                   opts->delta_atoms, beam, exp->wavelength, exp->bandwidth, samples,
+                                                   n, HKL_list, g_precision, (float *)res->F, res->ints);
+  } else {
+    st = spsim_b200_structure_factor_host(mol->natoms, mol->atomic_number, mol->pos, NULL, NULL, B,
+                                          opts ? opts->delta_atoms : 0, beam, n, HKL_list, g_precision,
+                                          (float *)res->F, res->ints);
+  }
   if (st) die("compute_pattern_on_list", st);
   if (opts && opts->verbosity_level > 0) /* src/diffraction.c:849-851 */
     printf("%g atoms.pixel/s\n", 1.0e6 * n * mol->natoms / (now_us() - t0));
@@ -212,35 +232,40 @@ static Diffraction_Pattern *pattern_on_list(Molecule *mol, float *HKL_list, int 
 /* src/diffraction.c:770 */
 Diffraction_Pattern *compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
                                              Experiment *exp, Options *opts) {
-  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts);
+  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts, 0);
 }
 
 /* src/diffraction.c:856 (the SSE path): same GPU evaluation */
 Diffraction_Pattern *vector_compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
                                                     Experiment *exp, Options *opts) {
-  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts);
+  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts, 0);
 }
 
 /* src/diffraction.cu:135 */
 Diffraction_Pattern *cuda_compute_pattern_on_list(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
                                                   Experiment *exp, Options *opts) {
-  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts);
+  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts, 0);
 }
 
-/* src/diffraction.cu:235 */
+/* src/diffraction.cu:235: the default CUDA path, including the spectrum */
 Diffraction_Pattern *cuda_compute_pattern_on_list2(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
                                                    Experiment *exp, Options *opts) {
-  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts);
+  return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts, 1);
 }
 
 /* src/spsim.c:110-144: the FFT / NFFT structure factors are other algorithms,
- * not provided; every direct-summation path runs on the GPU. */
+ * not provided; every direct-summation path runs on the GPU.  The dispatch
+ * follows the reference's: use_cuda == 2 is the first CUDA path, any other
+ * non-zero use_cuda the second (with the spectrum), use_cuda == 0 the CPU
+ * paths (monochromatic). */
 Diffraction_Pattern *compute_sf(Molecule *mol, float *HKL_list, int HKL_list_size, Options *opts) {
   if (opts->use_fft_for_sf || opts->use_nfft_for_sf) {
     fprintf(stderr, "spsim_b200: the FFT/NFFT structure factors are not supported\n");
     abort();
   }
-  Diffraction_Pattern *p = pattern_on_list(mol, HKL_list, HKL_list_size, opts->b_factor, opts->experiment, opts);
+  const int spectrum = opts->use_cuda != 0 && opts->use_cuda != 2;
+  Diffraction_Pattern *p =
+      pattern_on_list(mol, HKL_list, HKL_list_size, opts->b_factor, opts->experiment, opts, spectrum);
   p->rot = NULL;
   return p;
 }

@@ -280,6 +280,8 @@ extern "C" int spsim_b200_structure_factor_host_noalloc(int natoms, const int32_
   pat->per_atom_b = perb ? 1 : 0;
   pat->has_rot = 0;
   for (int k = 0; k < 9; ++k) pat->rot[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  pat->qscale = 1.0;
+  pat->s2scale = 1.0;
   pat->ff = (const double *)(dbase + d_ff);
   pat->npix = npix;
   pat->hkl = (const float *)(dbase + d_hkl);

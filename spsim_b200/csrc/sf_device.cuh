@@ -58,6 +58,8 @@ struct SfPattern {
   const float *hkl;        // AoS float3 q (1/m), or nullptr
   const double *q64;       // AoS double3 q (1/m), or nullptr
   double rot[9];           // row-major, applied as q' = R q
+  double qscale;           // phase-space q = qscale * R q (wavelength sample of a spectrum; 1 otherwise)
+  double s2scale;          // 1 / qscale^2: per-atom B factors use the unscaled |q|, like the form factors
   double center[3];        // molecule centre (m)
   float dq, inv_dq;        // pixel grid step (power of two) and its inverse
   double2 *acc;            // FP64 accumulator [npix] (zeroed before the forward)

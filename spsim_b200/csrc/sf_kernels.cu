@@ -69,6 +69,9 @@ __device__ __forceinline__ void load_q(const SfPattern &pt, long long p, double 
     q[1] = b;
     q[2] = c;
   }
+  q[0] *= pt.qscale;
+  q[1] *= pt.qscale;
+  q[2] *= pt.qscale;
 }
 
 // ---------------------------------------------------------------------------
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(NT) sf_f32_kernel(const SfPattern *__restrict_
       qlz[i] = (float)(q[2] - hz);
       // -(|q| 1e-10)^2 / 4 * log2(e): per-atom B factor exponent in base 2
       const double d2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20;
-      s2n[i] = (float)(-0.25 * d2 * 1.4426950408889634);
+      s2n[i] = (float)(-0.25 * d2 * pt.s2scale * 1.4426950408889634);
     }
     double fre[P], fim[P];
     float shc[P], slc[P], shs[P], sls[P];
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
         v[6][h] = (float)(q[0] - hx);
         v[7][h] = (float)(q[1] - hy);
         v[8][h] = (float)(q[2] - hz);
-        v[9][h] = (float)(-0.25 * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 1.4426950408889634);
+        v[9][h] = (float)(-0.25 * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * pt.s2scale * 1.4426950408889634);
       }
       qhx[j] = make_float2(v[0][0], v[0][1]);
       qhy[j] = make_float2(v[1][0], v[1][1]);
@@ -536,7 +539,7 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
       qx[i] = q[0];
       qy[i] = q[1];
       qz[i] = q[2];
-      s2n[i] = (float)(-0.25 * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 1.4426950408889634);
+      s2n[i] = (float)(-0.25 * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * pt.s2scale * 1.4426950408889634);
     }
     float2 shc[NP], slc[NP], shs[NP], sls[NP];
 #pragma unroll
@@ -692,7 +695,7 @@ __global__ void __launch_bounds__(256) sf_f64_kernel(const SfPattern *__restrict
   if (p >= pt.npix) return;
   double q[3];
   load_q(pt, p, q);
-  const double s2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 0.25;
+  const double s2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * 0.25 * pt.s2scale;
   double fr = 0.0, fi = 0.0, ar = 0.0, ai = 0.0;
   for (int k = 0; k < pt.n_tiles; ++k) {
     const TileDesc td = pt.tiles[k];
@@ -739,6 +742,32 @@ __global__ void sf_finalize_kernel(const SfPattern *__restrict__ pats, int patte
     sincospi(2.0 * t, &s, &c);
     pt.F[p] = make_float2((float)(a.x * c + a.y * s), (float)(a.y * c - a.x * s));
   }
+}
+
+// Polychromatic combination (src/diffraction.cu:415-476 semantics): the
+// patterns pattern0 .. pattern0+S-1 hold the centred FP64 amplitudes of one
+// detector at the phase-space scales lambda / lambda_j; F is their weighted
+// sum, each with its own centre phase e^{-2 pi i s_j q.c}, and I = |F|^2.
+__global__ void sf_spectrum_combine_kernel(const SfPattern *__restrict__ pats, int pattern0, int S,
+                                           const double *__restrict__ weight, float2 *__restrict__ F,
+                                           float *__restrict__ I, long long npix) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npix) return;
+  double re = 0.0, im = 0.0;
+  for (int j = 0; j < S; ++j) {
+    const SfPattern &pt = pats[pattern0 + j];
+    const double2 a = pt.acc[p];
+    double q[3];
+    load_q(pt, p, q);
+    double t = q[0] * pt.center[0] + q[1] * pt.center[1] + q[2] * pt.center[2];
+    t -= rint(t);
+    double s, c;
+    sincospi(2.0 * t, &s, &c);
+    re += weight[j] * (a.x * c + a.y * s);
+    im += weight[j] * (a.y * c - a.x * s);
+  }
+  if (F) F[p] = make_float2((float)re, (float)im);
+  if (I) I[p] = (float)(re * re + im * im);
 }
 
 // ---------------------------------------------------------------------------
@@ -917,6 +946,14 @@ bool sf_f32_variant_exists(int mode, int nt, int p, int packed) {
 cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cudaStream_t st) {
   if (npix <= 0) return cudaSuccess;
   sf_f64_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(pats, pattern);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spectrum_combine(const SfPattern *pats, int pattern0, int S, const double *weight, float *F,
+                                    float *I, long long npix, cudaStream_t st) {
+  if (npix <= 0) return cudaSuccess;
+  sf_spectrum_combine_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(pats, pattern0, S, weight, (float2 *)F, I,
+                                                                            npix);
   return cudaGetLastError();
 }
 

@@ -15,6 +15,8 @@ cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const 
 int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb);
 bool sf_f32_variant_exists(int mode, int nt, int p, int packed);
 cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cudaStream_t st);
+cudaError_t launch_spectrum_combine(const SfPattern *pats, int pattern0, int S, const double *weight, float *F,
+                                    float *I, long long npix, cudaStream_t st);
 cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st);
 cudaError_t launch_ewald(int nx, int ny, double width, double height, double distance, double cx, double cy,
                          double wavelength, int spherical, float *out32, double *out64, cudaStream_t st);
