@@ -61,6 +61,22 @@ Molecule *alloc_mol(void);                                               /* src/
 void add_atom_to_mol(Molecule *mol, int atomic_number, float x, float y, float z); /* src/molecule.c:402 */
 void free_mol(Molecule *mol);                                            /* src/molecule.c:413 */
 
+/* ---- molecule files: include/molecule.h:22-31, include/spsim.h (get_molecule) ----
+ * PDB ATOM/HETATM records (coordinates in Angstrom -> metres, element from
+ * columns 77-78) expanded by the REMARK 350 BIOMT operators; a chemical
+ * formula as random positions in the options' box; PDB writing; centring on
+ * the electron centre of mass.  Unidentifiable elements are skipped (the
+ * reference overwrites the previous atom's Z instead). */
+Molecule *get_Molecule_from_pdb(char *filename);                          /* src/molecule.c:65 */
+Molecule *get_Molecule_from_formula(Chem_Formula *form, Options *opts);   /* src/molecule.c:33 */
+void write_pdb_from_mol(char *filename, Molecule *mol);                   /* src/molecule.c:359 */
+void origin_to_center_of_mass(Molecule *mol);                             /* src/molecule.c:440 */
+Molecule *get_molecule(Options *opts);                                    /* src/spsim.c:83 */
+
+/* ---- VTK output: include/io.h ---- */
+void write_2D_array_to_vtk(float *F, int nx, int ny, char *filename);     /* src/io.c:29 */
+void write_3D_array_to_vtk(float *F, int nx, int ny, int nz, char *filename); /* src/io.c:60 */
+
 /* ---- distribution: include/mpi_comm.h:30-32 (single-process semantics;
  *      multi-GPU sharding lives in the Python layer over torch.distributed) ---- */
 void get_my_loop_start_and_end(int size, int *start, int *end);          /* src/mpi.c:30 */

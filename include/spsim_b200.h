@@ -281,6 +281,11 @@ int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
  * No reference counterpart: spsim allocates and frees per call. */
 void spsim_b200_release_scratch(void);
 
+/* Seed of the random positions get_Molecule_from_formula draws (the reference
+ * draws them from libspimage's p_drand48 stream, which is not available here;
+ * no counterpart). */
+void spsim_b200_set_formula_seed(unsigned long long seed);
+
 /* Autotuner: the kernel variant used for FP32 forwards: threads per CTA,
  * pixels per thread and form:
  *   0  compensated FP32 phase (hi/lo split), one pixel per lane

@@ -351,3 +351,65 @@ def ref_gpu_pattern(Z, pos, hkl, B=0.0, wavelength_samples=1, bandwidth=0.0, wav
         libc.free(ctypes.cast(ptr, c_void_p))
     libc.free(ctypes.cast(res, c_void_p))
     return Fr[0::2] + 1j * Fr[1::2], I
+
+
+# ---- spsim's own molecule.c / io.c (compiled into libspsim_ref.so)
+def _ref_mol_setup():
+    L = ref_lib()
+    L.get_Molecule_from_pdb.restype = POINTER(RefMolecule)
+    L.get_Molecule_from_pdb.argtypes = [ctypes.c_char_p]
+    L.write_pdb_from_mol.argtypes = [ctypes.c_char_p, POINTER(RefMolecule)]
+    L.origin_to_center_of_mass.argtypes = [POINTER(RefMolecule)]
+    L.write_3D_array_to_vtk.argtypes = [c_void_p, c_int, c_int, c_int, ctypes.c_char_p]
+    L.write_2D_array_to_vtk.argtypes = [c_void_p, c_int, c_int, ctypes.c_char_p]
+    return L
+
+
+def _mol_arrays(m):
+    n = m.contents.natoms
+    Z = np.ctypeslib.as_array(m.contents.atomic_number, shape=(max(n, 1),))[:n].copy()
+    pos = np.ctypeslib.as_array(m.contents.pos, shape=(max(3 * n, 1),))[:3 * n].copy().reshape(-1, 3)
+    return Z, pos
+
+
+def ref_read_pdb(path):
+    """spsim's get_Molecule_from_pdb (src/molecule.c:65-297): (Z int32 (N,), pos float32 (N,3))."""
+    L = _ref_mol_setup()
+    m = L.get_Molecule_from_pdb(path.encode())
+    Z, pos = _mol_arrays(m)
+    libc = ctypes.CDLL(None)
+    libc.free(ctypes.cast(m.contents.atomic_number, c_void_p))
+    libc.free(ctypes.cast(m.contents.pos, c_void_p))
+    libc.free(ctypes.cast(m, c_void_p))
+    return Z, pos
+
+
+def _ref_molecule(Z, pos):
+    Z = np.array(Z, np.int32)  # copies: the reference edits molecules in place
+    pos = np.array(pos, np.float32).reshape(-1)
+    return RefMolecule(len(Z), Z.ctypes.data_as(POINTER(c_int)), pos.ctypes.data_as(POINTER(c_float)), 0), Z, pos
+
+
+def ref_write_pdb(path, Z, pos):
+    """spsim's write_pdb_from_mol (src/molecule.c:359-379)."""
+    L = _ref_mol_setup()
+    m, Z, pos = _ref_molecule(Z, pos)
+    L.write_pdb_from_mol(path.encode(), ctypes.byref(m))
+
+
+def ref_center(Z, pos):
+    """spsim's origin_to_center_of_mass (src/molecule.c:440-464) on a copy."""
+    L = _ref_mol_setup()
+    m, Z, p = _ref_molecule(Z, pos)
+    L.origin_to_center_of_mass(ctypes.byref(m))
+    return p.reshape(-1, 3).copy()
+
+
+def ref_write_vtk(path, F, nx, ny, nz=None):
+    """spsim's write_3D_array_to_vtk / write_2D_array_to_vtk (src/io.c)."""
+    L = _ref_mol_setup()
+    F = np.ascontiguousarray(F, np.float32)
+    if nz is None:
+        L.write_2D_array_to_vtk(_p(F), nx, ny, path.encode())
+    else:
+        L.write_3D_array_to_vtk(_p(F), nx, ny, nz, path.encode())

@@ -7,8 +7,9 @@ statically and every symbol except the functions declared in include/*.h is
 hidden by a linker version script, so the library neither exports nor binds
 to another CUDA runtime loaded in the same process (PyTorch's, for example).
 
-Also builds spsim_b200/_lib/pipe_probe, the pipe-throughput probe bench.py
-runs for the measured FMA / MUFU peaks.
+Also builds spsim_b200/_lib/spsim, the spsim command-line program on the
+library (host/spsim_main.c), and spsim_b200/_lib/pipe_probe, the
+pipe-throughput probe bench.py runs for the measured FMA / MUFU peaks.
 
 Usage: python -m spsim_b200.build [--force] [--verbose]
 """
@@ -30,10 +31,11 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
-CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-result", "-I" + os.path.join(CUDA_HOME, "include")]
+CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-result", "-ffp-contract=off",
+            "-I" + os.path.join(CUDA_HOME, "include")]
 
 CU_SOURCES = ["sf_kernels.cu", "chain_kernels.cu", "adjoint_kernels.cu", "capi.cu", "noalloc.cu"]
-C_SOURCES = ["host/config.c", "host/legacy.c"]
+C_SOURCES = ["host/config.c", "host/legacy.c", "host/molecule.c"]
 
 
 def lib_path():
@@ -107,6 +109,10 @@ def build(force=False, verbose=False):
              ["-Xlinker", "--version-script=" + vmap, "-Xlinker", "-Bsymbolic", "-lrt", "-ldl", "-lpthread"],
              verbose)
         shutil.move(tmp, out)
+    cli = os.path.join(LIBDIR, "spsim")
+    csrc = os.path.join(CSRC, "host", "spsim_main.c")
+    if force or _newer(cli, [csrc, out]):
+        _run(["gcc"] + CC_FLAGS + ["-o", cli, csrc, "-L" + LIBDIR, "-l:" + LIBNAME, "-Wl,-rpath,$ORIGIN"], verbose)
     probe = os.path.join(LIBDIR, "pipe_probe")
     psrc = os.path.join(CSRC, "tools", "pipe_probe.cu")
     if force or _newer(probe, [psrc]):

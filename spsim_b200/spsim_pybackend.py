@@ -114,6 +114,13 @@ _PROTOS = {
     "alloc_mol": (P(Molecule), []),
     "add_atom_to_mol": (None, [P(Molecule), c_int, c_float, c_float, c_float]),
     "free_mol": (None, [P(Molecule)]),
+    "get_Molecule_from_pdb": (P(Molecule), [c_char_p]),
+    "get_Molecule_from_formula": (P(Molecule), [P(Chem_Formula), P(Options)]),
+    "write_pdb_from_mol": (None, [c_char_p, P(Molecule)]),
+    "origin_to_center_of_mass": (None, [P(Molecule)]),
+    "get_molecule": (P(Molecule), [P(Options)]),
+    "write_2D_array_to_vtk": (None, [P(c_float), c_int, c_int, c_char_p]),
+    "write_3D_array_to_vtk": (None, [P(c_float), c_int, c_int, c_int, c_char_p]),
     "get_my_loop_start_and_end": (None, [c_int, P(c_int), P(c_int)]),
     "syncronize_patterns": (None, [P(Diffraction_Pattern)]),
     "sum_patterns": (None, [P(Diffraction_Pattern)]),
@@ -300,3 +307,32 @@ def as_array(ptr, n, dtype=np.float32):
         raw = np.ctypeslib.as_array(ctypes.cast(ptr, POINTER(c_float)), shape=(2 * n,)).copy()
         return raw[0::2] + 1j * raw[1::2]
     return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
+
+
+# ---- molecule files and VTK output (src/molecule.c, src/io.c)
+def get_Molecule_from_pdb(filename):
+    return _fn("get_Molecule_from_pdb")(_path(filename))
+
+
+def get_Molecule_from_formula(form, opts):
+    return _fn("get_Molecule_from_formula")(form, opts)
+
+
+def write_pdb_from_mol(filename, mol):
+    _fn("write_pdb_from_mol")(_path(filename), mol)
+
+
+def origin_to_center_of_mass(mol):
+    _fn("origin_to_center_of_mass")(mol)
+
+
+def get_molecule(opts):
+    return _fn("get_molecule")(opts)
+
+
+def write_2D_array_to_vtk(F, nx, ny, filename):
+    _fn("write_2D_array_to_vtk")(_floats(F), int(nx), int(ny), _path(filename))
+
+
+def write_3D_array_to_vtk(F, nx, ny, nz, filename):
+    _fn("write_3D_array_to_vtk")(_floats(F), int(nx), int(ny), int(nz), _path(filename))
