@@ -73,6 +73,14 @@ void write_pdb_from_mol(char *filename, Molecule *mol);                   /* src
 void origin_to_center_of_mass(Molecule *mol);                             /* src/molecule.c:440 */
 Molecule *get_molecule(Options *opts);                                    /* src/spsim.c:83 */
 
+/* ---- crystal lattice: include/crystal.h:30-33 ----
+ * cell matrix rows A, B, C from crystal_cell (lengths in metres, angles in
+ * degrees); the lattice sum over crystal_size cells runs on the GPU in FP64 */
+void crystal_axis_to_cartesian(Options *opts, CrystalAxis axis, float *x, float *y, float *z); /* src/crystal.c:4 */
+void crystal_cell_matrix(Options *opts, float *matrix);                  /* src/crystal.c:23 */
+void calculate_pattern_from_crystal(float *I, Complex *F, float *HKL_list, int HKL_list_size,
+                                    Options *opts);                      /* src/crystal.c:39 */
+
 /* ---- VTK output: include/io.h ---- */
 void write_2D_array_to_vtk(float *F, int nx, int ny, char *filename);     /* src/io.c:29 */
 void write_3D_array_to_vtk(float *F, int nx, int ny, int nz, char *filename); /* src/io.c:60 */

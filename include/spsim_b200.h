@@ -255,6 +255,23 @@ int spsim_b200_hkl_for_detector(int nx, int ny, float width, float height, float
                                 float center_x, float center_y, float wavelength, int spherical,
                                 float *hkl_dev, void *stream);
 
+/* The reciprocal-space grid of a 3-D (volume) detector, spsim's
+ * get_HKL_list_for_3d_detector (src/diffraction.c:325-369): pixel centres
+ * ((i - (n-1)/2)/n) * extent - centre along x, y, z, times
+ * 1 / (distance * wavelength), FP64, stored as float (z outer, x inner). */
+int spsim_b200_hkl_for_3d_detector(int nx, int ny, int nz, float width, float height, float depth,
+                                   float distance, float center_x, float center_y, float center_z,
+                                   float wavelength, float *hkl_dev, void *stream);
+
+/* Crystal lattice sum, spsim's calculate_pattern_from_crystal
+ * (src/crystal.c:39-71), in place on device data: F <- F * sum over
+ * na x nb x nc cells of exp(-2 pi i q.(a A + b B + c C)), I = |F|^2 (I_dev may
+ * be NULL).  cell: the 3x3 cell matrix, rows A, B, C in metres (as
+ * crystal_cell_matrix returns it); hkl_dev: float q per pixel.  The lattice
+ * factor is the product of three one-dimensional sums, each in FP64. */
+int spsim_b200_crystal_lattice_sum(int64_t npix, const float *hkl_dev, const float *cell, int na, int nb, int nc,
+                                   float *F_dev, float *I_dev, void *stream);
+
 /* ---- completion, errors and timing -------------------------------------
  * Device-side failures of asynchronous calls (a bounded wait that gave up,
  * refined positions outside the molecule's bounds) are recorded in device

@@ -36,6 +36,9 @@ typedef struct {
 } SpRotation;
 #endif
 
+/* include/crystal.h:30 */
+typedef enum { CrystalA, CrystalB, CrystalC } CrystalAxis;
+
 /* include/config.h:44-48 */
 typedef struct {
   int n_elements;

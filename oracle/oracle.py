@@ -413,3 +413,64 @@ def ref_write_vtk(path, F, nx, ny, nz=None):
         L.write_2D_array_to_vtk(_p(F), nx, ny, path.encode())
     else:
         L.write_3D_array_to_vtk(_p(F), nx, ny, nz, path.encode())
+
+
+def hkl_3d_detector(nx, ny, nz, width, height, depth, distance, wavelength, center=(0.0, 0.0, 0.0)):
+    """The oracle's 3-D detector grid (float32 (nx*ny*nz, 3))."""
+    L = oracle_lib()
+    out = np.zeros(3 * nx * ny * nz, np.float32)
+    f = c_float
+    L.oracle_hkl_3d_detector.argtypes = [c_int, c_int, c_int, f, f, f, f, f, f, f, f, c_void_p]
+    L.oracle_hkl_3d_detector(nx, ny, nz, width, height, depth, distance, center[0], center[1], center[2], wavelength,
+                             _p(out))
+    return out.reshape(-1, 3)
+
+
+def ref_hkl_3d_detector(nx, ny, nz, width, height, depth, distance, wavelength, center=(0.0, 0.0, 0.0)):
+    """spsim's get_HKL_list_for_3d_detector (src/diffraction.c:325-369)."""
+    L = _ref_setup()
+    det = RefCCD(nx=nx, ny=ny, nz=nz, width=width, height=height, depth=depth, distance=distance,
+                 center_x=center[0], center_y=center[1], center_z=center[2])
+    exp = RefExperiment(wavelength=wavelength)
+    n = c_int(0)
+    L.get_HKL_list_for_3d_detector.restype = POINTER(c_float)
+    L.get_HKL_list_for_3d_detector.argtypes = [POINTER(RefCCD), POINTER(RefExperiment), POINTER(c_int)]
+    p = L.get_HKL_list_for_3d_detector(ctypes.byref(det), ctypes.byref(exp), ctypes.byref(n))
+    out = np.ctypeslib.as_array(p, shape=(n.value * 3,)).copy().reshape(-1, 3)
+    ctypes.CDLL(None).free(ctypes.cast(p, c_void_p))
+    return out
+
+
+def crystal(F, q, cell, size):
+    """The oracle's FP64 crystal lattice sum: (F complex128, I float64)."""
+    L = oracle_lib()
+    q = np.ascontiguousarray(q, np.float64).reshape(-1, 3)
+    Fr = np.ascontiguousarray(np.real(F), np.float64).copy()
+    Fi = np.ascontiguousarray(np.imag(F), np.float64).copy()
+    cell = np.ascontiguousarray(cell, np.float64).reshape(9)
+    I = np.zeros(q.shape[0])
+    L.oracle_crystal.argtypes = [ctypes.c_long, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]
+    L.oracle_crystal(q.shape[0], _p(q), _p(cell), int(size[0]), int(size[1]), int(size[2]), _p(Fr), _p(Fi), _p(I))
+    return Fr + 1j * Fi, I
+
+
+def ref_crystal(F, q, opts):
+    """spsim's calculate_pattern_from_crystal (src/crystal.c:39-71), float, on copies."""
+    L = ref_lib()
+    n = q.shape[0]
+    Fc = np.zeros(2 * n, np.float32)
+    Fc[0::2], Fc[1::2] = np.real(F), np.imag(F)
+    I = np.zeros(n, np.float32)
+    qf = np.ascontiguousarray(q, np.float32).reshape(-1)
+    L.calculate_pattern_from_crystal.argtypes = [c_void_p, c_void_p, c_void_p, c_int, POINTER(RefOptions)]
+    L.calculate_pattern_from_crystal(_p(I), _p(Fc), _p(qf), n, ctypes.byref(opts))
+    return Fc[0::2] + 1j * Fc[1::2], I
+
+
+def ref_cell_matrix(opts):
+    """spsim's crystal_cell_matrix (src/crystal.c:23-37)."""
+    L = ref_lib()
+    m = np.zeros(9, np.float32)
+    L.crystal_cell_matrix.argtypes = [POINTER(RefOptions), c_void_p]
+    L.crystal_cell_matrix(ctypes.byref(opts), _p(m))
+    return m

@@ -53,6 +53,8 @@ typedef struct {
 #define sp_max(a, b) (((a) > (b)) ? (a) : (b))
 
 static inline real sp_cabs(Complex a) { return (real)sqrt(a.re * a.re + a.im * a.im); }
+static inline real sp_cabs2(Complex a) { return a.re * a.re + a.im * a.im; }
+static inline real sp_carg(Complex a) { return (real)atan2(a.im, a.re); }
 static inline Complex sp_cinit(real re, real im) { Complex c; c.re = re; c.im = im; return c; }
 static inline Complex sp_cscale(Complex a, real s) { Complex c; c.re = a.re * s; c.im = a.im * s; return c; }
 

@@ -97,6 +97,48 @@ void oracle_hkl_detector(int nx, int ny, float width, float height, float distan
   }
 }
 
+/* src/crystal.c:39-71 in FP64: F <- F * sum over the na x nb x nc cells r =
+ * aA + bB + cC of exp(-2 pi i q.r) (cell rows A, B, C), I = |F|^2. */
+void oracle_crystal(long npix, const double *q, const double *cell, int na, int nb, int nc, double *F_re,
+                    double *F_im, double *I) {
+  for (long p = 0; p < npix; p++) {
+    double sr = 0.0, si = 0.0;
+    for (int a = 0; a < na; a++)
+      for (int b = 0; b < nb; b++)
+        for (int c = 0; c < nc; c++) {
+          const double r[3] = {cell[0] * a + cell[3] * b + cell[6] * c, cell[1] * a + cell[4] * b + cell[7] * c,
+                               cell[2] * a + cell[5] * b + cell[8] * c};
+          double t = q[3 * p] * r[0] + q[3 * p + 1] * r[1] + q[3 * p + 2] * r[2];
+          t -= rint(t);
+          sr += cos(2.0 * M_PI * t);
+          si -= sin(2.0 * M_PI * t);
+        }
+    const double re = F_re[p] * sr - F_im[p] * si, im = F_re[p] * si + F_im[p] * sr;
+    F_re[p] = re;
+    F_im[p] = im;
+    if (I) I[p] = re * re + im * im;
+  }
+}
+
+/* src/diffraction.c:325-369: the reciprocal-space grid of a 3-D detector,
+ * FP64, stored as float like the reference (z outer, x inner). */
+void oracle_hkl_3d_detector(int nx, int ny, int nz, float width, float height, float depth, float distance,
+                            float center_x, float center_y, float center_z, float wavelength, float *out) {
+  const float dl = distance * wavelength;
+  const double r2r = 1.0 / dl;
+  long idx = 0;
+  for (int z = 0; z < nz; z++)
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++) {
+        const double px = ((x - (nx - 1.0) / 2.0) / nx) * width - center_x;
+        const double py = ((y - (ny - 1.0) / 2.0) / ny) * height - center_y;
+        const double pz = ((z - (nz - 1.0) / 2.0) / nz) * depth - center_z;
+        out[idx++] = (float)(px * r2r);
+        out[idx++] = (float)(py * r2r);
+        out[idx++] = (float)(pz * r2r);
+      }
+}
+
 /*
  * src/diffraction.c:770-853 (compute_pattern_on_list), FP64:
  *   F(q) = sum_j f_Zj(|q|, B_j) * occ_j * sqrt(illum_j) * exp(-2 pi i q.r_j),  I = |F|^2

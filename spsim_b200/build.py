@@ -35,7 +35,7 @@ CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-result", "-ffp-c
             "-I" + os.path.join(CUDA_HOME, "include")]
 
 CU_SOURCES = ["sf_kernels.cu", "chain_kernels.cu", "adjoint_kernels.cu", "capi.cu", "noalloc.cu"]
-C_SOURCES = ["host/config.c", "host/legacy.c", "host/molecule.c"]
+C_SOURCES = ["host/config.c", "host/legacy.c", "host/molecule.c", "host/crystal.c"]
 
 
 def lib_path():

@@ -1346,6 +1346,27 @@ extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b20
 // ---------------------------------------------------------------------------
 // geometry and detector chain
 
+extern "C" int spsim_b200_crystal_lattice_sum(int64_t npix, const float *hkl_dev, const float *cell, int na, int nb,
+                                              int nc, float *F_dev, float *I_dev, void *stream) {
+  if (npix < 0 || (npix > 0 && (!hkl_dev || !F_dev)) || !cell)
+    return fail(SPSIM_ERR_INVALID_ARG, "crystal lattice sum: bad arguments");
+  if (na < 0 || nb < 0 || nc < 0) return fail(SPSIM_ERR_INVALID_ARG, "crystal size %d x %d x %d", na, nb, nc);
+  double c[9];
+  for (int k = 0; k < 9; ++k) c[k] = cell[k];
+  CUDA_TRY(launch_crystal(npix, hkl_dev, c, na, nb, nc, F_dev, I_dev, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_hkl_for_3d_detector(int nx, int ny, int nz, float width, float height, float depth,
+                                              float distance, float center_x, float center_y, float center_z,
+                                              float wavelength, float *hkl_dev, void *stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return fail(SPSIM_ERR_INVALID_ARG, "detector has %d x %d x %d pixels", nx, ny, nz);
+  if (!hkl_dev) return fail(SPSIM_ERR_INVALID_ARG, "hkl_dev is NULL");
+  CUDA_TRY(launch_volume(nx, ny, nz, width, height, depth, distance, center_x, center_y, center_z, wavelength, hkl_dev,
+                         (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
 extern "C" int spsim_b200_hkl_for_detector(int nx, int ny, float width, float height, float distance,
                                            float center_x, float center_y, float wavelength, int spherical,
                                            float *hkl_dev, void *stream) {

@@ -116,13 +116,18 @@ float *get_HKL_list_for_detector(CCD *det, Experiment *exp, int *HKL_list_size) 
   return out;
 }
 
-/* src/diffraction.c:325-369: the 3-D (volume) detector is not implemented. */
+/* src/diffraction.c:325-369, on the GPU in FP64, stored as float */
 float *get_HKL_list_for_3d_detector(CCD *det, Experiment *exp, int *HKL_list_size) {
-  (void)det;
-  (void)exp;
-  (void)HKL_list_size;
-  fprintf(stderr, "spsim_b200: 3-D detectors (nz > 1) are not supported\n");
-  abort();
+  const long long n = (long long)det->nx * det->ny * det->nz;
+  float *out = (float *)malloc(sizeof(float) * 3 * (n > 0 ? n : 1));
+  float *d = (float *)dev_alloc(SLOT_HKL, sizeof(float) * 3 * n);
+  int st = spsim_b200_hkl_for_3d_detector(det->nx, det->ny, det->nz, det->width, det->height, det->depth,
+                                          det->distance, det->center_x, det->center_y, det->center_z, exp->wavelength,
+                                          d, NULL);
+  if (st) die("get_HKL_list_for_3d_detector", st);
+  d2h(out, d, sizeof(float) * 3 * n);
+  *HKL_list_size = (int)n;
+  return out;
 }
 
 /* src/spsim.c:98-108 */

@@ -805,6 +805,56 @@ __global__ void ewald_kernel(int nx, int ny, double width, double height, double
   }
 }
 
+// Reciprocal-space grid of a 3-D (volume) detector (src/diffraction.c:325-369):
+// pixel centres scaled by 1 / (distance * wavelength), FP64 without
+// contraction as the reference computes them, stored as float.
+__global__ void volume_kernel(int nx, int ny, int nz, double width, double height, double depth, double cx, double cy,
+                              double cz, double r2r, float *__restrict__ out32) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nx * ny * nz) return;
+  const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
+  const double px = __dsub_rn(__dmul_rn(__ddiv_rn(__dsub_rn((double)x, (nx - 1.0) / 2.0), (double)nx), width), cx);
+  const double py = __dsub_rn(__dmul_rn(__ddiv_rn(__dsub_rn((double)y, (ny - 1.0) / 2.0), (double)ny), height), cy);
+  const double pz = __dsub_rn(__dmul_rn(__ddiv_rn(__dsub_rn((double)z, (nz - 1.0) / 2.0), (double)nz), depth), cz);
+  out32[3 * i] = (float)__dmul_rn(px, r2r);
+  out32[3 * i + 1] = (float)__dmul_rn(py, r2r);
+  out32[3 * i + 2] = (float)__dmul_rn(pz, r2r);
+}
+
+// Crystal lattice sum (src/crystal.c:39-71): F <- F * sum_{a,b,c} e^{-2 pi i q.(a A + b B + c C)}
+// over na x nb x nc cells, I = |F|^2.  The lattice factor separates into three
+// one-dimensional sums, each taken term by term in FP64 (no closed form, which
+// loses accuracy next to Bragg peaks).
+__device__ __forceinline__ double2 lattice_line(double u, int n) {
+  double re = 0.0, im = 0.0;
+  for (int a = 0; a < n; ++a) {
+    double t = u * a;
+    t -= rint(t);
+    double s, c;
+    sincospi(2.0 * t, &s, &c);
+    re += c;
+    im -= s;
+  }
+  return make_double2(re, im);
+}
+
+__global__ void crystal_kernel(long long npix, const float *__restrict__ hkl, double ax, double ay, double az,
+                               double bx, double by, double bz, double cx, double cy, double cz, int na, int nb,
+                               int nc, float2 *__restrict__ F, float *__restrict__ I) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npix) return;
+  const double qx = hkl[3 * p], qy = hkl[3 * p + 1], qz = hkl[3 * p + 2];
+  const double2 sa = lattice_line(qx * ax + qy * ay + qz * az, na);
+  const double2 sb = lattice_line(qx * bx + qy * by + qz * bz, nb);
+  const double2 sc = lattice_line(qx * cx + qy * cy + qz * cz, nc);
+  const double2 ab = make_double2(sa.x * sb.x - sa.y * sb.y, sa.x * sb.y + sa.y * sb.x);
+  const double2 s = make_double2(ab.x * sc.x - ab.y * sc.y, ab.x * sc.y + ab.y * sc.x);
+  const float2 f = F[p];
+  const double re = f.x * s.x - f.y * s.y, im = f.x * s.y + f.y * s.x;
+  F[p] = make_float2((float)re, (float)im);
+  if (I) I[p] = (float)(re * re + im * im);
+}
+
 // ---------------------------------------------------------------------------
 // refinement: rewrite atom records from device positions (caller order)
 
@@ -981,6 +1031,25 @@ cudaError_t launch_ewald(int nx, int ny, double width, double height, double dis
   const double fpy = 2 * sin(atan(py_size / distance) / 2) / wavelength;
   ewald_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nx, ny, width, height, distance, cx, cy, ewald, spherical,
                                                            fpx, fpy, px_size, py_size, out32, out64);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crystal(long long npix, const float *hkl, const double cell[9], int na, int nb, int nc, float *F,
+                           float *I, cudaStream_t st) {
+  if (npix <= 0) return cudaSuccess;
+  crystal_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(npix, hkl, cell[0], cell[1], cell[2], cell[3], cell[4],
+                                                                cell[5], cell[6], cell[7], cell[8], na, nb, nc,
+                                                                (float2 *)F, I);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_volume(int nx, int ny, int nz, float width, float height, float depth, float distance, float cx,
+                          float cy, float cz, float wavelength, float *out32, cudaStream_t st) {
+  const long long n = (long long)nx * ny * nz;
+  if (n <= 0) return cudaSuccess;
+  // 1.0 / (distance * wavelength): a float product, then a double quotient (src/diffraction.c:334)
+  const double r2r = 1.0 / (double)(distance * wavelength);
+  volume_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nx, ny, nz, width, height, depth, cx, cy, cz, r2r, out32);
   return cudaGetLastError();
 }
 

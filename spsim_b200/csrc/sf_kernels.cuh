@@ -17,6 +17,10 @@ bool sf_f32_variant_exists(int mode, int nt, int p, int packed);
 cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cudaStream_t st);
 cudaError_t launch_spectrum_combine(const SfPattern *pats, int pattern0, int S, const double *weight, float *F,
                                     float *I, long long npix, cudaStream_t st);
+cudaError_t launch_volume(int nx, int ny, int nz, float width, float height, float depth, float distance, float cx,
+                          float cy, float cz, float wavelength, float *out32, cudaStream_t st);
+cudaError_t launch_crystal(long long npix, const float *hkl, const double cell[9], int na, int nb, int nc, float *F,
+                           float *I, cudaStream_t st);
 cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st);
 cudaError_t launch_ewald(int nx, int ny, double width, double height, double distance, double cx, double cy,
                          double wavelength, int spherical, float *out32, double *out64, cudaStream_t st);

@@ -115,6 +115,9 @@ _PROTOS = {
     "add_atom_to_mol": (None, [P(Molecule), c_int, c_float, c_float, c_float]),
     "free_mol": (None, [P(Molecule)]),
     "get_Molecule_from_pdb": (P(Molecule), [c_char_p]),
+    "crystal_axis_to_cartesian": (None, [P(Options), c_int, P(c_float), P(c_float), P(c_float)]),
+    "crystal_cell_matrix": (None, [P(Options), P(c_float)]),
+    "calculate_pattern_from_crystal": (None, [P(c_float), P(Complex), P(c_float), c_int, P(Options)]),
     "get_Molecule_from_formula": (P(Molecule), [P(Chem_Formula), P(Options)]),
     "write_pdb_from_mol": (None, [c_char_p, P(Molecule)]),
     "origin_to_center_of_mass": (None, [P(Molecule)]),
@@ -336,3 +339,19 @@ def write_2D_array_to_vtk(F, nx, ny, filename):
 
 def write_3D_array_to_vtk(F, nx, ny, nz, filename):
     _fn("write_3D_array_to_vtk")(_floats(F), int(nx), int(ny), int(nz), _path(filename))
+
+
+# ---- crystal lattice (src/crystal.c)
+CrystalA, CrystalB, CrystalC = 0, 1, 2
+
+
+def crystal_axis_to_cartesian(opts, axis, x, y, z):
+    _fn("crystal_axis_to_cartesian")(opts, int(axis), x, y, z)
+
+
+def crystal_cell_matrix(opts, matrix):
+    _fn("crystal_cell_matrix")(opts, _floats(matrix))
+
+
+def calculate_pattern_from_crystal(I, F, HKL_list, HKL_list_size, opts):
+    _gpu_call("calculate_pattern_from_crystal", I, F, _floats(HKL_list), int(HKL_list_size), opts)
