@@ -211,6 +211,7 @@ def measured_pipe_peaks():
 # term, counted from the kernel source): FP32 = FP32 FMA/MUL/ADD, DFMA = FP64
 # FMA/ADD, IMAD = integer multiply-add, XU = MUFU / conversions.
 MIX = {
+    "sf_dpair_kernel": {"fp32": 15, "dfma": 3, "imad": 0.5, "xu": 0.875},  # half the terms FP64-anchored, half by FP32 step
     "sf_dphase_kernel": {"fp32": 12, "dfma": 6, "imad": 1, "xu": 1},   # FP64 phase + reduction, DHALF poly
     "sf_f32x2_kernel/f32": {"fp32": 27, "alu": 2},                   # compensated phase, HALF poly
     "sf_f32x2_kernel/f32_fast": {"fp32": 16, "xu": 2},               # compensated phase, MUFU sin/cos
@@ -526,7 +527,7 @@ def _adjoint_ratio(prec):
     return statistics.median(tb) / statistics.median(ta)
 
 
-PROFILE_VARIANTS = {"f32": (128, 8, 2), "f32_fast": (128, 6, 1)}  # the untuned defaults on the 1024^2 workload
+PROFILE_VARIANTS = {"f32": (128, 8, 3), "f32_fast": (128, 6, 1)}  # the untuned defaults on the 1024^2 workload
 
 
 def profile_case(precisions):
@@ -568,7 +569,8 @@ def sweep():
     I = torch.empty(qs.npix, device="cuda")
     for prec in ("f32", "f32_fast"):
         for v in [(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1),
-                  (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2)]:
+                  (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2), (128, 4, 3), (128, 8, 3),
+                  (256, 4, 3)]:
             core.set_variant(*v)
             for _ in range(2):
                 core.forward(mol, qs, precision=prec, F=F, I=I)

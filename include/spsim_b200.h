@@ -308,8 +308,12 @@ void spsim_b200_set_formula_seed(unsigned long long seed);
  *   0  compensated FP32 phase (hi/lo split), one pixel per lane
  *   1  compensated FP32 phase, pixel pairs in f32x2 instructions
  *   2  FP64 phase and half-cycle reduction, FP32 sin/cos and sums on pixel
- *      pairs (f32x2); the default, and free of the compensated forms' phase
- *      range limit (SPSIM_ERR_RANGE)
+ *      pairs (f32x2); free of the compensated forms' phase range limit
+ *      (SPSIM_ERR_RANGE)
+ *   3  form 2 on the first pixel of each neighbour pair (pixels 2m, 2m+1),
+ *      the second pixel's phase as the first's plus (q_b - q_a).r in FP32;
+ *      the default, used where |q_b - q_a| |r|max <= 1/8 cycle for every
+ *      pair of the q set (detector rows of even width), else form 2
  * threads < 0 restores automatic choice; autotune times every compiled
  * variant on the given workload and keeps the fastest for workloads of that
  * size class. */

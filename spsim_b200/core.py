@@ -337,8 +337,9 @@ def last_forward_stats():
 
 
 FORMS = {0: "compensated FP32, one pixel per lane", 1: "compensated FP32, pixel pairs (f32x2)",
-         2: "FP64 phase, FP32 sin/cos on pixel pairs (f32x2)"}
-KERNELS = {-1: "sf_f64_kernel", 0: "sf_f32_kernel", 1: "sf_f32x2_kernel", 2: "sf_dphase_kernel"}
+         2: "FP64 phase, FP32 sin/cos on pixel pairs (f32x2)",
+         3: "FP64 phase on the first pixel of neighbour pairs, FP32 step to the second"}
+KERNELS = {-1: "sf_f64_kernel", 0: "sf_f32_kernel", 1: "sf_f32x2_kernel", 2: "sf_dphase_kernel", 3: "sf_dpair_kernel"}
 
 
 def last_variant():
@@ -353,7 +354,7 @@ def kernel_name():
     return KERNELS[last_variant()[2]]
 
 
-def set_variant(threads=-1, pixels_per_thread=-1, form=2):
+def set_variant(threads=-1, pixels_per_thread=-1, form=3):
     """Force an FP32 kernel variant: threads per CTA, pixels per thread and the
     kernel form (FORMS); threads < 0 returns to automatic choice."""
     check(lib().spsim_b200_set_variant(int(threads), int(pixels_per_thread), int(form)))

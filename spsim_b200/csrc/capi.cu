@@ -390,6 +390,7 @@ struct spsim_b200_qset {
   float *d_hkl = nullptr;
   double *d_q64 = nullptr;
   double qmax = 0;
+  double pair_step = 0;  // largest |q[2m+1] - q[2m]| (the pixel-pair form's admission test)
   ~spsim_b200_qset() {
     cudaFree(d_hkl);
     cudaFree(d_q64);
@@ -425,6 +426,7 @@ extern "C" int spsim_b200_qset_from_list(int64_t npix, const float *hkl, int mem
     qm2 = std::max(qm2, a * a + b * b + c * c);
   }
   q->qmax = std::sqrt(qm2);
+  CUDA_TRY(pair_step(q->d_hkl, nullptr, q->npix, &q->pair_step));
   *out = q.release();
   return SPSIM_OK;
 }
@@ -484,6 +486,7 @@ extern "C" int spsim_b200_qset_from_detector(int nx, int ny, float width, float 
                         q->d_q64, 0));
   CUDA_TRY(cudaDeviceSynchronize());
   q->qmax = detector_qmax(nx, ny, width, height, distance, center_x, center_y, wavelength, spherical);
+  CUDA_TRY(pair_step(nullptr, q->d_q64, q->npix, &q->pair_step));
   *out = q.release();
   return SPSIM_OK;
 }
@@ -581,7 +584,7 @@ struct OneShot {  // per-thread scratch plan of uncached calls; lives until the 
 };
 static thread_local OneShot g_oneshot;
 static const size_t kMaxPlans = 8;
-static int g_force_nt = -1, g_force_p = -1, g_force_pk = 2;
+static int g_force_nt = -1, g_force_p = -1, g_force_pk = 3;
 struct Variant {
   int nt, p, packed;
 };
@@ -614,7 +617,7 @@ static Variant choose_variant(double terms, long long total_npix, int precision)
   // compensated pixel-pair form for FP32_FAST (MUFU sin/cos); more pixels per
   // thread once there are enough pixel tiles to fill every SM several times
   if (precision == SPSIM_PREC_F32_FAST) return {128, total_npix >= (1LL << 20) ? 6 : total_npix >= 65536 ? 4 : 2, 1};
-  return {128, total_npix >= (1LL << 20) ? 8 : total_npix >= 65536 ? 4 : 2, 2};
+  return {128, total_npix >= (1LL << 20) ? 8 : 4, 3};  // falls back to form 2 where a q set is not admitted
 }
 
 static bool is_orthonormal(const double *R) {
@@ -669,6 +672,20 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
 
   Variant var = {128, 4, 1};
   if (precision != SPSIM_PREC_FP64) var = choose_variant(terms, total_npix, precision);
+  if (var.packed == 3) {
+    // neighbour-pair form: every pattern needs |q_b - q_a| |r|max <= 1/8 cycle
+    bool ok = true;
+    for (int i = 0; i < npat && ok; ++i) {
+      double scale = spec ? std::fabs(spec->qscale[i]) : 1.0;
+      if (rot && !is_orthonormal(rot + 9 * (size_t)i)) {
+        double fro = 0;
+        for (int k = 0; k < 9; ++k) fro += rot[9 * (size_t)i + k] * rot[9 * (size_t)i + k];
+        scale *= std::sqrt(fro);
+      }
+      ok = qsets[i]->pair_step * scale * mols[i]->rbound <= (1.0 / 8) * (1.0 - 1e-9);
+    }
+    if (!ok) var.packed = 2;
+  }
   const int nt = var.nt, ppt = var.p;
   pl.nt = var.nt;
   pl.ppt = var.p;
@@ -720,7 +737,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     pt.I = I_dev ? I_dev[i] : nullptr;
     pl.max_npix = std::max(pl.max_npix, q->npix);
     pl.npix_of[i] = q->npix;
-    if (precision != SPSIM_PREC_FP64 && pl.packed == 2 && m->n_kept > 0 && q->npix > 0) {
+    if (precision != SPSIM_PREC_FP64 && pl.packed >= 2 && m->n_kept > 0 && q->npix > 0) {
       // FP64 phase: the half-cycle rounding needs |2 q.r| < 2^51
       const double qr = qmax * m->rbound;
       if (qr >= std::ldexp(1.0, 48))
@@ -1142,6 +1159,7 @@ static int host_session_qset(int64_t npix, const float *hkl, spsim_b200_qset **o
     qm2 = std::max(qm2, a * a + b * b + c * c);
   }
   q->qmax = std::sqrt(qm2);
+  CUDA_TRY(pair_step(q->d_hkl, nullptr, q->npix, &q->pair_step));
   *out = q;
   return SPSIM_OK;
 }
@@ -1267,7 +1285,7 @@ extern "C" int spsim_b200_set_variant(int threads, int pixels_per_thread, int pa
   std::lock_guard<std::mutex> lk(g_mu);
   if (threads < 0) {
     g_force_nt = g_force_p = -1;
-    g_force_pk = 2;
+    g_force_pk = 3;
     return SPSIM_OK;
   }
   if (!sf_f32_variant_exists(0, threads, pixels_per_thread, packed) ||
@@ -1285,7 +1303,8 @@ extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b20
   if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
   if (precision == SPSIM_PREC_FP64) return fail(SPSIM_ERR_INVALID_ARG, "the FP64 kernel has a single variant");
   const int cand[][3] = {{128, 2, 0}, {128, 4, 0}, {256, 4, 0}, {128, 2, 1}, {128, 4, 1}, {256, 4, 1},
-                         {128, 6, 1}, {128, 2, 2}, {128, 4, 2}, {256, 4, 2}, {128, 6, 2}, {128, 8, 2}};
+                         {128, 6, 1}, {128, 2, 2}, {128, 4, 2}, {256, 4, 2}, {128, 6, 2}, {128, 8, 2},
+                         {128, 4, 3}, {128, 8, 3}, {256, 4, 3}};
   float *dI = nullptr;
   CUDA_TRY(cudaMalloc(&dI, std::max<long long>(qs->npix, 1) * sizeof(float)));
   float best = 1e30f;
@@ -1535,7 +1554,7 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   const float dq = (float)std::ldexp(1.0, eq - kq);
   // FP32 adjoints follow the forward's kernel form: the FP64-phase one unless
   // a compensated form is forced with spsim_b200_set_variant
-  const bool dphase = precision == SPSIM_PREC_F32 && !(g_force_nt > 0 && g_force_pk != 2);
+  const bool dphase = precision == SPSIM_PREC_F32 && !(g_force_nt > 0 && g_force_pk < 2);
   if (dphase && qmax * m->rbound >= std::ldexp(1.0, 48))
     return fail(SPSIM_ERR_RANGE, "adjoint: |q|max*|r|max exceeds 2^48 cycles");
   if (precision != SPSIM_PREC_FP64 && !dphase && m->n_kept > 0) {

@@ -14,6 +14,8 @@ Three domains are generated:
   HALF:  |y| <= 1/4 + 1/16  (half-cycle reduction plus the phase cross-term)
   QUAD:  |y| <= 1/8 + 1/16  (quarter-cycle reduction plus the cross-term)
   DHALF: |y| <= 1/4         (half-cycle reduction of an FP64 phase, no cross-term)
+  WIDE:  |y| <= 3/8         (the second pixel of a neighbour pair: DHALF plus a
+                             step of at most 1/8 cycle)
 Degrees are the smallest whose float32 evaluation stays near the float32
 rounding floor (a higher sine degree on HALF only adds rounding error).
 
@@ -124,6 +126,7 @@ def main():
     emit("HALF", 0.25 + 1.0 / 16, 4, 5, out)
     emit("QUAD", 0.125 + 1.0 / 16, 4, 4, out)
     emit("DHALF", 0.25, 4, 4, out)
+    emit("WIDE", 0.375, 5, 5, out)
     out += ["#endif", ""]
     print("\n".join(out))
 

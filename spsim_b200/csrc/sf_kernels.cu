@@ -11,6 +11,7 @@
 #include "sf_kernels.cuh"
 
 #include <cstdio>
+#include <cstring>
 
 namespace spsim {
 
@@ -687,6 +688,257 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
 }
 
 // ---------------------------------------------------------------------------
+// FP64-anchored pixel pairs.  Pixels 2m and 2m+1 of a q set are neighbours on
+// a detector row, so their phases differ by a small delta = (q_b - q_a).r.
+// The first pixel of each pair takes the FP64 phase and exact half-cycle
+// reduction of sf_dphase_kernel (|y_a| <= 1/4, sign (-1)^k); the second is
+// y_b = y_a + delta with delta in FP32 from the float step q_b - q_a and the
+// atom's float position, and the same sign.  The host admits a q set only
+// when |q_b - q_a| * |r|max <= 1/8 cycle for every pair, so |y_b| <= 3/8
+// stays inside the WIDE polynomial's domain.  Per term this replaces 6 FP64
+// operations on every other pixel by 4 FP32 ones (and one more polynomial
+// step).  Threads hold P pixels as
+// P/2 pairs; two pairs' anchors and two pairs' seconds share each packed
+// f32x2 polynomial.
+
+template <int MODE, int NT, int P, bool PERB>
+__global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restrict__ pats,
+                                                      const WorkItem *__restrict__ items, int n_items,
+                                                      int *__restrict__ queue, int *__restrict__ err, uint32_t m31) {
+  static_assert(P % 4 == 0, "pixels per thread must be a multiple of 4 (two pairs per packed instruction)");
+  constexpr int NPR = P / 2;   // pixel pairs per thread
+  constexpr int NPK = P / 4;   // packed pair-of-pairs
+  __shared__ __align__(128) float4 ring[RING_STAGES][2 * TILE_ATOMS];
+  __shared__ __align__(16) double2 sacc[P * NT];  // per-thread FP64 pixel sums of the current work item
+  __shared__ __align__(8) uint64_t full_bar[RING_STAGES];
+  __shared__ int s_item;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < RING_STAGES; ++s) mbar_init(&full_bar[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  uint32_t g_issue = 0, g_cons = 0;
+  const long long kWaitCycles = 4000000000LL;
+  const double M52 = 6755399441055744.0;  // 1.5 * 2^52
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const WorkItem wi = items[it];
+    const SfPattern &pt = pats[wi.pattern];
+    const long long npix = pt.npix;
+    const AtomD *__restrict__ atomsd = pt.atomsd;
+    const TileDesc *__restrict__ tiles = pt.tiles;
+
+    // pair m of this thread: pixels pa = pix0 + 2 m NT and pa + 1
+    const long long pix0 = (long long)wi.pixel_tile * (NT * P) + 2 * tid;
+    double qx[NPR], qy[NPR], qz[NPR];
+    float dqx[NPR], dqy[NPR], dqz[NPR], s2a[NPR], s2b[NPR];
+#pragma unroll
+    for (int m = 0; m < NPR; ++m) {
+      const long long pa = pix0 + 2LL * m * NT;
+      double a[3] = {0.0, 0.0, 0.0}, b[3] = {0.0, 0.0, 0.0};
+      if (pa < npix) load_q(pt, pa, a);
+      if (pa + 1 < npix) load_q(pt, pa + 1, b);
+      else b[0] = a[0], b[1] = a[1], b[2] = a[2];
+      qx[m] = a[0];
+      qy[m] = a[1];
+      qz[m] = a[2];
+      dqx[m] = (float)(b[0] - a[0]);
+      dqy[m] = (float)(b[1] - a[1]);
+      dqz[m] = (float)(b[2] - a[2]);
+      s2a[m] = (float)(-0.25 * (a[0] * a[0] + a[1] * a[1] + a[2] * a[2]) * 1e-20 * pt.s2scale * 1.4426950408889634);
+      s2b[m] = (float)(-0.25 * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * 1e-20 * pt.s2scale * 1.4426950408889634);
+    }
+    // float-float element sums: [pair-of-pairs][first / second pixel]
+    float2 shc[NPK][2], slc[NPK][2], shs[NPK][2], sls[NPK][2];
+#pragma unroll
+    for (int j = 0; j < NPK; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) shc[j][h] = slc[j][h] = shs[j][h] = sls[j][h] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < P; ++i) sacc[i * NT + tid] = make_double2(0.0, 0.0);
+
+    const int k0 = wi.k0, k1 = wi.k1;
+    if (tid == 0) {
+      for (int k = k0; k < k1 && k < k0 + RING_STAGES; ++k) {
+        const TileDesc td = tiles[k];
+        const uint32_t st = g_issue % RING_STAGES;
+        const uint32_t bytes = (uint32_t)td.count * (uint32_t)sizeof(AtomD);
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atomsd + td.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+    }
+
+    for (int k = k0; k < k1; ++k) {
+      const uint32_t st = g_cons % RING_STAGES;
+      const uint32_t par = (g_cons / RING_STAGES) & 1u;
+      const bool ok = mbar_wait_bounded(&full_bar[st], par, kWaitCycles);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicOr(err, 1);
+          for (uint32_t g = g_cons; g < g_issue; ++g)
+            mbar_wait_bounded(&full_bar[g % RING_STAGES], (g / RING_STAGES) & 1u, kWaitCycles);
+        }
+        return;
+      }
+      const TileDesc td = tiles[k];
+      const float4 *__restrict__ ta = ring[st];
+      for (int a = 0; a < td.count; a += ATOM_GROUP) {
+        float2 bc[NPK][2], bs[NPK][2];
+#pragma unroll
+        for (int j = 0; j < NPK; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) bc[j][h] = bs[j][h] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int g = 0; g < ATOM_GROUP; ++g) {
+          const float4 d0 = ta[2 * (a + g)], d1 = ta[2 * (a + g) + 1];
+          const double rx = __hiloint2double(__float_as_int(d0.y), __float_as_int(d0.x));
+          const double ry = __hiloint2double(__float_as_int(d0.w), __float_as_int(d0.z));
+          const double rz = __hiloint2double(__float_as_int(d1.y), __float_as_int(d1.x));
+          const float W = d1.z;
+          const float2 fx = f2(__double2float_rn(rx)), fy = f2(__double2float_rn(ry)), fz = f2(__double2float_rn(rz));
+#pragma unroll
+          for (int j = 0; j < NPK; ++j) {
+            float ya[2];
+            uint32_t kb[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int m = 2 * j + h;
+              double u = qx[m] * rx;
+              u = fma(qy[m], ry, u);
+              u = fma(qz[m], rz, u);
+              if (MODE == PREC_MODE_POLY) {
+                const double t = fma(u, 2.0, M52);
+                ya[h] = __double2float_rn(fma(t - M52, -0.5, u));
+                kb[h] = (uint32_t)__double2loint(t);
+              } else {
+                const double t = u + M52;
+                ya[h] = __double2float_rn(u - (t - M52));
+                kb[h] = 0;
+              }
+            }
+            const float2 Ya = make_float2(ya[0], ya[1]);
+            // second pixels: y_b = y_a + (q_b - q_a).r in FP32
+            float2 dl = mul2(make_float2(dqx[2 * j], dqx[2 * j + 1]), fx);
+            dl = fma2(make_float2(dqy[2 * j], dqy[2 * j + 1]), fy, dl);
+            dl = fma2(make_float2(dqz[2 * j], dqz[2 * j + 1]), fz, dl);
+            const float2 Yb = add2(Ya, dl);
+            float2 wa = f2(W), wb = f2(W);
+            if (PERB) {
+              wa = make_float2(W * exp2f(d1.w * s2a[2 * j]), W * exp2f(d1.w * s2a[2 * j + 1]));
+              wb = make_float2(W * exp2f(d1.w * s2b[2 * j]), W * exp2f(d1.w * s2b[2 * j + 1]));
+            }
+            if (MODE == PREC_MODE_POLY) {
+              float2 Sa, Ca;
+              sincos_dhalf_poly2(Ya, Sa, Ca);
+              const float2 zb = mul2(Yb, Yb);
+              float2 ps = fma2(zb, f2(SPSIM_WIDE_S5), f2(SPSIM_WIDE_S4));
+              ps = fma2(zb, ps, f2(SPSIM_WIDE_S3));
+              ps = fma2(zb, ps, f2(SPSIM_WIDE_S2));
+              ps = fma2(zb, ps, f2(SPSIM_WIDE_S1));
+              ps = fma2(zb, ps, f2(SPSIM_WIDE_S0));
+              float2 pc = fma2(zb, f2(SPSIM_WIDE_C5), f2(SPSIM_WIDE_C4));
+              pc = fma2(zb, pc, f2(SPSIM_WIDE_C3));
+              pc = fma2(zb, pc, f2(SPSIM_WIDE_C2));
+              pc = fma2(zb, pc, f2(SPSIM_WIDE_C1));
+              pc = fma2(zb, pc, f2(SPSIM_WIDE_C0));
+              const float2 Sb = mul2(Yb, ps);
+              const float2 wsa = make_float2(sign_by_parity(wa.x, kb[0], m31), sign_by_parity(wa.y, kb[1], m31));
+              const float2 wsb = PERB ? make_float2(sign_by_parity(wb.x, kb[0], m31), sign_by_parity(wb.y, kb[1], m31))
+                                      : wsa;
+              bc[j][0] = fma2(wsa, Ca, bc[j][0]);
+              bs[j][0] = fma2(wsa, Sa, bs[j][0]);
+              bc[j][1] = fma2(wsb, pc, bc[j][1]);
+              bs[j][1] = fma2(wsb, Sb, bs[j][1]);
+            } else {
+              const float2 xa = mul2(Ya, f2(6.28318530717958648f)), xb = mul2(Yb, f2(6.28318530717958648f));
+              float2 sa, ca, sb, cb;
+              __sincosf(xa.x, &sa.x, &ca.x);
+              __sincosf(xa.y, &sa.y, &ca.y);
+              __sincosf(xb.x, &sb.x, &cb.x);
+              __sincosf(xb.y, &sb.y, &cb.y);
+              bc[j][0] = fma2(wa, ca, bc[j][0]);
+              bs[j][0] = fma2(wa, sa, bs[j][0]);
+              bc[j][1] = fma2(wb, cb, bc[j][1]);
+              bs[j][1] = fma2(wb, sb, bs[j][1]);
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < NPK; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            float2 s1 = add2(shc[j][h], bc[j][h]);
+            slc[j][h] = add2(slc[j][h], add2(bc[j][h], make_float2(-(s1.x - shc[j][h].x), -(s1.y - shc[j][h].y))));
+            shc[j][h] = s1;
+            float2 s2 = add2(shs[j][h], bs[j][h]);
+            sls[j][h] = add2(sls[j][h], add2(bs[j][h], make_float2(-(s2.x - shs[j][h].x), -(s2.y - shs[j][h].y))));
+            shs[j][h] = s2;
+          }
+      }
+      if (td.last || k == k1 - 1) {
+        const double *__restrict__ ffe = pt.ff + (long long)td.elem * npix;
+#pragma unroll
+        for (int j = 0; j < NPK; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h)      // first / second pixel of the pairs
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {  // which pair of the packed two
+              const int m = 2 * j + e;
+              const long long p = pix0 + 2LL * m * NT + h;
+              if (p < npix) {
+                const double f = ffe[p];
+                const double re = e ? (double)shc[j][h].y + (double)slc[j][h].y : (double)shc[j][h].x + (double)slc[j][h].x;
+                const double sm = e ? (double)shs[j][h].y + (double)sls[j][h].y : (double)shs[j][h].x + (double)sls[j][h].x;
+                double2 v = sacc[(2 * m + h) * NT + tid];
+                v.x = fma(f, re, v.x);
+                v.y = fma(-f, sm, v.y);
+                sacc[(2 * m + h) * NT + tid] = v;
+              }
+            }
+#pragma unroll
+        for (int j = 0; j < NPK; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) shc[j][h] = slc[j][h] = shs[j][h] = sls[j][h] = make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+      if (tid == 0 && k + RING_STAGES < k1) {
+        const TileDesc tn = tiles[k + RING_STAGES];
+        const uint32_t bytes = (uint32_t)tn.count * (uint32_t)sizeof(AtomD);
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atomsd + tn.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+      ++g_cons;
+    }
+    const bool whole = k0 == 0 && k1 == pt.n_tiles;
+#pragma unroll
+    for (int m = 0; m < NPR; ++m)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long long p = pix0 + 2LL * m * NT + h;
+        if (p < npix) {
+          const double2 v = sacc[(2 * m + h) * NT + tid];
+          if (whole) {
+            pt.acc[p] = v;
+          } else {
+            atomicAdd(&pt.acc[p].x, v.x);
+            atomicAdd(&pt.acc[p].y, v.y);
+          }
+        }
+      }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // plain FP64 forward: one thread per pixel, atoms read as warp-uniform loads
 
 __global__ void __launch_bounds__(256) sf_f64_kernel(const SfPattern *__restrict__ pats, int pattern) {
@@ -913,11 +1165,14 @@ cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix,
 
 // Variants: (mode, threads, pixels per thread, form).  form 0 selects the
 // scalar compensated kernel (sf_f32_kernel), 1 the pixel-pair compensated one
-// (sf_f32x2_kernel), 2 the pixel-pair FP64-phase one (sf_dphase_kernel).
+// (sf_f32x2_kernel), 2 the pixel-pair FP64-phase one (sf_dphase_kernel), 3 the
+// FP64-anchored neighbour pairs (sf_dpair_kernel).
 template <int MODE, int NT, int P, bool PERB, int PK>
 static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, int n_items, int *queue, int *err,
                                 int grid, cudaStream_t st) {
-  if constexpr (PK == 2)
+  if constexpr (PK == 3)
+    sf_dpair_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
+  else if constexpr (PK == 2)
     sf_dphase_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
   else if constexpr (PK == 1)
     sf_f32x2_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err);
@@ -929,7 +1184,9 @@ static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, in
 template <int MODE, int NT, int P, bool PERB, int PK>
 static int occupancy_t() {
   int n = 0;
-  if constexpr (PK == 2)
+  if constexpr (PK == 3)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dpair_kernel<MODE, NT, P, PERB>, NT, 0);
+  else if constexpr (PK == 2)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dphase_kernel<MODE, NT, P, PERB>, NT, 0);
   else if constexpr (PK == 1)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_f32x2_kernel<MODE, NT, P, PERB>, NT, 0);
@@ -962,7 +1219,13 @@ static int occupancy_t() {
   X(1, 128, 4, 2)             \
   X(1, 256, 4, 2)             \
   X(1, 128, 6, 2)             \
-  X(1, 128, 8, 2)
+  X(1, 128, 8, 2)             \
+  X(0, 128, 4, 3)             \
+  X(0, 128, 8, 3)             \
+  X(0, 256, 4, 3)             \
+  X(1, 128, 4, 3)             \
+  X(1, 128, 8, 3)             \
+  X(1, 256, 4, 3)
 
 cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
                           const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st) {
@@ -1041,6 +1304,40 @@ cudaError_t launch_crystal(long long npix, const float *hkl, const double cell[9
                                                                 cell[5], cell[6], cell[7], cell[8], na, nb, nc,
                                                                 (float2 *)F, I);
   return cudaGetLastError();
+}
+
+// Largest |q[2m+1] - q[2m]| over the pixel pairs of a q set (float or FP64
+// list), as the bits of a non-negative double (which order like integers).
+__global__ void pair_step_kernel(const float *__restrict__ hkl, const double *__restrict__ q64, long long npix,
+                                 unsigned long long *__restrict__ out) {
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (2 * m + 1 >= npix) return;
+  double d[3];
+  for (int c = 0; c < 3; ++c)
+    d[c] = hkl ? (double)hkl[3 * (2 * m + 1) + c] - (double)hkl[3 * (2 * m) + c]
+               : q64[3 * (2 * m + 1) + c] - q64[3 * (2 * m) + c];
+  const double n = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  atomicMax(out, (unsigned long long)__double_as_longlong(n));
+}
+
+cudaError_t pair_step(const float *hkl, const double *q64, long long npix, double *step) {
+  *step = 0.0;
+  if (npix < 2) return cudaSuccess;
+  unsigned long long *d = nullptr, h = 0;
+  cudaError_t e = cudaMalloc(&d, sizeof(*d));
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemset(d, 0, sizeof(*d))) == cudaSuccess) {
+    const long long pairs = npix / 2;
+    pair_step_kernel<<<(unsigned)((pairs + 255) / 256), 256>>>(hkl, q64, npix, d);
+    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (e == cudaSuccess) {
+    double v;
+    memcpy(&v, &h, sizeof(v));
+    *step = v;
+  }
+  return e;
 }
 
 cudaError_t launch_volume(int nx, int ny, int nz, float width, float height, float depth, float distance, float cx,

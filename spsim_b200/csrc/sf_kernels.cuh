@@ -21,6 +21,8 @@ cudaError_t launch_volume(int nx, int ny, int nz, float width, float height, flo
                           float cy, float cz, float wavelength, float *out32, cudaStream_t st);
 cudaError_t launch_crystal(long long npix, const float *hkl, const double cell[9], int na, int nb, int nc, float *F,
                            float *I, cudaStream_t st);
+// Largest |q[2m+1] - q[2m]| of a q set's pixel pairs (synchronous, small).
+cudaError_t pair_step(const float *hkl, const double *q64, long long npix, double *step);
 cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st);
 cudaError_t launch_ewald(int nx, int ny, double width, double height, double distance, double cx, double cy,
                          double wavelength, int spherical, float *out32, double *out64, cudaStream_t st);

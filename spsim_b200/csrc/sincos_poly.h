@@ -48,5 +48,22 @@
 #define SPSIM_DHALF_C2 6.493521881e+01f
 #define SPSIM_DHALF_C3 -8.525400543e+01f
 #define SPSIM_DHALF_C4 5.634064865e+01f
+/* WIDE: |y| <= 0.375000 cycles; float32 evaluation error vs float64:
+ *   sin max 2.583e-07 rms 4.398e-08, cos max 1.903e-07 rms 3.701e-08 */
+#define SPSIM_WIDE_YMAX 3.750000000e-01f
+#define SPSIM_WIDE_SIN_DEG 6
+#define SPSIM_WIDE_COS_DEG 6
+#define SPSIM_WIDE_S0 6.283185482e+00f
+#define SPSIM_WIDE_S1 -4.134171677e+01f
+#define SPSIM_WIDE_S2 8.160549164e+01f
+#define SPSIM_WIDE_S3 -7.670075226e+01f
+#define SPSIM_WIDE_S4 4.190143585e+01f
+#define SPSIM_WIDE_S5 -1.376170635e+01f
+#define SPSIM_WIDE_C0 1.000000000e+00f
+#define SPSIM_WIDE_C1 -1.973919868e+01f
+#define SPSIM_WIDE_C2 6.493840790e+01f
+#define SPSIM_WIDE_C3 -8.542442322e+01f
+#define SPSIM_WIDE_C4 5.977695465e+01f
+#define SPSIM_WIDE_C5 -2.333224869e+01f
 #endif
 

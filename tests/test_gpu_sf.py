@@ -193,7 +193,8 @@ def test_range_error_is_reported(cuda):
     assert np.abs(I.cpu().numpy() - I64).max() < 2e-7 * I64.max()
 
 
-VARIANTS = [(128, 2, 0), (256, 4, 0), (128, 4, 1), (128, 6, 1), (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 8, 2)]
+VARIANTS = [(128, 2, 0), (256, 4, 0), (128, 4, 1), (128, 6, 1), (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 8, 2),
+            (128, 4, 3), (128, 8, 3), (256, 4, 3)]
 
 
 @pytest.mark.parametrize("precision", ["f32", "f32_fast"])
@@ -214,3 +215,19 @@ def test_every_kernel_form_meets_tolerance(cuda, precision, variant):
     for got, want in ((I, I64), (Ib, I64b)):
         e_max, e_l2 = intensity_errors(got, want)
         assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1], (variant, e_max, e_l2)
+
+
+def test_neighbour_pair_form_admission(cuda):
+    # a detector of even width is admitted to the neighbour-pair form; a random
+    # HKL list (no neighbour structure) falls back to the FP64-phase form; both
+    # stay within tolerance
+    Z, pos = synth.random_molecule(2000, 3e-9, 31)
+    d = dict(nx=64, ny=40, width=64 * 150e-6, height=40 * 150e-6, distance=0.1, wavelength=0.2e-9)
+    q_det = O.hkl_detector(**d).astype(np.float32)
+    q_rand = np.random.Generator(np.random.PCG64(31)).normal(size=(2560, 3)).astype(np.float32) * 1e9
+    for q, kernel in ((q_det, "sf_dpair_kernel"), (q_rand, "sf_dphase_kernel")):
+        F, I = _run(Z, pos, q, "f32")
+        assert core.kernel_name() == kernel
+        _, I64 = O.structure_factor(Z, pos.astype(np.float64), q.astype(np.float64))
+        e_max, e_l2 = intensity_errors(I, I64)
+        assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (kernel, e_max, e_l2)
