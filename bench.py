@@ -266,7 +266,7 @@ def _peaks(props):
     return min(p_fma / OPS_PER_TERM_FMA, p_mufu / OPS_PER_TERM_MUFU), p_mufu, p_fma, sm_max, src
 
 
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "sf_dphase_precision50k_traffic.md")
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "sf_dpair_precision50k_traffic.md")
 
 
 def _traffic_per_launch():
