@@ -38,7 +38,7 @@ L2_FLUSH_BYTES = 256 << 20
 
 def workload_desc():
     return ("precision_50k: 50,000 atoms (C 62% N 17% O 20% S 1%, 12 nm ball), 1024x1024 pixels of 75 um at 0.1 m, "
-            "lambda 0.15 nm, compensated FP32 structure factor + detector chain (readout 10 e-, clamp 65535)")
+            "lambda 0.15 nm, FP32 structure factor (FP64 phase, FP32 sin/cos) + detector chain (readout 10 e-, clamp 65535)")
 
 
 # ----------------------------------------------------------------- CPU reference

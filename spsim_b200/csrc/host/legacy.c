@@ -9,6 +9,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/mman.h>
 #include <time.h>
 
 #include <cuda_runtime.h>
@@ -32,6 +33,29 @@ static void die(const char *where, int st) {
 static void cuda_die(const char *where, cudaError_t e) {
   fprintf(stderr, "spsim_b200: %s failed: %s\n", where, cudaGetErrorString(e));
   abort();
+}
+
+/* Output arrays the caller frees with free(), as the reference's are.  Large
+ * ones are 2 MiB aligned and advised for transparent huge pages, so that
+ * filling them (device-to-host copies) takes a few page faults instead of
+ * one per 4 KiB page; free() releases them like any malloc'd block. */
+static void *host_alloc(size_t bytes) {
+  if (!bytes) bytes = 4;
+  void *p = NULL;
+  if (bytes >= ((size_t)2 << 20)) {
+    const size_t huge = (size_t)2 << 20;
+    if (posix_memalign(&p, huge, (bytes + huge - 1) / huge * huge) == 0) {
+      madvise(p, (bytes + huge - 1) / huge * huge, MADV_HUGEPAGE);
+      return p;
+    }
+    p = NULL;
+  }
+  p = malloc(bytes);
+  if (!p) {
+    fprintf(stderr, "spsim_b200: out of host memory (%zu bytes)\n", bytes);
+    abort();
+  }
+  return p;
 }
 
 /* Device scratch of the reference-shaped calls: one grow-only buffer per
@@ -106,7 +130,7 @@ static double now_us(void) {
 /* src/diffraction.c:237-297, computed on the GPU in FP64, stored as float */
 float *get_HKL_list_for_detector(CCD *det, Experiment *exp, int *HKL_list_size) {
   const long long n = (long long)det->nx * det->ny;
-  float *out = (float *)malloc(sizeof(float) * 3 * (n > 0 ? n : 1));
+  float *out = (float *)host_alloc(sizeof(float) * 3 * (n > 0 ? n : 1));
   float *d = (float *)dev_alloc(SLOT_HKL, sizeof(float) * 3 * n);
   int st = spsim_b200_hkl_for_detector(det->nx, det->ny, det->width, det->height, det->distance, det->center_x,
                                        det->center_y, exp->wavelength, det->spherical, d, NULL);
@@ -119,7 +143,7 @@ float *get_HKL_list_for_detector(CCD *det, Experiment *exp, int *HKL_list_size) 
 /* src/diffraction.c:325-369, on the GPU in FP64, stored as float */
 float *get_HKL_list_for_3d_detector(CCD *det, Experiment *exp, int *HKL_list_size) {
   const long long n = (long long)det->nx * det->ny * det->nz;
-  float *out = (float *)malloc(sizeof(float) * 3 * (n > 0 ? n : 1));
+  float *out = (float *)host_alloc(sizeof(float) * 3 * (n > 0 ? n : 1));
   float *d = (float *)dev_alloc(SLOT_HKL, sizeof(float) * 3 * n);
   int st = spsim_b200_hkl_for_3d_detector(det->nx, det->ny, det->nz, det->width, det->height, det->depth,
                                           det->distance, det->center_x, det->center_y, det->center_z, exp->wavelength,
@@ -202,9 +226,9 @@ static Diffraction_Pattern *pattern_on_list(Molecule *mol, float *HKL_list, int 
                                             Options *opts, int spectrum) {
   double t0 = now_us();
   Diffraction_Pattern *res = (Diffraction_Pattern *)calloc(1, sizeof(Diffraction_Pattern));
-  res->F = (Complex *)malloc(sizeof(Complex) * (n > 0 ? n : 1));
-  res->ints = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
-  res->HKL_list = (float *)malloc(sizeof(float) * 3 * (n > 0 ? n : 1));
+  res->F = (Complex *)host_alloc(sizeof(Complex) * (n > 0 ? n : 1));
+  res->ints = (float *)host_alloc(sizeof(float) * (n > 0 ? n : 1));
+  res->HKL_list = (float *)host_alloc(sizeof(float) * 3 * (n > 0 ? n : 1));
   if (n > 0) memcpy(res->HKL_list, HKL_list, sizeof(float) * 3 * n);
   res->HKL_list_size = n;
   res->N_pix = n;
@@ -323,7 +347,7 @@ void calculate_thomson_correction(CCD *det, Experiment *exp) {
   float *d = (float *)dev_alloc(SLOT_THOMSON, sizeof(float) * n);
   int st = spsim_b200_thomson(&p, d, NULL);
   if (st) die("calculate_thomson_correction", st);
-  det->thomson_correction = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  det->thomson_correction = (float *)host_alloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->thomson_correction, d, sizeof(float) * n);
 }
 
@@ -334,7 +358,7 @@ void calculate_pixel_solid_angle(CCD *det) {
   float *d = (float *)dev_alloc(SLOT_SOLID, sizeof(float) * n);
   int st = spsim_b200_solid_angle(&p, d, NULL);
   if (st) die("calculate_pixel_solid_angle", st);
-  det->solid_angle = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  det->solid_angle = (float *)host_alloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->solid_angle, d, sizeof(float) * n);
 }
 
@@ -352,7 +376,7 @@ void calculate_photons_per_pixel(Diffraction_Pattern *pattern, Options *opts) {
   h2d(dI, pattern->ints, sizeof(float) * n);
   int st = spsim_b200_photons(n, dT, dO, dI, exp->beam_intensity, dP, NULL);
   if (st) die("calculate_photons_per_pixel", st);
-  det->photons_per_pixel = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  det->photons_per_pixel = (float *)host_alloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->photons_per_pixel, dP, sizeof(float) * n);
 }
 
@@ -368,7 +392,7 @@ void generate_poisson_noise(CCD *det) {
   h2d(dP, det->photons_per_pixel, sizeof(float) * n);
   int st = spsim_b200_photon_counts(&p, dP, dC, NULL);
   if (st) die("generate_poisson_noise", st);
-  det->photon_count = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  det->photon_count = (float *)host_alloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->photon_count, dC, sizeof(float) * n);
 }
 
@@ -384,7 +408,7 @@ void calculate_electrons_per_pixel(CCD *det, Experiment *experiment) {
   h2d(dC, det->photon_count, sizeof(float) * n);
   int st = spsim_b200_electrons(&p, dC, dE, NULL);
   if (st) die("calculate_electrons_per_pixel", st);
-  det->electrons_per_pixel = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+  det->electrons_per_pixel = (float *)host_alloc(sizeof(float) * (n > 0 ? n : 1));
   d2h(det->electrons_per_pixel, dE, sizeof(float) * n);
 }
 
@@ -400,7 +424,7 @@ void calculate_real_detector_output(CCD *det, Experiment *experiment) {
   h2d(dE, det->electrons_per_pixel, sizeof(float) * n);
   int st = spsim_b200_binned_outputs(&p, dE, NULL, dR, NULL, NULL);
   if (st) die("calculate_real_detector_output", st);
-  det->real_output = (float *)malloc(sizeof(float) * (nb > 0 ? nb : 1));
+  det->real_output = (float *)host_alloc(sizeof(float) * (nb > 0 ? nb : 1));
   d2h(det->real_output, dR, sizeof(float) * nb);
 }
 
@@ -416,7 +440,7 @@ void calculate_noiseless_detector_output(CCD *det, Experiment *experiment) {
   h2d(dP, det->photons_per_pixel, sizeof(float) * n);
   int st = spsim_b200_binned_outputs(&p, NULL, dP, NULL, dN, NULL);
   if (st) die("calculate_noiseless_detector_output", st);
-  det->noiseless_output = (float *)malloc(sizeof(float) * (nb > 0 ? nb : 1));
+  det->noiseless_output = (float *)host_alloc(sizeof(float) * (nb > 0 ? nb : 1));
   d2h(det->noiseless_output, dN, sizeof(float) * nb);
 }
 
@@ -456,7 +480,7 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
                     &det->electrons_per_pixel, &det->real_output, &det->noiseless_output};
   for (int k = 0; k < 7; k++) {
     const long long m = k < 5 ? np : nb;
-    *dst[k] = (float *)malloc(sizeof(float) * (m > 0 ? m : 1));
+    *dst[k] = (float *)host_alloc(sizeof(float) * (m > 0 ? m : 1));
     d2h(*dst[k], bufs[k], sizeof(float) * m);
   }
   g_pattern_counter++;
