@@ -209,10 +209,18 @@ def measured_pipe_peaks():
 
 # Per-term instruction mix of each kernel form (lane operations per atom.pixel
 # term, counted from the kernel source): FP32 = FP32 FMA/MUL/ADD, DFMA = FP64
-# FMA/ADD, IMAD = integer multiply-add, XU = MUFU / conversions.
+# FMA/ADD, IMAD = integer multiply-add, XU = MUFU and FP64->FP32 conversions,
+# I2F = int32->FP32 conversions (not a bound: the f32_fast sweep runs two MUFU
+# and one I2F per term faster than the probe's MUFU rate allows for three XU
+# operations, so I2F issues elsewhere).  "+word": the fixed-point phase word.
 MIX = {
-    "sf_dpair_kernel": {"fp32": 15, "dfma": 3, "imad": 0.5, "xu": 0.875},  # half the terms FP64-anchored, half by FP32 step
-    "sf_dphase_kernel": {"fp32": 12, "dfma": 6, "imad": 1, "xu": 1},   # FP64 phase + reduction, DHALF poly
+    # half the terms FP64-anchored, half by FP32 step
+    "sf_dpair_kernel": {"fp32": 15, "dfma": 3, "imad": 0.5, "xu": 0.875},
+    "sf_dpair_kernel+word": {"fp32": 15.5, "dfma": 1.5, "imad": 0.5, "alu": 0.5, "xu": 0.375, "i2f": 0.5},
+    # FP64 phase + reduction, DHALF poly
+    "sf_dphase_kernel": {"fp32": 12, "dfma": 6, "imad": 1, "xu": 1},
+    "sf_dphase_kernel+word/f32": {"fp32": 13, "dfma": 3, "imad": 1, "alu": 1, "i2f": 1},
+    "sf_dphase_kernel+word/f32_fast": {"fp32": 4, "dfma": 3, "xu": 2, "i2f": 1},
     "sf_f32x2_kernel/f32": {"fp32": 27, "alu": 2},                   # compensated phase, HALF poly
     "sf_f32x2_kernel/f32_fast": {"fp32": 16, "xu": 2},               # compensated phase, MUFU sin/cos
 }
@@ -360,7 +368,7 @@ def run_b200(args):
 
     elapsed_ms, sf_avg, clocks = timed(prec, args.steps, args.warmup)
     value = world * args.steps * terms / (elapsed_ms * 1e-3)
-    kname = core.kernel_name()
+    kname = core.kernel_name() + ("+word" if core.last_phase_word() else "")
 
     line = None
     if rank == 0:
@@ -428,9 +436,15 @@ def _modes(args, core, mol, qs, rot, terms, timed, prec):
     R = _peaks(props)[0]
     if prec != "f32_fast":
         ms, sf_ms, _ = timed("f32_fast", max(2, args.steps // 2), 1)
+        kname = core.kernel_name() + ("+word" if core.last_phase_word() else "")
+        bal = balanced_bound(kname, "f32_fast", measured_pipe_peaks())
+        if bal and sf_ms:
+            bal["frac"] = terms / (sf_ms * 1e-3) / bal["terms_per_s"]
         out["f32_fast"] = {"value": terms * max(2, args.steps // 2) / (ms * 1e-3), "unit": UNIT,
+                           "kernel": kname,
                            "kernel_terms_per_s": terms / (sf_ms * 1e-3) if sf_ms else None,
-                           "frac_of_R": terms / (sf_ms * 1e-3) / R if sf_ms else None}
+                           "frac_of_R": terms / (sf_ms * 1e-3) / R if sf_ms else None,
+                           "balanced": bal}
     q = qs.q()
     sub_rows = core.QSet.from_list(q.reshape(1024, 1024, 3)[::64].reshape(-1, 3))
     sub8 = core.QSet.from_list(q[::8])
@@ -477,23 +491,34 @@ def _e2e(args, w, Z, pos, terms, world):
     exp.wavelength, exp.beam_intensity, exp.exposure_time = d["wavelength"], 1e30, 1e-3
     o.verbosity_level = 0
     o.random_seed = 99
-    mol = S.get_molecule_from_atoms(Z, pos)
+    # two copies of the molecule, the second shifted by 1e-13 m, alternate from
+    # step to step: the library keeps the last molecule while the caller's atom
+    # arrays are unchanged, so alternating makes every step upload its atoms
+    mols = [S.get_molecule_from_atoms(Z, pos), S.get_molecule_from_atoms(Z, pos + 1e-13)]
     n = d["nx"] * d["ny"]
     nsteps = max(2, min(args.steps, 5))
-    for _ in range(1):
-        S.free_stuff(S.simulate_shot(mol, opts), opts)
+    for i in range(2):
+        S.free_stuff(S.simulate_shot(mols[i % 2], opts), opts)
     torch.cuda.synchronize()
     t = time.perf_counter()
-    for _ in range(nsteps):
-        S.free_stuff(S.simulate_shot(mol, opts), opts)
+    for i in range(nsteps):
+        S.free_stuff(S.simulate_shot(mols[i % 2], opts), opts)
     wall = (time.perf_counter() - t) / nsteps
-    S.free_mol(mol)
-    natoms = len(Z)
+    for m in mols:
+        S.free_mol(m)
+    # bytes per step: the molecule's device records (136 B per padded atom:
+    # two compensated layouts, the FP64 record, permutation, base weight, plus
+    # tiles and form-factor coefficients) up; HKL list, F, |F|^2 and the seven
+    # chain arrays down
+    counts = np.bincount(np.asarray(Z, np.int64), minlength=100)[1:]
+    n_pad = int(sum((c + 7) // 8 * 8 for c in counts if c))
+    n_tiles = int(sum((c + 7) // 8 * 8 // 128 + (1 if ((c + 7) // 8 * 8) % 128 else 0) for c in counts if c))
+    n_elem = int(np.count_nonzero(counts))
     return {"value": world * terms / wall, "unit": UNIT,
-            "h2d_bytes_per_step": 12 * n + 16 * natoms + 4 * n,
-            "d2h_bytes_per_step": 12 * n + 12 * n + 7 * 4 * n,
-            "call": "simulate_shot (reference-facing C ABI, host buffers)", "steps": nsteps,
-            "note": "reference semantics: no ADC clamp (extension) in this call"}
+            "h2d_bytes_per_step": 136 * n_pad + 16 * n_tiles + 36 * n_elem,
+            "d2h_bytes_per_step": 12 * n + 8 * n + 4 * n + 7 * 4 * n,
+            "call": "simulate_shot (reference-facing C ABI, host buffers, a new molecule upload every step)",
+            "steps": nsteps, "note": "reference semantics: no ADC clamp (extension) in this call"}
 
 
 def _adjoint_ratio(prec):
@@ -527,7 +552,7 @@ def _adjoint_ratio(prec):
     return statistics.median(tb) / statistics.median(ta)
 
 
-PROFILE_VARIANTS = {"f32": (128, 8, 3), "f32_fast": (128, 6, 1)}  # the untuned defaults on the 1024^2 workload
+PROFILE_VARIANTS = {"f32": (128, 12, 3), "f32_fast": (128, 8, 2)}  # the untuned defaults on the 1024^2 workload
 
 
 def profile_case(precisions):
@@ -570,7 +595,7 @@ def sweep():
     for prec in ("f32", "f32_fast"):
         for v in [(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1),
                   (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2), (128, 4, 3), (128, 8, 3),
-                  (256, 4, 3)]:
+                  (128, 12, 3), (256, 4, 3)]:
             core.set_variant(*v)
             for _ in range(2):
                 core.forward(mol, qs, precision=prec, F=F, I=I)

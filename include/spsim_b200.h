@@ -309,11 +309,15 @@ void spsim_b200_set_formula_seed(unsigned long long seed);
  *   1  compensated FP32 phase, pixel pairs in f32x2 instructions
  *   2  FP64 phase and half-cycle reduction, FP32 sin/cos and sums on pixel
  *      pairs (f32x2); free of the compensated forms' phase range limit
- *      (SPSIM_ERR_RANGE)
+ *      (SPSIM_ERR_RANGE); the SPSIM_PREC_F32_FAST default
  *   3  form 2 on the first pixel of each neighbour pair (pixels 2m, 2m+1),
  *      the second pixel's phase as the first's plus (q_b - q_a).r in FP32;
- *      the default, used where |q_b - q_a| |r|max <= 1/8 cycle for every
- *      pair of the q set (detector rows of even width), else form 2
+ *      the SPSIM_PREC_F32 default, used where |q_b - q_a| |r|max <= 1/8
+ *      cycle for every pair of the q set (detector rows of even width), else
+ *      form 2
+ * Forms 2 and 3 read the reduced phase from a fixed-point phase word (three
+ * FP64 FMAs) while |q|max |r - centre|max < 2^17 cycles, and reduce by FP64
+ * rounding (six FP64 operations, up to 2^48 cycles) beyond.
  * threads < 0 restores automatic choice; autotune times every compiled
  * variant on the given workload and keeps the fastest for workloads of that
  * size class. */
@@ -321,6 +325,10 @@ int spsim_b200_set_variant(int threads, int pixels_per_thread, int form);
 /* The kernel variant the last forward on this thread ran: threads per CTA,
  * pixels per thread and form (-1 for the plain FP64 kernel). */
 int spsim_b200_last_variant(int *threads, int *pixels_per_thread, int *form);
+/* Whether the last forward on this thread (forms 2 and 3) took the phase from
+ * the fixed-point phase word (1) or reduced it by FP64 rounding (0); 0 for the
+ * other forms and the plain FP64 kernel.  No reference counterpart. */
+int spsim_b200_last_phase_word(int *on);
 int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision, void *stream,
                         int *best_threads, int *best_pixels_per_thread, int *best_form);
 

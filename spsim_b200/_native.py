@@ -115,6 +115,7 @@ _SIGNATURES = {
     "spsim_b200_last_forward_stats": (c_int, [POINTER(c_double), POINTER(c_double)]),
     "spsim_b200_set_variant": (c_int, [c_int, c_int, c_int]),
     "spsim_b200_last_variant": (c_int, [POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "spsim_b200_last_phase_word": (c_int, [POINTER(c_int)]),
     "spsim_b200_release_scratch": (None, []),
     "spsim_b200_autotune": (c_int, [_P, _P, c_int, _P, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "spsim_b200_set_legacy_precision": (None, [c_int]),

@@ -21,7 +21,7 @@ from ._native import PRECISIONS, ChainOutputs, ChainParams, check, lib
 __all__ = [
     "Molecule", "QSet", "forward", "forward_batch", "adjoint", "detector_chain", "chain_params",
     "hkl_for_detector", "synchronize", "forward_spectrum", "timing", "autotune", "set_variant", "last_forward_stats",
-    "last_variant", "kernel_name",
+    "last_variant", "last_phase_word", "kernel_name",
 ]
 
 
@@ -347,6 +347,14 @@ def last_variant():
     t, p, f = c_int(0), c_int(0), c_int(0)
     check(lib().spsim_b200_last_variant(byref(t), byref(p), byref(f)))
     return t.value, p.value, f.value
+
+
+def last_phase_word():
+    """True when the last forward on this thread (forms 2, 3) took its phases
+    from the fixed-point phase word rather than FP64 rounding."""
+    on = c_int(0)
+    check(lib().spsim_b200_last_phase_word(byref(on)))
+    return bool(on.value)
 
 
 def kernel_name():

@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(NT) adj_kernel(AdjParams prm) {
 //   pf[2i]   = {qx, qy, qz, hr}  pf[2i+1] = {hi, s2, s2n, 0}   (FP32)
 // Per term the sign (-1)^k of the half-cycle reduction is applied to the two
 // products z = H conj(A) e^{-2 pi i u} with one integer multiply-add each.
-template <int NT, int A, bool PERB>
+template <int NT, int A, bool PERB, bool FIXW>
 __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t m31) {
   static_assert(A % 2 == 0, "atoms per thread must be even");
   constexpr int NP = A / 2;
@@ -229,8 +229,10 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
     for (int i = tid; i < ADJ_PIX_TILE; i += NT) {
       double q[3] = {0.0, 0.0, 0.0}, hr = 0.0, hi = 0.0, s2 = 0.0;
       if (i < n) adj_pixel(prm, blk.elem, base + i, q, hr, hi, s2);
-      pq[2 * i] = make_double2(q[0], q[1]);
-      pq[2 * i + 1] = make_double2(q[2], 0.0);
+      // FIXW: the phase word takes 2 q (half-cycle reduction)
+      const double qs = FIXW ? 2.0 : 1.0;
+      pq[2 * i] = make_double2(qs * q[0], qs * q[1]);
+      pq[2 * i + 1] = make_double2(qs * q[2], 0.0);
       pf[2 * i] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)hr);
       pf[2 * i + 1] = make_float4((float)hi, (float)s2, (float)(-s2 * 1.4426950408889634), 0.0f);
     }
@@ -250,15 +252,21 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int k = 2 * j + h;
-          double u = qa.x * rx[k];
-          u = fma(qa.y, ry[k], u);
-          u = fma(qb.x, rz[k], u);
-          const double t = fma(u, 2.0, M52);
-          y[h] = __double2float_rn(fma(t - M52, -0.5, u));
-          kb[h] = (uint32_t)__double2loint(t);
+          if (FIXW) {
+            const double t = phase_word(qa.x, qa.y, qb.x, rx[k], ry[k], rz[k], PHASE_WORD_BASE_HALF);
+            reduce_phase_word<PREC_MODE_POLY>(t, y[h], kb[h]);
+          } else {
+            double u = qa.x * rx[k];
+            u = fma(qa.y, ry[k], u);
+            u = fma(qb.x, rz[k], u);
+            const double t = fma(u, 2.0, M52);
+            y[h] = __double2float_rn(fma(t - M52, -0.5, u));
+            kb[h] = (uint32_t)__double2loint(t);
+          }
         }
         float2 S, C;
-        sincos_dhalf_poly2(make_float2(y[0], y[1]), S, C);
+        const float2 yy = make_float2(y[0], y[1]);
+        sincos_dhalf_poly2(FIXW ? mul2(yy, f2(word_to_cycles<PREC_MODE_POLY>())) : yy, S, C);
         // H conj(A) e^{-2 pi i u} = (hr C - hi S) - i (hr S + hi C), times (-1)^k
         float2 zr = fma2(nhi, S, mul2(hr, C));
         float2 zn = fma2(hi, C, mul2(hr, S));  // = -Im
@@ -380,10 +388,18 @@ cudaError_t launch_adjoint(int precision_mode, const AdjParams &prm, int n_items
     adj_f64_kernel<ADJ_THREADS><<<n_items, ADJ_THREADS, 0, st>>>(prm);
   } else if (precision_mode == 3) {
     if (prm.per_atom_b)
-      adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, true><<<n_items, ADJ_THREADS, 0, st>>>(prm, 0x80000000u);
+      adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, true, false><<<n_items, ADJ_THREADS, 0, st>>>(
+          prm, 0x80000000u);
     else
-      adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, false><<<n_items, ADJ_THREADS, 0, st>>>(prm,
-                                                                                                      0x80000000u);
+      adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, false, false><<<n_items, ADJ_THREADS, 0, st>>>(
+          prm, 0x80000000u);
+  } else if (precision_mode == 4) {
+    if (prm.per_atom_b)
+      adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, true, true><<<n_items, ADJ_THREADS, 0, st>>>(
+          prm, 0x80000000u);
+    else
+      adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, false, true><<<n_items, ADJ_THREADS, 0, st>>>(
+          prm, 0x80000000u);
   } else if (precision_mode == 0) {
     if (prm.per_atom_b)
       adj_kernel<0, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, true><<<n_items, ADJ_THREADS, 0, st>>>(prm);

@@ -41,7 +41,8 @@ struct AdjParams {
 };
 
 // precision_mode: 0 compensated FP32 polynomial, 1 compensated FP32 MUFU,
-// 2 plain FP64, 3 FP64 phase with FP32 polynomial (packed over atom pairs)
+// 2 plain FP64, 3 FP64 phase with FP32 polynomial (packed over atom pairs),
+// 4 the same with the fixed-point phase word (|q.(r - c)| < 2^17 cycles)
 cudaError_t launch_adjoint(int precision_mode, const AdjParams &prm, int n_items, cudaStream_t st);
 
 }  // namespace spsim

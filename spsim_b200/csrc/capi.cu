@@ -564,6 +564,7 @@ struct Plan {
   double terms = 0;
   int precision = 0, nt = 128, ppt = 4, packed = 1;
   bool perb = false;
+  bool fixw = false;  // FP64-phase forms: fixed-point phase word (every pattern within 2^17 cycles)
   std::vector<long long> npix_of;
   std::vector<SfPattern> host_pats;  // descriptors as last uploaded (rotations change per call)
   int spectrum = 0;                  // > 0: combine this many patterns into spec_F / spec_I
@@ -593,6 +594,7 @@ static bool g_timing = false;
 static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timing_events;
 static thread_local double g_last_terms = 0, g_last_ms = 0;
 static thread_local int g_last_variant[3] = {0, 0, -1};  // threads, pixels per thread, form (-1: FP64 kernel)
+static thread_local int g_last_phase_word = 0;            // forms 2/3: fixed-point phase word used
 static int g_num_sms = 0;
 
 static int num_sms() {
@@ -613,11 +615,12 @@ static Variant choose_variant(double terms, long long total_npix, int precision)
     return {g_force_nt, g_force_p, g_force_pk};
   auto it = g_tuned.find(size_class(terms) * 4 + precision);
   if (it != g_tuned.end()) return it->second;
-  // untuned defaults, from sweeps on B200: the FP64-phase form for FP32, the
-  // compensated pixel-pair form for FP32_FAST (MUFU sin/cos); more pixels per
-  // thread once there are enough pixel tiles to fill every SM several times
-  if (precision == SPSIM_PREC_F32_FAST) return {128, total_npix >= (1LL << 20) ? 6 : total_npix >= 65536 ? 4 : 2, 1};
-  return {128, total_npix >= (1LL << 20) ? 8 : 4, 3};  // falls back to form 2 where a q set is not admitted
+  // untuned defaults, from sweeps on B200: the neighbour-pair FP64-phase form
+  // for FP32, the FP64-phase form for FP32_FAST (MUFU sin/cos, where the
+  // neighbour step saves nothing); more pixels per thread once there are
+  // enough pixel tiles to fill every SM several times
+  if (precision == SPSIM_PREC_F32_FAST) return {128, total_npix >= (1LL << 20) ? 8 : 4, 2};
+  return {128, total_npix >= (1LL << 20) ? 12 : 4, 3};  // falls back to form 2 where a q set is not admitted
 }
 
 static bool is_orthonormal(const double *R) {
@@ -684,7 +687,11 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
       }
       ok = qsets[i]->pair_step * scale * mols[i]->rbound <= (1.0 / 8) * (1.0 - 1e-9);
     }
-    if (!ok) var.packed = 2;
+    if (!ok) {
+      var.packed = 2;
+      const int mode = precision == SPSIM_PREC_F32_FAST ? 1 : 0;
+      if (!sf_f32_variant_exists(mode, var.nt, var.p, 2)) var.p = 8;  // form 2 has no 12-pixel variant
+    }
   }
   const int nt = var.nt, ppt = var.p;
   pl.nt = var.nt;
@@ -756,6 +763,17 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
                     i, cmax, lim, qmax, m->rbound);
     }
   }
+  // the fixed-point phase word needs |q.(r - c)| < 2^18 cycles; 2^17 leaves a margin
+  pl.fixw = precision != SPSIM_PREC_FP64 && pl.packed >= 2;
+  for (int i = 0; i < npat && pl.fixw; ++i) {
+    double qmax = qsets[i]->qmax * (spec ? std::fabs(spec->qscale[i]) : 1.0);
+    if (rot && !is_orthonormal(rot + 9 * (size_t)i)) {
+      double fro = 0;
+      for (int k = 0; k < 9; ++k) fro += rot[9 * (size_t)i + k] * rot[9 * (size_t)i + k];
+      qmax *= std::sqrt(fro);
+    }
+    if (mols[i]->n_kept > 0 && qsets[i]->npix > 0 && qmax * mols[i]->rbound >= std::ldexp(1.0, 17)) pl.fixw = false;
+  }
   CUDA_TRY(cudaMemcpyAsync(pl.pats.p, pats.data(), npat * sizeof(SfPattern), cudaMemcpyHostToDevice, stream));
   pl.host_pats = pats;
   pl.spectrum = spec ? spec->samples : 0;
@@ -768,7 +786,8 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
 
   if (precision != SPSIM_PREC_FP64) {
     // work items: pixel tile x atom-tile range, cost-sorted (largest first)
-    const int occ = std::max(1, sf_f32_occupancy(precision == SPSIM_PREC_F32_FAST ? 1 : 0, nt, ppt, pl.packed, perb));
+    const int occ =
+        std::max(1, sf_f32_occupancy(precision == SPSIM_PREC_F32_FAST ? 1 : 0, nt, ppt, pl.packed, perb, pl.fixw));
     const long long slots = (long long)num_sms() * occ;
     long long total_ptiles = 0;
     for (int i = 0; i < npat; ++i) total_ptiles += (qsets[i]->npix + tile_pix - 1) / tile_pix;
@@ -841,7 +860,7 @@ static cudaError_t enqueue_plan(Plan &pl, cudaStream_t stream, cudaEvent_t ev0, 
     const int mode = pl.precision == SPSIM_PREC_F32_FAST ? PREC_MODE_MUFU : PREC_MODE_POLY;
     int *flags = (int *)pl.flags.p;
     if ((e = launch_sf_f32(mode, pl.nt, pl.ppt, pl.packed, pl.perb, (const SfPattern *)pl.pats.p, (const WorkItem *)pl.items.p,
-                           pl.n_items, flags, flags + 4, pl.grid, stream)))
+                           pl.n_items, flags, flags + 4, pl.grid, stream, pl.fixw)))
       return e;
   }
   if (ev1 && (e = cudaEventRecord(ev1, stream))) return e;
@@ -910,9 +929,11 @@ static int check_flags(Plan &pl) {
 }
 
 // cache == false: a one-shot plan (host convenience path), synchronised before return
+// cache == false and sync == false: the one-shot plan is enqueued and not
+// waited for; spsim_internal_shot_check reads its error flags afterwards.
 static int run_forward(int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
                        const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
-                       cudaStream_t stream, bool cache, const Spectrum *spec = nullptr) {
+                       cudaStream_t stream, bool cache, const Spectrum *spec = nullptr, bool sync = true) {
   if (npat < 0) return fail(SPSIM_ERR_INVALID_ARG, "npatterns < 0");
   if (npat == 0) return SPSIM_OK;
   if (!mols || !qsets) return fail(SPSIM_ERR_INVALID_ARG, "NULL molecule or q-set array");
@@ -972,6 +993,7 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
   g_last_variant[0] = pl->precision == SPSIM_PREC_FP64 ? 256 : pl->nt;
   g_last_variant[1] = pl->precision == SPSIM_PREC_FP64 ? 1 : pl->ppt;
   g_last_variant[2] = pl->precision == SPSIM_PREC_FP64 ? -1 : pl->packed;
+  g_last_phase_word = pl->precision != SPSIM_PREC_FP64 && pl->fixw ? 1 : 0;
   CUDA_TRY(refresh_rotations(*pl, rot, stream));
   if (g_timing || !cache || stream == nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -994,7 +1016,7 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
     }
     CUDA_TRY(cudaGraphLaunch(pl->exec, stream));
   }
-  if (!cache) {
+  if (!cache && sync) {
     CUDA_TRY(cudaStreamSynchronize(stream));
     return check_flags(*pl);
   }
@@ -1040,7 +1062,7 @@ static int spectrum_samples(float wavelength, float bandwidth, int samples, std:
 
 static int forward_spectrum(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot, float B,
                             int precision, float wavelength, float bandwidth, int samples, float *F_dev, float *I_dev,
-                            cudaStream_t stream, bool cache) {
+                            cudaStream_t stream, bool cache, bool sync = true) {
   if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
   if (samples < 1) return fail(SPSIM_ERR_INVALID_ARG, "wavelength samples must be >= 1 (got %d)", samples);
   if (bandwidth != 0.0f && !(wavelength > 0.0f))
@@ -1050,7 +1072,7 @@ static int forward_spectrum(const spsim_b200_molecule *m, const spsim_b200_qset 
   if (S == 1) {
     float *F[1] = {F_dev};
     float *I[1] = {I_dev};
-    return run_forward(1, &m, &qs, rot, B, precision, F, I, stream, cache);
+    return run_forward(1, &m, &qs, rot, B, precision, F, I, stream, cache, nullptr, sync);
   }
   std::vector<const spsim_b200_molecule *> mols(S, m);
   std::vector<const spsim_b200_qset *> qsets(S, qs);
@@ -1065,7 +1087,7 @@ static int forward_spectrum(const spsim_b200_molecule *m, const spsim_b200_qset 
   spec.F = F_dev;
   spec.I = I_dev;
   return run_forward(S, mols.data(), qsets.data(), rot ? rots.data() : nullptr, B, precision, none.data(), none.data(),
-                     stream, cache, &spec);
+                     stream, cache, &spec, sync);
 }
 
 extern "C" int spsim_b200_forward_spectrum(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot,
@@ -1093,6 +1115,7 @@ struct HostSession {
   std::vector<unsigned char> mol_inputs;  // natoms, Z, pos, occ, bfac, delta_atoms, beam, as passed
   spsim_b200_qset *qs = nullptr;
   DevBuf *F = nullptr, *I = nullptr;
+  DevBuf *stats = nullptr;  // two words for the device q-set statistics
 };
 static thread_local HostSession g_host;
 
@@ -1174,6 +1197,7 @@ extern "C" void spsim_internal_release_host_session(void) {
     if (g_host.qs) spsim_b200_qset_destroy(g_host.qs);
     delete g_host.F;
     delete g_host.I;
+    delete g_host.stats;
   }
   g_host = HostSession();
   if (g_oneshot.plan && g_oneshot.device == dev) delete g_oneshot.plan;
@@ -1210,6 +1234,75 @@ static int structure_factor_host(int natoms, const int32_t *Z, const float *pos,
   if (st) return st;
   if (F_host && npix) CUDA_TRY(cudaMemcpy(F_host, F[0], 2 * npix * sizeof(float), cudaMemcpyDeviceToHost));
   if (I_host && npix) CUDA_TRY(cudaMemcpy(I_host, I[0], npix * sizeof(float), cudaMemcpyDeviceToHost));
+  return SPSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The reference-shaped simulate_shot path (host/legacy.c): the structure
+// factor of host atom arrays on a float HKL list already in device memory,
+// F and I left in device memory.  Internal to the library (not exported).
+
+// The session q set takes a device float list: copied device to device, its
+// largest |q| and neighbour step measured on the device.
+static int host_session_qset_device(int64_t npix, const float *hkl_dev, cudaStream_t stream, spsim_b200_qset **out) {
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (!g_host.qs) {
+    g_host.qs = new spsim_b200_qset();
+    g_host.qs->device = dev;
+  }
+  spsim_b200_qset *q = g_host.qs;
+  const size_t need = 3 * (size_t)std::max<int64_t>(npix, 1) * sizeof(float);
+  if (!q->d_hkl || q->cap_bytes < need) {
+    cudaFree(q->d_hkl);
+    q->d_hkl = nullptr;
+    q->cap_bytes = 0;
+    CUDA_TRY(cudaMalloc(&q->d_hkl, need));
+    q->cap_bytes = need;
+  }
+  q->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
+  q->npix = npix;
+  if (npix)
+    CUDA_TRY(cudaMemcpyAsync(q->d_hkl, hkl_dev, 3 * npix * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+  if (!g_host.stats) g_host.stats = new DevBuf();
+  CUDA_TRY(g_host.stats->ensure(2 * sizeof(unsigned long long)));
+  CUDA_TRY(qset_stats(q->d_hkl, npix, (unsigned long long *)g_host.stats->p, &q->qmax, &q->pair_step, stream));
+  *out = q;
+  return SPSIM_OK;
+}
+
+// Enqueued on the legacy default stream and not waited for: the caller
+// synchronises, then calls spsim_internal_shot_check for kernel-side errors.
+extern "C" int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z, const float *pos, float B,
+                                                    int delta_atoms, const float *beam, float wavelength,
+                                                    float bandwidth, int samples, int64_t npix, const float *hkl_dev,
+                                                    int precision, float *F_dev, float *I_dev) {
+  if (npix < 0 || (npix > 0 && !hkl_dev)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (g_host.device != dev) {
+    g_host = HostSession();
+    g_host.device = dev;
+  }
+  spsim_b200_molecule *m = nullptr;
+  spsim_b200_qset *q = nullptr;
+  st = host_session_molecule(natoms, Z, pos, nullptr, nullptr, delta_atoms, beam, &m);
+  if (st) return st;
+  st = host_session_qset_device(npix, hkl_dev, nullptr, &q);
+  if (st) return st;
+  return forward_spectrum(m, q, nullptr, B, precision, wavelength, bandwidth, samples, F_dev, I_dev, nullptr, false,
+                          false);
+}
+
+extern "C" int spsim_internal_shot_check(void) {
+  if (!g_oneshot.plan) return SPSIM_OK;
+  return check_flags(*g_oneshot.plan);
+}
+
+extern "C" int spsim_internal_rotate_hkl(int64_t npix, const float R[9], float *hkl_dev) {
+  CUDA_TRY(launch_rotate_hkl(npix, R, hkl_dev, nullptr));
   return SPSIM_OK;
 }
 
@@ -1281,6 +1374,11 @@ extern "C" int spsim_b200_last_variant(int *threads, int *pixels_per_thread, int
   return SPSIM_OK;
 }
 
+extern "C" int spsim_b200_last_phase_word(int *on) {
+  if (on) *on = g_last_phase_word;
+  return SPSIM_OK;
+}
+
 extern "C" int spsim_b200_set_variant(int threads, int pixels_per_thread, int packed) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (threads < 0) {
@@ -1304,7 +1402,7 @@ extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b20
   if (precision == SPSIM_PREC_FP64) return fail(SPSIM_ERR_INVALID_ARG, "the FP64 kernel has a single variant");
   const int cand[][3] = {{128, 2, 0}, {128, 4, 0}, {256, 4, 0}, {128, 2, 1}, {128, 4, 1}, {256, 4, 1},
                          {128, 6, 1}, {128, 2, 2}, {128, 4, 2}, {256, 4, 2}, {128, 6, 2}, {128, 8, 2},
-                         {128, 4, 3}, {128, 8, 3}, {256, 4, 3}};
+                         {128, 4, 3}, {128, 8, 3}, {128, 12, 3}, {256, 4, 3}};
   float *dI = nullptr;
   CUDA_TRY(cudaMalloc(&dI, std::max<long long>(qs->npix, 1) * sizeof(float)));
   float best = 1e30f;
@@ -1632,7 +1730,10 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   prm.dpos = dpos_dev;
   prm.docc = docc_dev;
   prm.dB = dB_dev;
-  const int mode = precision == SPSIM_PREC_FP64 ? 2 : (precision == SPSIM_PREC_F32_FAST ? 1 : (dphase ? 3 : 0));
+  // mode 4: the FP64-phase adjoint with the fixed-point phase word (phases within 2^17 cycles)
+  const bool fixw = dphase && qmax * m->rbound < std::ldexp(1.0, 17);
+  const int mode =
+      precision == SPSIM_PREC_FP64 ? 2 : (precision == SPSIM_PREC_F32_FAST ? 1 : (dphase ? (fixw ? 4 : 3) : 0));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (g_timing) {
     CUDA_TRY(cudaEventCreate(&e0));

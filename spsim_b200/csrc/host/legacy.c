@@ -5,12 +5,14 @@
  * abort(), as the reference's sp_error_fatal paths do: there is no CPU fallback.
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <sys/mman.h>
 #include <time.h>
+#include <unistd.h>
 
 #include <cuda_runtime.h>
 
@@ -73,7 +75,7 @@ enum {
   SLOT_EL_C, SLOT_EL_E,
   SLOT_RO_E, SLOT_RO_R,
   SLOT_NL_P, SLOT_NL_N,
-  SLOT_SHOT_I, SLOT_SHOT_0,
+  SLOT_SHOT_I, SLOT_SHOT_F, SLOT_SHOT_0,
   N_SLOTS = SLOT_SHOT_0 + 7
 };
 static void *g_slot[N_SLOTS];
@@ -96,6 +98,30 @@ static void *dev_alloc(int slot, size_t bytes) {
 }
 
 void spsim_internal_release_host_session(void);
+/* library-internal (capi.cu): the simulate_shot structure factor on a device
+ * HKL list, its error check, and the float rotation of a device HKL list */
+int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z, const float *pos, float B, int delta_atoms,
+                                         const float *beam, float wavelength, float bandwidth, int samples,
+                                         int64_t npix, const float *hkl_dev, int precision, float *F_dev,
+                                         float *I_dev);
+int spsim_internal_shot_check(void);
+int spsim_internal_rotate_hkl(int64_t npix, const float R[9], float *hkl_dev);
+
+/* Pinned staging buffer of simulate_shot's device-to-host copies (grow-only,
+ * released by spsim_b200_release_scratch). */
+static void *g_pinned = NULL;
+static size_t g_pinned_bytes = 0;
+
+static void *pinned_alloc(size_t bytes) {
+  if (g_pinned && g_pinned_bytes >= bytes) return g_pinned;
+  if (g_pinned) cudaFreeHost(g_pinned);
+  g_pinned = NULL;
+  g_pinned_bytes = 0;
+  cudaError_t e = cudaHostAlloc(&g_pinned, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) cuda_die("cudaHostAlloc", e);
+  g_pinned_bytes = bytes;
+  return g_pinned;
+}
 
 void spsim_b200_release_scratch(void) {
   int dev = 0;
@@ -106,7 +132,59 @@ void spsim_b200_release_scratch(void) {
     g_slot[k] = NULL;
     g_slot_bytes[k] = 0;
   }
+  if (g_pinned) cudaFreeHost(g_pinned);
+  g_pinned = NULL;
+  g_pinned_bytes = 0;
   spsim_internal_release_host_session();
+}
+
+/* Host copies and first touches of large arrays, split over a few threads. */
+typedef struct {
+  char *dst;
+  const char *src; /* NULL: fill with zeros (first touch of fresh pages) */
+  size_t bytes;
+} HostCopy;
+
+static void *host_copy_worker(void *arg) {
+  HostCopy *c = (HostCopy *)arg;
+  if (c->src)
+    memcpy(c->dst, c->src, c->bytes);
+  else
+    memset(c->dst, 0, c->bytes);
+  return NULL;
+}
+
+static void host_copy(void *dst, const void *src, size_t bytes) {
+  enum { MAX_THREADS = 8 };
+  long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+  int nt = (int)(bytes >> 21); /* one thread per 2 MiB */
+  if (nt > MAX_THREADS) nt = MAX_THREADS;
+  if (nt > ncpu) nt = (int)ncpu;
+  if (nt < 2) {
+    if (src)
+      memcpy(dst, src, bytes);
+    else
+      memset(dst, 0, bytes);
+    return;
+  }
+  pthread_t th[MAX_THREADS];
+  HostCopy job[MAX_THREADS];
+  int started[MAX_THREADS] = {0};
+  const size_t chunk = (bytes / nt + 4095) & ~(size_t)4095;
+  for (int t = 0; t < nt; t++) {
+    const size_t off = (size_t)t * chunk;
+    job[t].dst = (char *)dst + (off < bytes ? off : bytes);
+    job[t].src = src ? (const char *)src + (off < bytes ? off : bytes) : NULL;
+    job[t].bytes = off < bytes ? (bytes - off < chunk ? bytes - off : chunk) : 0;
+    started[t] = t > 0 && pthread_create(&th[t], NULL, host_copy_worker, &job[t]) == 0;
+  }
+  host_copy_worker(&job[0]);
+  for (int t = 1; t < nt; t++) {
+    if (started[t])
+      pthread_join(th[t], NULL);
+    else
+      host_copy_worker(&job[t]);
+  }
 }
 
 static void h2d(void *d, const void *h, size_t bytes) {
@@ -196,7 +274,7 @@ static void rotation_matrix(Options *opts, double m[9]) {
 /* src/diffraction.c:300-323: q <- R q in float, like sp_matrix_vector_prod.
  * The returned rotation owns its data in the same allocation, so free() on it
  * (src/spsim.c:357-359) releases everything. */
-SpRotation *apply_orientation_to_HKL_list(float **HKL_list, int *HKL_list_size, Options *opts) {
+static SpRotation *new_rotation(Options *opts) {
   double m[9];
   rotation_matrix(opts, m);
   SpRotation *rot = (SpRotation *)malloc(sizeof(SpRotation) + 9 * sizeof(float));
@@ -204,6 +282,11 @@ SpRotation *apply_orientation_to_HKL_list(float **HKL_list, int *HKL_list_size, 
   rot->cols = 3;
   rot->data = (float *)(rot + 1);
   for (int k = 0; k < 9; k++) rot->data[k] = (float)m[k];
+  return rot;
+}
+
+SpRotation *apply_orientation_to_HKL_list(float **HKL_list, int *HKL_list_size, Options *opts) {
+  SpRotation *rot = new_rotation(opts);
   float *q = *HKL_list;
   for (long long i = 0; i < *HKL_list_size; i++) {
     float v[3] = {q[3 * i], q[3 * i + 1], q[3 * i + 2]};
@@ -446,7 +529,14 @@ void calculate_noiseless_detector_output(CCD *det, Experiment *experiment) {
 
 /* ------------------------------------------------------------ orchestration */
 
-/* src/spsim.c:281-346, with the detector chain fused into one GPU pass. */
+/* src/spsim.c:281-346 as one device pipeline with the reference's outputs:
+ * the HKL list is computed and rotated on the device (bit-identical to
+ * get_HKL_list and apply_orientation_to_HKL_list), the structure factor and
+ * the fused detector chain run on it without host round trips, and every
+ * output comes back through one pinned staging buffer.  While the structure
+ * factor runs, the host allocates and first-touches the output arrays and
+ * copies out the HKL list.  Outputs, ownership and values are those of the
+ * step-by-step reference sequence. */
 Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   CCD *det = opts->detector;
   Experiment *exp = opts->experiment;
@@ -458,33 +548,126 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
     fprintf(stderr, "spsim_b200: detector_gaussian_blurring is not supported\n");
     abort();
   }
+  if (opts->use_fft_for_sf || opts->use_nfft_for_sf) {
+    fprintf(stderr, "spsim_b200: the FFT/NFFT structure factors are not supported\n");
+    abort();
+  }
   if (opts->random_seed >= 0) spsim_b200_set_noise_seed((unsigned long long)opts->random_seed);
-  int n = 0;
-  float *HKL_list = get_HKL_list(opts, &n);
-  SpRotation *rot = apply_orientation_to_HKL_list(&HKL_list, &n, opts);
-  Diffraction_Pattern *pattern = compute_sf(mol, HKL_list, n, opts);
-  pattern->rot = rot;
+  const double t0 = now_us();
 
+  /* geometry (src/spsim.c:98-108, src/diffraction.c:300-323) */
+  const int vol = det->nz > 1;
+  const long long n = vol ? (long long)det->nx * det->ny * det->nz : (long long)det->nx * det->ny;
+  float *d_hkl = (float *)dev_alloc(SLOT_HKL, sizeof(float) * 3 * (n > 0 ? n : 1));
+  int st = vol ? spsim_b200_hkl_for_3d_detector(det->nx, det->ny, det->nz, det->width, det->height, det->depth,
+                                                 det->distance, det->center_x, det->center_y, det->center_z,
+                                                 exp->wavelength, d_hkl, NULL)
+               : spsim_b200_hkl_for_detector(det->nx, det->ny, det->width, det->height, det->distance,
+                                             det->center_x, det->center_y, exp->wavelength, det->spherical, d_hkl,
+                                             NULL);
+  if (st) die("simulate_shot geometry", st);
+  SpRotation *rot = new_rotation(opts);
+  st = spsim_internal_rotate_hkl(n, rot->data, d_hkl);
+  if (st) die("simulate_shot orientation", st);
+
+  /* staging layout: HKL list, F, ints, the five per-pixel and two binned chain arrays */
   const long long np = npix_of(det), nb = nbin_of(det);
+  if (np != n) {
+    fprintf(stderr, "spsim_b200: simulate_shot: detector of %lld pixels but %lld q vectors\n", np, n);
+    abort();
+  }
+  const size_t b_hkl = sizeof(float) * 3 * (size_t)n, b_F = sizeof(Complex) * (size_t)n, b_I = sizeof(float) * (size_t)n;
+  const size_t b_nb = sizeof(float) * (size_t)(nb > 0 ? nb : 0);
+  char *stage = (char *)pinned_alloc(b_hkl + b_F + b_I + 5 * b_I + 2 * b_nb + 64);
+  char *s_hkl = stage, *s_F = s_hkl + b_hkl, *s_I = s_F + b_F, *s_chain = s_I + b_I;
+  cudaEvent_t ev_hkl, ev_out;
+  cudaError_t e = cudaEventCreateWithFlags(&ev_hkl, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming);
+  if (e != cudaSuccess) cuda_die("cudaEventCreate", e);
+  if (n > 0) {
+    e = cudaMemcpyAsync(s_hkl, d_hkl, b_hkl, cudaMemcpyDeviceToHost, 0);
+    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync HKL", e);
+  }
+  cudaEventRecord(ev_hkl, 0);
+
+  /* structure factor (compute_sf, src/spsim.c:110-144): the CUDA dispatch decides the spectrum */
+  const int spectrum = opts->use_cuda != 0 && opts->use_cuda != 2;
+  int samples = 1;
+  if (spectrum) {
+    if (opts->wavelength_samples > 1 && (opts->wavelength_samples & 1) == 0) opts->wavelength_samples++;
+    samples = opts->wavelength_samples;
+  }
+  const int poly = spectrum && exp->bandwidth != 0.0f && samples != 1;
+  if (poly && samples < 1) {
+    fprintf(stderr, "spsim_b200: wavelength_samples must be >= 1 with a bandwidth (got %d)\n", samples);
+    abort();
+  }
+  const float beam[3] = {exp->beam_fwhm, exp->beam_center_x, exp->beam_center_y};
+  float *dF = (float *)dev_alloc(SLOT_SHOT_F, b_F > 0 ? b_F : 8);
+  float *dI = (float *)dev_alloc(SLOT_SHOT_I, b_I > 0 ? b_I : 4);
+  st = spsim_internal_shot_structure_factor(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
+                                            opts->delta_atoms, beam, poly ? exp->wavelength : 0.0f,
+                                            poly ? exp->bandwidth : 0.0f, poly ? samples : 1, n, d_hkl, g_precision,
+                                            dF, dI);
+  if (st) die("simulate_shot structure factor", st);
+
+  /* detector chain on the device intensities (src/spsim.c:300-336) */
   spsim_b200_chain_params p = chain_params(det, exp);
-  float *dI = (float *)dev_alloc(SLOT_SHOT_I, sizeof(float) * np);
   float *bufs[7];
   for (int k = 0; k < 5; k++) bufs[k] = (float *)dev_alloc(SLOT_SHOT_0 + k, sizeof(float) * np);
   bufs[5] = (float *)dev_alloc(SLOT_SHOT_0 + 5, sizeof(float) * nb);
   bufs[6] = (float *)dev_alloc(SLOT_SHOT_0 + 6, sizeof(float) * nb);
-  h2d(dI, pattern->ints, sizeof(float) * np);
   spsim_b200_chain_outputs o = {bufs[0], bufs[1], bufs[2], bufs[3], bufs[4], bufs[5], bufs[6]};
-  int st = spsim_b200_detector_chain(&p, dI, &o, NULL);
+  st = spsim_b200_detector_chain(&p, dI, &o, NULL);
   if (st) die("simulate_shot detector chain", st);
+  if (n > 0) {
+    e = cudaMemcpyAsync(s_F, dF, b_F, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s_I, dI, b_I, cudaMemcpyDeviceToHost, 0);
+    for (int k = 0; k < 7 && e == cudaSuccess; k++) {
+      const size_t b = k < 5 ? b_I : b_nb;
+      if (b) e = cudaMemcpyAsync(s_chain + (k < 5 ? k * b_I : 5 * b_I + (k - 5) * b_nb), bufs[k], b,
+                                 cudaMemcpyDeviceToHost, 0);
+    }
+    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync outputs", e);
+  }
+  cudaEventRecord(ev_out, 0);
+
+  /* meanwhile on the host: the reference-owned outputs, first touched now */
+  Diffraction_Pattern *pattern = (Diffraction_Pattern *)calloc(1, sizeof(Diffraction_Pattern));
+  pattern->F = (Complex *)host_alloc(b_F > 0 ? b_F : sizeof(Complex));
+  pattern->ints = (float *)host_alloc(b_I > 0 ? b_I : sizeof(float));
+  pattern->HKL_list = (float *)host_alloc(b_hkl > 0 ? b_hkl : 3 * sizeof(float));
+  pattern->HKL_list_size = (int)n;
+  pattern->N_pix = (int)n;
+  pattern->rot = rot;
   float **dst[7] = {&det->thomson_correction, &det->solid_angle, &det->photons_per_pixel, &det->photon_count,
                     &det->electrons_per_pixel, &det->real_output, &det->noiseless_output};
   for (int k = 0; k < 7; k++) {
-    const long long m = k < 5 ? np : nb;
-    *dst[k] = (float *)host_alloc(sizeof(float) * (m > 0 ? m : 1));
-    d2h(*dst[k], bufs[k], sizeof(float) * m);
+    const size_t b = k < 5 ? b_I : b_nb;
+    *dst[k] = (float *)host_alloc(b > 0 ? b : sizeof(float));
+    host_copy(*dst[k], NULL, b);
   }
+  host_copy(pattern->F, NULL, b_F);
+  host_copy(pattern->ints, NULL, b_I);
+  e = cudaEventSynchronize(ev_hkl);
+  if (e != cudaSuccess) cuda_die("simulate_shot HKL copy", e);
+  host_copy(pattern->HKL_list, s_hkl, b_hkl);
+
+  e = cudaEventSynchronize(ev_out);
+  if (e != cudaSuccess) cuda_die("simulate_shot outputs", e);
+  cudaEventDestroy(ev_hkl);
+  cudaEventDestroy(ev_out);
+  st = spsim_internal_shot_check();
+  if (st) die("simulate_shot structure factor", st);
+  host_copy(pattern->F, s_F, b_F);
+  host_copy(pattern->ints, s_I, b_I);
+  for (int k = 0; k < 7; k++) {
+    const size_t b = k < 5 ? b_I : b_nb;
+    host_copy(*dst[k], s_chain + (k < 5 ? k * b_I : 5 * b_I + (k - 5) * b_nb), b);
+  }
+  if (opts->verbosity_level > 0) /* src/diffraction.c:849-851 */
+    printf("%g atoms.pixel/s\n", 1.0e6 * n * mol->natoms / (now_us() - t0));
   g_pattern_counter++;
-  free(HKL_list);
   return pattern;
 }
 

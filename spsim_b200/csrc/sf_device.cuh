@@ -19,6 +19,9 @@
 
 namespace spsim {
 
+constexpr int PREC_MODE_POLY = 0;  // FMA-pipe minimax sin/cos (SPSIM_PREC_F32)
+constexpr int PREC_MODE_MUFU = 1;  // MUFU sin/cos (SPSIM_PREC_F32_FAST)
+
 constexpr int ATOM_GROUP = 8;        // segment padding and inner unroll
 constexpr int TILE_ATOMS = 128;      // atoms per shared-memory tile (4 KiB)
 constexpr int RING_STAGES = 3;       // bulk-copy ring depth
@@ -189,6 +192,63 @@ __device__ __forceinline__ float sign_by_parity(float w, uint32_t kbits, uint32_
   uint32_t r;
   asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(kbits), "r"(m31), "r"(__float_as_uint(w)));
   return __uint_as_float(r);
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-point phase word.  While |s q.(r - c)| < 2^19, the FP64 sum
+//   t = s q.(r - c) + base,  base = 1.5 * 2^20 (+ 1/2)
+// lies in [2^20, 2^21), where the ulp is 2^-32: the low 32 bits of t's
+// mantissa hold frac(s q.r + base) * 2^32 (as rounded by the three FMAs,
+// error <= 3 * 2^-33 of a cycle) and bit 0 of the high word holds the parity
+// of floor(s q.r + base) (1.5 * 2^20 is even).  The phase and its reduction
+// thus cost three DFMA instead of six, and the reduced phase reaches FP32
+// through one integer conversion.
+constexpr double PHASE_WORD_BASE = 1572864.0;       // 1.5 * 2^20
+constexpr double PHASE_WORD_BASE_HALF = 1572864.5;  // 1.5 * 2^20 + 1/2
+
+__device__ __forceinline__ double phase_word(double qx, double qy, double qz, double rx, double ry, double rz,
+                                             double base) {
+  double t = fma(qx, rx, base);
+  t = fma(qy, ry, t);
+  return fma(qz, rz, t);
+}
+
+// POLY (s = 2, base 1.5 * 2^20 + 1/2): with u = k/2 + y, k = rint(2u), the low
+// word is (2y + 1/2) 2^32; flipping its bit 31 gives 2y 2^32 as a signed
+// integer, and bit 0 of the high word is k mod 2.  The flip is a logic op:
+// the logic pipe is nearly idle in these kernels, where an integer add or
+// multiply-add would take FMA-pipe slots (measured slower on B200).
+// MUFU (s = 1, base 1.5 * 2^20): the low word as a signed integer is
+// (u - rint(u)) 2^32 (whole-cycle reduction; no sign).
+template <int MODE>
+__device__ __forceinline__ void reduce_phase_word(double t, float &yw, uint32_t &kbits) {
+  const int lo = __double2loint(t);
+  if (MODE == PREC_MODE_POLY) {
+    yw = __int2float_rn(lo ^ (int)0x80000000);
+    kbits = (uint32_t)__double2hiint(t);
+  } else {
+    yw = __int2float_rn(lo);
+    kbits = 0;
+  }
+}
+
+// reduce_phase_word's integer units -> cycles, and -> the kernels' sin/cos argument
+template <int MODE>
+__device__ __forceinline__ constexpr float word_to_cycles() {
+  return MODE == PREC_MODE_POLY ? 0x1p-33f : 0x1p-32f;
+}
+template <int MODE>
+__device__ __forceinline__ constexpr float word_to_phase() {
+  return MODE == PREC_MODE_POLY ? 0x1p-33f : 6.28318530717958648f * 0x1p-32f;
+}
+
+// Packed Fast2Sum: the block sums b of two pixels into their float-float
+// sums (hi, lo); s - hi and b - z as FMAs with -1, so every step stays packed.
+__device__ __forceinline__ void ff_accumulate2(float2 &hi, float2 &lo, float2 b) {
+  const float2 s = add2(hi, b);
+  const float2 z = fma2(hi, f2(-1.0f), s);
+  lo = add2(lo, fma2(z, f2(-1.0f), b));
+  hi = s;
 }
 
 // Fast2Sum-style float-float accumulation of a block sum b into (hi, lo).

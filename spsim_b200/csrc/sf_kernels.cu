@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
 // |q.r| < 2^50 cycles.  Atom records are AtomD (32 bytes), staged by the same
 // bulk-copy ring as the compensated kernels.
 
-template <int MODE, int NT, int P, bool PERB>
+template <int MODE, int NT, int P, bool PERB, bool FIXW>
 __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restrict__ pats,
                                                        const WorkItem *__restrict__ items, int n_items,
                                                        int *__restrict__ queue, int *__restrict__ err, uint32_t m31) {
@@ -517,6 +517,9 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
   uint32_t g_issue = 0, g_cons = 0;
   const long long kWaitCycles = 4000000000LL;
   const double M52 = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
+  // FIXW: pixel q pre-scaled by 2 (half-cycle reduction) and the phase summed onto kWordBase
+  constexpr double kQScale = (FIXW && MODE == PREC_MODE_POLY) ? 2.0 : 1.0;
+  constexpr double kWordBase = MODE == PREC_MODE_POLY ? PHASE_WORD_BASE_HALF : PHASE_WORD_BASE;
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(queue, 1);
@@ -537,9 +540,9 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
       const long long p = pix0 + i * NT;
       double q[3] = {0.0, 0.0, 0.0};
       if (p < npix) load_q(pt, p, q);
-      qx[i] = q[0];
-      qy[i] = q[1];
-      qz[i] = q[2];
+      qx[i] = kQScale * q[0];
+      qy[i] = kQScale * q[1];
+      qz[i] = kQScale * q[2];
       s2n[i] = (float)(-0.25 * (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) * 1e-20 * pt.s2scale * 1.4426950408889634);
     }
     float2 shc[NP], slc[NP], shs[NP], sls[NP];
@@ -574,12 +577,15 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
       }
       const TileDesc td = tiles[k];
       const float4 *__restrict__ ta = ring[st];
-      for (int a = 0; a < td.count; a += ATOM_GROUP) {
+      // atoms in groups of 2 x ATOM_GROUP (the last group of a tile may be
+      // ATOM_GROUP): FP32 sums within a group, Fast2Sum after it
+      for (int a = 0; a < td.count; a += 2 * ATOM_GROUP) {
         float2 bc[NP], bs[NP];
 #pragma unroll
         for (int j = 0; j < NP; ++j) bc[j] = bs[j] = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int g = 0; g < ATOM_GROUP; ++g) {
+        for (int g = 0; g < 2 * ATOM_GROUP; ++g) {
+          if (g == ATOM_GROUP && a + ATOM_GROUP >= td.count) break;
           const float4 d0 = ta[2 * (a + g)], d1 = ta[2 * (a + g) + 1];
           const double rx = __hiloint2double(__float_as_int(d0.y), __float_as_int(d0.x));
           const double ry = __hiloint2double(__float_as_int(d0.w), __float_as_int(d0.z));
@@ -592,21 +598,27 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
               const int i = 2 * j + h;
-              double u = qx[i] * rx;
-              u = fma(qy[i], ry, u);
-              u = fma(qz[i], rz, u);
-              if (MODE == PREC_MODE_POLY) {
-                const double t = fma(u, 2.0, M52);  // rint(2u) in the low bits
-                y[h] = __double2float_rn(fma(t - M52, -0.5, u));  // u - k/2, exact before the rounding
-                kb[h] = (uint32_t)__double2loint(t);
+              if (FIXW) {
+                const double t = phase_word(qx[i], qy[i], qz[i], rx, ry, rz, kWordBase);
+                reduce_phase_word<MODE>(t, y[h], kb[h]);
               } else {
-                const double t = u + M52;
-                y[h] = __double2float_rn(u - (t - M52));
-                kb[h] = 0;
+                double u = qx[i] * rx;
+                u = fma(qy[i], ry, u);
+                u = fma(qz[i], rz, u);
+                if (MODE == PREC_MODE_POLY) {
+                  const double t = fma(u, 2.0, M52);  // rint(2u) in the low bits
+                  y[h] = __double2float_rn(fma(t - M52, -0.5, u));  // u - k/2, exact before the rounding
+                  kb[h] = (uint32_t)__double2loint(t);
+                } else {
+                  const double t = u + M52;
+                  y[h] = __double2float_rn(u - (t - M52));
+                  kb[h] = 0;
+                }
               }
               w[h] = PERB ? W * exp2f(d1.w * s2n[i]) : W;
             }
-            const float2 yy = make_float2(y[0], y[1]);
+            const float2 yy = FIXW ? mul2(make_float2(y[0], y[1]), f2(word_to_phase<MODE>()))
+                                   : make_float2(y[0], y[1]);
             if (MODE == PREC_MODE_POLY) {
               // e^{2 pi i (k/2 + y)} = (-1)^k e^{2 pi i y}, |y| <= 1/4
               float2 S, pc;
@@ -615,7 +627,7 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
               bc[j] = fma2(ws, pc, bc[j]);
               bs[j] = fma2(ws, S, bs[j]);
             } else {
-              const float2 x = mul2(yy, f2(6.28318530717958648f));
+              const float2 x = FIXW ? yy : mul2(yy, f2(6.28318530717958648f));
               float2 sn, cs;
               __sincosf(x.x, &sn.x, &cs.x);
               __sincosf(x.y, &sn.y, &cs.y);
@@ -628,12 +640,8 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
           // Fast2Sum of the group sums into the float-float element sums
-          float2 s1 = add2(shc[j], bc[j]);
-          slc[j] = add2(slc[j], add2(bc[j], make_float2(-(s1.x - shc[j].x), -(s1.y - shc[j].y))));
-          shc[j] = s1;
-          float2 s2 = add2(shs[j], bs[j]);
-          sls[j] = add2(sls[j], add2(bs[j], make_float2(-(s2.x - shs[j].x), -(s2.y - shs[j].y))));
-          shs[j] = s2;
+          ff_accumulate2(shc[j], slc[j], bc[j]);
+          ff_accumulate2(shs[j], sls[j], bs[j]);
         }
       }
       if (td.last || k == k1 - 1) {
@@ -701,7 +709,7 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
 // P/2 pairs; two pairs' anchors and two pairs' seconds share each packed
 // f32x2 polynomial.
 
-template <int MODE, int NT, int P, bool PERB>
+template <int MODE, int NT, int P, bool PERB, bool FIXW>
 __global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restrict__ pats,
                                                       const WorkItem *__restrict__ items, int n_items,
                                                       int *__restrict__ queue, int *__restrict__ err, uint32_t m31) {
@@ -723,6 +731,8 @@ __global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restric
   uint32_t g_issue = 0, g_cons = 0;
   const long long kWaitCycles = 4000000000LL;
   const double M52 = 6755399441055744.0;  // 1.5 * 2^52
+  constexpr double kQScale = (FIXW && MODE == PREC_MODE_POLY) ? 2.0 : 1.0;
+  constexpr double kWordBase = MODE == PREC_MODE_POLY ? PHASE_WORD_BASE_HALF : PHASE_WORD_BASE;
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(queue, 1);
@@ -746,9 +756,9 @@ __global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restric
       if (pa < npix) load_q(pt, pa, a);
       if (pa + 1 < npix) load_q(pt, pa + 1, b);
       else b[0] = a[0], b[1] = a[1], b[2] = a[2];
-      qx[m] = a[0];
-      qy[m] = a[1];
-      qz[m] = a[2];
+      qx[m] = kQScale * a[0];
+      qy[m] = kQScale * a[1];
+      qz[m] = kQScale * a[2];
       dqx[m] = (float)(b[0] - a[0]);
       dqy[m] = (float)(b[1] - a[1]);
       dqz[m] = (float)(b[2] - a[2]);
@@ -790,14 +800,17 @@ __global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restric
       }
       const TileDesc td = tiles[k];
       const float4 *__restrict__ ta = ring[st];
-      for (int a = 0; a < td.count; a += ATOM_GROUP) {
+      // atoms in groups of 2 x ATOM_GROUP (the last group of a tile may be
+      // ATOM_GROUP): FP32 sums within a group, Fast2Sum after it
+      for (int a = 0; a < td.count; a += 2 * ATOM_GROUP) {
         float2 bc[NPK][2], bs[NPK][2];
 #pragma unroll
         for (int j = 0; j < NPK; ++j)
 #pragma unroll
           for (int h = 0; h < 2; ++h) bc[j][h] = bs[j][h] = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int g = 0; g < ATOM_GROUP; ++g) {
+        for (int g = 0; g < 2 * ATOM_GROUP; ++g) {
+          if (g == ATOM_GROUP && a + ATOM_GROUP >= td.count) break;
           const float4 d0 = ta[2 * (a + g)], d1 = ta[2 * (a + g) + 1];
           const double rx = __hiloint2double(__float_as_int(d0.y), __float_as_int(d0.x));
           const double ry = __hiloint2double(__float_as_int(d0.w), __float_as_int(d0.z));
@@ -811,20 +824,27 @@ __global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restric
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
               const int m = 2 * j + h;
-              double u = qx[m] * rx;
-              u = fma(qy[m], ry, u);
-              u = fma(qz[m], rz, u);
-              if (MODE == PREC_MODE_POLY) {
-                const double t = fma(u, 2.0, M52);
-                ya[h] = __double2float_rn(fma(t - M52, -0.5, u));
-                kb[h] = (uint32_t)__double2loint(t);
+              if (FIXW) {
+                const double t = phase_word(qx[m], qy[m], qz[m], rx, ry, rz, kWordBase);
+                reduce_phase_word<MODE>(t, ya[h], kb[h]);
               } else {
-                const double t = u + M52;
-                ya[h] = __double2float_rn(u - (t - M52));
-                kb[h] = 0;
+                double u = qx[m] * rx;
+                u = fma(qy[m], ry, u);
+                u = fma(qz[m], rz, u);
+                if (MODE == PREC_MODE_POLY) {
+                  const double t = fma(u, 2.0, M52);
+                  ya[h] = __double2float_rn(fma(t - M52, -0.5, u));
+                  kb[h] = (uint32_t)__double2loint(t);
+                } else {
+                  const double t = u + M52;
+                  ya[h] = __double2float_rn(u - (t - M52));
+                  kb[h] = 0;
+                }
               }
             }
-            const float2 Ya = make_float2(ya[0], ya[1]);
+            // anchors' reduced phases in cycles
+            const float2 Ya = FIXW ? mul2(make_float2(ya[0], ya[1]), f2(word_to_cycles<MODE>()))
+                                   : make_float2(ya[0], ya[1]);
             // second pixels: y_b = y_a + (q_b - q_a).r in FP32
             float2 dl = mul2(make_float2(dqx[2 * j], dqx[2 * j + 1]), fx);
             dl = fma2(make_float2(dqy[2 * j], dqy[2 * j + 1]), fy, dl);
@@ -875,12 +895,8 @@ __global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restric
         for (int j = 0; j < NPK; ++j)
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            float2 s1 = add2(shc[j][h], bc[j][h]);
-            slc[j][h] = add2(slc[j][h], add2(bc[j][h], make_float2(-(s1.x - shc[j][h].x), -(s1.y - shc[j][h].y))));
-            shc[j][h] = s1;
-            float2 s2 = add2(shs[j][h], bs[j][h]);
-            sls[j][h] = add2(sls[j][h], add2(bs[j][h], make_float2(-(s2.x - shs[j][h].x), -(s2.y - shs[j][h].y))));
-            shs[j][h] = s2;
+            ff_accumulate2(shc[j][h], slc[j][h], bc[j][h]);
+            ff_accumulate2(shs[j][h], sls[j][h], bs[j][h]);
           }
       }
       if (td.last || k == k1 - 1) {
@@ -1167,13 +1183,13 @@ cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix,
 // scalar compensated kernel (sf_f32_kernel), 1 the pixel-pair compensated one
 // (sf_f32x2_kernel), 2 the pixel-pair FP64-phase one (sf_dphase_kernel), 3 the
 // FP64-anchored neighbour pairs (sf_dpair_kernel).
-template <int MODE, int NT, int P, bool PERB, int PK>
+template <int MODE, int NT, int P, bool PERB, int PK, bool FW>
 static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, int n_items, int *queue, int *err,
                                 int grid, cudaStream_t st) {
   if constexpr (PK == 3)
-    sf_dpair_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
+    sf_dpair_kernel<MODE, NT, P, PERB, FW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
   else if constexpr (PK == 2)
-    sf_dphase_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
+    sf_dphase_kernel<MODE, NT, P, PERB, FW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
   else if constexpr (PK == 1)
     sf_f32x2_kernel<MODE, NT, P, PERB><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err);
   else
@@ -1181,13 +1197,13 @@ static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, in
   return cudaGetLastError();
 }
 
-template <int MODE, int NT, int P, bool PERB, int PK>
+template <int MODE, int NT, int P, bool PERB, int PK, bool FW>
 static int occupancy_t() {
   int n = 0;
   if constexpr (PK == 3)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dpair_kernel<MODE, NT, P, PERB>, NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dpair_kernel<MODE, NT, P, PERB, FW>, NT, 0);
   else if constexpr (PK == 2)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dphase_kernel<MODE, NT, P, PERB>, NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dphase_kernel<MODE, NT, P, PERB, FW>, NT, 0);
   else if constexpr (PK == 1)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_f32x2_kernel<MODE, NT, P, PERB>, NT, 0);
   else
@@ -1222,27 +1238,38 @@ static int occupancy_t() {
   X(1, 128, 8, 2)             \
   X(0, 128, 4, 3)             \
   X(0, 128, 8, 3)             \
+  X(0, 128, 12, 3)            \
   X(0, 256, 4, 3)             \
   X(1, 128, 4, 3)             \
   X(1, 128, 8, 3)             \
+  X(1, 128, 12, 3)            \
   X(1, 256, 4, 3)
 
+// fixw selects the fixed-point phase word in the FP64-phase forms (2, 3);
+// the compensated forms ignore it.
 cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
-                          const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st) {
-#define X(M, N, PP, PK)                                                                               \
-  if (mode == M && nt == N && p == PP && packed == PK) {                                              \
-    return perb ? launch_f32_t<M, N, PP, true, PK>(pats, items, n_items, queue, err, grid, st)        \
-                : launch_f32_t<M, N, PP, false, PK>(pats, items, n_items, queue, err, grid, st);      \
+                          const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st,
+                          bool fixw) {
+#define X(M, N, PP, PK)                                                                                   \
+  if (mode == M && nt == N && p == PP && packed == PK) {                                                  \
+    if (fixw && PK >= 2)                                                                                  \
+      return perb ? launch_f32_t<M, N, PP, true, PK, true>(pats, items, n_items, queue, err, grid, st)    \
+                  : launch_f32_t<M, N, PP, false, PK, true>(pats, items, n_items, queue, err, grid, st);  \
+    return perb ? launch_f32_t<M, N, PP, true, PK, false>(pats, items, n_items, queue, err, grid, st)     \
+                : launch_f32_t<M, N, PP, false, PK, false>(pats, items, n_items, queue, err, grid, st);   \
   }
   SPSIM_F32_VARIANTS(X)
 #undef X
   return cudaErrorInvalidConfiguration;
 }
 
-int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb) {
-#define X(M, N, PP, PK)                                 \
-  if (mode == M && nt == N && p == PP && packed == PK) \
-    return perb ? occupancy_t<M, N, PP, true, PK>() : occupancy_t<M, N, PP, false, PK>();
+int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw) {
+#define X(M, N, PP, PK)                                                                          \
+  if (mode == M && nt == N && p == PP && packed == PK) {                                         \
+    if (fixw && PK >= 2)                                                                         \
+      return perb ? occupancy_t<M, N, PP, true, PK, true>() : occupancy_t<M, N, PP, false, PK, true>(); \
+    return perb ? occupancy_t<M, N, PP, true, PK, false>() : occupancy_t<M, N, PP, false, PK, false>(); \
+  }
   SPSIM_F32_VARIANTS(X)
 #undef X
   return 0;
@@ -1338,6 +1365,71 @@ cudaError_t pair_step(const float *hkl, const double *q64, long long npix, doubl
     *step = v;
   }
   return e;
+}
+
+// q <- R q on a float HKL list with the operations of the reference's
+// apply_orientation_to_HKL_list loop (src/diffraction.c:300-323 through
+// sp_matrix_vector_prod): per row acc = 0, then acc += R[r][c] * v[c] for
+// c = 0, 1, 2, each product and sum rounded to float (no contraction), so the
+// device list is bit-identical to the host loop's.
+__global__ void rotate_hkl_kernel(long long n, float r0, float r1, float r2, float r3, float r4, float r5, float r6,
+                                  float r7, float r8, float *__restrict__ hkl) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float v0 = hkl[3 * i], v1 = hkl[3 * i + 1], v2 = hkl[3 * i + 2];
+  const float R[9] = {r0, r1, r2, r3, r4, r5, r6, r7, r8};
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    float acc = 0.0f;
+    acc = __fadd_rn(acc, __fmul_rn(R[3 * r], v0));
+    acc = __fadd_rn(acc, __fmul_rn(R[3 * r + 1], v1));
+    acc = __fadd_rn(acc, __fmul_rn(R[3 * r + 2], v2));
+    hkl[3 * i + r] = acc;
+  }
+}
+
+cudaError_t launch_rotate_hkl(long long n, const float R[9], float *hkl, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  rotate_hkl_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7],
+                                                                R[8], hkl);
+  return cudaGetLastError();
+}
+
+// Largest |q|^2 and largest |q[2m+1] - q[2m]|^2 of a float HKL list, as the
+// bits of non-negative doubles (which order like integers) in out[0], out[1].
+__global__ void qset_stats_kernel(const float *__restrict__ hkl, long long npix, unsigned long long *__restrict__ out) {
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (2 * m >= npix) return;
+  double a[3], b[3];
+  for (int c = 0; c < 3; ++c) a[c] = hkl[3 * (2 * m) + c];
+  double qq = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+  double dd = 0.0;
+  if (2 * m + 1 < npix) {
+    for (int c = 0; c < 3; ++c) b[c] = hkl[3 * (2 * m + 1) + c];
+    qq = fmax(qq, b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+    dd = (b[0] - a[0]) * (b[0] - a[0]) + (b[1] - a[1]) * (b[1] - a[1]) + (b[2] - a[2]) * (b[2] - a[2]);
+  }
+  atomicMax(out, (unsigned long long)__double_as_longlong(qq));
+  atomicMax(out + 1, (unsigned long long)__double_as_longlong(dd));
+}
+
+cudaError_t qset_stats(const float *hkl, long long npix, unsigned long long *scratch2, double *qmax, double *step,
+                       cudaStream_t st) {
+  *qmax = *step = 0.0;
+  if (npix <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(scratch2, 0, 2 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  const long long pairs = (npix + 1) / 2;
+  qset_stats_kernel<<<(unsigned)((pairs + 255) / 256), 256, 0, st>>>(hkl, npix, scratch2);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  unsigned long long h[2] = {0, 0};
+  if ((e = cudaMemcpyAsync(h, scratch2, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  double v[2];
+  memcpy(v, h, sizeof(v));
+  *qmax = sqrt(v[0]);
+  *step = sqrt(v[1]);
+  return cudaSuccess;
 }
 
 cudaError_t launch_volume(int nx, int ny, int nz, float width, float height, float depth, float distance, float cx,

@@ -5,14 +5,15 @@
 
 namespace spsim {
 
-constexpr int PREC_MODE_POLY = 0;  // FMA-pipe minimax sin/cos (SPSIM_PREC_F32)
-constexpr int PREC_MODE_MUFU = 1;  // MUFU sin/cos (SPSIM_PREC_F32_FAST)
 
 cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix, int n_elem, const float *coeffs,
                             double B, int delta_atoms, double *ff, cudaStream_t st);
+// fixw: the FP64-phase forms (2, 3) take the fixed-point phase word, valid
+// while |q|max |r - c|max < 2^18 cycles (the host checks 2^17)
 cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
-                          const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st);
-int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb);
+                          const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st,
+                          bool fixw = false);
+int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw = false);
 bool sf_f32_variant_exists(int mode, int nt, int p, int packed);
 cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cudaStream_t st);
 cudaError_t launch_spectrum_combine(const SfPattern *pats, int pattern0, int S, const double *weight, float *F,
@@ -21,6 +22,12 @@ cudaError_t launch_volume(int nx, int ny, int nz, float width, float height, flo
                           float cy, float cz, float wavelength, float *out32, cudaStream_t st);
 cudaError_t launch_crystal(long long npix, const float *hkl, const double cell[9], int na, int nb, int nc, float *F,
                            float *I, cudaStream_t st);
+// q <- R q in float on a device HKL list, bit-identical to the reference's host loop.
+cudaError_t launch_rotate_hkl(long long n, const float R[9], float *hkl, cudaStream_t st);
+// Largest |q| and largest |q[2m+1] - q[2m]| of a device float HKL list
+// (scratch2: two device words; waits for `st`).
+cudaError_t qset_stats(const float *hkl, long long npix, unsigned long long *scratch2, double *qmax, double *step,
+                       cudaStream_t st);
 // Largest |q[2m+1] - q[2m]| of a q set's pixel pairs (synchronous, small).
 cudaError_t pair_step(const float *hkl, const double *q64, long long npix, double *step);
 cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st);

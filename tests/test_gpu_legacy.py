@@ -121,3 +121,75 @@ def test_host_entry_point_reuses_scratch_safely(cuda):
     L.spsim_b200_release_scratch()
     e_max, _ = intensity_errors(call(Z, pos, hkl), want(Z, pos, hkl))
     assert e_max < 1e-5
+
+
+@pytest.mark.parametrize("use_cuda", [1, 2])
+def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda):
+    # simulate_shot runs geometry, orientation, structure factor and the chain
+    # as one device pipeline; its outputs must be those of the reference's
+    # step-by-step sequence (src/spsim.c:281-346) through the public calls:
+    # HKL list bit for bit (device rotation = host float loop), F and |F|^2
+    # bit for bit, the chain arrays as the fused chain gives them (within a
+    # few ulps of the per-stage functions; noise from the same streams)
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        opts = S.set_defaults()
+        S.read_options_file(os.path.join(GOLDEN, "config", "example.conf"), opts)
+        o = opts.contents
+        det, exp = o.detector.contents, o.experiment.contents
+        det.width = det.height = 48 * det.pixel_width
+        det.nx = det.ny = 48
+        det.readout_noise = 3.0
+        o.verbosity_level = 0
+        o.use_cuda = use_cuda
+        o.random_orientation = 0
+        o.euler_orientation[0], o.euler_orientation[1], o.euler_orientation[2] = 0.3, -1.1, 2.2
+        o.random_seed = 4242
+        S.set_noise_seed(4242)
+        g = golden("sf_small.npz")
+        mol = _mol(g["Z"], g["pos"])
+        n = 48 * 48
+
+        # the reference sequence, step by step (no pattern counter step in between)
+        size = ctypes.c_int(0)
+        hkl = S.get_HKL_list(opts, ctypes.byref(size))
+        hp = ctypes.pointer(hkl)
+        rot = S.apply_orientation_to_HKL_list(hp, ctypes.byref(size), opts)
+        pat = S.compute_sf(mol, hp.contents, size.value, opts)
+        S.calculate_thomson_correction(o.detector, o.experiment)
+        S.calculate_pixel_solid_angle(o.detector)
+        S.calculate_photons_per_pixel(pat, opts)
+        S.generate_poisson_noise(o.detector)
+        S.calculate_electrons_per_pixel(o.detector, o.experiment)
+        S.calculate_real_detector_output(o.detector, o.experiment)
+        S.calculate_noiseless_detector_output(o.detector, o.experiment)
+        names = ["thomson_correction", "solid_angle", "photons_per_pixel", "photon_count", "electrons_per_pixel",
+                 "real_output", "noiseless_output"]
+        step = {k: S.as_array(getattr(det, k), n).copy() for k in names}
+        step_hkl = S.as_array(pat.contents.HKL_list, 3 * n).copy()
+        step_F = S.as_array(pat.contents.F, n).copy()
+        step_I = S.as_array(pat.contents.ints, n).copy()
+        step_rot = np.ctypeslib.as_array(rot.contents.data, shape=(9,)).copy()
+        S.free_diffraction_pattern(pat)
+        S.free_output_in_options(opts)
+
+        shot = S.simulate_shot(mol, opts)
+        np.testing.assert_array_equal(S.as_array(shot.contents.HKL_list, 3 * n), step_hkl)
+        np.testing.assert_array_equal(np.ctypeslib.as_array(shot.contents.rot.contents.data, shape=(9,)), step_rot)
+        np.testing.assert_array_equal(S.as_array(shot.contents.F, n), step_F)
+        np.testing.assert_array_equal(S.as_array(shot.contents.ints, n), step_I)
+        got = {k: S.as_array(getattr(det, k), n) for k in names}
+        np.testing.assert_allclose(got["thomson_correction"], step["thomson_correction"], rtol=2.4e-7)
+        np.testing.assert_allclose(got["solid_angle"], step["solid_angle"], rtol=2.4e-7)
+        np.testing.assert_allclose(got["photons_per_pixel"], step["photons_per_pixel"], rtol=6e-7)
+        np.testing.assert_allclose(got["noiseless_output"], step["noiseless_output"], rtol=1e-6)
+        assert np.mean(got["photon_count"] == step["photon_count"]) > 0.995
+        same = got["photon_count"] == step["photon_count"]
+        np.testing.assert_allclose(got["electrons_per_pixel"][same], step["electrons_per_pixel"][same], rtol=1e-6)
+        np.testing.assert_allclose(got["real_output"][same], step["real_output"][same], rtol=1e-5, atol=1e-3)
+        assert shot.contents.HKL_list_size == n
+        S.free_stuff(shot, opts)
+        S.free_mol(mol)
+    finally:
+        os.chdir(cwd)

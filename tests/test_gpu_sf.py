@@ -4,8 +4,8 @@ Tolerances (relative |F|^2 error against FP64, floored at 1e-3 of the mean
 intensity, and L2 over the pattern; every path stores F and I as float32, so
 one float ulp, ~6e-8, is the floor):
   fp64      2e-7  / 1e-7
-  f32       1e-5  / 1e-6     compensated phase, FMA-pipe sin/cos
-  f32_fast  2e-4  / 1e-5     compensated phase, MUFU sin/cos
+  f32       1e-5  / 1e-6     FP64 or compensated FP32 phase, FMA-pipe sin/cos
+  f32_fast  2e-4  / 1e-5     FP64 or compensated FP32 phase, MUFU sin/cos
 and against the reference's float results, its own error band (2e-5 / 2e-6).
 """
 import numpy as np
@@ -193,8 +193,32 @@ def test_range_error_is_reported(cuda):
     assert np.abs(I.cpu().numpy() - I64).max() < 2e-7 * I64.max()
 
 
+@pytest.mark.parametrize("precision", ["f32", "f32_fast"])
+def test_wide_phase_range_uses_fp64_rounding(cuda, precision):
+    # |q|max |r - c|max of ~6e5 cycles is above the fixed-point phase word's
+    # 2^17-cycle range: the FP64-phase forms reduce by FP64 rounding instead
+    rng = np.random.Generator(np.random.PCG64(5))
+    Z = rng.choice([6, 7, 8, 16], 64).astype(np.int32)
+    pos = rng.uniform(-3e-5, 3e-5, (64, 3)).astype(np.float32)
+    # pixel pairs 2m, 2m+1 a few 100 1/m apart, so that the neighbour-pair form is admitted too
+    qa = rng.normal(size=(1024, 3)) * 3e9
+    hkl = np.stack([qa, qa + rng.normal(size=(1024, 3)) * 3e2], axis=1).reshape(-1, 3).astype(np.float32)
+    qr = np.linalg.norm(hkl.astype(np.float64), axis=1).max() * np.linalg.norm(pos - pos.mean(0), axis=1).max()
+    assert qr > 2.0 ** 17
+    _, I64 = O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64))
+    for form in (2, 3):
+        try:
+            core.set_variant(128, 4, form)
+            _, I = _run(Z, pos, hkl, precision)
+            assert core.last_variant()[2] == form and not core.last_phase_word()
+        finally:
+            core.set_variant(-1)
+        e_max, e_l2 = intensity_errors(I, I64)
+        assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1], (form, e_max, e_l2)
+
+
 VARIANTS = [(128, 2, 0), (256, 4, 0), (128, 4, 1), (128, 6, 1), (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 8, 2),
-            (128, 4, 3), (128, 8, 3), (256, 4, 3)]
+            (128, 4, 3), (128, 8, 3), (128, 12, 3), (256, 4, 3)]
 
 
 @pytest.mark.parametrize("precision", ["f32", "f32_fast"])
@@ -227,7 +251,7 @@ def test_neighbour_pair_form_admission(cuda):
     q_rand = np.random.Generator(np.random.PCG64(31)).normal(size=(2560, 3)).astype(np.float32) * 1e9
     for q, kernel in ((q_det, "sf_dpair_kernel"), (q_rand, "sf_dphase_kernel")):
         F, I = _run(Z, pos, q, "f32")
-        assert core.kernel_name() == kernel
+        assert core.kernel_name() == kernel and core.last_phase_word()
         _, I64 = O.structure_factor(Z, pos.astype(np.float64), q.astype(np.float64))
         e_max, e_l2 = intensity_errors(I, I64)
         assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (kernel, e_max, e_l2)

@@ -24,8 +24,8 @@ TOL = {_native.PREC_F32: (1e-5, 1e-6), _native.PREC_F32_FAST: (2e-4, 1e-5), _nat
 
 def _call(fn, Z, pos, hkl, precision, B=0.0):
     n = hkl.shape[0]
-    F = np.empty(2 * n, np.float32)
-    I = np.empty(n, np.float32)
+    F = np.zeros(2 * n, np.float32)
+    I = np.zeros(n, np.float32)
     Z = np.ascontiguousarray(Z, np.int32)
     pos = np.ascontiguousarray(pos, np.float32)
     hkl = np.ascontiguousarray(hkl, np.float32)
