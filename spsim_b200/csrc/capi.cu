@@ -152,6 +152,29 @@ void spsim_internal_atomsf_row(int Z, float out[9]) {
 
 static unsigned long long g_next_id = 1;
 
+// A grow-only device buffer (no copies; swap hands a buffer to another owner).
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { cudaFree(p); }
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+  void swap(DevBuf &o) {
+    std::swap(p, o.p);
+    std::swap(cap, o.cap);
+  }
+};
+
 struct spsim_b200_molecule {
   unsigned long long id = 0;
   int device = 0;
@@ -168,6 +191,7 @@ struct spsim_b200_molecule {
   int er = 0, kr = 11;
   float dr = 1, inv_dr = 1;
   int per_atom_b = 0, delta_atoms = 0;
+  // device views of the buffers below
   float4 *d_atoms = nullptr;
   float4 *d_atoms2 = nullptr;  // pixel-pair layout of the same records
   AtomD *d_atomsd = nullptr;   // FP64-phase records
@@ -176,15 +200,18 @@ struct spsim_b200_molecule {
   float *d_wbase = nullptr;
   float *d_coeffs = nullptr;
   int *d_flags = nullptr;  // [0] range error
-  ~spsim_b200_molecule() {
-    cudaFree(d_atoms);
-    cudaFree(d_atoms2);
-    cudaFree(d_atomsd);
-    cudaFree(d_tiles);
-    cudaFree(d_perm);
-    cudaFree(d_wbase);
-    cudaFree(d_coeffs);
-    cudaFree(d_flags);
+  // owned device memory; a new molecule may take over a dropped one's buffers
+  DevBuf b_atoms, b_atoms2, b_atomsd, b_tiles, b_perm, b_wbase, b_coeffs, b_flags, b_inputs;
+  void take_buffers(spsim_b200_molecule &o) {
+    b_atoms.swap(o.b_atoms);
+    b_atoms2.swap(o.b_atoms2);
+    b_atomsd.swap(o.b_atomsd);
+    b_tiles.swap(o.b_tiles);
+    b_perm.swap(o.b_perm);
+    b_wbase.swap(o.b_wbase);
+    b_coeffs.swap(o.b_coeffs);
+    b_flags.swap(o.b_flags);
+    b_inputs.swap(o.b_inputs);
   }
 };
 
@@ -197,9 +224,12 @@ static int ceil_log2_bound(double x) {
   return e;
 }
 
+// recycle: a molecule about to be destroyed, whose device buffers (not in use
+// by queued work) the new one takes over instead of allocating its own.
 template <typename PosT>
 static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, const float *occ, const float *bfac,
-                                int delta_atoms, const float *beam, spsim_b200_molecule **out) {
+                                int delta_atoms, const float *beam, spsim_b200_molecule **out,
+                                spsim_b200_molecule *recycle = nullptr) {
   if (!out) return fail(SPSIM_ERR_INVALID_ARG, "out is NULL");
   *out = nullptr;
   if (natoms < 0) return fail(SPSIM_ERR_INVALID_ARG, "natoms < 0");
@@ -264,8 +294,6 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
   seg_begin.push_back(n_pad);
   m->n_padded = n_pad;
   m->perm.assign(n_pad, -1);
-  std::vector<float4> rec(2 * (size_t)std::max(n_pad, 1), make_float4(0, 0, 0, 0));
-  std::vector<AtomD> recd((size_t)std::max(n_pad, 1), AtomD{0.0, 0.0, 0.0, 0.0f, 0.0f});
   std::vector<float> wbase(std::max(n_pad, 1), 0.0f);
   {
     std::vector<int> fill(m->n_elem, 0);
@@ -276,7 +304,7 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
       const int e = slot_of_z[Z[j]];
       const int idx = seg_begin[e] + fill[e]++;
       m->perm[idx] = j;
-      // weight: occ * sqrt(illumination) (src/diffraction.c:223-235, :834), float like the reference
+      // weight: sqrt(illumination) (src/diffraction.c:223-235, :834), float like the reference
       float w = 1.0f;
       if (!delta_atoms) {
         float illum = 1.0f;
@@ -289,15 +317,6 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
         w = (float)std::sqrt((double)illum);
       }
       wbase[idx] = w;
-      const float o = occ ? occ[j] : 1.0f;
-      double r[3];
-      for (int k = 0; k < 3; ++k) r[k] = (double)pos[3 * j + k] - m->center[k];
-      const double hx = std::rint(r[0] * m->inv_dr) * m->dr;
-      const double hy = std::rint(r[1] * m->inv_dr) * m->dr;
-      const double hz = std::rint(r[2] * m->inv_dr) * m->dr;
-      rec[2 * idx] = make_float4((float)hx, (float)hy, (float)hz, o * w);
-      rec[2 * idx + 1] = make_float4((float)(r[0] - hx), (float)(r[1] - hy), (float)(r[2] - hz), bfac ? bfac[j] : 0.0f);
-      recd[idx] = AtomD{r[0], r[1], r[2], o * w, bfac ? bfac[j] : 0.0f};
     }
   }
   // tile table
@@ -311,36 +330,51 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
       m->tiles.push_back(t);
     }
   }
-  // upload
+  // device buffers (taken over from `recycle` where they are large enough)
+  if (recycle) m->take_buffers(*recycle);
   const size_t na = std::max(n_pad, 1);
-  CUDA_TRY(cudaMalloc(&m->d_atoms, 2 * na * sizeof(float4)));
-  CUDA_TRY(cudaMemcpy(m->d_atoms, rec.data(), 2 * na * sizeof(float4), cudaMemcpyHostToDevice));
-  {
-    std::vector<float4> dup(4 * na);
-    for (size_t j = 0; j < na; ++j) {
-      const float4 a0 = rec[2 * j], a1 = rec[2 * j + 1];
-      dup[4 * j] = make_float4(a0.x, a0.x, a0.y, a0.y);
-      dup[4 * j + 1] = make_float4(a0.z, a0.z, a0.w, a0.w);
-      dup[4 * j + 2] = make_float4(a1.x, a1.x, a1.y, a1.y);
-      dup[4 * j + 3] = make_float4(a1.z, a1.z, a1.w, a1.w);
-    }
-    CUDA_TRY(cudaMalloc(&m->d_atoms2, 4 * na * sizeof(float4)));
-    CUDA_TRY(cudaMemcpy(m->d_atoms2, dup.data(), 4 * na * sizeof(float4), cudaMemcpyHostToDevice));
+  const size_t nin = (size_t)std::max(natoms, 1);
+  const size_t in_pos = 3 * nin * sizeof(PosT), in_occ = nin * sizeof(float);
+  const size_t in_bytes = in_pos + (occ ? in_occ : 0) + (bfac ? in_occ : 0);
+  CUDA_TRY(m->b_atoms.ensure(2 * na * sizeof(float4)));
+  CUDA_TRY(m->b_atoms2.ensure(4 * na * sizeof(float4)));
+  CUDA_TRY(m->b_atomsd.ensure(na * sizeof(AtomD)));
+  CUDA_TRY(m->b_tiles.ensure(std::max<size_t>(m->tiles.size(), 1) * sizeof(TileDesc)));
+  CUDA_TRY(m->b_perm.ensure(na * sizeof(int)));
+  CUDA_TRY(m->b_wbase.ensure(na * sizeof(float)));
+  CUDA_TRY(m->b_coeffs.ensure(std::max<size_t>(m->coeffs.size(), 1) * sizeof(float)));
+  CUDA_TRY(m->b_flags.ensure(4 * sizeof(int)));
+  CUDA_TRY(m->b_inputs.ensure(std::max<size_t>(in_bytes, 16)));
+  m->d_atoms = (float4 *)m->b_atoms.p;
+  m->d_atoms2 = (float4 *)m->b_atoms2.p;
+  m->d_atomsd = (AtomD *)m->b_atomsd.p;
+  m->d_tiles = (TileDesc *)m->b_tiles.p;
+  m->d_perm = (int *)m->b_perm.p;
+  m->d_wbase = (float *)m->b_wbase.p;
+  m->d_coeffs = (float *)m->b_coeffs.p;
+  m->d_flags = (int *)m->b_flags.p;
+  // upload the caller's arrays and the host-built tables; the records are
+  // built on the device (atoms_build_kernel, the host's arithmetic)
+  char *din = (char *)m->b_inputs.p;
+  const PosT *d_pos = (const PosT *)din;
+  const float *d_occ = occ ? (const float *)(din + in_pos) : nullptr;
+  const float *d_bfac = bfac ? (const float *)(din + in_pos + (occ ? in_occ : 0)) : nullptr;
+  if (natoms > 0) {
+    CUDA_TRY(cudaMemcpy(din, pos, 3 * (size_t)natoms * sizeof(PosT), cudaMemcpyHostToDevice));
+    if (occ) CUDA_TRY(cudaMemcpy((void *)d_occ, occ, (size_t)natoms * sizeof(float), cudaMemcpyHostToDevice));
+    if (bfac) CUDA_TRY(cudaMemcpy((void *)d_bfac, bfac, (size_t)natoms * sizeof(float), cudaMemcpyHostToDevice));
   }
-  CUDA_TRY(cudaMalloc(&m->d_atomsd, na * sizeof(AtomD)));
-  CUDA_TRY(cudaMemcpy(m->d_atomsd, recd.data(), na * sizeof(AtomD), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMalloc(&m->d_tiles, std::max<size_t>(m->tiles.size(), 1) * sizeof(TileDesc)));
   if (!m->tiles.empty())
     CUDA_TRY(cudaMemcpy(m->d_tiles, m->tiles.data(), m->tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMalloc(&m->d_perm, na * sizeof(int)));
   if (n_pad) CUDA_TRY(cudaMemcpy(m->d_perm, m->perm.data(), n_pad * sizeof(int), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMalloc(&m->d_wbase, na * sizeof(float)));
   CUDA_TRY(cudaMemcpy(m->d_wbase, wbase.data(), na * sizeof(float), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMalloc(&m->d_coeffs, std::max<size_t>(m->coeffs.size(), 1) * sizeof(float)));
   if (!m->coeffs.empty())
     CUDA_TRY(cudaMemcpy(m->d_coeffs, m->coeffs.data(), m->coeffs.size() * sizeof(float), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMalloc(&m->d_flags, 4 * sizeof(int)));
   CUDA_TRY(cudaMemset(m->d_flags, 0, 4 * sizeof(int)));
+  CUDA_TRY(launch_atoms_build<PosT>(m->d_atoms, m->d_atoms2, m->d_atomsd, m->d_perm, n_pad, d_pos, d_occ, d_bfac,
+                                    m->d_wbase, m->center, (double)m->dr, (double)m->inv_dr, nullptr));
+  // complete before return, so that work on any stream (non-blocking ones too) sees the records
+  CUDA_TRY(cudaStreamSynchronize(nullptr));
   *out = m.release();
   return SPSIM_OK;
 }
@@ -527,20 +561,6 @@ extern "C" int spsim_b200_qset_destroy(spsim_b200_qset *qs) {
 // ---------------------------------------------------------------------------
 // forward planning
 
-struct DevBuf {
-  void *p = nullptr;
-  size_t cap = 0;
-  ~DevBuf() { cudaFree(p); }
-  cudaError_t ensure(size_t bytes) {
-    if (bytes <= cap) return cudaSuccess;
-    cudaFree(p);
-    p = nullptr;
-    cap = 0;
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e == cudaSuccess) cap = bytes;
-    return e;
-  }
-};
 
 // A polychromatic forward: the plan's npat patterns are the wavelength
 // samples of one detector (phase-space scales qscale[j]); their amplitudes are
@@ -1142,12 +1162,14 @@ static int host_session_molecule(int natoms, const int32_t *Z, const float *pos,
     return SPSIM_OK;
   }
   spsim_b200_molecule *m = nullptr;
-  int st = spsim_b200_molecule_create(natoms, Z, pos, occ, bfac, delta_atoms, beam, &m);
+  // the kept molecule's records may still be read by queued work: wait, then
+  // hand its device buffers to the new molecule
+  if (g_host.mol) CUDA_TRY(cudaDeviceSynchronize());
+  int st = molecule_create_impl<float>(natoms, Z, pos, occ, bfac, delta_atoms, beam, &m, g_host.mol);
+  if (g_host.mol) spsim_b200_molecule_destroy(g_host.mol);
+  g_host.mol = nullptr;
+  g_host.mol_inputs.clear();
   if (st) return st;
-  if (g_host.mol) {
-    cudaDeviceSynchronize();  // its records may still be read by queued work
-    spsim_b200_molecule_destroy(g_host.mol);
-  }
   g_host.mol = m;
   g_host.mol_inputs.swap(key);
   *out = m;

@@ -111,6 +111,8 @@ int spsim_internal_rotate_hkl(int64_t npix, const float R[9], float *hkl_dev);
  * released by spsim_b200_release_scratch). */
 static void *g_pinned = NULL;
 static size_t g_pinned_bytes = 0;
+static cudaStream_t g_copy_stream = NULL; /* non-blocking side stream of simulate_shot */
+static int g_copy_stream_device = -1;
 
 static void *pinned_alloc(size_t bytes) {
   if (g_pinned && g_pinned_bytes >= bytes) return g_pinned;
@@ -135,55 +137,73 @@ void spsim_b200_release_scratch(void) {
   if (g_pinned) cudaFreeHost(g_pinned);
   g_pinned = NULL;
   g_pinned_bytes = 0;
+  if (g_copy_stream && g_copy_stream_device == dev) cudaStreamDestroy(g_copy_stream);
+  g_copy_stream = NULL;
+  g_copy_stream_device = -1;
   spsim_internal_release_host_session();
 }
 
-/* Host copies and first touches of large arrays, split over a few threads. */
+/* Host copies and first touches of large arrays: a batch of (dst, src, bytes)
+ * jobs (src NULL: fill with zeros, the first touch of fresh pages) cut into
+ * equal byte ranges over a few threads. */
 typedef struct {
   char *dst;
-  const char *src; /* NULL: fill with zeros (first touch of fresh pages) */
+  const char *src;
   size_t bytes;
 } HostCopy;
 
+typedef struct {
+  const HostCopy *jobs;
+  int njobs;
+  size_t begin, end; /* byte range of the concatenated jobs */
+} HostCopyRange;
+
 static void *host_copy_worker(void *arg) {
-  HostCopy *c = (HostCopy *)arg;
-  if (c->src)
-    memcpy(c->dst, c->src, c->bytes);
-  else
-    memset(c->dst, 0, c->bytes);
+  const HostCopyRange *r = (const HostCopyRange *)arg;
+  size_t base = 0;
+  for (int j = 0; j < r->njobs; j++) {
+    const HostCopy *c = &r->jobs[j];
+    const size_t lo = r->begin > base ? r->begin - base : 0;
+    const size_t hi = r->end - base < c->bytes ? r->end - base : c->bytes;
+    if (r->end > base && lo < hi && lo < c->bytes) {
+      if (c->src)
+        memcpy(c->dst + lo, c->src + lo, hi - lo);
+      else
+        memset(c->dst + lo, 0, hi - lo);
+    }
+    base += c->bytes;
+    if (base >= r->end) break;
+  }
   return NULL;
 }
 
-static void host_copy(void *dst, const void *src, size_t bytes) {
+static void host_copy_batch(const HostCopy *jobs, int njobs) {
   enum { MAX_THREADS = 8 };
+  size_t total = 0;
+  for (int j = 0; j < njobs; j++) total += jobs[j].bytes;
   long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
-  int nt = (int)(bytes >> 21); /* one thread per 2 MiB */
+  int nt = (int)(total >> 21); /* one thread per 2 MiB */
   if (nt > MAX_THREADS) nt = MAX_THREADS;
   if (nt > ncpu) nt = (int)ncpu;
-  if (nt < 2) {
-    if (src)
-      memcpy(dst, src, bytes);
-    else
-      memset(dst, 0, bytes);
-    return;
-  }
+  if (nt < 1) nt = 1;
   pthread_t th[MAX_THREADS];
-  HostCopy job[MAX_THREADS];
+  HostCopyRange rg[MAX_THREADS];
   int started[MAX_THREADS] = {0};
-  const size_t chunk = (bytes / nt + 4095) & ~(size_t)4095;
+  const size_t chunk = (total / nt + 4095) & ~(size_t)4095;
   for (int t = 0; t < nt; t++) {
-    const size_t off = (size_t)t * chunk;
-    job[t].dst = (char *)dst + (off < bytes ? off : bytes);
-    job[t].src = src ? (const char *)src + (off < bytes ? off : bytes) : NULL;
-    job[t].bytes = off < bytes ? (bytes - off < chunk ? bytes - off : chunk) : 0;
-    started[t] = t > 0 && pthread_create(&th[t], NULL, host_copy_worker, &job[t]) == 0;
+    rg[t].jobs = jobs;
+    rg[t].njobs = njobs;
+    rg[t].begin = (size_t)t * chunk < total ? (size_t)t * chunk : total;
+    rg[t].end = (size_t)(t + 1) * chunk < total ? (size_t)(t + 1) * chunk : total;
+    if (t == nt - 1) rg[t].end = total;
+    started[t] = t > 0 && pthread_create(&th[t], NULL, host_copy_worker, &rg[t]) == 0;
   }
-  host_copy_worker(&job[0]);
+  host_copy_worker(&rg[0]);
   for (int t = 1; t < nt; t++) {
     if (started[t])
       pthread_join(th[t], NULL);
     else
-      host_copy_worker(&job[t]);
+      host_copy_worker(&rg[t]);
   }
 }
 
@@ -584,11 +604,21 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   cudaError_t e = cudaEventCreateWithFlags(&ev_hkl, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming);
   if (e != cudaSuccess) cuda_die("cudaEventCreate", e);
-  if (n > 0) {
-    e = cudaMemcpyAsync(s_hkl, d_hkl, b_hkl, cudaMemcpyDeviceToHost, 0);
-    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync HKL", e);
+  /* the HKL list goes down on a side stream, beside the structure factor */
+  int cur_dev = 0;
+  cudaGetDevice(&cur_dev);
+  if (!g_copy_stream || g_copy_stream_device != cur_dev) { /* a stream left on another device is kept */
+    e = cudaStreamCreateWithFlags(&g_copy_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) cuda_die("cudaStreamCreate", e);
+    g_copy_stream_device = cur_dev;
   }
   cudaEventRecord(ev_hkl, 0);
+  cudaStreamWaitEvent(g_copy_stream, ev_hkl, 0);
+  if (n > 0) {
+    e = cudaMemcpyAsync(s_hkl, d_hkl, b_hkl, cudaMemcpyDeviceToHost, g_copy_stream);
+    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync HKL", e);
+  }
+  cudaEventRecord(ev_hkl, g_copy_stream);
 
   /* structure factor (compute_sf, src/spsim.c:110-144): the CUDA dispatch decides the spectrum */
   const int spectrum = opts->use_cuda != 0 && opts->use_cuda != 2;
@@ -642,16 +672,22 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   pattern->rot = rot;
   float **dst[7] = {&det->thomson_correction, &det->solid_angle, &det->photons_per_pixel, &det->photon_count,
                     &det->electrons_per_pixel, &det->real_output, &det->noiseless_output};
+  HostCopy out[9];
+  out[0] = (HostCopy){(char *)pattern->F, s_F, b_F};
+  out[1] = (HostCopy){(char *)pattern->ints, s_I, b_I};
   for (int k = 0; k < 7; k++) {
     const size_t b = k < 5 ? b_I : b_nb;
     *dst[k] = (float *)host_alloc(b > 0 ? b : sizeof(float));
-    host_copy(*dst[k], NULL, b);
+    out[2 + k] = (HostCopy){(char *)*dst[k], s_chain + (k < 5 ? k * b_I : 5 * b_I + (k - 5) * b_nb), b};
   }
-  host_copy(pattern->F, NULL, b_F);
-  host_copy(pattern->ints, NULL, b_I);
+  HostCopy touch[10];
+  for (int k = 0; k < 9; k++) touch[k] = (HostCopy){out[k].dst, NULL, out[k].bytes};
+  touch[9] = (HostCopy){(char *)pattern->HKL_list, NULL, b_hkl};
+  host_copy_batch(touch, 10);
   e = cudaEventSynchronize(ev_hkl);
   if (e != cudaSuccess) cuda_die("simulate_shot HKL copy", e);
-  host_copy(pattern->HKL_list, s_hkl, b_hkl);
+  const HostCopy hk = {(char *)pattern->HKL_list, s_hkl, b_hkl};
+  host_copy_batch(&hk, 1);
 
   e = cudaEventSynchronize(ev_out);
   if (e != cudaSuccess) cuda_die("simulate_shot outputs", e);
@@ -659,12 +695,7 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   cudaEventDestroy(ev_out);
   st = spsim_internal_shot_check();
   if (st) die("simulate_shot structure factor", st);
-  host_copy(pattern->F, s_F, b_F);
-  host_copy(pattern->ints, s_I, b_I);
-  for (int k = 0; k < 7; k++) {
-    const size_t b = k < 5 ? b_I : b_nb;
-    host_copy(*dst[k], s_chain + (k < 5 ? k * b_I : 5 * b_I + (k - 5) * b_nb), b);
-  }
+  host_copy_batch(out, 9);
   if (opts->verbosity_level > 0) /* src/diffraction.c:849-851 */
     printf("%g atoms.pixel/s\n", 1.0e6 * n * mol->natoms / (now_us() - t0));
   g_pattern_counter++;

@@ -1168,6 +1168,61 @@ __global__ void atoms_update_kernel(float4 *__restrict__ atoms, float4 *__restri
   atomsd[j] = AtomD{r[0], r[1], r[2], a0.w, a1.w};
 }
 
+// Molecule creation on the device: the atom records of padded atom j from the
+// caller's positions (atom perm[j]; perm < 0 is segment padding, all zero),
+// with the host's arithmetic: r = pos - centre in FP64, the coarse part
+// rint(r / dr) dr and the remainder, the weight occ * wbase in float.
+template <typename PosT>
+__global__ void atoms_build_kernel(float4 *__restrict__ atoms, float4 *__restrict__ atoms2, AtomD *__restrict__ atomsd,
+                                   const int *__restrict__ perm, int n_padded, const PosT *__restrict__ pos,
+                                   const float *__restrict__ occ, const float *__restrict__ bfac,
+                                   const float *__restrict__ wbase, double cx, double cy, double cz, double dr,
+                                   double inv_dr) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_padded) return;
+  const int src = perm[j];
+  if (src < 0) {
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    atoms[2 * j] = atoms[2 * j + 1] = z;
+    atoms2[4 * j] = atoms2[4 * j + 1] = atoms2[4 * j + 2] = atoms2[4 * j + 3] = z;
+    atomsd[j] = AtomD{0.0, 0.0, 0.0, 0.0f, 0.0f};
+    return;
+  }
+  const double r0 = __dsub_rn((double)pos[3 * src], cx);
+  const double r1 = __dsub_rn((double)pos[3 * src + 1], cy);
+  const double r2 = __dsub_rn((double)pos[3 * src + 2], cz);
+  const double hx = __dmul_rn(rint(__dmul_rn(r0, inv_dr)), dr);
+  const double hy = __dmul_rn(rint(__dmul_rn(r1, inv_dr)), dr);
+  const double hz = __dmul_rn(rint(__dmul_rn(r2, inv_dr)), dr);
+  const float w = __fmul_rn(occ ? occ[src] : 1.0f, wbase[j]);
+  const float b = bfac ? bfac[src] : 0.0f;
+  const float4 a0 = make_float4((float)hx, (float)hy, (float)hz, w);
+  const float4 a1 = make_float4((float)__dsub_rn(r0, hx), (float)__dsub_rn(r1, hy), (float)__dsub_rn(r2, hz), b);
+  atoms[2 * j] = a0;
+  atoms[2 * j + 1] = a1;
+  atoms2[4 * j] = make_float4(a0.x, a0.x, a0.y, a0.y);
+  atoms2[4 * j + 1] = make_float4(a0.z, a0.z, a0.w, a0.w);
+  atoms2[4 * j + 2] = make_float4(a1.x, a1.x, a1.y, a1.y);
+  atoms2[4 * j + 3] = make_float4(a1.z, a1.z, a1.w, a1.w);
+  atomsd[j] = AtomD{r0, r1, r2, w, b};
+}
+
+template <typename PosT>
+cudaError_t launch_atoms_build(float4 *atoms, float4 *atoms2, AtomD *atomsd, const int *perm, int n_padded,
+                               const PosT *pos, const float *occ, const float *bfac, const float *wbase,
+                               const double c[3], double dr, double inv_dr, cudaStream_t st) {
+  if (n_padded <= 0) return cudaSuccess;
+  atoms_build_kernel<PosT><<<(n_padded + 255) / 256, 256, 0, st>>>(atoms, atoms2, atomsd, perm, n_padded, pos, occ,
+                                                                  bfac, wbase, c[0], c[1], c[2], dr, inv_dr);
+  return cudaGetLastError();
+}
+template cudaError_t launch_atoms_build<float>(float4 *, float4 *, AtomD *, const int *, int, const float *,
+                                               const float *, const float *, const float *, const double[3], double,
+                                               double, cudaStream_t);
+template cudaError_t launch_atoms_build<double>(float4 *, float4 *, AtomD *, const int *, int, const double *,
+                                                const float *, const float *, const float *, const double[3], double,
+                                                double, cudaStream_t);
+
 // ---------------------------------------------------------------------------
 // launch wrappers
 

@@ -33,6 +33,12 @@ cudaError_t pair_step(const float *hkl, const double *q64, long long npix, doubl
 cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st);
 cudaError_t launch_ewald(int nx, int ny, double width, double height, double distance, double cx, double cy,
                          double wavelength, int spherical, float *out32, double *out64, cudaStream_t st);
+// Atom records of a new molecule from the caller's positions (float or double),
+// arithmetic identical to the host's record building.
+template <typename PosT>
+cudaError_t launch_atoms_build(float4 *atoms, float4 *atoms2, AtomD *atomsd, const int *perm, int n_padded,
+                               const PosT *pos, const float *occ, const float *bfac, const float *wbase,
+                               const double c[3], double dr, double inv_dr, cudaStream_t st);
 cudaError_t launch_atoms_update(float4 *atoms, float4 *atoms2, AtomD *atomsd, const int *perm, int n_padded, const float *pos32,
                                 const double *pos64, const float *occ, const float *bfac, const float *wbase,
                                 const double c[3], float dr, float inv_dr, double rbound, int *range_err,
