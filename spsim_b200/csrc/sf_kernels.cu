@@ -1390,16 +1390,33 @@ cudaError_t launch_crystal(long long npix, const float *hkl, const double cell[9
 
 // Largest |q[2m+1] - q[2m]| over the pixel pairs of a q set (float or FP64
 // list), as the bits of a non-negative double (which order like integers).
-__global__ void pair_step_kernel(const float *__restrict__ hkl, const double *__restrict__ q64, long long npix,
-                                 unsigned long long *__restrict__ out) {
+// Block-wide maximum of a non-negative double (256 threads), then one atomic
+// per block on its bits: a million same-address atomics would serialise.
+__device__ __forceinline__ void block_max_to(double v, unsigned long long *out) {
+  __shared__ double wmax[8];
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = wmax[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) pair_step_kernel(const float *__restrict__ hkl, const double *__restrict__ q64,
+                                                        long long npix, unsigned long long *__restrict__ out) {
   const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (2 * m + 1 >= npix) return;
-  double d[3];
-  for (int c = 0; c < 3; ++c)
-    d[c] = hkl ? (double)hkl[3 * (2 * m + 1) + c] - (double)hkl[3 * (2 * m) + c]
-               : q64[3 * (2 * m + 1) + c] - q64[3 * (2 * m) + c];
-  const double n = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-  atomicMax(out, (unsigned long long)__double_as_longlong(n));
+  double n = 0.0;
+  if (2 * m + 1 < npix) {
+    double d[3];
+    for (int c = 0; c < 3; ++c)
+      d[c] = hkl ? (double)hkl[3 * (2 * m + 1) + c] - (double)hkl[3 * (2 * m) + c]
+                 : q64[3 * (2 * m + 1) + c] - q64[3 * (2 * m) + c];
+    n = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  }
+  block_max_to(n, out);
 }
 
 cudaError_t pair_step(const float *hkl, const double *q64, long long npix, double *step) {
@@ -1452,20 +1469,22 @@ cudaError_t launch_rotate_hkl(long long n, const float R[9], float *hkl, cudaStr
 
 // Largest |q|^2 and largest |q[2m+1] - q[2m]|^2 of a float HKL list, as the
 // bits of non-negative doubles (which order like integers) in out[0], out[1].
-__global__ void qset_stats_kernel(const float *__restrict__ hkl, long long npix, unsigned long long *__restrict__ out) {
+__global__ void __launch_bounds__(256) qset_stats_kernel(const float *__restrict__ hkl, long long npix,
+                                                         unsigned long long *__restrict__ out) {
   const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (2 * m >= npix) return;
-  double a[3], b[3];
-  for (int c = 0; c < 3; ++c) a[c] = hkl[3 * (2 * m) + c];
-  double qq = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
-  double dd = 0.0;
-  if (2 * m + 1 < npix) {
-    for (int c = 0; c < 3; ++c) b[c] = hkl[3 * (2 * m + 1) + c];
-    qq = fmax(qq, b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
-    dd = (b[0] - a[0]) * (b[0] - a[0]) + (b[1] - a[1]) * (b[1] - a[1]) + (b[2] - a[2]) * (b[2] - a[2]);
+  double qq = 0.0, dd = 0.0;
+  if (2 * m < npix) {
+    double a[3], b[3];
+    for (int c = 0; c < 3; ++c) a[c] = hkl[3 * (2 * m) + c];
+    qq = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+    if (2 * m + 1 < npix) {
+      for (int c = 0; c < 3; ++c) b[c] = hkl[3 * (2 * m + 1) + c];
+      qq = fmax(qq, b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+      dd = (b[0] - a[0]) * (b[0] - a[0]) + (b[1] - a[1]) * (b[1] - a[1]) + (b[2] - a[2]) * (b[2] - a[2]);
+    }
   }
-  atomicMax(out, (unsigned long long)__double_as_longlong(qq));
-  atomicMax(out + 1, (unsigned long long)__double_as_longlong(dd));
+  block_max_to(qq, out);
+  block_max_to(dd, out + 1);
 }
 
 cudaError_t qset_stats(const float *hkl, long long npix, unsigned long long *scratch2, double *qmax, double *step,
