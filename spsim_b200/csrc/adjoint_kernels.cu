@@ -186,29 +186,45 @@ __global__ void __launch_bounds__(NT) adj_kernel(AdjParams prm) {
 
 // FP64-phase adjoint: the phase u = q.(r - c) and its half-cycle reduction in
 // FP64 (as in the FP64-phase forward), sin/cos and the five gradient sums in
-// packed f32x2 over pairs of atoms.  Each thread holds A atoms (A/2 pairs) in
-// registers; a CTA streams pixel records through shared memory:
-//   pq[2i]   = {qx, qy}  pq[2i+1] = {qz, 0}          (FP64)
-//   pf[2i]   = {qx, qy, qz, hr}  pf[2i+1] = {hi, s2, s2n, 0}   (FP32)
-// Per term the sign (-1)^k of the half-cycle reduction is applied to the two
-// products z = H conj(A) e^{-2 pi i u} with one integer multiply-add each.
+// packed f32x2 over pairs of atoms.  Each thread holds A consecutive atoms
+// (A/2 pairs, one element) in registers; a CTA's block of atoms spans at most
+// two element segments, and the CTA streams the pixel records of each of its
+// elements through shared memory.  With the
+// fixed-point phase word (FIXW), H = |H| e^{i phi} enters as a phase and a
+// magnitude, so the polynomial's cos / sin are the products z themselves:
+//   pq[2i]   = {2 qx, 2 qy}  pq[2i+1] = {2 qz, word constant + phi / pi}   (FP64)
+//   pf[2i]   = {|H| qx, |H| qy, |H| qz, |H|}  pf[2i+1] = {|H| s2, s2n, 0, 0}   (FP32)
+// and otherwise (FP64 rounding reduction, phases beyond 2^17 cycles)
+//   pq[2i]   = {qx, qy}  pq[2i+1] = {qz, 0}
+//   pf[2i]   = {qx, qy, qz, hr}  pf[2i+1] = {hi, s2, s2n, 0}
+// with z = H conj(A) e^{-2 pi i u} formed per term.  The sign (-1)^k of the
+// half-cycle reduction is applied to the two products with one integer
+// multiply-add each.
 template <int NT, int A, bool PERB, bool FIXW>
 __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t m31) {
   static_assert(A % 2 == 0, "atoms per thread must be even");
   constexpr int NP = A / 2;
-  __shared__ __align__(16) double2 pq[ADJ_PIX_TILE * 2];
-  __shared__ __align__(16) float4 pf[ADJ_PIX_TILE * 2];
+  // pixel records of the block's (at most two) elements
+  __shared__ __align__(16) double2 pq_all[2][ADJ_PIX_TILE * 2];
+  __shared__ __align__(16) float4 pf_all[2][ADJ_PIX_TILE * 2];
   const int tid = threadIdx.x;
   const AdjItem item = prm.items[blockIdx.x];
   const AdjBlock blk = prm.blocks[item.block];
   const double M52 = 6755399441055744.0;  // 1.5 * 2^52
+  // this thread's A consecutive atoms lie in one element segment (segments are
+  // padded to multiples of 8, blocks start and split on multiples of A)
+  const int a_first = blk.atom_begin + A * tid;
+  const int slot = (blk.elem2 >= 0 && a_first >= blk.split) ? 1 : 0;
+  const int nslot = blk.elem2 >= 0 ? 2 : 1;
+  const double2 *__restrict__ pq = pq_all[slot];
+  const float4 *__restrict__ pf = pf_all[slot];
 
   double rx[A], ry[A], rz[A];
   float bfac[A];
   int aidx[A];
 #pragma unroll
   for (int k = 0; k < A; ++k) {
-    aidx[k] = blk.atom_begin + tid + k * NT;
+    aidx[k] = a_first + k;
     rx[k] = ry[k] = rz[k] = 0.0;
     bfac[k] = 0.0f;
     if (aidx[k] < blk.atom_end) {
@@ -226,15 +242,28 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
   for (long long base = item.pix_begin; base < item.pix_end; base += ADJ_PIX_TILE) {
     const int n = (int)min((long long)ADJ_PIX_TILE, item.pix_end - base);
     __syncthreads();
-    for (int i = tid; i < ADJ_PIX_TILE; i += NT) {
+    for (int c = tid; c < ADJ_PIX_TILE * nslot; c += NT) {
+      const int i = c % ADJ_PIX_TILE, sl = c / ADJ_PIX_TILE;
+      double2 *__restrict__ pq = pq_all[sl];
+      float4 *__restrict__ pf = pf_all[sl];
       double q[3] = {0.0, 0.0, 0.0}, hr = 0.0, hi = 0.0, s2 = 0.0;
-      if (i < n) adj_pixel(prm, blk.elem, base + i, q, hr, hi, s2);
-      // FIXW: the phase word takes 2 q (half-cycle reduction)
-      const double qs = FIXW ? 2.0 : 1.0;
-      pq[2 * i] = make_double2(qs * q[0], qs * q[1]);
-      pq[2 * i + 1] = make_double2(qs * q[2], 0.0);
-      pf[2 * i] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)hr);
-      pf[2 * i + 1] = make_float4((float)hi, (float)s2, (float)(-s2 * 1.4426950408889634), 0.0f);
+      if (i < n) adj_pixel(prm, sl ? blk.elem2 : blk.elem, base + i, q, hr, hi, s2);
+      if (FIXW) {
+        // H = |H| e^{i phi}: H e^{2 pi i u} = |H| e^{2 pi i (u + phi / 2 pi)}, so the
+        // pixel's phase goes into the phase word's constant (2 q and 2 u + phi / pi
+        // + 1/2 + 1.5 * 2^20, the half-cycle reduction) and |H| into its factors
+        const double mag = hypot(hr, hi);
+        const double phi = mag > 0.0 ? atan2(hi, hr) : 0.0;
+        pq[2 * i] = make_double2(2.0 * q[0], 2.0 * q[1]);
+        pq[2 * i + 1] = make_double2(2.0 * q[2], PHASE_WORD_BASE_HALF + phi * 0.31830988618379067);
+        pf[2 * i] = make_float4((float)(mag * q[0]), (float)(mag * q[1]), (float)(mag * q[2]), (float)mag);
+        pf[2 * i + 1] = make_float4((float)(mag * s2), (float)(-s2 * 1.4426950408889634), 0.0f, 0.0f);
+      } else {
+        pq[2 * i] = make_double2(q[0], q[1]);
+        pq[2 * i + 1] = make_double2(q[2], 0.0);
+        pf[2 * i] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)hr);
+        pf[2 * i + 1] = make_float4((float)hi, (float)s2, (float)(-s2 * 1.4426950408889634), 0.0f);
+      }
     }
     __syncthreads();
     // sums of z_i = -Im part (so that dL/dr = -4 pi w sum z_i q) and z_r
@@ -244,6 +273,36 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
     for (int i = 0; i < n; ++i) {
       const double2 qa = pq[2 * i], qb = pq[2 * i + 1];
       const float4 f0 = pf[2 * i], f1 = pf[2 * i + 1];
+      if (FIXW) {
+        // cos / sin of 2 pi (u + phi / 2 pi), signed by the half-cycle parity, are
+        // z_r / |H| and -Im / |H|: the five sums take them with |H|-scaled factors
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          float y[2];
+          uint32_t kb[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int k = 2 * j + h;
+            const double t = phase_word(qa.x, qa.y, qb.x, rx[k], ry[k], rz[k], qb.y);
+            reduce_phase_word<PREC_MODE_POLY>(t, y[h], kb[h]);
+          }
+          float2 S, C;
+          sincos_dhalf_poly2(mul2(make_float2(y[0], y[1]), f2(word_to_cycles<PREC_MODE_POLY>())), S, C);
+          float2 zr = make_float2(sign_by_parity(C.x, kb[0], m31), sign_by_parity(C.y, kb[1], m31));
+          float2 zn = make_float2(sign_by_parity(S.x, kb[0], m31), sign_by_parity(S.y, kb[1], m31));
+          if (PERB) {
+            const float2 E = make_float2(exp2f(bfac[2 * j] * f1.y), exp2f(bfac[2 * j + 1] * f1.y));
+            zr = mul2(zr, E);
+            zn = mul2(zn, E);
+          }
+          fx[j] = fma2(zn, f2(f0.x), fx[j]);
+          fy[j] = fma2(zn, f2(f0.y), fy[j]);
+          fz[j] = fma2(zn, f2(f0.z), fz[j]);
+          fo[j] = fma2(zr, f2(f0.w), fo[j]);
+          fb[j] = fma2(zr, f2(f1.x), fb[j]);
+        }
+        continue;
+      }
       const float2 hr = f2(f0.w), nhi = f2(-f1.x), hi = f2(f1.x);
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
@@ -252,10 +311,7 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int k = 2 * j + h;
-          if (FIXW) {
-            const double t = phase_word(qa.x, qa.y, qb.x, rx[k], ry[k], rz[k], PHASE_WORD_BASE_HALF);
-            reduce_phase_word<PREC_MODE_POLY>(t, y[h], kb[h]);
-          } else {
+          {
             double u = qa.x * rx[k];
             u = fma(qa.y, ry[k], u);
             u = fma(qb.x, rz[k], u);
@@ -265,8 +321,7 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
           }
         }
         float2 S, C;
-        const float2 yy = make_float2(y[0], y[1]);
-        sincos_dhalf_poly2(FIXW ? mul2(yy, f2(word_to_cycles<PREC_MODE_POLY>())) : yy, S, C);
+        sincos_dhalf_poly2(make_float2(y[0], y[1]), S, C);
         // H conj(A) e^{-2 pi i u} = (hr C - hi S) - i (hr S + hi C), times (-1)^k
         float2 zr = fma2(nhi, S, mul2(hr, C));
         float2 zn = fma2(hi, C, mul2(hr, S));  // = -Im

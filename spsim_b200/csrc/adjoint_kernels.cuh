@@ -11,8 +11,11 @@ constexpr int ADJ_BLOCK_ATOMS = ADJ_THREADS * ADJ_ATOMS_PER_THREAD;
 constexpr int ADJ_DPHASE_ATOMS_PER_THREAD = 4;
 constexpr int ADJ_DPHASE_BLOCK_ATOMS = ADJ_THREADS * ADJ_DPHASE_ATOMS_PER_THREAD;
 
-struct AdjBlock {   // atoms [atom_begin, atom_end) of one element
-  int atom_begin, atom_end, elem, pad;
+// atoms [atom_begin, atom_end): of element `elem`, or, in the FP64-phase
+// adjoint's blocks, of `elem` below `split` and of `elem2` from `split` on
+// (elem2 < 0: one element)
+struct AdjBlock {
+  int atom_begin, atom_end, elem, elem2, split, pad;
 };
 
 struct AdjItem {    // one CTA: an atom block x a range of (pattern, pixel) indices

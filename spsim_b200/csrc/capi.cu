@@ -1692,24 +1692,49 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   if (dB_dev) CUDA_TRY(cudaMemsetAsync(dB_dev, 0, (size_t)m->natoms_in * sizeof(double), st));
   if (m->n_kept == 0 || total == 0) return SPSIM_OK;
 
-  // atom blocks (single element each) x pixel chunks
+  // atom blocks x pixel chunks.  The FP64-phase adjoint's blocks are
+  // consecutive runs of the element-sorted atoms that may span two element
+  // segments (each thread's atoms stay in one), so short segments do not leave
+  // blocks mostly empty; the other adjoints take one element per block.
   const int block_atoms =
       precision == SPSIM_PREC_FP64 ? ADJ_THREADS : (dphase ? ADJ_DPHASE_BLOCK_ATOMS : ADJ_BLOCK_ATOMS);
   std::vector<AdjBlock> blocks;
   {
+    struct Seg {
+      int elem, begin, end;
+    };
+    std::vector<Seg> segs;
     int e = -1, seg0 = 0;
     for (size_t k = 0; k <= m->tiles.size(); ++k) {
       const bool end = k == m->tiles.size();
       if (end || m->tiles[k].elem != e) {
-        if (e >= 0) {
-          const int seg1 = m->tiles[k - 1].atom_begin + m->tiles[k - 1].count;
-          for (int a = seg0; a < seg1; a += block_atoms) blocks.push_back({a, std::min(a + block_atoms, seg1), e, 0});
-        }
+        if (e >= 0) segs.push_back({e, seg0, m->tiles[k - 1].atom_begin + m->tiles[k - 1].count});
         if (!end) {
           e = m->tiles[k].elem;
           seg0 = m->tiles[k].atom_begin;
         }
       }
+    }
+    if (dphase) {
+      size_t s0 = 0;
+      int a = segs.empty() ? 0 : segs[0].begin;
+      while (s0 < segs.size()) {
+        AdjBlock b = {a, std::min(a + block_atoms, segs[s0].end), segs[s0].elem, -1, 0, 0};
+        b.split = b.atom_end;
+        if (b.atom_end == segs[s0].end && b.atom_end - a < block_atoms && s0 + 1 < segs.size()) {
+          // fill the rest of the block from the next segment (segments are contiguous)
+          b.elem2 = segs[s0 + 1].elem;
+          b.split = segs[s0 + 1].begin;
+          b.atom_end = std::min(a + block_atoms, segs[s0 + 1].end);
+        }
+        blocks.push_back(b);
+        a = b.atom_end;
+        while (s0 < segs.size() && a >= segs[s0].end) ++s0;
+      }
+    } else {
+      for (const Seg &sg : segs)
+        for (int a = sg.begin; a < sg.end; a += block_atoms)
+          blocks.push_back({a, std::min(a + block_atoms, sg.end), sg.elem, -1, std::min(a + block_atoms, sg.end), 0});
     }
   }
   const long long want = 8LL * num_sms();

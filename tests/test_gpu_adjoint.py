@@ -105,3 +105,25 @@ def test_refinement_positions_update_in_place(cuda):
     F, I = core.forward(mol, qs, rot=R[0])
     F64, I64 = O.structure_factor(Z, shifted, q)
     assert np.max(np.abs(I.cpu().numpy() - I64) / np.maximum(I64, 1e-3 * I64.mean())) < 1e-5
+
+
+def test_adjoint_wide_phase_range_uses_fp64_rounding(cuda):
+    # |q|max |r - c|max above 2^17 cycles: the FP64-phase adjoint leaves the
+    # fixed-point phase word (and its amplitude/phase folding of the pixel
+    # factor) for the FP64 rounding reduction
+    rng = np.random.Generator(np.random.PCG64(21))
+    Z = rng.choice([6, 7, 8], 48).astype(np.int32)
+    pos = rng.uniform(-3e-5, 3e-5, (48, 3)).astype(np.float32)
+    occ = rng.uniform(0.5, 1.0, 48).astype(np.float32)
+    q = (rng.normal(size=(512, 3)) * 3e9).astype(np.float32)
+    qr = np.linalg.norm(q.astype(np.float64), axis=1).max() * np.linalg.norm(pos - pos.mean(0), axis=1).max()
+    assert qr > 2.0 ** 17
+    g = rng.normal(size=512).astype(np.float32)
+    mol = core.Molecule(Z, pos, occ=occ)
+    qs = core.QSet.from_list(q)
+    F, I = core.forward(mol, qs, precision="f32")
+    dpos, docc, _ = core.adjoint(mol, qs, F, torch.from_numpy(g).cuda(), precision="f32")
+    torch.cuda.synchronize()
+    dp, do, _ = O.structure_factor_vjp(Z, pos.astype(np.float64), q.astype(np.float64), g.astype(np.float64), occ=occ)
+    assert _rel(dpos.cpu().numpy(), dp) < 1e-4
+    assert _rel(docc.cpu().numpy(), do) < 1e-4
