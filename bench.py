@@ -558,11 +558,26 @@ PROFILE_VARIANTS = {"f32": (128, 12, 3), "f32_fast": (128, 8, 2)}  # the untuned
 def profile_case(precisions):
     """One forward per precision on the 20,000-atom / 256^2 case (~1.3e9 terms),
     each with the kernel variant the benchmark workload runs by default: a
-    short, small-memory command for ncu captures."""
+    short, small-memory command for ncu captures.  "adjoint" instead runs one
+    FP32 forward and one adjoint of the refinement shape (5,000 atoms, 512^2
+    pixels, 2 orientations, ~2.6e9 terms each)."""
     import torch
 
     from spsim_b200 import core, synth
 
+    if "adjoint" in precisions:
+        w = synth.WORKLOADS["adjoint_5k"]
+        Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+        d = w["det"]
+        mol = core.Molecule(Z, pos, occ=np.ones(len(Z), np.float32))
+        qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+        R = synth.haar_rotations(2, w["rot_seed"])
+        F, I = core.forward_batch([mol] * 2, [qs] * 2, rots=R, precision="f32")
+        core.adjoint(mol, qs, torch.cat(F), torch.rand(2 * qs.npix, device="cuda"), rots=R, precision="f32")
+        torch.cuda.synchronize()
+        core.synchronize()
+        print("profile case ok")
+        return 0
     w = synth.WORKLOADS["orientations_20k"]
     Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
     d = w["det"]
@@ -709,7 +724,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-modes", action="store_true", help="skip the f32_fast / fp64 / accuracy extras")
     ap.add_argument("--profile-case", default=None,
-                    help="comma-separated precisions: one forward each on the 20,000-atom x 256^2 case (for ncu)")
+                    help="comma-separated precisions: one forward each on the 20,000-atom x 256^2 case, or "
+                         "\"adjoint\": one forward and one adjoint of the 5,000-atom refinement shape (for ncu)")
     ap.add_argument("--sweep", action="store_true", help="time every compiled FP32 kernel variant")
     ap.add_argument("--workloads", action="store_true", help="time the batched workloads (orientations, uneven, "
                                                               "adjoint)")

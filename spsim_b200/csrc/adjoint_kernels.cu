@@ -437,6 +437,34 @@ __global__ void __launch_bounds__(NT) adj_f64_kernel(AdjParams prm) {
   if (prm.dB) atomicAdd(&prm.dB[src], -2.0 * w * gb);
 }
 
+int adjoint_occupancy(int precision_mode, bool perb) {
+  int n = 0;
+  if (precision_mode == 2)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adj_f64_kernel<ADJ_THREADS>, ADJ_THREADS, 0);
+  else if (precision_mode == 3 || precision_mode == 4) {
+    const bool fw = precision_mode == 4;
+    if (perb)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, fw ? adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, true, true>
+                 : adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, true, false>,
+          ADJ_THREADS, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, fw ? adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, false, true>
+                 : adj_dphase_kernel<ADJ_THREADS, ADJ_DPHASE_ATOMS_PER_THREAD, false, false>,
+          ADJ_THREADS, 0);
+  } else if (precision_mode == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &n, perb ? adj_kernel<0, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, true> : adj_kernel<0, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, false>,
+        ADJ_THREADS, 0);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &n, perb ? adj_kernel<1, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, true> : adj_kernel<1, ADJ_THREADS, ADJ_ATOMS_PER_THREAD, false>,
+        ADJ_THREADS, 0);
+  }
+  return n;
+}
+
 cudaError_t launch_adjoint(int precision_mode, const AdjParams &prm, int n_items, cudaStream_t st) {
   if (n_items <= 0) return cudaSuccess;
   if (precision_mode == 2) {

@@ -47,5 +47,7 @@ struct AdjParams {
 // 2 plain FP64, 3 FP64 phase with FP32 polynomial (packed over atom pairs),
 // 4 the same with the fixed-point phase word (|q.(r - c)| < 2^17 cycles)
 cudaError_t launch_adjoint(int precision_mode, const AdjParams &prm, int n_items, cudaStream_t st);
+// resident CTAs per SM of the adjoint kernel launch_adjoint picks for this mode
+int adjoint_occupancy(int precision_mode, bool perb);
 
 }  // namespace spsim

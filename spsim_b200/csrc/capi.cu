@@ -1737,8 +1737,15 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
           blocks.push_back({a, std::min(a + block_atoms, sg.end), sg.elem, -1, std::min(a + block_atoms, sg.end), 0});
     }
   }
-  const long long want = 8LL * num_sms();
-  long long nchunk = std::max<long long>(1, (want + (long long)blocks.size() - 1) / (long long)blocks.size());
+  // mode 4: the FP64-phase adjoint with the fixed-point phase word (phases within 2^17 cycles)
+  const bool fixw = dphase && qmax * m->rbound < std::ldexp(1.0, 17);
+  const int mode =
+      precision == SPSIM_PREC_FP64 ? 2 : (precision == SPSIM_PREC_F32_FAST ? 1 : (dphase ? (fixw ? 4 : 3) : 0));
+  // pixel chunks per block so that the equal-cost CTAs fill at most four whole
+  // waves of the resident slots (a last wave of a few CTAs would leave the GPU
+  // idle for one item's length: 1,190 CTAs on 592 slots ran as three waves)
+  const long long slots = (long long)num_sms() * std::max(1, adjoint_occupancy(mode, m->per_atom_b != 0));
+  long long nchunk = std::max<long long>(1, 4 * slots / (long long)blocks.size());
   long long chunk = (total + nchunk - 1) / nchunk;
   chunk = (chunk + 255) / 256 * 256;
   std::vector<AdjItem> items;
@@ -1781,10 +1788,6 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   prm.dpos = dpos_dev;
   prm.docc = docc_dev;
   prm.dB = dB_dev;
-  // mode 4: the FP64-phase adjoint with the fixed-point phase word (phases within 2^17 cycles)
-  const bool fixw = dphase && qmax * m->rbound < std::ldexp(1.0, 17);
-  const int mode =
-      precision == SPSIM_PREC_FP64 ? 2 : (precision == SPSIM_PREC_F32_FAST ? 1 : (dphase ? (fixw ? 4 : 3) : 0));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (g_timing) {
     CUDA_TRY(cudaEventCreate(&e0));
