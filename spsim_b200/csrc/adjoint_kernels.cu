@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(NT) adj_kernel(AdjParams prm) {
         float zr = p2.y * C - p2.z * S;
         float zi = -(p2.y * S + p2.z * C);
         if (PERB) {
-          const float E = exp2f(a1[k].w * s2n);
+          const float E = ex2_approx(a1[k].w * s2n);
           zr *= E;
           zi *= E;
         }
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
           float2 zr = make_float2(sign_by_parity(C.x, kb[0], m31), sign_by_parity(C.y, kb[1], m31));
           float2 zn = make_float2(sign_by_parity(S.x, kb[0], m31), sign_by_parity(S.y, kb[1], m31));
           if (PERB) {
-            const float2 E = make_float2(exp2f(bfac[2 * j] * f1.y), exp2f(bfac[2 * j + 1] * f1.y));
+            const float2 E = make_float2(ex2_approx(bfac[2 * j] * f1.y), ex2_approx(bfac[2 * j + 1] * f1.y));
             zr = mul2(zr, E);
             zn = mul2(zn, E);
           }
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
         zr = make_float2(sign_by_parity(zr.x, kb[0], m31), sign_by_parity(zr.y, kb[1], m31));
         zn = make_float2(sign_by_parity(zn.x, kb[0], m31), sign_by_parity(zn.y, kb[1], m31));
         if (PERB) {
-          const float2 E = make_float2(exp2f(bfac[2 * j] * f1.z), exp2f(bfac[2 * j + 1] * f1.z));
+          const float2 E = make_float2(ex2_approx(bfac[2 * j] * f1.z), ex2_approx(bfac[2 * j + 1] * f1.z));
           zr = mul2(zr, E);
           zn = mul2(zn, E);
         }

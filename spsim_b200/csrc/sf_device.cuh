@@ -242,6 +242,16 @@ __device__ __forceinline__ constexpr float word_to_phase() {
   return MODE == PREC_MODE_POLY ? 0x1p-33f : 6.28318530717958648f * 0x1p-32f;
 }
 
+// 2^x with the XU pipe's approximation (PTX ex2.approx.ftz.f32, relative
+// error ~2^-22; results below 2^-126 flush to zero): the per-atom B-factor
+// weight exp(-B s^2) of one term, where the library exp2f spends extra FMA-pipe
+// instructions on full-range accuracy that a weight in (0, 1] does not need.
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Packed Fast2Sum: the block sums b of two pixels into their float-float
 // sums (hi, lo); s - hi and b - z as FMAs with -1, so every step stays packed.
 __device__ __forceinline__ void ff_accumulate2(float2 &hi, float2 &lo, float2 b) {

@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(NT) sf_f32_kernel(const SfPattern *__restrict_
           const float4 a1 = ta[2 * (a + g) + 1];
 #pragma unroll
           for (int i = 0; i < P; ++i) {
-            const float w = PERB ? a0.w * exp2f(a1.w * s2n[i]) : a0.w;
+            const float w = PERB ? a0.w * ex2_approx(a1.w * s2n[i]) : a0.w;
             sf_term<MODE>(a0, a1, w, qhx[i], qhy[i], qhz[i], qx[i], qy[i], qz[i], qlx[i], qly[i], qlz[i], bc[i],
                           bs[i]);
           }
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
 #pragma unroll
           for (int j = 0; j < NP; ++j) {
             float2 w = W;
-            if (PERB) w = make_float2(W.x * exp2f(d3.z * s2n[j].x), W.y * exp2f(d3.w * s2n[j].y));
+            if (PERB) w = make_float2(W.x * ex2_approx(d3.z * s2n[j].x), W.y * ex2_approx(d3.w * s2n[j].y));
             float2 u = mul2(qhx[j], Hx);
             u = fma2(qhy[j], Hy, u);
             u = fma2(qhz[j], Hz, u);
@@ -615,7 +615,7 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
                   kb[h] = 0;
                 }
               }
-              w[h] = PERB ? W * exp2f(d1.w * s2n[i]) : W;
+              w[h] = PERB ? W * ex2_approx(d1.w * s2n[i]) : W;
             }
             const float2 yy = FIXW ? mul2(make_float2(y[0], y[1]), f2(word_to_phase<MODE>()))
                                    : make_float2(y[0], y[1]);
@@ -852,8 +852,8 @@ __global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restric
             const float2 Yb = add2(Ya, dl);
             float2 wa = f2(W), wb = f2(W);
             if (PERB) {
-              wa = make_float2(W * exp2f(d1.w * s2a[2 * j]), W * exp2f(d1.w * s2a[2 * j + 1]));
-              wb = make_float2(W * exp2f(d1.w * s2b[2 * j]), W * exp2f(d1.w * s2b[2 * j + 1]));
+              wa = make_float2(W * ex2_approx(d1.w * s2a[2 * j]), W * ex2_approx(d1.w * s2a[2 * j + 1]));
+              wb = make_float2(W * ex2_approx(d1.w * s2b[2 * j]), W * ex2_approx(d1.w * s2b[2 * j + 1]));
             }
             if (MODE == PREC_MODE_POLY) {
               float2 Sa, Ca;
