@@ -399,13 +399,17 @@ def run_b200(args):
             "clocks": clocks.summary(),
             "gpu_launches": 3 * args.steps,
         }
-    # the other precisions on the same workload, and accuracy against the FP64 GPU kernel
-    extra = _modes(args, core, mol, qs, rot, terms, timed, prec) if rank == 0 and not args.no_modes else None
+    # the other precisions on the same workload, and accuracy against the FP64
+    # GPU kernel: single-GPU extras (their timing takes no collective steps the
+    # other ranks would have to match)
+    extra = _modes(args, core, mol, qs, rot, terms, timed, prec) if world == 1 and not args.no_modes else None
     if rank == 0 and extra:
         line.update(extra)
-    # end to end through the reference-facing simulate_shot (host buffers)
-    if rank == 0 and not args.no_e2e:
-        line["e2e"] = _e2e(args, w, Z, pos, terms, world)
+    # end to end through the reference-facing simulate_shot (host buffers), on every rank
+    if not args.no_e2e:
+        e2e = _e2e(args, w, Z, pos, terms, world, dist)
+        if rank == 0:
+            line["e2e"] = e2e
     if rank == 0 and pool is not None:
         v, desc = _cpu_sample(Z, pos, _hkl_host(w), pool, nproc, target_s=12.0)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nproc, "kind": _ref_kind(), "sample": desc}
@@ -472,9 +476,11 @@ def _modes(args, core, mol, qs, rot, terms, timed, prec):
     return out
 
 
-def _e2e(args, w, Z, pos, terms, world):
+def _e2e(args, w, Z, pos, terms, world, dist=None):
     """simulate_shot (src/spsim.c:281) with host buffers: geometry, structure factor
-    and the detector chain, every host<->device copy inside the timed region."""
+    and the detector chain, every host<->device copy inside the timed region.
+    Under torchrun every rank runs it on its own GPU at the same time (barrier
+    before, the slowest rank's time after)."""
     import torch
 
     from spsim_b200 import spsim as S
@@ -500,10 +506,16 @@ def _e2e(args, w, Z, pos, terms, world):
     for i in range(2):
         S.free_stuff(S.simulate_shot(mols[i % 2], opts), opts)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t = time.perf_counter()
     for i in range(nsteps):
         S.free_stuff(S.simulate_shot(mols[i % 2], opts), opts)
     wall = (time.perf_counter() - t) / nsteps
+    if dist:
+        tw = torch.tensor([wall], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tw, op=dist.ReduceOp.MAX)
+        wall = float(tw.item())
     for m in mols:
         S.free_mol(m)
     # bytes per step: the molecule's device records (136 B per padded atom:
