@@ -564,7 +564,7 @@ def _adjoint_ratio(prec):
     return statistics.median(tb) / statistics.median(ta)
 
 
-PROFILE_VARIANTS = {"f32": (128, 12, 3), "f32_fast": (128, 8, 2)}  # the untuned defaults on the 1024^2 workload
+PROFILE_VARIANTS = {"f32": (128, 8, 3), "f32_fast": (128, 8, 2)}  # the untuned defaults on the 1024^2 workload
 
 
 def profile_case(precisions):

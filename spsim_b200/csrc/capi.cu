@@ -637,14 +637,11 @@ static Variant choose_variant(double terms, long long total_npix, int precision)
   if (it != g_tuned.end()) return it->second;
   // untuned defaults, from sweeps on B200: the neighbour-pair FP64-phase form
   // for FP32, the FP64-phase form for FP32_FAST (MUFU sin/cos, where the
-  // neighbour step saves nothing); more pixels per thread once there are
-  // enough pixel tiles to fill every SM several times, and 12 (two CTAs per
-  // SM) only where a work item's per-pixel set-up is spread over >= 10,000
-  // atoms (5,000-atom patterns ran 20 % slower at 12 than at 8)
+  // neighbour step saves nothing); 8 pixels per thread (two CTAs per SM) once
+  // there are enough pixel tiles to fill every SM several times (fastest on
+  // both the 50,000- and the 5,000-atom workloads)
   if (precision == SPSIM_PREC_F32_FAST) return {128, total_npix >= (1LL << 20) ? 8 : 4, 2};
-  const double atoms_per_pixel = terms / (double)std::max<long long>(total_npix, 1);
-  const int p = total_npix < (1LL << 20) ? 4 : atoms_per_pixel >= 10000 ? 12 : 8;
-  return {128, p, 3};  // falls back to form 2 where a q set is not admitted
+  return {128, total_npix >= (1LL << 20) ? 8 : 4, 3};  // falls back to form 2 where a q set is not admitted
 }
 
 static bool is_orthonormal(const double *R) {

@@ -15,6 +15,15 @@
 
 namespace spsim {
 
+// Minimum resident CTAs per SM requested of the compiler for the structure-
+// factor kernels.  The FMA-polynomial kernels run fastest with every register
+// they can use (1: the 128 x 8 neighbour-pair kernel takes 188 registers
+// without spilling, where the compiler's own choice was 128 with spills, and
+// runs 6 % faster); the MUFU kernels, bound by the XU pipe, keep the
+// compiler's own choice (0), which leaves more warps per SM (asking for 1
+// gave them up to 252 registers and cost 5 %).
+__host__ __device__ constexpr int sf_min_blocks(int mode) { return mode == PREC_MODE_POLY ? 1 : 0; }
+
 // ---------------------------------------------------------------------------
 // form factors
 
@@ -116,7 +125,7 @@ __device__ __forceinline__ void sf_term(const float4 a0, const float4 a1, float 
 }
 
 template <int MODE, int NT, int P, bool PERB>
-__global__ void __launch_bounds__(NT) sf_f32_kernel(const SfPattern *__restrict__ pats,
+__global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_f32_kernel(const SfPattern *__restrict__ pats,
                                                     const WorkItem *__restrict__ items, int n_items,
                                                     int *__restrict__ queue, int *__restrict__ err) {
   __shared__ __align__(128) float4 ring[RING_STAGES][2 * TILE_ATOMS];
@@ -267,7 +276,7 @@ __global__ void __launch_bounds__(NT) sf_f32_kernel(const SfPattern *__restrict_
 
 
 template <int MODE, int NT, int P, bool PERB>
-__global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restrict__ pats,
+__global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_f32x2_kernel(const SfPattern *__restrict__ pats,
                                                       const WorkItem *__restrict__ items, int n_items,
                                                       int *__restrict__ queue, int *__restrict__ err) {
   static_assert(P % 2 == 0, "pixels per thread must be even");
@@ -497,7 +506,7 @@ __global__ void __launch_bounds__(NT) sf_f32x2_kernel(const SfPattern *__restric
 // bulk-copy ring as the compensated kernels.
 
 template <int MODE, int NT, int P, bool PERB, bool FIXW>
-__global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restrict__ pats,
+__global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dphase_kernel(const SfPattern *__restrict__ pats,
                                                        const WorkItem *__restrict__ items, int n_items,
                                                        int *__restrict__ queue, int *__restrict__ err, uint32_t m31) {
   static_assert(P % 2 == 0, "pixels per thread must be even");
@@ -710,7 +719,7 @@ __global__ void __launch_bounds__(NT) sf_dphase_kernel(const SfPattern *__restri
 // f32x2 polynomial.
 
 template <int MODE, int NT, int P, bool PERB, bool FIXW>
-__global__ void __launch_bounds__(NT) sf_dpair_kernel(const SfPattern *__restrict__ pats,
+__global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const SfPattern *__restrict__ pats,
                                                       const WorkItem *__restrict__ items, int n_items,
                                                       int *__restrict__ queue, int *__restrict__ err, uint32_t m31) {
   static_assert(P % 4 == 0, "pixels per thread must be a multiple of 4 (two pairs per packed instruction)");
