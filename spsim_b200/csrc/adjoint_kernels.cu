@@ -270,6 +270,9 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
     float2 fx[NP], fy[NP], fz[NP], fo[NP], fb[NP];
 #pragma unroll
     for (int j = 0; j < NP; ++j) fx[j] = fy[j] = fz[j] = fo[j] = fb[j] = make_float2(0.f, 0.f);
+    // four pixels per iteration: independent chains for the scheduler (each
+    // thread's two atom pairs alone left it waiting on fixed-latency results)
+#pragma unroll 4
     for (int i = 0; i < n; ++i) {
       const double2 qa = pq[2 * i], qb = pq[2 * i + 1];
       const float4 f0 = pf[2 * i], f1 = pf[2 * i + 1];
