@@ -5,8 +5,10 @@
 // with A_p = e^{+2 pi i q_p.c} F_p the centred amplitude, u_pj = q_p.(r_j - c),
 // E_pj = exp(-B_j s_p^2) (1 without per-atom B) and s^2 = (|q| 1e-10)^2 / 4.
 // Phases are recomputed with the forward's arithmetic (compensated FP32 or the
-// FP64-phase form); nothing of size atoms x pixels is stored.  One CTA owns a block of atoms of one element
-// (registers) and streams a range of pixel records through shared memory.
+// FP64-phase form); nothing of size atoms x pixels is stored.  One CTA owns a
+// block of atoms (registers; one element, or in the FP64-phase adjoint up to
+// two element segments) and streams a range of pixel records through shared
+// memory.
 #include "adjoint_kernels.cuh"
 
 namespace spsim {
