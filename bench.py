@@ -518,16 +518,18 @@ def _e2e(args, w, Z, pos, terms, world, dist=None):
         wall = float(tw.item())
     for m in mols:
         S.free_mol(m)
-    # bytes per step: the molecule's device records (136 B per padded atom:
-    # two compensated layouts, the FP64 record, permutation, base weight, plus
-    # tiles and form-factor coefficients) up; HKL list, F, |F|^2 and the seven
-    # chain arrays down
+    # bytes per step up: the new molecule's positions (12 B per atom), its
+    # permutation and base weights (8 B per padded atom; the device builds the
+    # atom records from them), tiles and form-factor coefficients, and the
+    # plan's pattern descriptor (232 B) and work items (16 B per 1,024-pixel
+    # tile); down: HKL list, F, |F|^2 and the seven chain arrays
     counts = np.bincount(np.asarray(Z, np.int64), minlength=100)[1:]
     n_pad = int(sum((c + 7) // 8 * 8 for c in counts if c))
     n_tiles = int(sum((c + 7) // 8 * 8 // 128 + (1 if ((c + 7) // 8 * 8) % 128 else 0) for c in counts if c))
     n_elem = int(np.count_nonzero(counts))
+    n_items = (n + 1023) // 1024
     return {"value": world * terms / wall, "unit": UNIT,
-            "h2d_bytes_per_step": 136 * n_pad + 16 * n_tiles + 36 * n_elem,
+            "h2d_bytes_per_step": 12 * len(Z) + 8 * n_pad + 16 * n_tiles + 36 * n_elem + 232 + 16 * n_items,
             "d2h_bytes_per_step": 12 * n + 8 * n + 4 * n + 7 * 4 * n,
             "call": "simulate_shot (reference-facing C ABI, host buffers, a new molecule upload every step)",
             "steps": nsteps, "note": "reference semantics: no ADC clamp (extension) in this call"}
