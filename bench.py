@@ -700,9 +700,14 @@ def workloads(prec, n_orient=512):
         cost += float(len(Zm)) * qsets[-1].npix
     with torch.cuda.stream(stream):
         F, I = core.forward_batch(mols, qsets, precision=prec, want_F=False)
+        t_d = ev_time(lambda: core.forward_batch(mols, qsets, precision=prec, I=I, want_F=False))
+        # the autotuner picks the tile shape for this batch (kept for its size class)
+        tuned = core.autotune_batch(mols, qsets, precision=prec, stream=stream)
         t_u = ev_time(lambda: core.forward_batch(mols, qsets, precision=prec, I=I, want_F=False))
     print(json.dumps({"workload": "uneven_64", "precision": prec, "terms": cost, "batch_ms": t_u,
-                      "terms_per_s": cost / t_u * 1e3, "frac_of_R": cost / t_u * 1e3 / R0}), flush=True)
+                      "terms_per_s": cost / t_u * 1e3, "frac_of_R": cost / t_u * 1e3 / R0,
+                      "autotuned_variant": {"threads": tuned[0], "pixels_per_thread": tuned[1], "form": tuned[2]},
+                      "untuned_default_ms": t_d}), flush=True)
     del mols, qsets, F, I
 
     # adjoint

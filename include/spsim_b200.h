@@ -331,6 +331,16 @@ int spsim_b200_last_variant(int *threads, int *pixels_per_thread, int *form);
 int spsim_b200_last_phase_word(int *on);
 int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision, void *stream,
                         int *best_threads, int *best_pixels_per_thread, int *best_form);
+/* The same over a batch (the arguments of spsim_b200_forward_batch, without
+ * B and outputs): every variant is timed on the whole batched launch, and the
+ * fastest is kept for batches of that size class (total atom.pixel terms).
+ * No reference counterpart. */
+int spsim_b200_autotune_batch(int npatterns, const spsim_b200_molecule *const *mols,
+                              const spsim_b200_qset *const *qsets, const double *rot, int precision, void *stream,
+                              int *best_threads, int *best_pixels_per_thread, int *best_form);
+/* Forget every autotuned choice (later forwards use the untuned defaults
+ * again).  No reference counterpart. */
+int spsim_b200_clear_tuning(void);
 
 #ifdef __cplusplus
 }

@@ -118,6 +118,9 @@ _SIGNATURES = {
     "spsim_b200_last_phase_word": (c_int, [POINTER(c_int)]),
     "spsim_b200_release_scratch": (None, []),
     "spsim_b200_autotune": (c_int, [_P, _P, c_int, _P, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "spsim_b200_autotune_batch": (c_int, [c_int, _P, _P, _P, c_int, _P, POINTER(c_int), POINTER(c_int),
+                                          POINTER(c_int)]),
+    "spsim_b200_clear_tuning": (c_int, []),
     "spsim_b200_set_legacy_precision": (None, [c_int]),
     "spsim_b200_get_legacy_precision": (c_int, []),
     "spsim_b200_set_noise_seed": (None, [c_uint64]),

@@ -21,7 +21,7 @@ from ._native import PRECISIONS, ChainOutputs, ChainParams, check, lib
 __all__ = [
     "Molecule", "QSet", "forward", "forward_batch", "adjoint", "detector_chain", "chain_params",
     "hkl_for_detector", "synchronize", "forward_spectrum", "timing", "autotune", "set_variant", "last_forward_stats",
-    "last_variant", "last_phase_word", "kernel_name",
+    "last_variant", "last_phase_word", "kernel_name", "autotune_batch", "clear_tuning",
 ]
 
 
@@ -375,6 +375,35 @@ def autotune(mol, qs, precision="f32", stream=None):
     check(lib().spsim_b200_autotune(mol.handle, qs.handle, _prec(precision), _stream_ptr(stream), byref(bt),
                                     byref(bp), byref(bk)))
     return bt.value, bp.value, bk.value
+
+
+def autotune_batch(mols, qsets, rots=None, precision="f32", stream=None):
+    """Time every compiled FP32 kernel variant on one batched forward of these
+    patterns (arguments as forward_batch) and keep the fastest for batches of
+    this size; returns (threads, pixels_per_thread, form)."""
+    if rots is not None:
+        npat = len(rots)
+    else:
+        npat = len(mols) if isinstance(mols, (list, tuple)) else len(qsets)
+    mols = list(mols) if isinstance(mols, (list, tuple)) else [mols] * npat
+    qsets = list(qsets) if isinstance(qsets, (list, tuple)) else [qsets] * npat
+    if len(mols) != npat or len(qsets) != npat:
+        raise ValueError("molecules, q sets and rotations disagree on the number of patterns")
+    _native.use_device(mols[0].device)
+    MA = c_void_p * npat
+    mh = MA(*[m.handle.value for m in mols])
+    qh = MA(*[q.handle.value for q in qsets])
+    r = _rot_array(rots, npat)
+    bt, bp, bk = c_int(0), c_int(0), c_int(0)
+    check(lib().spsim_b200_autotune_batch(npat, ctypes.cast(mh, c_void_p), ctypes.cast(qh, c_void_p),
+                                          r.ctypes.data_as(c_void_p) if r is not None else None, _prec(precision),
+                                          _stream_ptr(stream), byref(bt), byref(bp), byref(bk)))
+    return bt.value, bp.value, bk.value
+
+
+def clear_tuning():
+    """Forget every autotuned choice: later forwards use the untuned defaults."""
+    check(lib().spsim_b200_clear_tuning())
 
 
 def npix_of(qs):

@@ -1419,15 +1419,33 @@ extern "C" int spsim_b200_set_variant(int threads, int pixels_per_thread, int pa
   return SPSIM_OK;
 }
 
-extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision,
-                                   void *stream, int *best_threads, int *best_pixels_per_thread, int *best_packed) {
-  if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
+// Times every compiled FP32 variant on one forward of the given patterns and
+// keeps the fastest for workloads of that size class (total terms).
+static int autotune_impl(int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
+                         const double *rot, int precision, cudaStream_t stream, int *best_threads,
+                         int *best_pixels_per_thread, int *best_packed) {
+  if (npat < 1 || !mols || !qsets) return fail(SPSIM_ERR_INVALID_ARG, "no patterns to tune on");
+  double terms = 0;
+  long long total = 0;
+  for (int i = 0; i < npat; ++i) {
+    if (!mols[i] || !qsets[i]) return fail(SPSIM_ERR_INVALID_ARG, "pattern %d: NULL handle", i);
+    terms += (double)qsets[i]->npix * mols[i]->n_kept;
+    total += qsets[i]->npix;
+  }
   if (precision == SPSIM_PREC_FP64) return fail(SPSIM_ERR_INVALID_ARG, "the FP64 kernel has a single variant");
   const int cand[][3] = {{128, 2, 0}, {128, 4, 0}, {256, 4, 0}, {128, 2, 1}, {128, 4, 1}, {256, 4, 1},
                          {128, 6, 1}, {128, 2, 2}, {128, 4, 2}, {256, 4, 2}, {128, 6, 2}, {128, 8, 2},
                          {128, 4, 3}, {128, 8, 3}, {128, 12, 3}, {256, 4, 3}};
   float *dI = nullptr;
-  CUDA_TRY(cudaMalloc(&dI, std::max<long long>(qs->npix, 1) * sizeof(float)));
+  CUDA_TRY(cudaMalloc(&dI, std::max<long long>(total, 1) * sizeof(float)));
+  std::vector<float *> I(npat), F(npat, nullptr);
+  {
+    long long off = 0;
+    for (int i = 0; i < npat; ++i) {
+      I[i] = dI + off;
+      off += qsets[i]->npix;
+    }
+  }
   float best = 1e30f;
   int bt = 128, bp = 4, bk = 2;
   const int saved_nt = g_force_nt, saved_p = g_force_p, saved_pk = g_force_pk;
@@ -1437,21 +1455,17 @@ extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b20
     g_force_nt = c[0];
     g_force_p = c[1];
     g_force_pk = c[2];
-    float *I[1] = {dI};
-    float *F[1] = {nullptr};
-    const spsim_b200_molecule *mm = m;
-    const spsim_b200_qset *qq = qs;
     // warm-up, then three timed launches
-    st = run_forward(1, &mm, &qq, nullptr, 0.0f, precision, F, I, (cudaStream_t)stream, false);
+    st = run_forward(npat, mols, qsets, rot, 0.0f, precision, F.data(), I.data(), stream, false);
     if (st) break;
     float tot = 0;
     for (int r = 0; r < 3 && !st; ++r) {
       cudaEvent_t a, b;
       cudaEventCreate(&a);
       cudaEventCreate(&b);
-      cudaEventRecord(a, (cudaStream_t)stream);
-      st = run_forward(1, &mm, &qq, nullptr, 0.0f, precision, F, I, (cudaStream_t)stream, false);
-      cudaEventRecord(b, (cudaStream_t)stream);
+      cudaEventRecord(a, stream);
+      st = run_forward(npat, mols, qsets, rot, 0.0f, precision, F.data(), I.data(), stream, false);
+      cudaEventRecord(b, stream);
       cudaEventSynchronize(b);
       float t = 0;
       cudaEventElapsedTime(&t, a, b);
@@ -1475,12 +1489,33 @@ extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b20
   if (st) return st;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    g_tuned[size_class((double)qs->npix * m->n_kept) * 4 + precision] = {bt, bp, bk};
+    g_tuned[size_class(terms) * 4 + precision] = {bt, bp, bk};
   }
   if (best_threads) *best_threads = bt;
   if (best_pixels_per_thread) *best_pixels_per_thread = bp;
   if (best_packed) *best_packed = bk;
   return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision,
+                                   void *stream, int *best_threads, int *best_pixels_per_thread, int *best_packed) {
+  if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
+  return autotune_impl(1, &m, &qs, nullptr, precision, (cudaStream_t)stream, best_threads, best_pixels_per_thread,
+                       best_packed);
+}
+
+extern "C" int spsim_b200_clear_tuning(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_tuned.clear();
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_autotune_batch(int npatterns, const spsim_b200_molecule *const *mols,
+                                         const spsim_b200_qset *const *qsets, const double *rot, int precision,
+                                         void *stream, int *best_threads, int *best_pixels_per_thread,
+                                         int *best_form) {
+  return autotune_impl(npatterns, mols, qsets, rot, precision, (cudaStream_t)stream, best_threads,
+                       best_pixels_per_thread, best_form);
 }
 
 // ---------------------------------------------------------------------------

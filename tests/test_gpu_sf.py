@@ -255,3 +255,39 @@ def test_neighbour_pair_form_admission(cuda):
         _, I64 = O.structure_factor(Z, pos.astype(np.float64), q.astype(np.float64))
         e_max, e_l2 = intensity_errors(I, I64)
         assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (kernel, e_max, e_l2)
+
+
+CANDIDATES = {(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1), (128, 2, 2),
+              (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2), (128, 4, 3), (128, 8, 3), (128, 12, 3), (256, 4, 3)}
+
+
+def test_autotune_single_and_batch(cuda):
+    # the autotuners time every compiled variant, keep the fastest for the
+    # workload's size class, and the forwards that follow use it and stay
+    # within tolerance; clearing the tuning restores the untuned defaults
+    Z, pos = synth.random_molecule(1500, 2.5e-9, 61)
+    d = dict(nx=48, ny=40, width=48 * 150e-6, height=40 * 150e-6, distance=0.1, wavelength=0.2e-9)
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(**d)
+    q = O.hkl_detector(**d)
+    R = synth.haar_rotations(3, 62)
+    try:
+        best = core.autotune(mol, qs, precision="f32")
+        assert best in CANDIDATES
+        _, I = core.forward(mol, qs, precision="f32")
+        assert core.last_variant()[:2] == best[:2]
+        _, I64 = O.structure_factor(Z, pos.astype(np.float64), q)
+        e_max, e_l2 = intensity_errors(I.cpu().numpy(), I64)
+        assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1]
+        best_b = core.autotune_batch([mol] * 3, [qs] * 3, rots=R, precision="f32")
+        assert best_b in CANDIDATES
+        _, Ib = core.forward_batch([mol] * 3, [qs] * 3, rots=R, precision="f32")
+        assert core.last_variant()[:2] == best_b[:2]
+        for r, Ir in zip(R, Ib):
+            _, I64r = O.structure_factor(Z, pos.astype(np.float64), q @ r.T)
+            e_max, e_l2 = intensity_errors(Ir.cpu().numpy(), I64r)
+            assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1]
+    finally:
+        core.clear_tuning()
+    core.forward(mol, qs, precision="f32")
+    assert core.last_variant() == (128, 4, 3)  # the untuned default again
