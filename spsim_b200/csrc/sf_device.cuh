@@ -252,6 +252,13 @@ __device__ __forceinline__ float ex2_approx(float x) {
   return y;
 }
 
+// log2(x) by the XU pipe's approximation (PTX lg2.approx.ftz.f32; -inf at 0)
+__device__ __forceinline__ float lg2_approx(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Packed Fast2Sum: the block sums b of two pixels into their float-float
 // sums (hi, lo); s - hi and b - z as FMAs with -1, so every step stays packed.
 __device__ __forceinline__ void ff_accumulate2(float2 &hi, float2 &lo, float2 b) {

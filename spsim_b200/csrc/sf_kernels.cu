@@ -529,6 +529,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dphase_kernel(cons
   // FIXW: pixel q pre-scaled by 2 (half-cycle reduction) and the phase summed onto kWordBase
   constexpr double kQScale = (FIXW && MODE == PREC_MODE_POLY) ? 2.0 : 1.0;
   constexpr double kWordBase = MODE == PREC_MODE_POLY ? PHASE_WORD_BASE_HALF : PHASE_WORD_BASE;
+  // per-atom B factors with the half-cycle phase word: the weight folded into the exponent
+  constexpr bool LOGW = PERB && FIXW && MODE == PREC_MODE_POLY;
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(queue, 1);
@@ -600,6 +602,10 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dphase_kernel(cons
           const double ry = __hiloint2double(__float_as_int(d0.w), __float_as_int(d0.z));
           const double rz = __hiloint2double(__float_as_int(d1.y), __float_as_int(d1.x));
           const float W = d1.z;
+          // LOGW: W exp2(b s2) as exp2(b s2 + log2|W|), the sign of W as one more
+          // half cycle in the phase word (its parity bit flips the term's sign)
+          const float lw = LOGW ? lg2_approx(fabsf(W)) : 0.0f;
+          const double wbase = LOGW && W < 0.0f ? kWordBase + 1.0 : kWordBase;
 #pragma unroll
           for (int j = 0; j < NP; ++j) {
             float y[2], w[2];
@@ -608,7 +614,7 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dphase_kernel(cons
             for (int h = 0; h < 2; ++h) {
               const int i = 2 * j + h;
               if (FIXW) {
-                const double t = phase_word(qx[i], qy[i], qz[i], rx, ry, rz, kWordBase);
+                const double t = phase_word(qx[i], qy[i], qz[i], rx, ry, rz, wbase);
                 reduce_phase_word<MODE>(t, y[h], kb[h]);
               } else {
                 double u = qx[i] * rx;
@@ -624,7 +630,7 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dphase_kernel(cons
                   kb[h] = 0;
                 }
               }
-              w[h] = PERB ? W * ex2_approx(d1.w * s2n[i]) : W;
+              w[h] = LOGW ? ex2_approx(fmaf(d1.w, s2n[i], lw)) : PERB ? W * ex2_approx(d1.w * s2n[i]) : W;
             }
             const float2 yy = FIXW ? mul2(make_float2(y[0], y[1]), f2(word_to_phase<MODE>()))
                                    : make_float2(y[0], y[1]);
@@ -742,6 +748,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
   const double M52 = 6755399441055744.0;  // 1.5 * 2^52
   constexpr double kQScale = (FIXW && MODE == PREC_MODE_POLY) ? 2.0 : 1.0;
   constexpr double kWordBase = MODE == PREC_MODE_POLY ? PHASE_WORD_BASE_HALF : PHASE_WORD_BASE;
+  // per-atom B factors with the half-cycle phase word: the weight folded into the exponent
+  constexpr bool LOGW = PERB && FIXW && MODE == PREC_MODE_POLY;
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(queue, 1);
@@ -826,6 +834,10 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
           const double rz = __hiloint2double(__float_as_int(d1.y), __float_as_int(d1.x));
           const float W = d1.z;
           const float2 fx = f2(__double2float_rn(rx)), fy = f2(__double2float_rn(ry)), fz = f2(__double2float_rn(rz));
+          // LOGW: W exp2(b s2) as exp2(b s2 + log2|W|), the sign of W as one more
+          // half cycle in the phase word (its parity bit flips both pixels' sign)
+          const float lw = LOGW ? lg2_approx(fabsf(W)) : 0.0f;
+          const double wbase = LOGW && W < 0.0f ? kWordBase + 1.0 : kWordBase;
 #pragma unroll
           for (int j = 0; j < NPK; ++j) {
             float ya[2];
@@ -834,7 +846,7 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
             for (int h = 0; h < 2; ++h) {
               const int m = 2 * j + h;
               if (FIXW) {
-                const double t = phase_word(qx[m], qy[m], qz[m], rx, ry, rz, kWordBase);
+                const double t = phase_word(qx[m], qy[m], qz[m], rx, ry, rz, wbase);
                 reduce_phase_word<MODE>(t, ya[h], kb[h]);
               } else {
                 double u = qx[m] * rx;
@@ -860,7 +872,10 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
             dl = fma2(make_float2(dqz[2 * j], dqz[2 * j + 1]), fz, dl);
             const float2 Yb = add2(Ya, dl);
             float2 wa = f2(W), wb = f2(W);
-            if (PERB) {
+            if (LOGW) {
+              wa = make_float2(ex2_approx(fmaf(d1.w, s2a[2 * j], lw)), ex2_approx(fmaf(d1.w, s2a[2 * j + 1], lw)));
+              wb = make_float2(ex2_approx(fmaf(d1.w, s2b[2 * j], lw)), ex2_approx(fmaf(d1.w, s2b[2 * j + 1], lw)));
+            } else if (PERB) {
               wa = make_float2(W * ex2_approx(d1.w * s2a[2 * j]), W * ex2_approx(d1.w * s2a[2 * j + 1]));
               wb = make_float2(W * ex2_approx(d1.w * s2b[2 * j]), W * ex2_approx(d1.w * s2b[2 * j + 1]));
             }

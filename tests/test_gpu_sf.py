@@ -291,3 +291,26 @@ def test_autotune_single_and_batch(cuda):
         core.clear_tuning()
     core.forward(mol, qs, precision="f32")
     assert core.last_variant() == (128, 4, 3)  # the untuned default again
+
+
+@pytest.mark.parametrize("form", [2, 3])
+def test_b_factors_with_negative_and_zero_occupancies(cuda, form):
+    # per-atom B factors fold the atom weight into the exponent, exp2(b s^2 +
+    # log2|w|), and carry the weight's sign as an extra half cycle of phase:
+    # negative and zero occupancies (refinement can produce both) must come out
+    # as with the plain product
+    g = golden("sf_plain1k.npz")
+    rng = np.random.Generator(np.random.PCG64(71))
+    n = len(g["Z"])
+    occ = rng.uniform(-0.6, 1.0, n).astype(np.float32)
+    occ[::17] = 0.0
+    bfac = rng.uniform(0, 40, n).astype(np.float32)
+    _, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64), occ=occ, bfac=bfac)
+    try:
+        core.set_variant(128, 4, form)
+        _, I = _run(g["Z"], g["pos"], g["hkl"], "f32", occ=occ, bfac=bfac)
+        assert core.last_variant()[2] == form and core.last_phase_word()
+    finally:
+        core.set_variant(-1)
+    e_max, e_l2 = intensity_errors(I, I64)
+    assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (e_max, e_l2)
