@@ -293,12 +293,16 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
           }
           float2 S, C;
           sincos_dhalf_poly2(mul2(make_float2(y[0], y[1]), f2(word_to_cycles<PREC_MODE_POLY>())), S, C);
-          float2 zr = make_float2(sign_by_parity(C.x, kb[0], m31), sign_by_parity(C.y, kb[1], m31));
-          float2 zn = make_float2(sign_by_parity(S.x, kb[0], m31), sign_by_parity(S.y, kb[1], m31));
+          float2 zr, zn;
           if (PERB) {
-            const float2 E = make_float2(ex2_approx(bfac[2 * j] * f1.y), ex2_approx(bfac[2 * j + 1] * f1.y));
-            zr = mul2(zr, E);
-            zn = mul2(zn, E);
+            // the sign once, on the B-factor weight E, which then scales both
+            const float2 E = make_float2(sign_by_parity(ex2_approx(bfac[2 * j] * f1.y), kb[0], m31),
+                                         sign_by_parity(ex2_approx(bfac[2 * j + 1] * f1.y), kb[1], m31));
+            zr = mul2(C, E);
+            zn = mul2(S, E);
+          } else {
+            zr = make_float2(sign_by_parity(C.x, kb[0], m31), sign_by_parity(C.y, kb[1], m31));
+            zn = make_float2(sign_by_parity(S.x, kb[0], m31), sign_by_parity(S.y, kb[1], m31));
           }
           fx[j] = fma2(zn, f2(f0.x), fx[j]);
           fy[j] = fma2(zn, f2(f0.y), fy[j]);
