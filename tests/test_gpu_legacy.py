@@ -123,8 +123,9 @@ def test_host_entry_point_reuses_scratch_safely(cuda):
     assert e_max < 1e-5
 
 
+@pytest.mark.parametrize("bandwidth", [0.0, 0.3])
 @pytest.mark.parametrize("use_cuda", [1, 2])
-def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda):
+def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda, bandwidth):
     # simulate_shot runs geometry, orientation, structure factor and the chain
     # as one device pipeline; its outputs must be those of the reference's
     # step-by-step sequence (src/spsim.c:281-346) through the public calls:
@@ -142,7 +143,9 @@ def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda):
         det.nx = det.ny = 48
         det.readout_noise = 3.0
         o.verbosity_level = 0
-        o.use_cuda = use_cuda
+        o.use_cuda = use_cuda  # 1: the spectrum path when there is a bandwidth
+        o.wavelength_samples = 4
+        exp.bandwidth = bandwidth
         o.random_orientation = 0
         o.euler_orientation[0], o.euler_orientation[1], o.euler_orientation[2] = 0.3, -1.1, 2.2
         o.random_seed = 4242
