@@ -1139,6 +1139,7 @@ struct HostSession {
   DevBuf *stats = nullptr;  // two words for the device q-set statistics
 };
 static thread_local HostSession g_host;
+static thread_local spsim_b200_molecule *g_shot_mol = nullptr;  // set by spsim_internal_shot_molecule
 
 static void append_bytes(std::vector<unsigned char> &v, const void *p, size_t n) {
   const unsigned char *b = (const unsigned char *)p;
@@ -1223,6 +1224,7 @@ extern "C" void spsim_internal_release_host_session(void) {
     delete g_host.stats;
   }
   g_host = HostSession();
+  g_shot_mol = nullptr;
   if (g_oneshot.plan && g_oneshot.device == dev) delete g_oneshot.plan;
   g_oneshot = OneShot();
 }
@@ -1295,6 +1297,28 @@ static int host_session_qset_device(int64_t npix, const float *hkl_dev, cudaStre
   return SPSIM_OK;
 }
 
+// The session molecule for the caller's atom arrays, made ready before the
+// shot's geometry is queued (a changed molecule synchronises the device before
+// it takes over the old one's buffers, and then finds it idle); the structure
+// factor call that follows uses it without comparing the arrays again.
+
+extern "C" int spsim_internal_shot_molecule(int natoms, const int32_t *Z, const float *pos, int delta_atoms,
+                                            const float *beam) {
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (g_host.device != dev) {
+    g_host = HostSession();
+    g_host.device = dev;
+  }
+  g_shot_mol = nullptr;
+  spsim_b200_molecule *m = nullptr;
+  st = host_session_molecule(natoms, Z, pos, nullptr, nullptr, delta_atoms, beam, &m);
+  if (st) return st;
+  g_shot_mol = m;
+  return SPSIM_OK;
+}
+
 // Enqueued on the legacy default stream and not waited for: the caller
 // synchronises, then calls spsim_internal_shot_check for kernel-side errors.
 extern "C" int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z, const float *pos, float B,
@@ -1309,10 +1333,13 @@ extern "C" int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z
     g_host = HostSession();
     g_host.device = dev;
   }
-  spsim_b200_molecule *m = nullptr;
+  spsim_b200_molecule *m = g_shot_mol;
+  g_shot_mol = nullptr;
   spsim_b200_qset *q = nullptr;
-  st = host_session_molecule(natoms, Z, pos, nullptr, nullptr, delta_atoms, beam, &m);
-  if (st) return st;
+  if (!m || m != g_host.mol) {
+    st = host_session_molecule(natoms, Z, pos, nullptr, nullptr, delta_atoms, beam, &m);
+    if (st) return st;
+  }
   st = host_session_qset_device(npix, hkl_dev, nullptr, &q);
   if (st) return st;
   return forward_spectrum(m, q, nullptr, B, precision, wavelength, bandwidth, samples, F_dev, I_dev, nullptr, false,

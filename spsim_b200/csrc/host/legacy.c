@@ -105,6 +105,7 @@ int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z, const flo
                                          int64_t npix, const float *hkl_dev, int precision, float *F_dev,
                                          float *I_dev);
 int spsim_internal_shot_check(void);
+int spsim_internal_shot_molecule(int natoms, const int32_t *Z, const float *pos, int delta_atoms, const float *beam);
 int spsim_internal_rotate_hkl(int64_t npix, const float R[9], float *hkl_dev);
 
 /* Pinned staging buffer of simulate_shot's device-to-host copies (grow-only,
@@ -574,12 +575,16 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   }
   if (opts->random_seed >= 0) spsim_b200_set_noise_seed((unsigned long long)opts->random_seed);
   const double t0 = now_us();
+  const float beam[3] = {exp->beam_fwhm, exp->beam_center_x, exp->beam_center_y};
+  /* the molecule first: a changed one waits for the device, which is idle now */
+  int st = spsim_internal_shot_molecule(mol->natoms, mol->atomic_number, mol->pos, opts->delta_atoms, beam);
+  if (st) die("simulate_shot molecule", st);
 
   /* geometry (src/spsim.c:98-108, src/diffraction.c:300-323) */
   const int vol = det->nz > 1;
   const long long n = vol ? (long long)det->nx * det->ny * det->nz : (long long)det->nx * det->ny;
   float *d_hkl = (float *)dev_alloc(SLOT_HKL, sizeof(float) * 3 * (n > 0 ? n : 1));
-  int st = vol ? spsim_b200_hkl_for_3d_detector(det->nx, det->ny, det->nz, det->width, det->height, det->depth,
+  st = vol ? spsim_b200_hkl_for_3d_detector(det->nx, det->ny, det->nz, det->width, det->height, det->depth,
                                                  det->distance, det->center_x, det->center_y, det->center_z,
                                                  exp->wavelength, d_hkl, NULL)
                : spsim_b200_hkl_for_detector(det->nx, det->ny, det->width, det->height, det->distance,
@@ -632,7 +637,6 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
     fprintf(stderr, "spsim_b200: wavelength_samples must be >= 1 with a bandwidth (got %d)\n", samples);
     abort();
   }
-  const float beam[3] = {exp->beam_fwhm, exp->beam_center_x, exp->beam_center_y};
   float *dF = (float *)dev_alloc(SLOT_SHOT_F, b_F > 0 ? b_F : 8);
   float *dI = (float *)dev_alloc(SLOT_SHOT_I, b_I > 0 ? b_I : 4);
   st = spsim_internal_shot_structure_factor(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
@@ -640,6 +644,18 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
                                             poly ? exp->bandwidth : 0.0f, poly ? samples : 1, n, d_hkl, g_precision,
                                             dF, dI);
   if (st) die("simulate_shot structure factor", st);
+
+  /* F and |F|^2 go down ahead of the chain, so the host can copy them out
+   * while the chain's arrays are still in flight */
+  cudaEvent_t ev_fi;
+  e = cudaEventCreateWithFlags(&ev_fi, cudaEventDisableTiming);
+  if (e != cudaSuccess) cuda_die("cudaEventCreate", e);
+  if (n > 0) {
+    e = cudaMemcpyAsync(s_F, dF, b_F, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s_I, dI, b_I, cudaMemcpyDeviceToHost, 0);
+    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync F, I", e);
+  }
+  cudaEventRecord(ev_fi, 0);
 
   /* detector chain on the device intensities (src/spsim.c:300-336) */
   spsim_b200_chain_params p = chain_params(det, exp);
@@ -651,8 +667,6 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   st = spsim_b200_detector_chain(&p, dI, &o, NULL);
   if (st) die("simulate_shot detector chain", st);
   if (n > 0) {
-    e = cudaMemcpyAsync(s_F, dF, b_F, cudaMemcpyDeviceToHost, 0);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(s_I, dI, b_I, cudaMemcpyDeviceToHost, 0);
     for (int k = 0; k < 7 && e == cudaSuccess; k++) {
       const size_t b = k < 5 ? b_I : b_nb;
       if (b) e = cudaMemcpyAsync(s_chain + (k < 5 ? k * b_I : 5 * b_I + (k - 5) * b_nb), bufs[k], b,
@@ -688,14 +702,18 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   if (e != cudaSuccess) cuda_die("simulate_shot HKL copy", e);
   const HostCopy hk = {(char *)pattern->HKL_list, s_hkl, b_hkl};
   host_copy_batch(&hk, 1);
+  e = cudaEventSynchronize(ev_fi);
+  if (e != cudaSuccess) cuda_die("simulate_shot F, I", e);
+  host_copy_batch(out, 2);
 
   e = cudaEventSynchronize(ev_out);
   if (e != cudaSuccess) cuda_die("simulate_shot outputs", e);
   cudaEventDestroy(ev_hkl);
+  cudaEventDestroy(ev_fi);
   cudaEventDestroy(ev_out);
   st = spsim_internal_shot_check();
   if (st) die("simulate_shot structure factor", st);
-  host_copy_batch(out, 9);
+  host_copy_batch(out + 2, 7);
   if (opts->verbosity_level > 0) /* src/diffraction.c:849-851 */
     printf("%g atoms.pixel/s\n", 1.0e6 * n * mol->natoms / (now_us() - t0));
   g_pattern_counter++;
