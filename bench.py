@@ -212,11 +212,14 @@ def measured_pipe_peaks():
 # FMA/ADD, IMAD = integer multiply-add, XU = MUFU and FP64->FP32 conversions,
 # I2F = int32->FP32 conversions (not a bound: the f32_fast sweep runs two MUFU
 # and one I2F per term faster than the probe's MUFU rate allows for three XU
-# operations, so I2F issues elsewhere).  "+word": the fixed-point phase word.
+# operations, so I2F issues elsewhere).  "+word": the fixed-point phase word;
+# "+narrow": the neighbour pairs' second pixels on the NARROW polynomial.
 MIX = {
     # half the terms FP64-anchored, half by FP32 step
     "sf_dpair_kernel": {"fp32": 15, "dfma": 3, "imad": 0.5, "xu": 0.875},
     "sf_dpair_kernel+word": {"fp32": 15.5, "dfma": 1.5, "imad": 0.5, "alu": 0.5, "xu": 0.375, "i2f": 0.5},
+    # second pixels on the NARROW polynomial: one FMA fewer per second-pixel term
+    "sf_dpair_kernel+word+narrow": {"fp32": 15.0, "dfma": 1.5, "imad": 0.5, "alu": 0.5, "xu": 0.375, "i2f": 0.5},
     # FP64 phase + reduction, DHALF poly
     "sf_dphase_kernel": {"fp32": 12, "dfma": 6, "imad": 1, "xu": 1},
     "sf_dphase_kernel+word/f32": {"fp32": 13, "dfma": 3, "imad": 1, "alu": 1, "i2f": 1},
@@ -224,6 +227,13 @@ MIX = {
     "sf_f32x2_kernel/f32": {"fp32": 27, "alu": 2},                   # compensated phase, HALF poly
     "sf_f32x2_kernel/f32_fast": {"fp32": 16, "xu": 2},               # compensated phase, MUFU sin/cos
 }
+
+
+def _kernel_key():
+    """MIX key of the structure-factor kernel the last forward ran."""
+    from spsim_b200 import core
+    return (core.kernel_name() + ("+word" if core.last_phase_word() else "")
+            + ("+narrow" if core.last_pair_narrow() else ""))
 
 
 def balanced_bound(kernel, prec, probe):
@@ -368,7 +378,7 @@ def run_b200(args):
 
     elapsed_ms, sf_avg, clocks = timed(prec, args.steps, args.warmup)
     value = world * args.steps * terms / (elapsed_ms * 1e-3)
-    kname = core.kernel_name() + ("+word" if core.last_phase_word() else "")
+    kname = _kernel_key()
 
     line = None
     if rank == 0:
@@ -440,7 +450,7 @@ def _modes(args, core, mol, qs, rot, terms, timed, prec):
     R = _peaks(props)[0]
     if prec != "f32_fast":
         ms, sf_ms, _ = timed("f32_fast", max(2, args.steps // 2), 1)
-        kname = core.kernel_name() + ("+word" if core.last_phase_word() else "")
+        kname = _kernel_key()
         bal = balanced_bound(kname, "f32_fast", measured_pipe_peaks())
         if bal and sf_ms:
             bal["frac"] = terms / (sf_ms * 1e-3) / bal["terms_per_s"]

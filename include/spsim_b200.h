@@ -329,6 +329,11 @@ int spsim_b200_last_variant(int *threads, int *pixels_per_thread, int *form);
  * the fixed-point phase word (1) or reduced it by FP64 rounding (0); 0 for the
  * other forms and the plain FP64 kernel.  No reference counterpart. */
 int spsim_b200_last_phase_word(int *on);
+/* Whether the last forward on this thread ran the neighbour-pair form with
+ * every pair's step within 0.07 cycle, so that its second pixels took the
+ * shorter NARROW sin/cos polynomial (1), or not (0).  No reference
+ * counterpart. */
+int spsim_b200_last_pair_narrow(int *on);
 int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision, void *stream,
                         int *best_threads, int *best_pixels_per_thread, int *best_form);
 /* The same over a batch (the arguments of spsim_b200_forward_batch, without

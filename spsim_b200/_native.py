@@ -116,6 +116,7 @@ _SIGNATURES = {
     "spsim_b200_set_variant": (c_int, [c_int, c_int, c_int]),
     "spsim_b200_last_variant": (c_int, [POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "spsim_b200_last_phase_word": (c_int, [POINTER(c_int)]),
+    "spsim_b200_last_pair_narrow": (c_int, [POINTER(c_int)]),
     "spsim_b200_release_scratch": (None, []),
     "spsim_b200_autotune": (c_int, [_P, _P, c_int, _P, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "spsim_b200_autotune_batch": (c_int, [c_int, _P, _P, _P, c_int, _P, POINTER(c_int), POINTER(c_int),

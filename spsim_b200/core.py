@@ -21,7 +21,7 @@ from ._native import PRECISIONS, ChainOutputs, ChainParams, check, lib
 __all__ = [
     "Molecule", "QSet", "forward", "forward_batch", "adjoint", "detector_chain", "chain_params",
     "hkl_for_detector", "synchronize", "forward_spectrum", "timing", "autotune", "set_variant", "last_forward_stats",
-    "last_variant", "last_phase_word", "kernel_name", "autotune_batch", "clear_tuning",
+    "last_variant", "last_phase_word", "last_pair_narrow", "kernel_name", "autotune_batch", "clear_tuning",
 ]
 
 
@@ -354,6 +354,15 @@ def last_phase_word():
     from the fixed-point phase word rather than FP64 rounding."""
     on = c_int(0)
     check(lib().spsim_b200_last_phase_word(byref(on)))
+    return bool(on.value)
+
+
+def last_pair_narrow():
+    """True when the last forward on this thread ran the neighbour-pair form
+    (3) with every pair's step within 0.07 cycle, its second pixels on the
+    shorter NARROW sin/cos polynomial."""
+    on = c_int(0)
+    check(lib().spsim_b200_last_pair_narrow(byref(on)))
     return bool(on.value)
 
 

@@ -585,6 +585,7 @@ struct Plan {
   int precision = 0, nt = 128, ppt = 4, packed = 1;
   bool perb = false;
   bool fixw = false;  // FP64-phase forms: fixed-point phase word (every pattern within 2^17 cycles)
+  bool narrow = false;  // neighbour pairs: every step within 0.07 cycle (the NARROW second-pixel polynomial)
   std::vector<long long> npix_of;
   std::vector<SfPattern> host_pats;  // descriptors as last uploaded (rotations change per call)
   int spectrum = 0;                  // > 0: combine this many patterns into spec_F / spec_I
@@ -615,6 +616,7 @@ static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timing_events;
 static thread_local double g_last_terms = 0, g_last_ms = 0;
 static thread_local int g_last_variant[3] = {0, 0, -1};  // threads, pixels per thread, form (-1: FP64 kernel)
 static thread_local int g_last_phase_word = 0;            // forms 2/3: fixed-point phase word used
+static thread_local int g_last_pair_narrow = 0;           // form 3: NARROW second-pixel polynomial used
 static int g_num_sms = 0;
 
 static int num_sms() {
@@ -699,6 +701,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
   if (var.packed == 3) {
     // neighbour-pair form: every pattern needs |q_b - q_a| |r|max <= 1/8 cycle
     bool ok = true;
+    double max_step = 0.0;
     for (int i = 0; i < npat && ok; ++i) {
       double scale = spec ? std::fabs(spec->qscale[i]) : 1.0;
       if (rot && !is_orthonormal(rot + 9 * (size_t)i)) {
@@ -707,7 +710,9 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
         scale *= std::sqrt(fro);
       }
       ok = qsets[i]->pair_step * scale * mols[i]->rbound <= (1.0 / 8) * (1.0 - 1e-9);
+      max_step = std::max(max_step, qsets[i]->pair_step * scale * mols[i]->rbound);
     }
+    pl.narrow = ok && max_step <= 0.07 * (1.0 - 1e-6);
     if (!ok) {
       var.packed = 2;
       const int mode = precision == SPSIM_PREC_F32_FAST ? 1 : 0;
@@ -808,7 +813,8 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
   if (precision != SPSIM_PREC_FP64) {
     // work items: pixel tile x atom-tile range, cost-sorted (largest first)
     const int occ =
-        std::max(1, sf_f32_occupancy(precision == SPSIM_PREC_F32_FAST ? 1 : 0, nt, ppt, pl.packed, perb, pl.fixw));
+        std::max(1, sf_f32_occupancy(precision == SPSIM_PREC_F32_FAST ? 1 : 0, nt, ppt, pl.packed, perb, pl.fixw,
+                                     pl.narrow));
     const long long slots = (long long)num_sms() * occ;
     long long total_ptiles = 0;
     for (int i = 0; i < npat; ++i) total_ptiles += (qsets[i]->npix + tile_pix - 1) / tile_pix;
@@ -881,7 +887,7 @@ static cudaError_t enqueue_plan(Plan &pl, cudaStream_t stream, cudaEvent_t ev0, 
     const int mode = pl.precision == SPSIM_PREC_F32_FAST ? PREC_MODE_MUFU : PREC_MODE_POLY;
     int *flags = (int *)pl.flags.p;
     if ((e = launch_sf_f32(mode, pl.nt, pl.ppt, pl.packed, pl.perb, (const SfPattern *)pl.pats.p, (const WorkItem *)pl.items.p,
-                           pl.n_items, flags, flags + 4, pl.grid, stream, pl.fixw)))
+                           pl.n_items, flags, flags + 4, pl.grid, stream, pl.fixw, pl.narrow)))
       return e;
   }
   if (ev1 && (e = cudaEventRecord(ev1, stream))) return e;
@@ -1015,6 +1021,7 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
   g_last_variant[1] = pl->precision == SPSIM_PREC_FP64 ? 1 : pl->ppt;
   g_last_variant[2] = pl->precision == SPSIM_PREC_FP64 ? -1 : pl->packed;
   g_last_phase_word = pl->precision != SPSIM_PREC_FP64 && pl->fixw ? 1 : 0;
+  g_last_pair_narrow = pl->precision == SPSIM_PREC_F32 && pl->packed == 3 && pl->fixw && pl->narrow ? 1 : 0;
   CUDA_TRY(refresh_rotations(*pl, rot, stream));
   if (g_timing || !cache || stream == nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1426,6 +1433,11 @@ extern "C" int spsim_b200_last_variant(int *threads, int *pixels_per_thread, int
 
 extern "C" int spsim_b200_last_phase_word(int *on) {
   if (on) *on = g_last_phase_word;
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_last_pair_narrow(int *on) {
+  if (on) *on = g_last_pair_narrow;
   return SPSIM_OK;
 }
 

@@ -10,12 +10,14 @@ float32 Horner evaluation (with fused multiply-add, as the kernel does it) is
 measured and printed into the header.  No library sin/cos internals are used:
 the reference values come from numpy's float64 sin/cos.
 
-Three domains are generated:
+The domains generated:
   HALF:  |y| <= 1/4 + 1/16  (half-cycle reduction plus the phase cross-term)
   QUAD:  |y| <= 1/8 + 1/16  (quarter-cycle reduction plus the cross-term)
   DHALF: |y| <= 1/4         (half-cycle reduction of an FP64 phase, no cross-term)
   WIDE:  |y| <= 3/8         (the second pixel of a neighbour pair: DHALF plus a
                              step of at most 1/8 cycle)
+  NARROW: |y| <= 0.32       (the same where every step is at most 0.07 cycle:
+                             one sine coefficient fewer at WIDE's accuracy)
 Degrees are the smallest whose float32 evaluation stays near the float32
 rounding floor (a higher sine degree on HALF only adds rounding error).
 
@@ -127,6 +129,7 @@ def main():
     emit("QUAD", 0.125 + 1.0 / 16, 4, 4, out)
     emit("DHALF", 0.25, 4, 4, out)
     emit("WIDE", 0.375, 5, 5, out)
+    emit("NARROW", 0.32, 4, 5, out)
     out += ["#endif", ""]
     print("\n".join(out))
 

@@ -724,7 +724,9 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dphase_kernel(cons
 // P/2 pairs; two pairs' anchors and two pairs' seconds share each packed
 // f32x2 polynomial.
 
-template <int MODE, int NT, int P, bool PERB, bool FIXW>
+// NARROW: every pair's step is at most 0.07 cycle (host-checked), so the
+// second pixel's |y| <= 0.32 takes the NARROW polynomial, one FMA shorter.
+template <int MODE, int NT, int P, bool PERB, bool FIXW, bool NARROW = false>
 __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const SfPattern *__restrict__ pats,
                                                       const WorkItem *__restrict__ items, int n_items,
                                                       int *__restrict__ queue, int *__restrict__ err, uint32_t m31) {
@@ -883,16 +885,29 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
               float2 Sa, Ca;
               sincos_dhalf_poly2(Ya, Sa, Ca);
               const float2 zb = mul2(Yb, Yb);
-              float2 ps = fma2(zb, f2(SPSIM_WIDE_S5), f2(SPSIM_WIDE_S4));
-              ps = fma2(zb, ps, f2(SPSIM_WIDE_S3));
-              ps = fma2(zb, ps, f2(SPSIM_WIDE_S2));
-              ps = fma2(zb, ps, f2(SPSIM_WIDE_S1));
-              ps = fma2(zb, ps, f2(SPSIM_WIDE_S0));
-              float2 pc = fma2(zb, f2(SPSIM_WIDE_C5), f2(SPSIM_WIDE_C4));
-              pc = fma2(zb, pc, f2(SPSIM_WIDE_C3));
-              pc = fma2(zb, pc, f2(SPSIM_WIDE_C2));
-              pc = fma2(zb, pc, f2(SPSIM_WIDE_C1));
-              pc = fma2(zb, pc, f2(SPSIM_WIDE_C0));
+              float2 ps, pc;
+              if (NARROW) {
+                ps = fma2(zb, f2(SPSIM_NARROW_S4), f2(SPSIM_NARROW_S3));
+                ps = fma2(zb, ps, f2(SPSIM_NARROW_S2));
+                ps = fma2(zb, ps, f2(SPSIM_NARROW_S1));
+                ps = fma2(zb, ps, f2(SPSIM_NARROW_S0));
+                pc = fma2(zb, f2(SPSIM_NARROW_C5), f2(SPSIM_NARROW_C4));
+                pc = fma2(zb, pc, f2(SPSIM_NARROW_C3));
+                pc = fma2(zb, pc, f2(SPSIM_NARROW_C2));
+                pc = fma2(zb, pc, f2(SPSIM_NARROW_C1));
+                pc = fma2(zb, pc, f2(SPSIM_NARROW_C0));
+              } else {
+                ps = fma2(zb, f2(SPSIM_WIDE_S5), f2(SPSIM_WIDE_S4));
+                ps = fma2(zb, ps, f2(SPSIM_WIDE_S3));
+                ps = fma2(zb, ps, f2(SPSIM_WIDE_S2));
+                ps = fma2(zb, ps, f2(SPSIM_WIDE_S1));
+                ps = fma2(zb, ps, f2(SPSIM_WIDE_S0));
+                pc = fma2(zb, f2(SPSIM_WIDE_C5), f2(SPSIM_WIDE_C4));
+                pc = fma2(zb, pc, f2(SPSIM_WIDE_C3));
+                pc = fma2(zb, pc, f2(SPSIM_WIDE_C2));
+                pc = fma2(zb, pc, f2(SPSIM_WIDE_C1));
+                pc = fma2(zb, pc, f2(SPSIM_WIDE_C0));
+              }
               const float2 Sb = mul2(Yb, ps);
               const float2 wsa = make_float2(sign_by_parity(wa.x, kb[0], m31), sign_by_parity(wa.y, kb[1], m31));
               const float2 wsb = PERB ? make_float2(sign_by_parity(wb.x, kb[0], m31), sign_by_parity(wb.y, kb[1], m31))
@@ -1262,11 +1277,11 @@ cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix,
 // scalar compensated kernel (sf_f32_kernel), 1 the pixel-pair compensated one
 // (sf_f32x2_kernel), 2 the pixel-pair FP64-phase one (sf_dphase_kernel), 3 the
 // FP64-anchored neighbour pairs (sf_dpair_kernel).
-template <int MODE, int NT, int P, bool PERB, int PK, bool FW>
+template <int MODE, int NT, int P, bool PERB, int PK, bool FW, bool NW = false>
 static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, int n_items, int *queue, int *err,
                                 int grid, cudaStream_t st) {
   if constexpr (PK == 3)
-    sf_dpair_kernel<MODE, NT, P, PERB, FW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
+    sf_dpair_kernel<MODE, NT, P, PERB, FW, NW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
   else if constexpr (PK == 2)
     sf_dphase_kernel<MODE, NT, P, PERB, FW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
   else if constexpr (PK == 1)
@@ -1276,11 +1291,11 @@ static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, in
   return cudaGetLastError();
 }
 
-template <int MODE, int NT, int P, bool PERB, int PK, bool FW>
+template <int MODE, int NT, int P, bool PERB, int PK, bool FW, bool NW = false>
 static int occupancy_t() {
   int n = 0;
   if constexpr (PK == 3)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dpair_kernel<MODE, NT, P, PERB, FW>, NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dpair_kernel<MODE, NT, P, PERB, FW, NW>, NT, 0);
   else if constexpr (PK == 2)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dphase_kernel<MODE, NT, P, PERB, FW>, NT, 0);
   else if constexpr (PK == 1)
@@ -1328,9 +1343,12 @@ static int occupancy_t() {
 // the compensated forms ignore it.
 cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
                           const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st,
-                          bool fixw) {
+                          bool fixw, bool narrow) {
 #define X(M, N, PP, PK)                                                                                   \
   if (mode == M && nt == N && p == PP && packed == PK) {                                                  \
+    if (narrow && fixw && PK == 3 && M == PREC_MODE_POLY)                                                 \
+      return perb ? launch_f32_t<M, N, PP, true, PK, true, true>(pats, items, n_items, queue, err, grid, st) \
+                  : launch_f32_t<M, N, PP, false, PK, true, true>(pats, items, n_items, queue, err, grid, st); \
     if (fixw && PK >= 2)                                                                                  \
       return perb ? launch_f32_t<M, N, PP, true, PK, true>(pats, items, n_items, queue, err, grid, st)    \
                   : launch_f32_t<M, N, PP, false, PK, true>(pats, items, n_items, queue, err, grid, st);  \
@@ -1342,9 +1360,12 @@ cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const 
   return cudaErrorInvalidConfiguration;
 }
 
-int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw) {
+int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw, bool narrow) {
 #define X(M, N, PP, PK)                                                                          \
   if (mode == M && nt == N && p == PP && packed == PK) {                                         \
+    if (narrow && fixw && PK == 3 && M == PREC_MODE_POLY)                                        \
+      return perb ? occupancy_t<M, N, PP, true, PK, true, true>()                                \
+                  : occupancy_t<M, N, PP, false, PK, true, true>();                              \
     if (fixw && PK >= 2)                                                                         \
       return perb ? occupancy_t<M, N, PP, true, PK, true>() : occupancy_t<M, N, PP, false, PK, true>(); \
     return perb ? occupancy_t<M, N, PP, true, PK, false>() : occupancy_t<M, N, PP, false, PK, false>(); \

@@ -9,11 +9,13 @@ namespace spsim {
 cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix, int n_elem, const float *coeffs,
                             double B, int delta_atoms, double *ff, cudaStream_t st);
 // fixw: the FP64-phase forms (2, 3) take the fixed-point phase word, valid
-// while |q|max |r - c|max < 2^18 cycles (the host checks 2^17)
+// while |q|max |r - c|max < 2^18 cycles (the host checks 2^17); narrow: the
+// neighbour-pair form (3, FP32 polynomial, fixw) with every pair's step at
+// most 0.07 cycle evaluates its second pixels with the NARROW polynomial
 cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
                           const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st,
-                          bool fixw = false);
-int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw = false);
+                          bool fixw = false, bool narrow = false);
+int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw = false, bool narrow = false);
 bool sf_f32_variant_exists(int mode, int nt, int p, int packed);
 cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cudaStream_t st);
 cudaError_t launch_spectrum_combine(const SfPattern *pats, int pattern0, int S, const double *weight, float *F,

@@ -257,6 +257,39 @@ def test_neighbour_pair_form_admission(cuda):
         assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (kernel, e_max, e_l2)
 
 
+@pytest.mark.parametrize("step,narrow", [(0.065, True), (0.11, False)])
+def test_neighbour_pair_step_selects_second_pixel_polynomial(cuda, step, narrow):
+    # pairs whose step |q_b - q_a| times the molecule's bound (its bounding-box
+    # radius plus the refinement margin) stays within 0.07 cycle evaluate the
+    # second pixel with the shorter NARROW polynomial; steps up to 1/8 cycle
+    # keep the WIDE one; both stay within tolerance, on the steepest step the
+    # admission allows, with and without per-atom B factors
+    Z, pos = synth.random_molecule(3000, 3e-9, 41)
+    p64 = pos.astype(np.float64)
+    c = 0.5 * (p64.min(0) + p64.max(0))
+    rmax = np.linalg.norm(p64 - c, axis=1).max()
+    rbound = rmax + max(0.05 * rmax, 5e-10)
+    rng = np.random.Generator(np.random.PCG64(42))
+    qa = rng.normal(size=(4096, 3)) * 1.5e9
+    u = rng.normal(size=(4096, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    hkl = np.stack([qa, qa + u * (step / rbound)], axis=1).reshape(-1, 3).astype(np.float32)
+    bfac = rng.uniform(0, 40, len(Z)).astype(np.float32)
+    for kw in ({}, {"bfac": bfac}):
+        _, I64 = O.structure_factor(Z, p64, hkl.astype(np.float64), **kw)
+        try:
+            core.set_variant(128, 8, 3)
+            _, I = _run(Z, pos, hkl, "f32", **kw)
+            assert core.kernel_name() == "sf_dpair_kernel" and core.last_phase_word()
+            assert core.last_pair_narrow() == narrow
+        finally:
+            core.set_variant(-1)
+        e_max, e_l2 = intensity_errors(I, I64)
+        assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (step, kw.keys(), e_max, e_l2)
+        _, I = _run(Z, pos, hkl, "f32_fast", **kw)
+        assert not core.last_pair_narrow()  # the MUFU forms have no polynomial
+
+
 CANDIDATES = {(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1), (128, 2, 2),
               (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2), (128, 4, 3), (128, 8, 3), (128, 12, 3), (256, 4, 3)}
 
