@@ -481,9 +481,45 @@ def _modes(args, core, mol, qs, rot, terms, timed, prec):
     torch.cuda.synchronize()
     out["accuracy"] = {"reference": "plain FP64 GPU kernel", "pixels": "every 64th detector row (16,384)",
                        "floor": "1e-3 x mean intensity", **acc}
+    out["nufft"] = _nufft_mode(core, mol, qs, rot, terms, sub_rows, I64)
     out["fp64_plain"] = {"kernel_terms_per_s": fp64_rate, "sample": "every 8th pixel",
                          "f32_speedup": None, "f32_fast_speedup": None}
     return out
+
+
+def _nufft_mode(core, mol, qs, rot, terms, sub_rows, I64, eps=1e-9, steps=5):
+    """The same structure factor by the type-3 NUFFT (spsim_b200_forward_nufft,
+    the reference's use_nfft_for_sf path): device-resident time per pattern
+    (CUDA events around the call, L2 flushed between calls), the equivalent
+    atom.pixel terms/s, and its |F|^2 error on the accuracy rows."""
+    import torch
+
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    F = torch.empty(qs.npix, dtype=torch.complex64, device="cuda")
+    I = torch.empty(qs.npix, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        core.forward_nufft(mol, qs, rot=rot, eps=eps, F=F, I=I)
+    torch.cuda.synchronize()
+    core.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in evs:
+        flush.zero_()
+        a.record()
+        core.forward_nufft(mol, qs, rot=rot, eps=eps, F=F, I=I)
+        b.record()
+    torch.cuda.synchronize()
+    core.synchronize()
+    ms = statistics.median(a.elapsed_time(b) for a, b in evs)
+    w1, w2, n2 = core.last_nufft_grid()
+    _, In = core.forward_nufft(mol, sub_rows, rot=rot, eps=eps)
+    In = In.double().cpu().numpy()
+    den = np.maximum(I64, 1e-3 * I64.mean())
+    return {"ms_per_pattern": ms, "equivalent_terms_per_s": terms / (ms * 1e-3), "eps": eps,
+            "kernel_widths": [w1, w2], "fft_grid": list(n2),
+            "accuracy": {"floored_max_rel": float(np.max(np.abs(In - I64) / den)),
+                         "l2_rel": float(np.linalg.norm(In - I64) / np.linalg.norm(I64))},
+            "note": "type-3 NUFFT per element (spread, pad, cuFFT Z2Z, interpolate; FP64 grids), "
+                    "a different algorithm from the direct sum the headline value times"}
 
 
 def _e2e(args, w, Z, pos, terms, world, dist=None):
@@ -589,6 +625,20 @@ def profile_case(precisions):
 
     from spsim_b200 import core, synth
 
+    if "nufft" in precisions or "nufft_small" in precisions:
+        # the NUFFT structure factor: the 50,000-atom / 1024^2 workload, or the
+        # 20,000-atom / 256^2 case; two calls (the first sizes the grids)
+        w = synth.WORKLOADS["precision_50k" if "nufft" in precisions else "orientations_20k"]
+        Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+        d = w["det"]
+        mol = core.Molecule(Z, pos)
+        qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
+        for _ in range(2):
+            core.forward_nufft(mol, qs)
+        torch.cuda.synchronize()
+        core.synchronize()
+        print("profile case ok", core.last_nufft_grid())
+        return 0
     if "adjoint" in precisions:
         w = synth.WORKLOADS["adjoint_5k"]
         Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
@@ -754,7 +804,9 @@ def main():
     ap.add_argument("--no-modes", action="store_true", help="skip the f32_fast / fp64 / accuracy extras")
     ap.add_argument("--profile-case", default=None,
                     help="comma-separated precisions: one forward each on the 20,000-atom x 256^2 case, or "
-                         "\"adjoint\": one forward and one adjoint of the 5,000-atom refinement shape (for ncu)")
+                         "\"adjoint\": one forward and one adjoint of the 5,000-atom refinement shape, "
+                         "\"nufft\" / \"nufft_small\": two NUFFT forwards of the 50,000-atom / 1024^2 workload or "
+                         "the 20,000-atom / 256^2 case (for ncu)")
     ap.add_argument("--sweep", action="store_true", help="time every compiled FP32 kernel variant")
     ap.add_argument("--workloads", action="store_true", help="time the batched workloads (orientations, uneven, "
                                                               "adjoint)")

@@ -39,6 +39,8 @@ Diffraction_Pattern *cuda_compute_pattern_on_list(Molecule *mol, float *HKL_list
                                                   Experiment *exp, Options *opts);   /* src/diffraction.cu:135 */
 Diffraction_Pattern *cuda_compute_pattern_on_list2(Molecule *mol, float *HKL_list, int HKL_list_size, float B,
                                                    Experiment *exp, Options *opts);  /* src/diffraction.cu:235 */
+Diffraction_Pattern *compute_pattern_on_list_by_nfft(Molecule *mol, float *HKL_list, int HKL_list_size, CCD *det,
+                                                     float B, Options *opts);        /* src/diffraction.c:528 */
 Diffraction_Pattern *compute_sf(Molecule *mol, float *HKL_list, int HKL_list_size, Options *opts); /* src/spsim.c:110 */
 
 /* ---- detector chain: include/diffraction.h:85-89, include/noise.h:33, include/amplification.h:24-26 ---- */
@@ -97,6 +99,11 @@ void sum_patterns(Diffraction_Pattern *pat);                             /* src/
  * of the noise stages (simulate_shot sets it from opts->random_seed). */
 void spsim_b200_set_legacy_precision(int precision);
 int spsim_b200_get_legacy_precision(void);
+/* Relative error of the NUFFT structure factor behind
+ * compute_pattern_on_list_by_nfft and use_nfft_for_sf (default 1e-9; see
+ * spsim_b200_forward_nufft). */
+void spsim_b200_set_legacy_nufft_eps(double eps);
+double spsim_b200_get_legacy_nufft_eps(void);
 void spsim_b200_set_noise_seed(unsigned long long seed);
 
 #ifdef __cplusplus

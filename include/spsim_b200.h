@@ -153,6 +153,36 @@ int spsim_b200_structure_factor_host_spectrum(int natoms, const int32_t *Z, cons
                                               float wavelength, float bandwidth, int samples, int64_t npix,
                                               const float *hkl, int precision, float *F_host, float *I_host);
 
+/* ---- non-uniform FFT structure factor --------------------------------------
+ * The same F(q) = sum_e f_e(|q|) sum_{j in e} w_j exp(-2 pi i q.r_j) as
+ * spsim_b200_forward, computed per element as a type-3 non-uniform FFT
+ * (atoms spread onto a real-space grid, one batched 3-D FFT, interpolation at
+ * every pixel's q; FP64 grids) in O(atoms w^3 + grid log grid + pixels w^3)
+ * instead of O(atoms x pixels).  Replaces the reference's NNFFT path
+ * (compute_pattern_on_list_by_nfft, src/diffraction.c:528-675, dispatched by
+ * compute_sf when use_nfft_for_sf is set, src/spsim.c:120-126), which runs
+ * the NFFT library with a cut-off of m = 2.
+ * eps: requested relative L2 error of F against the exact sum, in
+ * [1e-14, 1e-2]; it sets the kernel width w = ceil(-log10 eps) + 1 grid points
+ * (interpolation) and w + 1 (spreading), up to 15.  The grid follows the
+ * bounding box of R q and the molecule's radius: (4 S_d |r - c|max * 2 + w)
+ * * 2 points per axis (S_d: half-width of the q box along d).
+ * Not supported: per-atom B factors (SPSIM_ERR_INVALID_ARG).  F_dev, I_dev
+ * as spsim_b200_forward; enqueued on `stream` after a one-time read-back of
+ * the q box per (q set, rotation); atoms that moved outside the creation-time
+ * bounds are left out and reported as SPSIM_ERR_RANGE by
+ * spsim_b200_synchronize.  No reference counterpart beyond the NNFFT path. */
+int spsim_b200_forward_nufft(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot, float B,
+                             double eps, float *F_dev, float *I_dev, void *stream);
+/* Kernel widths (spreading, interpolation) and FFT grid (x, y, z) of the last
+ * NUFFT forward on this thread. */
+int spsim_b200_last_nufft_grid(int *w_spread, int *w_interp, int *n2);
+/* The NUFFT structure factor of host arrays with unit atom weights (the
+ * reference NNFFT's semantics: no illumination weights), host F (complex64)
+ * and I out; synchronous. */
+int spsim_b200_structure_factor_host_nufft(int natoms, const int32_t *Z, const float *pos, float B, int delta_atoms,
+                                           int64_t npix, const float *hkl, double eps, float *F_host, float *I_host);
+
 /* ---- allocation-free variant (no counterpart in the reference) ------------
  * The same computation, arguments and results as
  * spsim_b200_structure_factor_host, for callers that may not allocate device

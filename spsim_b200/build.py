@@ -35,7 +35,7 @@ CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-result", "-Werro
             "-ffp-contract=off",
             "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["sf_kernels.cu", "chain_kernels.cu", "adjoint_kernels.cu", "capi.cu", "noalloc.cu"]
+CU_SOURCES = ["sf_kernels.cu", "chain_kernels.cu", "adjoint_kernels.cu", "nufft_kernels.cu", "capi.cu", "noalloc.cu"]
 C_SOURCES = ["host/config.c", "host/legacy.c", "host/molecule.c", "host/crystal.c"]
 
 
@@ -107,7 +107,9 @@ def build(force=False, verbose=False):
     if force or _newer(out, objs + [vmap]):
         tmp = out + ".tmp"
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs +
-             ["-Xlinker", "--version-script=" + vmap, "-Xlinker", "-Bsymbolic", "-lrt", "-ldl", "-lpthread"],
+             ["-Xlinker", "--version-script=" + vmap, "-Xlinker", "-Bsymbolic",
+              "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft",
+              "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64"), "-lrt", "-ldl", "-lpthread"],
              verbose)
         shutil.move(tmp, out)
     cli = os.path.join(LIBDIR, "spsim")

@@ -16,6 +16,9 @@
 #include "chain_kernels.cuh"
 #include "adjoint_kernels.cuh"
 #include "sf_kernels.cuh"
+#include "nufft_kernels.cuh"
+
+#include <cufft.h>
 
 using namespace spsim;
 
@@ -1353,7 +1356,16 @@ extern "C" int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z
                           false);
 }
 
+static int nufft_check_flags(int dev);
+
 extern "C" int spsim_internal_shot_check(void) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int st = nufft_check_flags(dev);
+    if (st) return st;
+  }
   if (!g_oneshot.plan) return SPSIM_OK;
   return check_flags(*g_oneshot.plan);
 }
@@ -1381,6 +1393,302 @@ extern "C" int spsim_b200_structure_factor_host_spectrum(int natoms, const int32
 }
 
 // ---------------------------------------------------------------------------
+// Non-uniform FFT structure factor (nufft_kernels.cuh): the same F(q) as the
+// direct sum, computed per element by spreading the atoms onto a real-space
+// grid, one batched 3-D FFT and interpolation at every pixel's q, with FP64
+// grids.  Its cost is O(atoms w^3 + grid log grid + pixels w^3) instead of
+// O(atoms x pixels).  One context per device, under g_mu; calls on different
+// streams are ordered by the context's completion event.
+
+struct NufftCtx {
+  DevBuf small, fine, dec, seg, keys, flags;
+  cufftHandle fft = 0;
+  int fft_dims[4] = {0, 0, 0, 0};  // n2z, n2y, n2x, elements
+  std::vector<double> geom_key;
+  unsigned long long seg_mol = 0;  // molecule whose segment table is on the device
+  NufftGeom g;
+  int n_coef = 0;
+  double psi_a[NUFFT_MAX_COEF];
+  unsigned long long *h_keys = nullptr;  // pinned bounds read-back
+  cudaEvent_t done = nullptr;
+  bool has_done = false;
+};
+static std::map<int, NufftCtx> g_nufft;
+static thread_local int g_last_nufft_w[2] = {0, 0};
+static thread_local int g_last_nufft_n2[3] = {0, 0, 0};
+
+static int fft_size(int n) {  // smallest even size >= n with prime factors 2, 3, 5, 7
+  for (int m = std::max(n, 2);; ++m) {
+    if (m & 1) continue;
+    int r = m;
+    for (int f : {2, 3, 5, 7})
+      while (r % f == 0) r /= f;
+    if (r == 1) return m;
+  }
+}
+
+static double es_host(double u, double w, double beta) {
+  const double t = 2.0 * u / w, a = 1.0 - t * t;
+  return a >= 0.0 ? std::exp(beta * (std::sqrt(a) - 1.0)) : 0.0;
+}
+
+// Fourier transform of the ES kernel, int es(u) e^{-2 pi i xi u} du, by the
+// trapezoid rule at spacing d (spectrally accurate: the kernel is smooth and
+// vanishes to e^{-beta} at its ends)
+static double es_hat_host(double xi, double w, double beta, double d) {
+  const int n = (int)std::floor(0.5 * w / d);
+  double s = 0.5 * es_host(0.0, w, beta);
+  for (int i = 1; i <= n; ++i) s += es_host(i * d, w, beta) * std::cos(2.0 * M_PI * xi * i * d);
+  return 2.0 * d * s;
+}
+
+// Kernel width (grid points) for a requested relative error of F: measured
+// relative L2 errors against the direct sum are ~5 x 10^-w at sigma = 2.
+static int nufft_width(double eps) {
+  const int w = (int)std::ceil(-std::log10(eps)) + 1;
+  return std::min(std::max(w, NUFFT_MIN_W), NUFFT_MAX_W - 1);
+}
+
+static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot, float B,
+                         double eps, float *F_dev, float *I_dev, cudaStream_t st) {
+  if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
+  if (!(eps >= 1e-14 && eps <= 1e-2)) return fail(SPSIM_ERR_INVALID_ARG, "eps %g outside [1e-14, 1e-2]", eps);
+  if (m->per_atom_b)
+    return fail(SPSIM_ERR_INVALID_ARG, "per-atom B factors are not supported by the NUFFT structure factor");
+  int dev;
+  int st0 = current_device(&dev);
+  if (st0) return st0;
+  if (m->device != dev || qs->device != dev) return fail(SPSIM_ERR_INVALID_ARG, "handle belongs to another device");
+  const long long npix = qs->npix;
+  if (npix == 0) return SPSIM_OK;
+  if (m->n_kept == 0) {
+    if (F_dev) CUDA_TRY(cudaMemsetAsync(F_dev, 0, 2 * npix * sizeof(float), st));
+    if (I_dev) CUDA_TRY(cudaMemsetAsync(I_dev, 0, npix * sizeof(float), st));
+    return SPSIM_OK;
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  NufftCtx &c = g_nufft[dev];
+  if (!c.h_keys) CUDA_TRY(cudaMallocHost(&c.h_keys, 6 * sizeof(unsigned long long)));
+  if (!c.done) CUDA_TRY(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+  if (c.has_done) CUDA_TRY(cudaStreamWaitEvent(st, c.done, 0));  // the buffers' previous user
+  CUDA_TRY(c.flags.ensure(sizeof(int)));
+  if (!c.has_done) CUDA_TRY(cudaMemsetAsync(c.flags.p, 0, sizeof(int), st));
+
+  const int n_elem = m->n_elem;
+  std::vector<double> key = {(double)qs->id, (double)npix, m->rbound, (double)n_elem, eps, rot ? 1.0 : 0.0};
+  if (rot) key.insert(key.end(), rot, rot + 9);
+  if (key != c.geom_key) {
+    // q box of R q over the list (one read-back), then the grids
+    c.geom_key.clear();
+    CUDA_TRY(c.keys.ensure(6 * sizeof(unsigned long long)));
+    unsigned long long *dk = (unsigned long long *)c.keys.p;
+    CUDA_TRY(nufft_bounds(qs->d_hkl, qs->d_q64, npix, rot, dk, st));
+    CUDA_TRY(cudaMemcpyAsync(c.h_keys, dk, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = nufft_key_to_double(c.h_keys[d]);
+      hi[d] = nufft_key_to_double(c.h_keys[3 + d]);
+      if (!(std::isfinite(lo[d]) && std::isfinite(hi[d])))
+        return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: non-finite q in the list");
+    }
+    const int w = nufft_width(eps);
+    const double sigma1 = 2.0, sigma2 = 2.0;
+    NufftGeom g;
+    std::memset(&g, 0, sizeof(g));
+    g.w1 = w + 1;
+    g.w2 = w;
+    g.beta1 = 0.97 * M_PI * g.w1 * (1.0 - 0.5 / sigma1);
+    g.beta2 = 0.97 * M_PI * g.w2 * (1.0 - 0.5 / sigma2);
+    const double X = m->rbound;
+    size_t cells1 = 1, cells2 = 1;
+    for (int d = 0; d < 3; ++d) {
+      g.cq[d] = 0.5 * (lo[d] + hi[d]);
+      const double S = std::max(0.5 * (hi[d] - lo[d]), 1e-3 / X);
+      g.h[d] = 1.0 / (2.0 * sigma1 * S);
+      g.inv_h[d] = 2.0 * sigma1 * S;
+      const double n1 = std::ceil(2.0 * X * g.inv_h[d]) + g.w1 + 2;
+      if (n1 > 4096) return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: %.0f grid points along axis %d; use the direct sum", n1, d);
+      g.n1[d] = (int)n1 + ((int)n1 & 1);
+      g.n2[d] = fft_size((int)std::ceil(sigma2 * g.n1[d]));
+      g.L[d] = g.h[d] * g.n2[d];
+      cells1 *= (size_t)g.n1[d];
+      cells2 *= (size_t)g.n2[d];
+    }
+    const size_t bytes1 = cells1 * n_elem * sizeof(double2), bytes2 = cells2 * n_elem * sizeof(double2);
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const size_t have = free_b + c.small.cap + c.fine.cap;
+    if (bytes1 + 2 * bytes2 > have / 10 * 9)
+      return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: grids of %.3g GB do not fit; use the direct sum",
+                  (bytes1 + 2.0 * bytes2) * 1e-9);
+    // 1 / phi2hat per spreading-grid index, and psi1hat's trapezoid coefficients
+    std::vector<double> dec;
+    for (int d = 0; d < 3; ++d)
+      for (int l = 0; l < g.n1[d]; ++l)
+        dec.push_back(1.0 / es_hat_host((double)(l - g.n1[d] / 2) / g.n2[d], g.w2, g.beta2, 0.01));
+    c.n_coef = (int)std::floor(0.5 * g.w1 / 0.25) + 1;
+    for (int k = 0; k < c.n_coef; ++k) c.psi_a[k] = 0.25 * (k == 0 ? 1.0 : 2.0) * es_host(0.25 * k, g.w1, g.beta1);
+    CUDA_TRY(c.small.ensure(bytes1));
+    CUDA_TRY(c.fine.ensure(bytes2));
+    CUDA_TRY(c.dec.ensure(dec.size() * sizeof(double)));
+    CUDA_TRY(cudaMemcpyAsync(c.dec.p, dec.data(), dec.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    const int dims[4] = {g.n2[2], g.n2[1], g.n2[0], n_elem};
+    if (!c.fft || std::memcmp(dims, c.fft_dims, sizeof(dims)) != 0) {
+      if (c.fft) {
+        cufftDestroy(c.fft);
+        c.fft = 0;
+      }
+      int n[3] = {dims[0], dims[1], dims[2]};
+      const int dist = dims[0] * dims[1] * dims[2];
+      if (cufftPlanMany(&c.fft, 3, n, nullptr, 1, dist, nullptr, 1, dist, CUFFT_Z2Z, n_elem) != CUFFT_SUCCESS) {
+        c.fft = 0;
+        return fail(SPSIM_ERR_CUDA, "NUFFT: cuFFT plan %d x %d x %d x %d failed", dims[0], dims[1], dims[2], n_elem);
+      }
+      std::memcpy(c.fft_dims, dims, sizeof(dims));
+    }
+    // the read-back and the dec upload above are complete when this returns
+    CUDA_TRY(cudaStreamSynchronize(st));
+    c.g = g;
+    c.geom_key = key;
+  }
+  if (c.seg_mol != m->id) {
+    // element segments of the padded atom records
+    std::vector<int> seg(n_elem + 1, 0);
+    for (const TileDesc &t : m->tiles) seg[t.elem + 1] = std::max(seg[t.elem + 1], t.atom_begin + t.count);
+    CUDA_TRY(c.seg.ensure(seg.size() * sizeof(int)));
+    CUDA_TRY(cudaMemcpy(c.seg.p, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice));
+    c.seg_mol = m->id;
+  }
+  NufftGeom g = c.g;
+  for (int d = 0; d < 3; ++d) g.center[d] = m->center[d];
+  size_t cells1 = (size_t)g.n1[0] * g.n1[1] * g.n1[2];
+  CUDA_TRY(cudaMemsetAsync(c.small.p, 0, cells1 * n_elem * sizeof(double2), st));
+  CUDA_TRY(nufft_spread(m->d_atomsd, (const int *)c.seg.p, n_elem, m->n_padded, g, (double2 *)c.small.p,
+                        (int *)c.flags.p, st));
+  CUDA_TRY(nufft_pad((const double2 *)c.small.p, (double2 *)c.fine.p, g, n_elem, (const double *)c.dec.p, st));
+  if (cufftSetStream(c.fft, st) != CUFFT_SUCCESS) return fail(SPSIM_ERR_CUDA, "NUFFT: cufftSetStream failed");
+  if (cufftExecZ2Z(c.fft, (cufftDoubleComplex *)c.fine.p, (cufftDoubleComplex *)c.fine.p, CUFFT_FORWARD) !=
+      CUFFT_SUCCESS)
+    return fail(SPSIM_ERR_CUDA, "NUFFT: cuFFT execution failed");
+  NufftInterp a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = g;
+  a.hkl = qs->d_hkl;
+  a.q64 = qs->d_q64;
+  a.npix = npix;
+  a.has_rot = rot != nullptr;
+  for (int k = 0; k < 9; ++k) a.rot[k] = rot ? rot[k] : 0.0;
+  a.grid = (const double2 *)c.fine.p;
+  a.cell2 = (long long)g.n2[0] * g.n2[1] * g.n2[2];
+  a.n_elem = n_elem;
+  a.coeffs = m->d_coeffs;
+  a.B = (double)B;
+  a.delta_atoms = m->delta_atoms;
+  a.n_coef = c.n_coef;
+  std::memcpy(a.psi_a, c.psi_a, sizeof(a.psi_a));
+  a.F = (float2 *)F_dev;
+  a.I = I_dev;
+  CUDA_TRY(nufft_interp(a, st));
+  CUDA_TRY(cudaEventRecord(c.done, st));
+  c.has_done = true;
+  g_last_nufft_w[0] = g.w1;
+  g_last_nufft_w[1] = g.w2;
+  for (int d = 0; d < 3; ++d) g_last_nufft_n2[d] = g.n2[d];
+  return SPSIM_OK;
+}
+
+// Sticky error word of this device's NUFFT context (atoms outside the grid).
+static int nufft_check_flags(int dev) {
+  auto it = g_nufft.find(dev);
+  if (it == g_nufft.end() || !it->second.flags.p) return SPSIM_OK;
+  int h = 0;
+  CUDA_TRY(cudaMemcpy(&h, it->second.flags.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    CUDA_TRY(cudaMemset(it->second.flags.p, 0, sizeof(int)));
+    return fail(SPSIM_ERR_RANGE, "NUFFT: atoms outside the molecule's creation-time bounds");
+  }
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_b200_forward_nufft(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot,
+                                        float B, double eps, float *F_dev, float *I_dev, void *stream) {
+  return nufft_forward(m, qs, rot, B, eps, F_dev, I_dev, (cudaStream_t)stream);
+}
+
+extern "C" int spsim_b200_last_nufft_grid(int *w_spread, int *w_interp, int *n2) {
+  if (w_spread) *w_spread = g_last_nufft_w[0];
+  if (w_interp) *w_interp = g_last_nufft_w[1];
+  if (n2)
+    for (int d = 0; d < 3; ++d) n2[d] = g_last_nufft_n2[d];
+  return SPSIM_OK;
+}
+
+// Host arrays in and out (the reference-shaped NFFT path): the session
+// molecule and q set of the direct host calls, synchronised before return.
+extern "C" int spsim_b200_structure_factor_host_nufft(int natoms, const int32_t *Z, const float *pos, float B,
+                                                      int delta_atoms, int64_t npix, const float *hkl, double eps,
+                                                      float *F_host, float *I_host) {
+  if (npix < 0 || (npix > 0 && !hkl)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (g_host.device != dev) {
+    g_host = HostSession();
+    g_host.device = dev;
+  }
+  spsim_b200_molecule *m = nullptr;
+  spsim_b200_qset *q = nullptr;
+  st = host_session_molecule(natoms, Z, pos, nullptr, nullptr, delta_atoms, nullptr, &m);
+  if (st) return st;
+  st = host_session_qset(npix, hkl, &q);
+  if (st) return st;
+  if (!g_host.F) g_host.F = new DevBuf();
+  if (!g_host.I) g_host.I = new DevBuf();
+  CUDA_TRY(g_host.F->ensure(2 * std::max<int64_t>(npix, 1) * sizeof(float)));
+  CUDA_TRY(g_host.I->ensure(std::max<int64_t>(npix, 1) * sizeof(float)));
+  float *F = F_host ? (float *)g_host.F->p : nullptr;
+  float *I = I_host ? (float *)g_host.I->p : nullptr;
+  st = nufft_forward(m, q, nullptr, B, eps, F, I, nullptr);
+  if (st) return st;
+  CUDA_TRY(cudaStreamSynchronize(nullptr));
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    st = nufft_check_flags(dev);
+  }
+  if (st) return st;
+  if (F_host && npix) CUDA_TRY(cudaMemcpy(F_host, F, 2 * npix * sizeof(float), cudaMemcpyDeviceToHost));
+  if (I_host && npix) CUDA_TRY(cudaMemcpy(I_host, I, npix * sizeof(float), cudaMemcpyDeviceToHost));
+  return SPSIM_OK;
+}
+
+// simulate_shot with use_nfft_for_sf: the session molecule (unit weights) on
+// the device HKL list, enqueued on the legacy default stream like
+// spsim_internal_shot_structure_factor.
+extern "C" int spsim_internal_shot_structure_factor_nufft(int natoms, const int32_t *Z, const float *pos, float B,
+                                                          int delta_atoms, int64_t npix, const float *hkl_dev,
+                                                          double eps, float *F_dev, float *I_dev) {
+  if (npix < 0 || (npix > 0 && !hkl_dev)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (g_host.device != dev) {
+    g_host = HostSession();
+    g_host.device = dev;
+  }
+  spsim_b200_molecule *m = g_shot_mol;
+  g_shot_mol = nullptr;
+  spsim_b200_qset *q = nullptr;
+  if (!m || m != g_host.mol) {
+    st = host_session_molecule(natoms, Z, pos, nullptr, nullptr, delta_atoms, nullptr, &m);
+    if (st) return st;
+  }
+  st = host_session_qset_device(npix, hkl_dev, nullptr, &q);
+  if (st) return st;
+  return nufft_forward(m, q, nullptr, B, eps, F_dev, I_dev, nullptr);
+}
+
+// ---------------------------------------------------------------------------
 // completion, timing, statistics, variants
 
 extern "C" int spsim_b200_synchronize(void *stream) {
@@ -1390,7 +1698,9 @@ extern "C" int spsim_b200_synchronize(void *stream) {
     int st = check_flags(*p);
     if (st) return st;
   }
-  return SPSIM_OK;
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  return nufft_check_flags(dev);
 }
 
 extern "C" int spsim_b200_timing_enable(int enable) {

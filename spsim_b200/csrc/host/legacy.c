@@ -20,11 +20,14 @@
 #include "../../../include/spsim_b200.h"
 
 static int g_precision = SPSIM_PREC_F32;
+static double g_nufft_eps = 1e-9;
 static unsigned long long g_seed = 0x5eed5eedULL;
 static uint32_t g_pattern_counter = 0;
 
 void spsim_b200_set_legacy_precision(int precision) { g_precision = precision; }
 int spsim_b200_get_legacy_precision(void) { return g_precision; }
+void spsim_b200_set_legacy_nufft_eps(double eps) { g_nufft_eps = eps; }
+double spsim_b200_get_legacy_nufft_eps(void) { return g_nufft_eps; }
 void spsim_b200_set_noise_seed(unsigned long long seed) { g_seed = seed; }
 
 static void die(const char *where, int st) {
@@ -104,6 +107,9 @@ int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z, const flo
                                          const float *beam, float wavelength, float bandwidth, int samples,
                                          int64_t npix, const float *hkl_dev, int precision, float *F_dev,
                                          float *I_dev);
+int spsim_internal_shot_structure_factor_nufft(int natoms, const int32_t *Z, const float *pos, float B,
+                                               int delta_atoms, int64_t npix, const float *hkl_dev, double eps,
+                                               float *F_dev, float *I_dev);
 int spsim_internal_shot_check(void);
 int spsim_internal_shot_molecule(int natoms, const int32_t *Z, const float *pos, int delta_atoms, const float *beam);
 int spsim_internal_rotate_hkl(int64_t npix, const float R[9], float *hkl_dev);
@@ -386,15 +392,51 @@ Diffraction_Pattern *cuda_compute_pattern_on_list2(Molecule *mol, float *HKL_lis
   return pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts, 1);
 }
 
-/* src/spsim.c:110-144: the FFT / NFFT structure factors are other algorithms,
- * not provided; every direct-summation path runs on the GPU.  The dispatch
+/* src/diffraction.c:528-675: the NNFFT structure factor on a q list, with
+ * unit atom weights (no illumination), the form factor of |q| with the B
+ * factor and delta_atoms as the direct sum.  Here a type-3 NUFFT on the GPU
+ * (spsim_b200_forward_nufft) at relative error g_nufft_eps; the reference ran
+ * the NFFT library with a cut-off of m = 2.  The detector is not used (as in
+ * the reference); HKL_list is copied into the result, which the reference
+ * leaves uninitialised. */
+Diffraction_Pattern *compute_pattern_on_list_by_nfft(Molecule *mol, float *HKL_list, int HKL_list_size, CCD *det,
+                                                     float B, Options *opts) {
+  (void)det;
+  double t0 = now_us();
+  const int n = HKL_list_size;
+  Diffraction_Pattern *res = (Diffraction_Pattern *)calloc(1, sizeof(Diffraction_Pattern));
+  res->F = (Complex *)host_alloc(sizeof(Complex) * (n > 0 ? n : 1));
+  res->ints = (float *)host_alloc(sizeof(float) * (n > 0 ? n : 1));
+  res->HKL_list = (float *)host_alloc(sizeof(float) * 3 * (n > 0 ? n : 1));
+  if (n > 0) memcpy(res->HKL_list, HKL_list, sizeof(float) * 3 * n);
+  res->HKL_list_size = n;
+  res->N_pix = n;
+  int st = spsim_b200_structure_factor_host_nufft(mol->natoms, mol->atomic_number, mol->pos, B,
+                                                  opts ? opts->delta_atoms : 0, n, HKL_list, g_nufft_eps,
+                                                  (float *)res->F, res->ints);
+  if (st) die("compute_pattern_on_list_by_nfft", st);
+  if (opts && opts->verbosity_level > 0)
+    printf("%g atoms.pixel/s\n", 1.0e6 * n * mol->natoms / (now_us() - t0));
+  return res;
+}
+
+/* src/spsim.c:110-144: use_nfft_for_sf takes the NUFFT structure factor
+ * (compute_pattern_on_list_by_nfft, as the reference's dispatch); the FFT of
+ * a gridded electron density (use_fft_for_sf) is another algorithm, not
+ * provided.  Every direct-summation path runs on the GPU.  The dispatch
  * follows the reference's: use_cuda == 2 is the first CUDA path, any other
  * non-zero use_cuda the second (with the spectrum), use_cuda == 0 the CPU
  * paths (monochromatic). */
 Diffraction_Pattern *compute_sf(Molecule *mol, float *HKL_list, int HKL_list_size, Options *opts) {
-  if (opts->use_fft_for_sf || opts->use_nfft_for_sf) {
-    fprintf(stderr, "spsim_b200: the FFT/NFFT structure factors are not supported\n");
+  if (opts->use_fft_for_sf) {
+    fprintf(stderr, "spsim_b200: the FFT structure factor (use_fft_for_sf) is not supported\n");
     abort();
+  }
+  if (opts->use_nfft_for_sf) {
+    Diffraction_Pattern *p =
+        compute_pattern_on_list_by_nfft(mol, HKL_list, HKL_list_size, opts->detector, opts->b_factor, opts);
+    p->rot = NULL;
+    return p;
   }
   const int spectrum = opts->use_cuda != 0 && opts->use_cuda != 2;
   Diffraction_Pattern *p =
@@ -569,15 +611,17 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
     fprintf(stderr, "spsim_b200: detector_gaussian_blurring is not supported\n");
     abort();
   }
-  if (opts->use_fft_for_sf || opts->use_nfft_for_sf) {
-    fprintf(stderr, "spsim_b200: the FFT/NFFT structure factors are not supported\n");
+  if (opts->use_fft_for_sf) {
+    fprintf(stderr, "spsim_b200: the FFT structure factor (use_fft_for_sf) is not supported\n");
     abort();
   }
   if (opts->random_seed >= 0) spsim_b200_set_noise_seed((unsigned long long)opts->random_seed);
   const double t0 = now_us();
   const float beam[3] = {exp->beam_fwhm, exp->beam_center_x, exp->beam_center_y};
   /* the molecule first: a changed one waits for the device, which is idle now */
-  int st = spsim_internal_shot_molecule(mol->natoms, mol->atomic_number, mol->pos, opts->delta_atoms, beam);
+  /* the NNFFT path weighs every atom by 1 (no illumination) */
+  int st = spsim_internal_shot_molecule(mol->natoms, mol->atomic_number, mol->pos, opts->delta_atoms,
+                                        opts->use_nfft_for_sf ? NULL : beam);
   if (st) die("simulate_shot molecule", st);
 
   /* geometry (src/spsim.c:98-108, src/diffraction.c:300-323) */
@@ -639,10 +683,14 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   }
   float *dF = (float *)dev_alloc(SLOT_SHOT_F, b_F > 0 ? b_F : 8);
   float *dI = (float *)dev_alloc(SLOT_SHOT_I, b_I > 0 ? b_I : 4);
-  st = spsim_internal_shot_structure_factor(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
-                                            opts->delta_atoms, beam, poly ? exp->wavelength : 0.0f,
-                                            poly ? exp->bandwidth : 0.0f, poly ? samples : 1, n, d_hkl, g_precision,
-                                            dF, dI);
+  if (opts->use_nfft_for_sf)
+    st = spsim_internal_shot_structure_factor_nufft(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
+                                                    opts->delta_atoms, n, d_hkl, g_nufft_eps, dF, dI);
+  else
+    st = spsim_internal_shot_structure_factor(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
+                                              opts->delta_atoms, beam, poly ? exp->wavelength : 0.0f,
+                                              poly ? exp->bandwidth : 0.0f, poly ? samples : 1, n, d_hkl,
+                                              g_precision, dF, dI);
   if (st) die("simulate_shot structure factor", st);
 
   /* F and |F|^2 go down ahead of the chain, so the host can copy them out

@@ -99,6 +99,8 @@ _PROTOS = {
                                                               P(Experiment), P(Options)]),
     "cuda_compute_pattern_on_list2": (P(Diffraction_Pattern), [P(Molecule), P(c_float), c_int, c_float,
                                                                P(Experiment), P(Options)]),
+    "compute_pattern_on_list_by_nfft": (P(Diffraction_Pattern), [P(Molecule), P(c_float), c_int, P(CCD), c_float,
+                                                                 P(Options)]),
     "compute_sf": (P(Diffraction_Pattern), [P(Molecule), P(c_float), c_int, P(Options)]),
     "calculate_thomson_correction": (None, [P(CCD), P(Experiment)]),
     "calculate_pixel_solid_angle": (None, [P(CCD)]),
@@ -205,6 +207,10 @@ def cuda_compute_pattern_on_list(mol, HKL_list, HKL_list_size, B, exp, opts):
 
 def cuda_compute_pattern_on_list2(mol, HKL_list, HKL_list_size, B, exp, opts):
     return _gpu_call("cuda_compute_pattern_on_list2", mol, _floats(HKL_list), HKL_list_size, B, exp, opts)
+
+
+def compute_pattern_on_list_by_nfft(mol, HKL_list, HKL_list_size, det, B, opts):
+    return _gpu_call("compute_pattern_on_list_by_nfft", mol, _floats(HKL_list), HKL_list_size, det, B, opts)
 
 
 def compute_sf(mol, HKL_list, HKL_list_size, opts):
