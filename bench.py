@@ -487,7 +487,7 @@ def _modes(args, core, mol, qs, rot, terms, timed, prec):
     return out
 
 
-def _nufft_mode(core, mol, qs, rot, terms, sub_rows, I64, eps=1e-9, steps=5):
+def _nufft_mode(core, mol, qs, rot, terms, sub_rows, I64, eps=1e-8, steps=5):
     """The same structure factor by the type-3 NUFFT (spsim_b200_forward_nufft,
     the reference's use_nfft_for_sf path): device-resident time per pattern
     (CUDA events around the call, L2 flushed between calls), the equivalent

@@ -100,7 +100,7 @@ void sum_patterns(Diffraction_Pattern *pat);                             /* src/
 void spsim_b200_set_legacy_precision(int precision);
 int spsim_b200_get_legacy_precision(void);
 /* Relative error of the NUFFT structure factor behind
- * compute_pattern_on_list_by_nfft and use_nfft_for_sf (default 1e-9; see
+ * compute_pattern_on_list_by_nfft and use_nfft_for_sf (default 1e-8; see
  * spsim_b200_forward_nufft). */
 void spsim_b200_set_legacy_nufft_eps(double eps);
 double spsim_b200_get_legacy_nufft_eps(void);

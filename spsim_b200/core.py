@@ -167,7 +167,7 @@ def forward(mol, qs, rot=None, B=0.0, precision="f32", F=None, I=None, want_F=Tr
     return (F if want_F else None), (I if want_I else None)
 
 
-def forward_nufft(mol, qs, rot=None, B=0.0, eps=1e-9, F=None, I=None, want_F=True, want_I=True, stream=None):
+def forward_nufft(mol, qs, rot=None, B=0.0, eps=1e-8, F=None, I=None, want_F=True, want_I=True, stream=None):
     """The structure factor of forward() by a type-3 non-uniform FFT per
     element (FP64 grids, cuFFT), for large molecules: relative L2 error of F
     about eps against the exact sum.  Replaces spsim's NNFFT path

@@ -1401,9 +1401,12 @@ extern "C" int spsim_b200_structure_factor_host_spectrum(int natoms, const int32
 // streams are ordered by the context's completion event.
 
 struct NufftCtx {
-  DevBuf small, fine, dec, seg, keys, flags;
-  cufftHandle fft = 0;
-  int fft_dims[4] = {0, 0, 0, 0};  // n2z, n2y, n2x, elements
+  DevBuf small, fine, packed, dec, seg, keys, flags;
+  // the FFT of the padded grid, element by element: 2-D (y, x) transforms of
+  // the planes that hold data (the n1z / 2 planes at either end of z), then
+  // the z transform of every (y, x) column
+  cufftHandle fft_yx = 0, fft_z = 0;
+  int fft_dims[4] = {0, 0, 0, 0};  // n2z, n2y, n2x, n1z
   std::vector<double> geom_key;
   unsigned long long seg_mol = 0;  // molecule whose segment table is on the device
   NufftGeom g;
@@ -1442,8 +1445,10 @@ static double es_hat_host(double xi, double w, double beta, double d) {
   return 2.0 * d * s;
 }
 
-// Kernel width (grid points) for a requested relative error of F: measured
-// relative L2 errors against the direct sum are ~5 x 10^-w at sigma = 2.
+// Interpolation kernel width (grid points) for a requested relative error of
+// F: measured relative L2 errors against the direct sum are ~5 x 10^-w with
+// an FFT grid upsampled 2x, and the spreading kernel w + 4 points wide on a
+// grid upsampled 1.5x adds about as much.
 static int nufft_width(double eps) {
   const int w = (int)std::ceil(-std::log10(eps)) + 1;
   return std::min(std::max(w, NUFFT_MIN_W), NUFFT_MAX_W - 1);
@@ -1493,10 +1498,10 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
         return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: non-finite q in the list");
     }
     const int w = nufft_width(eps);
-    const double sigma1 = 2.0, sigma2 = 2.0;
+    const double sigma1 = 1.5, sigma2 = 2.0;
     NufftGeom g;
     std::memset(&g, 0, sizeof(g));
-    g.w1 = w + 1;
+    g.w1 = std::min(w + 4, NUFFT_MAX_W);
     g.w2 = w;
     g.beta1 = 0.97 * M_PI * g.w1 * (1.0 - 0.5 / sigma1);
     g.beta2 = 0.97 * M_PI * g.w2 * (1.0 - 0.5 / sigma2);
@@ -1516,12 +1521,13 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
       cells2 *= (size_t)g.n2[d];
     }
     const size_t bytes1 = cells1 * n_elem * sizeof(double2), bytes2 = cells2 * n_elem * sizeof(double2);
+    const size_t bytes3 = cells2 * nufft_pack_groups(n_elem) * nufft_pack_halves(n_elem) * sizeof(float4);
     size_t free_b = 0, total_b = 0;
     CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-    const size_t have = free_b + c.small.cap + c.fine.cap;
-    if (bytes1 + 2 * bytes2 > have / 10 * 9)
+    const size_t have = free_b + c.small.cap + c.fine.cap + c.packed.cap;
+    if (bytes1 + 2 * bytes2 + bytes3 > have / 10 * 9)  // cuFFT's work area about the size of the grid
       return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: grids of %.3g GB do not fit; use the direct sum",
-                  (bytes1 + 2.0 * bytes2) * 1e-9);
+                  (bytes1 + 2.0 * bytes2 + bytes3) * 1e-9);
     // 1 / phi2hat per spreading-grid index, and psi1hat's trapezoid coefficients
     std::vector<double> dec;
     for (int d = 0; d < 3; ++d)
@@ -1531,19 +1537,24 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
     for (int k = 0; k < c.n_coef; ++k) c.psi_a[k] = 0.25 * (k == 0 ? 1.0 : 2.0) * es_host(0.25 * k, g.w1, g.beta1);
     CUDA_TRY(c.small.ensure(bytes1));
     CUDA_TRY(c.fine.ensure(bytes2));
+    CUDA_TRY(c.packed.ensure(bytes3));
     CUDA_TRY(c.dec.ensure(dec.size() * sizeof(double)));
     CUDA_TRY(cudaMemcpyAsync(c.dec.p, dec.data(), dec.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    const int dims[4] = {g.n2[2], g.n2[1], g.n2[0], n_elem};
-    if (!c.fft || std::memcmp(dims, c.fft_dims, sizeof(dims)) != 0) {
-      if (c.fft) {
-        cufftDestroy(c.fft);
-        c.fft = 0;
-      }
-      int n[3] = {dims[0], dims[1], dims[2]};
-      const int dist = dims[0] * dims[1] * dims[2];
-      if (cufftPlanMany(&c.fft, 3, n, nullptr, 1, dist, nullptr, 1, dist, CUFFT_Z2Z, n_elem) != CUFFT_SUCCESS) {
-        c.fft = 0;
-        return fail(SPSIM_ERR_CUDA, "NUFFT: cuFFT plan %d x %d x %d x %d failed", dims[0], dims[1], dims[2], n_elem);
+    const int dims[4] = {g.n2[2], g.n2[1], g.n2[0], g.n1[2]};
+    if (!c.fft_yx || std::memcmp(dims, c.fft_dims, sizeof(dims)) != 0) {
+      if (c.fft_yx) cufftDestroy(c.fft_yx);
+      if (c.fft_z) cufftDestroy(c.fft_z);
+      c.fft_yx = c.fft_z = 0;
+      int nyx[2] = {dims[1], dims[2]}, nz[1] = {dims[0]};
+      const int plane = dims[1] * dims[2];
+      bool ok = cufftPlanMany(&c.fft_yx, 2, nyx, nullptr, 1, plane, nullptr, 1, plane, CUFFT_Z2Z, dims[3] / 2) ==
+                CUFFT_SUCCESS;
+      ok = ok && cufftPlanMany(&c.fft_z, 1, nz, nz, plane, 1, nz, plane, 1, CUFFT_Z2Z, plane) == CUFFT_SUCCESS;
+      if (!ok) {
+        if (c.fft_yx) cufftDestroy(c.fft_yx);
+        if (c.fft_z) cufftDestroy(c.fft_z);
+        c.fft_yx = c.fft_z = 0;
+        return fail(SPSIM_ERR_CUDA, "NUFFT: cuFFT plans for %d x %d x %d failed", dims[0], dims[1], dims[2]);
       }
       std::memcpy(c.fft_dims, dims, sizeof(dims));
     }
@@ -1567,10 +1578,19 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   CUDA_TRY(nufft_spread(m->d_atomsd, (const int *)c.seg.p, n_elem, m->n_padded, g, (double2 *)c.small.p,
                         (int *)c.flags.p, st));
   CUDA_TRY(nufft_pad((const double2 *)c.small.p, (double2 *)c.fine.p, g, n_elem, (const double *)c.dec.p, st));
-  if (cufftSetStream(c.fft, st) != CUFFT_SUCCESS) return fail(SPSIM_ERR_CUDA, "NUFFT: cufftSetStream failed");
-  if (cufftExecZ2Z(c.fft, (cufftDoubleComplex *)c.fine.p, (cufftDoubleComplex *)c.fine.p, CUFFT_FORWARD) !=
-      CUFFT_SUCCESS)
-    return fail(SPSIM_ERR_CUDA, "NUFFT: cuFFT execution failed");
+  if (cufftSetStream(c.fft_yx, st) != CUFFT_SUCCESS || cufftSetStream(c.fft_z, st) != CUFFT_SUCCESS)
+    return fail(SPSIM_ERR_CUDA, "NUFFT: cufftSetStream failed");
+  const long long cells2 = (long long)g.n2[0] * g.n2[1] * g.n2[2];
+  const long long plane = (long long)g.n2[0] * g.n2[1];
+  for (int e = 0; e < n_elem; ++e) {
+    cufftDoubleComplex *base = (cufftDoubleComplex *)c.fine.p + e * cells2;
+    cufftDoubleComplex *upper = base + (long long)(g.n2[2] - g.n1[2] / 2) * plane;
+    if (cufftExecZ2Z(c.fft_yx, base, base, CUFFT_FORWARD) != CUFFT_SUCCESS ||
+        cufftExecZ2Z(c.fft_yx, upper, upper, CUFFT_FORWARD) != CUFFT_SUCCESS ||
+        cufftExecZ2Z(c.fft_z, base, base, CUFFT_FORWARD) != CUFFT_SUCCESS)
+      return fail(SPSIM_ERR_CUDA, "NUFFT: cuFFT execution failed");
+  }
+  CUDA_TRY(nufft_pack((const double2 *)c.fine.p, (float4 *)c.packed.p, cells2, n_elem, st));
   NufftInterp a;
   std::memset(&a, 0, sizeof(a));
   a.g = g;
@@ -1579,8 +1599,10 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   a.npix = npix;
   a.has_rot = rot != nullptr;
   for (int k = 0; k < 9; ++k) a.rot[k] = rot ? rot[k] : 0.0;
-  a.grid = (const double2 *)c.fine.p;
-  a.cell2 = (long long)g.n2[0] * g.n2[1] * g.n2[2];
+  a.packed = (const float4 *)c.packed.p;
+  a.cell2 = cells2;
+  a.halves = nufft_pack_halves(n_elem);
+  a.n_groups = nufft_pack_groups(n_elem);
   a.n_elem = n_elem;
   a.coeffs = m->d_coeffs;
   a.B = (double)B;

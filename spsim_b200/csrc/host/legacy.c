@@ -20,7 +20,7 @@
 #include "../../../include/spsim_b200.h"
 
 static int g_precision = SPSIM_PREC_F32;
-static double g_nufft_eps = 1e-9;
+static double g_nufft_eps = 1e-8;
 static unsigned long long g_seed = 0x5eed5eedULL;
 static uint32_t g_pattern_counter = 0;
 

@@ -149,13 +149,21 @@ __global__ void __launch_bounds__(32 * SPREAD_WARPS) nufft_spread_kernel(const A
   const double cr = (double)a.w * cs, ci = -(double)a.w * sn;
   const long long n1x = g.n1[0], n1y = g.n1[1];
   double2 *base = grid + (long long)e * n1x * n1y * g.n1[2] + ((long long)l0[2] * n1y + l0[1]) * n1x + l0[0];
-  const int ww = w * w;
-  for (int c = lane; c < ww * w; c += 32) {
-    const int iz = c / ww, r = c - iz * ww, iy = r / w, ix = r - iy * w;
-    const double v = kv[warp][2][iz] * kv[warp][1][iy] * kv[warp][0][ix];
-    double2 *p = base + ((long long)iz * n1y + iy) * n1x + ix;
-    atomicAdd(&p->x, v * cr);
-    atomicAdd(&p->y, v * ci);
+  // lane = (y parity, x offset): half-warps cover two stencil rows per step
+  static_assert(NUFFT_MAX_W <= 16, "one stencil row per half-warp");
+  const int ix = lane & 15, iy0 = lane >> 4;
+  if (ix < w) {
+    const double kxr = kv[warp][0][ix] * cr, kxi = kv[warp][0][ix] * ci;
+    for (int iz = 0; iz < w; ++iz) {
+      const double kz = kv[warp][2][iz];
+      double2 *plane = base + (long long)iz * n1y * n1x + ix;
+      for (int iy = iy0; iy < w; iy += 2) {
+        const double v = kz * kv[warp][1][iy];
+        double2 *p = plane + (long long)iy * n1x;
+        atomicAdd(&p->x, v * kxr);
+        atomicAdd(&p->y, v * kxi);
+      }
+    }
   }
 }
 
@@ -168,50 +176,87 @@ cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_a
 }
 
 // ---------------------------------------------------------------------------
-// step 2: deconvolution by phi2hat and zero-padding into the FFT grid.
-// Spreading-grid index l holds mode m = l - n1/2, stored at FFT index m mod n2.
+// step 2: deconvolution by phi2hat into the zeroed FFT grid.  Spreading-grid
+// index l holds mode m = l - n1/2, stored at FFT index m mod n2.
 
-__global__ void nufft_pad_kernel(const double2 *__restrict__ small, double2 *__restrict__ fine, const NufftGeom g,
-                                 int n_elem, const double *__restrict__ dec) {
-  const int n2x = g.n2[0], n2y = g.n2[1], n2z = g.n2[2];
+__global__ void nufft_scatter_kernel(const double2 *__restrict__ small, double2 *__restrict__ fine, const NufftGeom g,
+                                     int n_elem, const double *__restrict__ dec) {
   const int n1x = g.n1[0], n1y = g.n1[1], n1z = g.n1[2];
+  const int n2x = g.n2[0], n2y = g.n2[1], n2z = g.n2[2];
   const double *decx = dec, *decy = dec + n1x, *decz = dec + n1x + n1y;
-  const int py = blockIdx.y;
-  const int my = (py < n2y / 2 ? py : py - n2y) + n1y / 2;
-  const bool iny = my >= 0 && my < n1y;
-  for (int ez = blockIdx.z; ez < n_elem * n2z; ez += gridDim.z) {
-    const int e = ez / n2z, pz = ez - e * n2z;
-    const int mz = (pz < n2z / 2 ? pz : pz - n2z) + n1z / 2;
-    const bool inyz = iny && mz >= 0 && mz < n1z;
+  const int ly = blockIdx.y;
+  for (int ez = blockIdx.z; ez < n_elem * n1z; ez += gridDim.z) {
+    const int e = ez / n1z, lz = ez - e * n1z;
+    const int pz = lz - n1z / 2 < 0 ? lz - n1z / 2 + n2z : lz - n1z / 2;
+    const int py = ly - n1y / 2 < 0 ? ly - n1y / 2 + n2y : ly - n1y / 2;
+    const double dyz = decy[ly] * decz[lz];
+    const double2 *in = small + (((long long)e * n1z + lz) * n1y + ly) * n1x;
     double2 *out = fine + (((long long)e * n2z + pz) * n2y + py) * n2x;
-    const double2 *in = inyz ? small + (((long long)e * n1z + mz) * n1y + my) * n1x : small;
-    const double dyz = inyz ? decy[my] * decz[mz] : 0.0;
-    for (int px = blockIdx.x * blockDim.x + threadIdx.x; px < n2x; px += gridDim.x * blockDim.x) {
-      const int mx = (px < n2x / 2 ? px : px - n2x) + n1x / 2;
-      double2 v = make_double2(0.0, 0.0);
-      if (inyz && mx >= 0 && mx < n1x) {
-        const double2 b = in[mx];
-        const double d = dyz * decx[mx];
-        v = make_double2(b.x * d, b.y * d);
-      }
-      out[px] = v;
+    for (int lx = blockIdx.x * blockDim.x + threadIdx.x; lx < n1x; lx += gridDim.x * blockDim.x) {
+      const int px = lx - n1x / 2 < 0 ? lx - n1x / 2 + n2x : lx - n1x / 2;
+      const double2 b = in[lx];
+      const double d = dyz * decx[lx];
+      out[px] = make_double2(b.x * d, b.y * d);
     }
   }
 }
 
 cudaError_t nufft_pad(const double2 *small, double2 *fine, const NufftGeom &g, int n_elem, const double *dec,
                       cudaStream_t st) {
+  const size_t cells2 = (size_t)g.n2[0] * g.n2[1] * g.n2[2];
+  cudaError_t e = cudaMemsetAsync(fine, 0, cells2 * n_elem * sizeof(double2), st);
+  if (e != cudaSuccess) return e;
   const int threads = 128;
-  dim3 grid((unsigned)std::min((g.n2[0] + threads - 1) / threads, 8), (unsigned)g.n2[1],
-            (unsigned)std::min(n_elem * g.n2[2], 65535));
-  nufft_pad_kernel<<<grid, threads, 0, st>>>(small, fine, g, n_elem, dec);
+  dim3 grid((unsigned)std::min((g.n1[0] + threads - 1) / threads, 8), (unsigned)g.n1[1],
+            (unsigned)std::min(n_elem * g.n1[2], 65535));
+  nufft_scatter_kernel<<<grid, threads, 0, st>>>(small, fine, g, n_elem, dec);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// step 3b: the FFT output, FP64 [e][z][y][x], packed for the interpolation as
+// FP32 complex with the elements interleaved: [group][z][y][x][H float4], each
+// float4 holding two elements (re, im, re, im); absent elements are zero.  FP32
+// storage adds a relative error of ~4e-9 to F, below the rounding of the
+// complex64 output.
+
+template <int H>
+__global__ void nufft_pack_kernel(const double2 *__restrict__ fine, float4 *__restrict__ packed, long long cells2,
+                                  int n_elem, int n_groups) {
+  const long long total = cells2 * n_groups;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long grp = i / cells2, c = i - grp * cells2;
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      const int e0 = (int)grp * 2 * H + 2 * h;
+      double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+      if (e0 < n_elem) a = fine[(long long)e0 * cells2 + c];
+      if (e0 + 1 < n_elem) b = fine[(long long)(e0 + 1) * cells2 + c];
+      packed[i * H + h] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+    }
+  }
+}
+
+int nufft_pack_halves(int n_elem) { return n_elem <= 2 ? 1 : 2; }
+int nufft_pack_groups(int n_elem) { return (n_elem + 2 * nufft_pack_halves(n_elem) - 1) / (2 * nufft_pack_halves(n_elem)); }
+
+cudaError_t nufft_pack(const double2 *fine, float4 *packed, long long cells2, int n_elem, cudaStream_t st) {
+  const int H = nufft_pack_halves(n_elem), G = nufft_pack_groups(n_elem);
+  const long long total = cells2 * G;
+  const unsigned blocks = (unsigned)std::min<long long>((total + 255) / 256, 148 * 16);
+  if (H == 1)
+    nufft_pack_kernel<1><<<blocks, 256, 0, st>>>(fine, packed, cells2, n_elem, G);
+  else
+    nufft_pack_kernel<2><<<blocks, 256, 0, st>>>(fine, packed, cells2, n_elem, G);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // step 4: interpolation at each pixel's q, form factors, deconvolution by
-// psi1hat, centre phase.  One thread per pixel; the stencil is W^3 FFT-grid
-// points, each element's grid read at the same offsets.
+// psi1hat, centre phase.  One thread per pixel; the stencil is W^3 grid points,
+// all elements of a group read together.  Each x row of the stencil is
+// contracted in FP32 (W terms), the rows summed in FP64.
 
 __device__ __forceinline__ double psi1_hat(double xi, const double *__restrict__ a, int n) {
   // sum_k a_k cos(2 pi xi k / 4) by Clenshaw's recurrence in T_k(cos(pi xi / 2))
@@ -225,7 +270,14 @@ __device__ __forceinline__ double psi1_hat(double xi, const double *__restrict__
   return fma(x, b1, a[0] - b2);
 }
 
-template <int W>
+// 32 bytes (four elements, FP32 complex) in one 256-bit load; p 32-byte aligned
+__device__ __forceinline__ void ld_cell32(const float4 *p, float4 &a, float4 &b) {
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+               : "l"(p));
+}
+
+template <int W, int H>
 __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant__ NufftInterp a) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.npix) return;
@@ -255,18 +307,19 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
     t[d] = qp * g.L[d];
     const double p0 = ceil(t[d] - 0.5 * W);
     t[d] -= p0;  // stencil offsets: t - i, i = 0 .. W-1
-    int s = (int)p0 % g.n2[d];
+    const int s = (int)p0 % g.n2[d];
     b[d] = s < 0 ? s + g.n2[d] : s;
     D *= psi1_hat(g.h[d] * qp, a.psi_a, a.n_coef);
   }
   const double ihw = 2.0 / W;
-  double kx[W], ky[W];
+  float kx[W];
+  double ky[W];
   int ix[W], iy[W];
 #pragma unroll
   for (int i = 0; i < W; ++i) {
-    kx[i] = es_kernel(t[0] - i, ihw, g.beta2);
+    kx[i] = (float)es_kernel(t[0] - i, ihw, g.beta2);
     ky[i] = es_kernel(t[1] - i, ihw, g.beta2);
-    ix[i] = b[0] + i >= n2x ? b[0] + i - n2x : b[0] + i;
+    ix[i] = (b[0] + i >= n2x ? b[0] + i - n2x : b[0] + i) * H;
     iy[i] = b[1] + i >= n2y ? b[1] + i - n2y : b[1] + i;
   }
   // |q| of the unrotated list for the form factors, as the direct path
@@ -274,51 +327,57 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
     const double d = sqrt(h0 * h0 + h1 * h1 + h2 * h2) * 1e-10;
     return d * d * 0.25;
   }();
+  const long long row_stride = (long long)n2x * H, plane_stride = row_stride * n2y;
   double fr = 0.0, fi = 0.0;
-  for (int e0 = 0; e0 < a.n_elem; e0 += 4) {
-    const int ne = min(4, a.n_elem - e0);
-    const double2 *gr = a.grid + (long long)e0 * a.cell2;
-    double ar[4] = {0.0, 0.0, 0.0, 0.0}, ai[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int grp = 0; grp < a.n_groups; ++grp) {
+    const float4 *gr = a.packed + (long long)grp * a.cell2 * H;
+    double acc[4 * H];
+#pragma unroll
+    for (int k = 0; k < 4 * H; ++k) acc[k] = 0.0;
     for (int iz = 0; iz < W; ++iz) {
       const double kz = es_kernel(t[2] - iz, ihw, g.beta2);
       const int zz = b[2] + iz >= n2z ? b[2] + iz - n2z : b[2] + iz;
-      const double2 *plane = gr + (long long)zz * n2y * n2x;
+      const float4 *plane = gr + (long long)zz * plane_stride;
 #pragma unroll
       for (int jy = 0; jy < W; ++jy) {
-        const double2 *row = plane + (long long)iy[jy] * n2x;
-        double sr[4] = {0.0, 0.0, 0.0, 0.0}, si[4] = {0.0, 0.0, 0.0, 0.0};
+        const float4 *row = plane + (long long)iy[jy] * row_stride;
+        float s[4 * H];
+#pragma unroll
+        for (int k = 0; k < 4 * H; ++k) s[k] = 0.0f;
 #pragma unroll
         for (int jx = 0; jx < W; ++jx) {
+          float4 v[H];
+          if constexpr (H == 2)
+            ld_cell32(row + ix[jx], v[0], v[1]);
+          else
+            v[0] = __ldg(row + ix[jx]);
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            if (e < ne) {
-              const double2 v = __ldg(row + (long long)e * a.cell2 + ix[jx]);
-              sr[e] = fma(kx[jx], v.x, sr[e]);
-              si[e] = fma(kx[jx], v.y, si[e]);
-            }
+          for (int h = 0; h < H; ++h) {
+            s[4 * h + 0] = fmaf(kx[jx], v[h].x, s[4 * h + 0]);
+            s[4 * h + 1] = fmaf(kx[jx], v[h].y, s[4 * h + 1]);
+            s[4 * h + 2] = fmaf(kx[jx], v[h].z, s[4 * h + 2]);
+            s[4 * h + 3] = fmaf(kx[jx], v[h].w, s[4 * h + 3]);
           }
         }
         const double kzy = kz * ky[jy];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          ar[e] = fma(kzy, sr[e], ar[e]);
-          ai[e] = fma(kzy, si[e], ai[e]);
-        }
+        for (int k = 0; k < 4 * H; ++k) acc[k] = fma(kzy, (double)s[k], acc[k]);
       }
     }
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      if (e >= ne) break;
+    for (int k = 0; k < 2 * H; ++k) {
+      const int e = grp * 2 * H + k;
+      if (e >= a.n_elem) break;
       double f = 1.0;
       if (!a.delta_atoms) {
         // src/diffraction.c:183-193, as ff_table_kernel
-        const float *c = a.coeffs + 9 * (e0 + e);
+        const float *c = a.coeffs + 9 * e;
         f = 0.0;
         for (int i = 0; i < 4; ++i) f += (double)c[i] * exp(-((double)c[i + 4] + a.B) * s2);
         f += (double)c[8] * exp(-a.B * s2);
       }
-      fr = fma(f, ar[e], fr);
-      fi = fma(f, ai[e], fi);
+      fr = fma(f, acc[2 * k], fr);
+      fi = fma(f, acc[2 * k + 1], fi);
     }
   }
   const double inv = 1.0 / D;
@@ -337,12 +396,16 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
 template <int W>
 static cudaError_t interp_t(const NufftInterp &a, cudaStream_t st) {
   const unsigned blocks = (unsigned)((a.npix + 127) / 128);
-  nufft_interp_kernel<W><<<blocks, 128, 0, st>>>(a);
+  if (a.halves == 1)
+    nufft_interp_kernel<W, 1><<<blocks, 128, 0, st>>>(a);
+  else
+    nufft_interp_kernel<W, 2><<<blocks, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t nufft_interp(const NufftInterp &a, cudaStream_t st) {
   if (a.npix <= 0) return cudaSuccess;
+  if (a.halves != 1 && a.halves != 2) return cudaErrorInvalidValue;
   switch (a.g.w2) {
     case 4: return interp_t<4>(a, st);
     case 5: return interp_t<5>(a, st);
@@ -356,7 +419,6 @@ cudaError_t nufft_interp(const NufftInterp &a, cudaStream_t st) {
     case 13: return interp_t<13>(a, st);
     case 14: return interp_t<14>(a, st);
     case 15: return interp_t<15>(a, st);
-    case 16: return interp_t<16>(a, st);
     default: return cudaErrorInvalidValue;
   }
 }

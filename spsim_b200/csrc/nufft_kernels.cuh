@@ -8,11 +8,12 @@
 //   2. pad      b_l / phi2hat((l - n1/2) / n2) into an n2 = sigma2 n1 grid at
 //               index (l - n1/2) mod n2, zeros elsewhere
 //   3. FFT      forward (e^{-2 pi i m p / n2}) over the n2 grid (cuFFT, batched
-//               over elements)
+//               over elements), then packed as FP32 with the elements interleaved
 //   4. interp   T(q') = sum_p g_p phi2(n2 h q' - p), F = e^{-2 pi i q.c}
 //               sum_e f_e T_e(q') / prod_d psi1hat(h_d q'_d)
 // psi1, phi2: "exponential of semicircle" kernels exp(beta (sqrt(1 - (2u/w)^2) - 1))
-// of width w grid points; q' = q - C.  Sums and grids in FP64.
+// of width w grid points; q' = q - C.  Spreading, FFT and the interpolation's
+// row sums in FP64; the packed grid and its contraction along x in FP32.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -22,7 +23,7 @@
 namespace spsim {
 
 constexpr int NUFFT_MIN_W = 4;
-constexpr int NUFFT_MAX_W = 16;
+constexpr int NUFFT_MAX_W = 16;  // spreading; the interpolation goes to 15
 constexpr int NUFFT_MAX_COEF = 2 * NUFFT_MAX_W + 2;  // psi1hat trapezoid nodes at spacing 1/4 over [0, w/2]
 
 struct NufftGeom {
@@ -44,8 +45,10 @@ struct NufftInterp {
   long long npix;
   int has_rot;
   double rot[9];      // q' = R q (row-major)
-  const double2 *grid;  // [n_elem][n2z][n2y][n2x] after the FFT
-  long long cell2;      // n2x n2y n2z
+  const float4 *packed;  // [n_groups][n2z][n2y][n2x][halves] (nufft_pack)
+  long long cell2;       // n2x n2y n2z
+  int halves;            // float4 per cell and group (two elements each)
+  int n_groups;
   int n_elem;
   const float *coeffs;  // n_elem x 9 atomsf coefficients
   double B;
@@ -68,9 +71,15 @@ unsigned long long nufft_double_to_key(double d);
 // grid is skipped and sets err[0].
 cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_atoms, const NufftGeom &g,
                          double2 *grid, int *err, cudaStream_t st);
-// Step 2.  dec: 1 / phi2hat per spreading-grid index, x then y then z.
+// Step 2: zero `fine` and scatter the deconvolved spreading grid into it.
+// dec: 1 / phi2hat per spreading-grid index, x then y then z.
 cudaError_t nufft_pad(const double2 *small, double2 *fine, const NufftGeom &g, int n_elem, const double *dec,
                       cudaStream_t st);
+// Step 3b: FP32 element-interleaved copy of the FFT output for step 4
+// (nufft_pack_groups(n_elem) x cells2 x nufft_pack_halves(n_elem) float4).
+int nufft_pack_halves(int n_elem);
+int nufft_pack_groups(int n_elem);
+cudaError_t nufft_pack(const double2 *fine, float4 *packed, long long cells2, int n_elem, cudaStream_t st);
 // Step 4.
 cudaError_t nufft_interp(const NufftInterp &a, cudaStream_t st);
 
