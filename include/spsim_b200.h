@@ -82,7 +82,9 @@ int spsim_b200_molecule_create_f64(int natoms, const int32_t *Z, const double *p
  * in the caller's original atom order, on `stream`, keeping the element
  * order and grid chosen at creation.  pos_dev is float (pos_is_f64 == 0) or
  * double; occ_dev / bfac_dev may be NULL (unchanged).  Positions that leave the
- * creation-time bounds raise SPSIM_ERR_RANGE at the next forward. */
+ * creation-time bounds (the radius about the centre plus 5 % or 0.5 nm) make
+ * the next forward (direct or NUFFT) report SPSIM_ERR_RANGE through
+ * spsim_b200_synchronize; each update clears the molecule's range word. */
 int spsim_b200_molecule_update_device(spsim_b200_molecule *m, const void *pos_dev, int pos_is_f64,
                                       const float *occ_dev, const float *bfac_dev, void *stream);
 int spsim_b200_molecule_natoms(const spsim_b200_molecule *m, int *natoms);
@@ -160,7 +162,7 @@ int spsim_b200_structure_factor_host_spectrum(int natoms, const int32_t *Z, cons
  * every pixel's q; FP64 grids) in O(atoms w^3 + grid log grid + pixels w^3)
  * instead of O(atoms x pixels).  Replaces the reference's NNFFT path
  * (compute_pattern_on_list_by_nfft, src/diffraction.c:528-675, dispatched by
- * compute_sf when use_nfft_for_sf is set, src/spsim.c:120-126), which runs
+ * compute_sf when use_nfft_for_sf is set, src/spsim.c:119-123), which runs
  * the NFFT library with a cut-off of m = 2.
  * eps: requested relative L2 error of F against the exact sum, in
  * [1e-14, 1e-2]; it sets the kernel width w = ceil(-log10 eps) + 1 grid points

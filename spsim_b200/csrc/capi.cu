@@ -399,6 +399,7 @@ extern "C" int spsim_b200_molecule_update_device(spsim_b200_molecule *m, const v
   if (!m || !pos_dev) return fail(SPSIM_ERR_INVALID_ARG, "molecule or positions NULL");
   if (bfac_dev && !m->per_atom_b)
     return fail(SPSIM_ERR_INVALID_ARG, "molecule was created without per-atom B factors");
+  CUDA_TRY(cudaMemsetAsync(m->d_flags, 0, sizeof(int), (cudaStream_t)stream));  // the range word of this update
   CUDA_TRY(launch_atoms_update(m->d_atoms, m->d_atoms2, m->d_atomsd, m->d_perm, m->n_padded, pos_is_f64 ? nullptr : (const float *)pos_dev,
                                pos_is_f64 ? (const double *)pos_dev : nullptr, occ_dev, bfac_dev, m->d_wbase,
                                m->center, m->dr, m->inv_dr, m->rbound, m->d_flags, (cudaStream_t)stream));
@@ -764,6 +765,8 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     pt.s2scale = 1.0 / (pt.qscale * pt.qscale);
     qmax *= std::fabs(pt.qscale);
     memcpy(pt.center, m->center, sizeof(pt.center));
+    pt.mol_err = m->d_flags;
+    pt.plan_err = (int *)pl.flags.p + 5;
     const int eq = ceil_log2_bound(std::max(qmax, 1e-300));
     const int kq = 22 - m->kr;
     pt.dq = (float)std::ldexp(1.0, eq - kq);
@@ -954,6 +957,11 @@ static int check_flags(Plan &pl) {
     int z = 0;
     cudaMemcpy((int *)pl.flags.p + 4, &z, sizeof(int), cudaMemcpyHostToDevice);
     return fail(SPSIM_ERR_TIMEOUT, "structure-factor kernel: an atom-tile copy did not complete in time");
+  }
+  if (h[5]) {
+    int z = 0;
+    cudaMemcpy((int *)pl.flags.p + 5, &z, sizeof(int), cudaMemcpyHostToDevice);
+    return fail(SPSIM_ERR_RANGE, "atoms moved outside the molecule's creation-time bounds");
   }
   return SPSIM_OK;
 }

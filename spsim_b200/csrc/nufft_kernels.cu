@@ -2,7 +2,7 @@
 // spreading, deconvolution/zero-padding and interpolation at the pixels' q.
 // The FFT between the last two steps is cuFFT's.  The transform replaces the
 // reference's per-element NNFFT (src/diffraction.c:528-675, dispatched from
-// src/spsim.c:120-126): atoms -> q list, unit atom weights, then the
+// src/spsim.c:119-123): atoms -> q list, unit atom weights, then the
 // form factor of |q| with the B factor (src/diffraction.c:390-400).
 #include "nufft_kernels.cuh"
 

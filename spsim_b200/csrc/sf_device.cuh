@@ -69,6 +69,8 @@ struct SfPattern {
   float2 *F;               // complex64 output [npix] or nullptr
   float *I;                // intensity output [npix] or nullptr
   long long tile0;         // first pixel-tile index of this pattern in a grid-mapped launch
+  const int *mol_err;      // the molecule's range word (atoms moved past its bounds), or nullptr
+  int *plan_err;           // where the finalizing kernel reports it
 };
 
 struct WorkItem {      // one CTA's unit of work

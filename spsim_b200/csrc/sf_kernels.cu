@@ -1037,6 +1037,7 @@ __global__ void __launch_bounds__(256) sf_f64_kernel(const SfPattern *__restrict
 __global__ void sf_finalize_kernel(const SfPattern *__restrict__ pats, int pattern0) {
   const SfPattern &pt = pats[pattern0 + blockIdx.y];
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0 && pt.mol_err && *pt.mol_err) atomicOr(pt.plan_err, 1);
   if (p >= pt.npix) return;
   const double2 a = pt.acc[p];
   if (pt.I) pt.I[p] = (float)(a.x * a.x + a.y * a.y);
@@ -1059,6 +1060,7 @@ __global__ void sf_spectrum_combine_kernel(const SfPattern *__restrict__ pats, i
                                            const double *__restrict__ weight, float2 *__restrict__ F,
                                            float *__restrict__ I, long long npix) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0 && pats[pattern0].mol_err && *pats[pattern0].mol_err) atomicOr(pats[pattern0].plan_err, 1);
   if (p >= npix) return;
   double re = 0.0, im = 0.0;
   for (int j = 0; j < S; ++j) {

@@ -347,3 +347,28 @@ def test_b_factors_with_negative_and_zero_occupancies(cuda, form):
         core.set_variant(-1)
     e_max, e_l2 = intensity_errors(I, I64)
     assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (e_max, e_l2)
+
+
+def test_atoms_moved_outside_bounds_are_reported(cuda):
+    # refinement moves past the creation-time radius (and its margin) are
+    # reported as SPSIM_ERR_RANGE by the next forward's synchronisation, for
+    # cached (graph) and FP64 plans alike; moving back clears it
+    from spsim_b200._native import SpsimError, SPSIM_ERR_RANGE
+
+    Z, pos = synth.random_molecule(300, 1e-9, 16)
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_list((np.random.default_rng(4).normal(size=(700, 3)) * 1e9).astype(np.float32))
+    moved = pos.astype(np.float64).copy()
+    moved[5] += 3e-8
+    for precision in ("f32", "fp64"):
+        mol.update_device(torch.from_numpy(moved).cuda())
+        core.forward(mol, qs, precision=precision)
+        with pytest.raises(SpsimError) as e:
+            core.synchronize()
+        assert e.value.status == SPSIM_ERR_RANGE
+        mol.update_device(torch.from_numpy(pos.astype(np.float64)).cuda())
+        _, I = core.forward(mol, qs, precision=precision)
+        core.synchronize()
+        _, I64 = O.structure_factor(Z, pos.astype(np.float64), qs.q().astype(np.float64))
+        e_max, _ = intensity_errors(I.cpu().numpy(), I64)
+        assert e_max < 1e-5
