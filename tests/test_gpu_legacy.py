@@ -123,15 +123,17 @@ def test_host_entry_point_reuses_scratch_safely(cuda):
     assert e_max < 1e-5
 
 
-@pytest.mark.parametrize("bandwidth", [0.0, 0.3])
-@pytest.mark.parametrize("use_cuda", [1, 2])
-def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda, bandwidth):
+@pytest.mark.parametrize("use_cuda,bandwidth,nfft", [(1, 0.0, 0), (2, 0.0, 0), (1, 0.3, 0), (2, 0.3, 0), (1, 0.0, 1)],
+                         ids=["cuda1", "cuda2", "cuda1_bw", "cuda2_bw", "nfft"])
+def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda, bandwidth, nfft):
     # simulate_shot runs geometry, orientation, structure factor and the chain
     # as one device pipeline; its outputs must be those of the reference's
     # step-by-step sequence (src/spsim.c:281-346) through the public calls:
     # HKL list bit for bit (device rotation = host float loop), F and |F|^2
-    # bit for bit, the chain arrays as the fused chain gives them (within a
-    # few ulps of the per-stage functions; noise from the same streams)
+    # bit for bit (to 1e-6 of the maximum for the NUFFT, whose spreading adds
+    # in FP64 atomics of unspecified order), the chain arrays as the fused
+    # chain gives them (within a few ulps of the per-stage functions; noise
+    # from the same streams)
     cwd = os.getcwd()
     os.chdir(tmp_path)
     try:
@@ -144,6 +146,7 @@ def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda, ba
         det.readout_noise = 3.0
         o.verbosity_level = 0
         o.use_cuda = use_cuda  # 1: the spectrum path when there is a bandwidth
+        o.use_nfft_for_sf = nfft
         o.wavelength_samples = 4
         exp.bandwidth = bandwidth
         o.random_orientation = 0
@@ -180,8 +183,14 @@ def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda, ba
         shot = S.simulate_shot(mol, opts)
         np.testing.assert_array_equal(S.as_array(shot.contents.HKL_list, 3 * n), step_hkl)
         np.testing.assert_array_equal(np.ctypeslib.as_array(shot.contents.rot.contents.data, shape=(9,)), step_rot)
-        np.testing.assert_array_equal(S.as_array(shot.contents.F, n), step_F)
-        np.testing.assert_array_equal(S.as_array(shot.contents.ints, n), step_I)
+        if nfft:
+            assert np.abs(S.as_array(shot.contents.F, n) - step_F).max() <= 1e-6 * np.abs(step_F).max()
+            assert np.abs(S.as_array(shot.contents.ints, n) - step_I).max() <= 2e-6 * step_I.max()
+            F64, _ = O.structure_factor(g["Z"], g["pos"].astype(np.float64), step_hkl.reshape(-1, 3).astype(np.float64))
+            assert np.linalg.norm(step_F - F64) / np.linalg.norm(F64) < 2e-7
+        else:
+            np.testing.assert_array_equal(S.as_array(shot.contents.F, n), step_F)
+            np.testing.assert_array_equal(S.as_array(shot.contents.ints, n), step_I)
         got = {k: S.as_array(getattr(det, k), n) for k in names}
         np.testing.assert_allclose(got["thomson_correction"], step["thomson_correction"], rtol=2.4e-7)
         np.testing.assert_allclose(got["solid_angle"], step["solid_angle"], rtol=2.4e-7)
