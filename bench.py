@@ -748,6 +748,22 @@ def workloads(prec, n_orient=512):
                       "batch_ms": t_batch, "terms_per_s": terms / t_batch * 1e3, "frac_of_R": terms / t_batch * 1e3 / R0,
                       "loop_of_single_calls_ms": t_loop, "batch_speedup": t_loop / t_batch}), flush=True)
     del F, I
+    # the same orientations by the NUFFT batch (one grid for every rotation)
+    with torch.cuda.stream(stream):
+        Fn, In = core.forward_nufft_batch(mol, qs, R, stream=stream, want_F=False)
+        t_nufft = ev_time(lambda: core.forward_nufft_batch(mol, qs, R, I=In, want_F=False, stream=stream))
+        errs = []
+        for i in range(4):
+            _, I64 = core.forward(mol, qs, rot=R[i], precision="fp64")
+            I64 = I64.double()
+            errs.append(float(((In[i].double() - I64).abs() / torch.clamp(I64, min=1e-3 * float(I64.mean()))).max()))
+        torch.cuda.synchronize()
+    w1, w2, n2 = core.last_nufft_grid()
+    print(json.dumps({"workload": "orientations_20k", "method": "nufft_batch", "orientations": n_orient,
+                      "batch_ms": t_nufft, "equivalent_terms_per_s": terms / t_nufft * 1e3,
+                      "speedup_vs_direct_batch": t_batch / t_nufft, "kernel_widths": [w1, w2], "fft_grid": list(n2),
+                      "floored_max_rel_vs_fp64_first4": max(errs)}), flush=True)
+    del Fn, In
 
     # uneven molecules
     mols, qsets, cost = [], [], 0.0

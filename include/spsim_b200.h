@@ -176,6 +176,16 @@ int spsim_b200_structure_factor_host_spectrum(int natoms, const int32_t *Z, cons
  * spsim_b200_synchronize.  No reference counterpart beyond the NNFFT path. */
 int spsim_b200_forward_nufft(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot, float B,
                              double eps, float *F_dev, float *I_dev, void *stream);
+/* npatterns orientations of one molecule on one q set (pattern i at rot[9 i],
+ * or all unrotated if rot is NULL), outputs [npatterns][npix] in F_dev / I_dev.
+ * The grid is sized for the ball |R q| <= |q|max, which holds for every
+ * rotation: the atoms are spread and transformed once, every pattern is one
+ * interpolation pass, and nothing is read back to the host.  Otherwise as
+ * spsim_b200_forward_nufft (which sizes its grid for the box of the one
+ * rotated list); npatterns in [1, 65535]. */
+int spsim_b200_forward_nufft_batch(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int npatterns,
+                                   const double *rot, float B, double eps, float *F_dev, float *I_dev,
+                                   void *stream);
 /* Kernel widths (spreading, interpolation) and FFT grid (x, y, z) of the last
  * NUFFT forward on this thread. */
 int spsim_b200_last_nufft_grid(int *w_spread, int *w_interp, int *n2);

@@ -22,7 +22,7 @@ __all__ = [
     "Molecule", "QSet", "forward", "forward_batch", "adjoint", "detector_chain", "chain_params",
     "hkl_for_detector", "synchronize", "forward_spectrum", "timing", "autotune", "set_variant", "last_forward_stats",
     "last_variant", "last_phase_word", "last_pair_narrow", "kernel_name", "autotune_batch", "clear_tuning",
-    "forward_nufft", "last_nufft_grid",
+    "forward_nufft", "forward_nufft_batch", "last_nufft_grid",
 ]
 
 
@@ -182,6 +182,25 @@ def forward_nufft(mol, qs, rot=None, B=0.0, eps=1e-8, F=None, I=None, want_F=Tru
     check(lib().spsim_b200_forward_nufft(mol.handle, qs.handle, r.ctypes.data_as(c_void_p) if r is not None else None,
                                          float(B), float(eps), _dev(F) if want_F else None,
                                          _dev(I) if want_I else None, _stream_ptr(stream)))
+    return (F if want_F else None), (I if want_I else None)
+
+
+def forward_nufft_batch(mol, qs, rots, B=0.0, eps=1e-8, F=None, I=None, want_F=True, want_I=True, stream=None):
+    """Many orientations of one molecule by the NUFFT: the grid is sized for
+    every rotation, the atoms are spread and transformed once, each pattern is
+    one interpolation pass.  rots: (npat, 3, 3).  Returns (F, I) of shape
+    (npat, npix)."""
+    _native.use_device(mol.device)
+    dev = torch.device("cuda", mol.device)
+    r = np.ascontiguousarray(np.asarray(rots, np.float64).reshape(-1, 9))
+    npat = r.shape[0]
+    if want_F and F is None:
+        F = torch.empty(npat, qs.npix, dtype=torch.complex64, device=dev)
+    if want_I and I is None:
+        I = torch.empty(npat, qs.npix, dtype=torch.float32, device=dev)
+    check(lib().spsim_b200_forward_nufft_batch(mol.handle, qs.handle, int(npat), r.ctypes.data_as(c_void_p),
+                                               float(B), float(eps), _dev(F) if want_F else None,
+                                               _dev(I) if want_I else None, _stream_ptr(stream)))
     return (F if want_F else None), (I if want_I else None)
 
 

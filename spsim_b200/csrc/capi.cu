@@ -1409,7 +1409,7 @@ extern "C" int spsim_b200_structure_factor_host_spectrum(int natoms, const int32
 // streams are ordered by the context's completion event.
 
 struct NufftCtx {
-  DevBuf small, fine, packed, dec, seg, keys, flags;
+  DevBuf small, fine, packed, dec, seg, keys, flags, rots;
   // the FFT of the padded grid, element by element: 2-D (y, x) transforms of
   // the planes that hold data (the n1z / 2 planes at either end of z), then
   // the z transform of every (y, x) column
@@ -1462,9 +1462,14 @@ static int nufft_width(double eps) {
   return std::min(std::max(w, NUFFT_MIN_W), NUFFT_MAX_W - 1);
 }
 
-static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot, float B,
-                         double eps, float *F_dev, float *I_dev, cudaStream_t st) {
+// npat patterns of one molecule and q set, pattern i rotated by rot[9 i] (or
+// none), outputs [npat][npix].  ball: size the grid for the ball |R q| <=
+// |q|max instead of the box of the rotated list, so that it holds for every
+// rotation (no read-back; the grid of a batch of orientations).
+static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int npat, const double *rot,
+                         bool ball, float B, double eps, float *F_dev, float *I_dev, cudaStream_t st) {
   if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
+  if (npat < 1 || npat > 65535) return fail(SPSIM_ERR_INVALID_ARG, "npatterns %d outside [1, 65535]", npat);
   if (!(eps >= 1e-14 && eps <= 1e-2)) return fail(SPSIM_ERR_INVALID_ARG, "eps %g outside [1e-14, 1e-2]", eps);
   if (m->per_atom_b)
     return fail(SPSIM_ERR_INVALID_ARG, "per-atom B factors are not supported by the NUFFT structure factor");
@@ -1475,10 +1480,18 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   const long long npix = qs->npix;
   if (npix == 0) return SPSIM_OK;
   if (m->n_kept == 0) {
-    if (F_dev) CUDA_TRY(cudaMemsetAsync(F_dev, 0, 2 * npix * sizeof(float), st));
-    if (I_dev) CUDA_TRY(cudaMemsetAsync(I_dev, 0, npix * sizeof(float), st));
+    if (F_dev) CUDA_TRY(cudaMemsetAsync(F_dev, 0, 2 * npix * npat * sizeof(float), st));
+    if (I_dev) CUDA_TRY(cudaMemsetAsync(I_dev, 0, npix * npat * sizeof(float), st));
     return SPSIM_OK;
   }
+  double qball = qs->qmax;  // |R q| <= |q|max ||R||, ||R|| = 1 for rotations, <= Frobenius otherwise
+  if (rot)
+    for (int i = 0; i < npat; ++i)
+      if (!is_orthonormal(rot + 9 * (size_t)i)) {
+        double fro = 0;
+        for (int k = 0; k < 9; ++k) fro += rot[9 * (size_t)i + k] * rot[9 * (size_t)i + k];
+        qball = std::max(qball, qs->qmax * std::sqrt(fro));
+      }
   std::lock_guard<std::mutex> lk(g_mu);
   NufftCtx &c = g_nufft[dev];
   if (!c.h_keys) CUDA_TRY(cudaMallocHost(&c.h_keys, 6 * sizeof(unsigned long long)));
@@ -1488,22 +1501,35 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   if (!c.has_done) CUDA_TRY(cudaMemsetAsync(c.flags.p, 0, sizeof(int), st));
 
   const int n_elem = m->n_elem;
-  std::vector<double> key = {(double)qs->id, (double)npix, m->rbound, (double)n_elem, eps, rot ? 1.0 : 0.0};
-  if (rot) key.insert(key.end(), rot, rot + 9);
+  std::vector<double> key;
+  if (ball) {
+    key = {-1.0, qball, m->rbound, (double)n_elem, eps};
+  } else {
+    key = {(double)qs->id, (double)npix, m->rbound, (double)n_elem, eps, rot ? 1.0 : 0.0};
+    if (rot) key.insert(key.end(), rot, rot + 9);
+  }
   if (key != c.geom_key) {
-    // q box of R q over the list (one read-back), then the grids
     c.geom_key.clear();
-    CUDA_TRY(c.keys.ensure(6 * sizeof(unsigned long long)));
-    unsigned long long *dk = (unsigned long long *)c.keys.p;
-    CUDA_TRY(nufft_bounds(qs->d_hkl, qs->d_q64, npix, rot, dk, st));
-    CUDA_TRY(cudaMemcpyAsync(c.h_keys, dk, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
     double lo[3], hi[3];
-    for (int d = 0; d < 3; ++d) {
-      lo[d] = nufft_key_to_double(c.h_keys[d]);
-      hi[d] = nufft_key_to_double(c.h_keys[3 + d]);
-      if (!(std::isfinite(lo[d]) && std::isfinite(hi[d])))
-        return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: non-finite q in the list");
+    if (ball) {
+      if (!std::isfinite(qball)) return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: non-finite q in the list");
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = -qball;
+        hi[d] = qball;
+      }
+    } else {
+      // q box of R q over the list (one read-back), then the grids
+      CUDA_TRY(c.keys.ensure(6 * sizeof(unsigned long long)));
+      unsigned long long *dk = (unsigned long long *)c.keys.p;
+      CUDA_TRY(nufft_bounds(qs->d_hkl, qs->d_q64, npix, rot, dk, st));
+      CUDA_TRY(cudaMemcpyAsync(c.h_keys, dk, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaStreamSynchronize(st));
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = nufft_key_to_double(c.h_keys[d]);
+        hi[d] = nufft_key_to_double(c.h_keys[3 + d]);
+        if (!(std::isfinite(lo[d]) && std::isfinite(hi[d])))
+          return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: non-finite q in the list");
+      }
     }
     const int w = nufft_width(eps);
     const double sigma1 = 1.5, sigma2 = 2.0;
@@ -1605,8 +1631,15 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   a.hkl = qs->d_hkl;
   a.q64 = qs->d_q64;
   a.npix = npix;
-  a.has_rot = rot != nullptr;
-  for (int k = 0; k < 9; ++k) a.rot[k] = rot ? rot[k] : 0.0;
+  a.npat = npat;
+  if (npat > 1 && rot) {
+    CUDA_TRY(c.rots.ensure(9 * (size_t)npat * sizeof(double)));
+    CUDA_TRY(cudaMemcpyAsync(c.rots.p, rot, 9 * (size_t)npat * sizeof(double), cudaMemcpyHostToDevice, st));
+    a.rots = (const double *)c.rots.p;
+  } else {
+    a.has_rot = rot != nullptr;
+    for (int k = 0; k < 9; ++k) a.rot[k] = rot ? rot[k] : 0.0;
+  }
   a.packed = (const float4 *)c.packed.p;
   a.cell2 = cells2;
   a.halves = nufft_pack_halves(n_elem);
@@ -1643,7 +1676,13 @@ static int nufft_check_flags(int dev) {
 
 extern "C" int spsim_b200_forward_nufft(const spsim_b200_molecule *m, const spsim_b200_qset *qs, const double *rot,
                                         float B, double eps, float *F_dev, float *I_dev, void *stream) {
-  return nufft_forward(m, qs, rot, B, eps, F_dev, I_dev, (cudaStream_t)stream);
+  return nufft_forward(m, qs, 1, rot, false, B, eps, F_dev, I_dev, (cudaStream_t)stream);
+}
+
+extern "C" int spsim_b200_forward_nufft_batch(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int npatterns,
+                                              const double *rot, float B, double eps, float *F_dev, float *I_dev,
+                                              void *stream) {
+  return nufft_forward(m, qs, npatterns, rot, true, B, eps, F_dev, I_dev, (cudaStream_t)stream);
 }
 
 extern "C" int spsim_b200_last_nufft_grid(int *w_spread, int *w_interp, int *n2) {
@@ -1679,7 +1718,7 @@ extern "C" int spsim_b200_structure_factor_host_nufft(int natoms, const int32_t 
   CUDA_TRY(g_host.I->ensure(std::max<int64_t>(npix, 1) * sizeof(float)));
   float *F = F_host ? (float *)g_host.F->p : nullptr;
   float *I = I_host ? (float *)g_host.I->p : nullptr;
-  st = nufft_forward(m, q, nullptr, B, eps, F, I, nullptr);
+  st = nufft_forward(m, q, 1, nullptr, false, B, eps, F, I, nullptr);
   if (st) return st;
   CUDA_TRY(cudaStreamSynchronize(nullptr));
   {
@@ -1715,7 +1754,7 @@ extern "C" int spsim_internal_shot_structure_factor_nufft(int natoms, const int3
   }
   st = host_session_qset_device(npix, hkl_dev, nullptr, &q);
   if (st) return st;
-  return nufft_forward(m, q, nullptr, B, eps, F_dev, I_dev, nullptr);
+  return nufft_forward(m, q, 1, nullptr, false, B, eps, F_dev, I_dev, nullptr);
 }
 
 // ---------------------------------------------------------------------------

@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.npix) return;
   const NufftGeom &g = a.g;
+  const long long out = (long long)blockIdx.y * a.npix + p;
   double h0, h1, h2;
   if (a.hkl) {
     h0 = a.hkl[3 * p];
@@ -293,10 +294,11 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
     h2 = a.q64[3 * p + 2];
   }
   double q[3] = {h0, h1, h2};
-  if (a.has_rot) {
-    q[0] = a.rot[0] * h0 + a.rot[1] * h1 + a.rot[2] * h2;
-    q[1] = a.rot[3] * h0 + a.rot[4] * h1 + a.rot[5] * h2;
-    q[2] = a.rot[6] * h0 + a.rot[7] * h1 + a.rot[8] * h2;
+  const double *R = a.rots ? a.rots + 9 * blockIdx.y : (a.has_rot ? a.rot : nullptr);
+  if (R) {
+    q[0] = R[0] * h0 + R[1] * h1 + R[2] * h2;
+    q[1] = R[3] * h0 + R[4] * h1 + R[5] * h2;
+    q[2] = R[6] * h0 + R[7] * h1 + R[8] * h2;
   }
   const int n2x = g.n2[0], n2y = g.n2[1], n2z = g.n2[2];
   double t[3];
@@ -383,23 +385,23 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
   const double inv = 1.0 / D;
   fr *= inv;
   fi *= inv;
-  if (a.I) a.I[p] = (float)(fr * fr + fi * fi);
+  if (a.I) a.I[out] = (float)(fr * fr + fi * fi);
   if (a.F) {
     double tc = q[0] * g.center[0] + q[1] * g.center[1] + q[2] * g.center[2];
     tc -= rint(tc);
     double sn, cs;
     sincospi(2.0 * tc, &sn, &cs);
-    a.F[p] = make_float2((float)(fr * cs + fi * sn), (float)(fi * cs - fr * sn));
+    a.F[out] = make_float2((float)(fr * cs + fi * sn), (float)(fi * cs - fr * sn));
   }
 }
 
 template <int W>
 static cudaError_t interp_t(const NufftInterp &a, cudaStream_t st) {
-  const unsigned blocks = (unsigned)((a.npix + 127) / 128);
+  const dim3 grid((unsigned)((a.npix + 127) / 128), (unsigned)std::max(a.npat, 1));
   if (a.halves == 1)
-    nufft_interp_kernel<W, 1><<<blocks, 128, 0, st>>>(a);
+    nufft_interp_kernel<W, 1><<<grid, 128, 0, st>>>(a);
   else
-    nufft_interp_kernel<W, 2><<<blocks, 128, 0, st>>>(a);
+    nufft_interp_kernel<W, 2><<<grid, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 

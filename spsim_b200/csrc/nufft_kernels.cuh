@@ -45,6 +45,8 @@ struct NufftInterp {
   long long npix;
   int has_rot;
   double rot[9];      // q' = R q (row-major)
+  int npat;           // patterns (blockIdx.y); outputs [npat][npix]
+  const double *rots; // device, 9 per pattern (row-major), or nullptr (then has_rot / rot)
   const float4 *packed;  // [n_groups][n2z][n2y][n2x][halves] (nufft_pack)
   long long cell2;       // n2x n2y n2z
   int halves;            // float4 per cell and group (two elements each)

@@ -168,3 +168,23 @@ def test_reference_shaped_nfft_path(cuda):
     assert np.linalg.norm(F - F64) / np.linalg.norm(F64) < 2e-7
     S.free_diffraction_pattern(pat)
     S.free_mol(mol)
+
+
+def test_orientation_batch_matches_oracle_and_single_calls(cuda):
+    # a batch of orientations on one grid sized for every rotation (the ball
+    # |q| <= |q|max): each pattern as the oracle, and as single NUFFT calls
+    Z, pos = synth.random_molecule(2500, 3.5e-9, 21)
+    d = dict(nx=48, ny=40, width=48 * 300e-6, height=40 * 300e-6, distance=0.1, wavelength=0.2e-9)
+    q0 = O.hkl_detector(**d)
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(**d)
+    R = synth.haar_rotations(5, 22)
+    F, I = core.forward_nufft_batch(mol, qs, R, B=10.0)
+    core.synchronize()
+    assert F.shape == (5, qs.npix) and I.shape == (5, qs.npix)
+    for i, r in enumerate(R):
+        F64, _ = O.structure_factor(Z, pos.astype(np.float64), q0 @ r.T, B=10.0)
+        _check_F(_np(F[i]), F64, 1e-8)
+        Fs, _ = core.forward_nufft(mol, qs, rot=r, B=10.0)
+        core.synchronize()
+        assert np.abs(_np(Fs) - _np(F[i])).max() < 2e-6 * np.abs(F64).max()
