@@ -17,8 +17,8 @@ import heapq
 import torch
 import torch.distributed as dist
 
-__all__ = ["slab_range", "balanced_assignment", "rank_world", "forward_sharded", "gather_to", "allreduce_",
-           "sharded_intensity"]
+__all__ = ["slab_range", "balanced_assignment", "rank_world", "forward_sharded", "sharded_orientations",
+           "gather_to", "allreduce_", "sharded_intensity"]
 
 
 def rank_world(group=None):
@@ -60,6 +60,19 @@ def forward_sharded(units, compute, costs=None, group=None):
         s, e = slab_range(n, rank, world)
         mine = range(s, e)
     return {i: compute(i) for i in mine}
+
+
+def sharded_orientations(rots, compute_batch, group=None):
+    """This rank's contiguous slab of orientations in one batched call, e.g.
+    compute_batch = lambda r: core.forward_nufft_batch(mol, qs, r)[1] (one NUFFT
+    grid per rank for all its orientations) or a core.forward_batch call.
+    Returns ({index: pattern}, (start, end)); no collective is issued."""
+    rank, world = rank_world(group)
+    s, e = slab_range(len(rots), rank, world)
+    if e <= s:
+        return {}, (s, e)
+    out = compute_batch(rots[s:e])
+    return {s + i: out[i] for i in range(e - s)}, (s, e)
 
 
 def gather_to(local, n_units, shape, dtype, dst=0, group=None, device=None):

@@ -87,6 +87,32 @@ def test_sharded_forward_gather_equals_single_process():
     np.testing.assert_allclose(res["full.npy"], ref, rtol=1e-12)
 
 
+def _sharded_orientation_batch(rank, world, out):
+    from oracle import oracle as O
+
+    Z, pos, R, q0 = _case()
+
+    def batch(rots):  # stands in for a batched GPU call (forward_nufft_batch / forward_batch)
+        return torch.from_numpy(np.stack([O.structure_factor(Z, pos.astype(np.float64), q0 @ r.T, nthreads=1)[1]
+                                          for r in rots]))
+
+    local, (s, e) = D.sharded_orientations(R, batch)
+    np.save(os.path.join(out, "range_%d.npy" % rank), np.array([s, e]))
+    full = D.gather_to(local, len(R), (q0.shape[0],), torch.float64)
+    if rank == 0:
+        np.save(os.path.join(out, "full.npy"), full.numpy())
+
+
+def test_sharded_orientation_batch_gather_equals_single_process():
+    from oracle import oracle as O
+
+    res = _run(_sharded_orientation_batch)
+    Z, pos, R, q0 = _case()
+    assert list(res["range_0.npy"]) == [0, 2] and list(res["range_1.npy"]) == [2, 5]
+    ref = np.stack([O.structure_factor(Z, pos.astype(np.float64), q0 @ r.T)[1] for r in R])
+    np.testing.assert_allclose(res["full.npy"], ref, rtol=1e-12)
+
+
 def _gradient_allreduce(rank, world, out):
     from oracle import oracle as O
 
