@@ -76,7 +76,8 @@ def test_cli_formula_molecule(cuda, tmp_path):
     assert not np.array_equal(p0, p1)  # independent noise per shot
 
 
-def test_cli_pdb_molecule_scattering_factors(cuda, tmp_path):
+@pytest.mark.parametrize("nfft", [0, 1], ids=["direct", "nfft"])
+def test_cli_pdb_molecule_scattering_factors(cuda, tmp_path, nfft):
     rng = np.random.Generator(np.random.PCG64(11))
     lines = []
     ops = [np.eye(3), np.array([[0, -1, 0], [1, 0, 0], [0, 0, 1.0]])]
@@ -91,6 +92,8 @@ def test_cli_pdb_molecule_scattering_factors(cuda, tmp_path):
                      % (i + 1, e, 1, x, y, z, e))
     (tmp_path / "mol.pdb").write_text("".join(lines) + "END\n")
     conf = 'number_of_dimensions = 2;\ninput_type = "pdb";\npdb_filename = "mol.pdb";\n' + DETECTOR
+    if nfft:  # compute_sf's NFFT branch (src/spsim.c:119-123), through simulate_shot
+        conf += "use_nfft_for_sf = 1;\n"
     _run(tmp_path, conf)
     m = S.get_Molecule_from_pdb(str(tmp_path / "mol.pdb"))
     n = m.contents.natoms
