@@ -1419,6 +1419,7 @@ struct NufftCtx {
   unsigned long long seg_mol = 0;  // molecule whose segment table is on the device
   NufftGeom g;
   int n_coef = 0;
+  int copies = 1;  // spreading-grid copies
   double psi_a[NUFFT_MAX_COEF];
   unsigned long long *h_keys = nullptr;  // pinned bounds read-back
   cudaEvent_t done = nullptr;
@@ -1554,7 +1555,12 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
       cells1 *= (size_t)g.n1[d];
       cells2 *= (size_t)g.n2[d];
     }
-    const size_t bytes1 = cells1 * n_elem * sizeof(double2), bytes2 = cells2 * n_elem * sizeof(double2);
+    // copies of the spreading grid while they stay small next to L2 (32 MB):
+    // about 1,000 updates of one cell from 20,000 atoms on a 40 x 40 x 18 grid
+    // otherwise serialise in the atomic units
+    const size_t one1 = cells1 * n_elem * sizeof(double2);
+    c.copies = (int)std::max<size_t>(1, std::min<size_t>(8, (32u << 20) / std::max<size_t>(one1, 1)));
+    const size_t bytes1 = one1 * c.copies, bytes2 = cells2 * n_elem * sizeof(double2);
     const size_t bytes3 = cells2 * nufft_pack_groups(n_elem) * nufft_pack_halves(n_elem) * sizeof(float4);
     size_t free_b = 0, total_b = 0;
     CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
@@ -1608,10 +1614,11 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   NufftGeom g = c.g;
   for (int d = 0; d < 3; ++d) g.center[d] = m->center[d];
   size_t cells1 = (size_t)g.n1[0] * g.n1[1] * g.n1[2];
-  CUDA_TRY(cudaMemsetAsync(c.small.p, 0, cells1 * n_elem * sizeof(double2), st));
-  CUDA_TRY(nufft_spread(m->d_atomsd, (const int *)c.seg.p, n_elem, m->n_padded, g, (double2 *)c.small.p,
+  CUDA_TRY(cudaMemsetAsync(c.small.p, 0, cells1 * n_elem * c.copies * sizeof(double2), st));
+  CUDA_TRY(nufft_spread(m->d_atomsd, (const int *)c.seg.p, n_elem, m->n_padded, g, (double2 *)c.small.p, c.copies,
                         (int *)c.flags.p, st));
-  CUDA_TRY(nufft_pad((const double2 *)c.small.p, (double2 *)c.fine.p, g, n_elem, (const double *)c.dec.p, st));
+  CUDA_TRY(nufft_pad((const double2 *)c.small.p, (double2 *)c.fine.p, g, n_elem, c.copies, (const double *)c.dec.p,
+                     st));
   if (cufftSetStream(c.fft_yx, st) != CUFFT_SUCCESS || cufftSetStream(c.fft_z, st) != CUFFT_SUCCESS)
     return fail(SPSIM_ERR_CUDA, "NUFFT: cufftSetStream failed");
   const long long cells2 = (long long)g.n2[0] * g.n2[1] * g.n2[2];

@@ -113,7 +113,7 @@ constexpr int SPREAD_WARPS = 8;
 __global__ void __launch_bounds__(32 * SPREAD_WARPS) nufft_spread_kernel(const AtomD *__restrict__ atoms,
                                                                          const int *__restrict__ seg, int n_elem,
                                                                          int n_atoms, const NufftGeom g,
-                                                                         double2 *__restrict__ grid,
+                                                                         double2 *__restrict__ grid, int copies,
                                                                          int *__restrict__ err) {
   __shared__ double kv[SPREAD_WARPS][3][NUFFT_MAX_W];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -148,7 +148,10 @@ __global__ void __launch_bounds__(32 * SPREAD_WARPS) nufft_spread_kernel(const A
   sincospi(2.0 * t, &sn, &cs);
   const double cr = (double)a.w * cs, ci = -(double)a.w * sn;
   const long long n1x = g.n1[0], n1y = g.n1[1];
-  double2 *base = grid + (long long)e * n1x * n1y * g.n1[2] + ((long long)l0[2] * n1y + l0[1]) * n1x + l0[0];
+  // warps take the grid copies in turn: fewer updates of one cell in flight
+  const long long cells1 = n1x * n1y * g.n1[2];
+  double2 *base = grid + ((long long)(j % copies) * n_elem + e) * cells1 + ((long long)l0[2] * n1y + l0[1]) * n1x +
+                  l0[0];
   // lane = (y parity, x offset): half-warps cover two stencil rows per step
   static_assert(NUFFT_MAX_W <= 16, "one stencil row per half-warp");
   const int ix = lane & 15, iy0 = lane >> 4;
@@ -168,10 +171,11 @@ __global__ void __launch_bounds__(32 * SPREAD_WARPS) nufft_spread_kernel(const A
 }
 
 cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_atoms, const NufftGeom &g,
-                         double2 *grid, int *err, cudaStream_t st) {
+                         double2 *grid, int copies, int *err, cudaStream_t st) {
   if (n_atoms <= 0) return cudaSuccess;
   const unsigned blocks = (unsigned)((n_atoms + SPREAD_WARPS - 1) / SPREAD_WARPS);
-  nufft_spread_kernel<<<blocks, 32 * SPREAD_WARPS, 0, st>>>(atoms, seg, n_elem, n_atoms, g, grid, err);
+  nufft_spread_kernel<<<blocks, 32 * SPREAD_WARPS, 0, st>>>(atoms, seg, n_elem, n_atoms, g, grid, std::max(copies, 1),
+                                                            err);
   return cudaGetLastError();
 }
 
@@ -180,7 +184,7 @@ cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_a
 // index l holds mode m = l - n1/2, stored at FFT index m mod n2.
 
 __global__ void nufft_scatter_kernel(const double2 *__restrict__ small, double2 *__restrict__ fine, const NufftGeom g,
-                                     int n_elem, const double *__restrict__ dec) {
+                                     int n_elem, int copies, const double *__restrict__ dec) {
   const int n1x = g.n1[0], n1y = g.n1[1], n1z = g.n1[2];
   const int n2x = g.n2[0], n2y = g.n2[1], n2z = g.n2[2];
   const double *decx = dec, *decy = dec + n1x, *decz = dec + n1x + n1y;
@@ -192,24 +196,30 @@ __global__ void nufft_scatter_kernel(const double2 *__restrict__ small, double2 
     const double dyz = decy[ly] * decz[lz];
     const double2 *in = small + (((long long)e * n1z + lz) * n1y + ly) * n1x;
     double2 *out = fine + (((long long)e * n2z + pz) * n2y + py) * n2x;
+    const long long copy_stride = (long long)n_elem * n1z * n1y * n1x;
     for (int lx = blockIdx.x * blockDim.x + threadIdx.x; lx < n1x; lx += gridDim.x * blockDim.x) {
       const int px = lx - n1x / 2 < 0 ? lx - n1x / 2 + n2x : lx - n1x / 2;
-      const double2 b = in[lx];
+      double2 b = in[lx];
+      for (int k = 1; k < copies; ++k) {
+        const double2 c = in[k * copy_stride + lx];
+        b.x += c.x;
+        b.y += c.y;
+      }
       const double d = dyz * decx[lx];
       out[px] = make_double2(b.x * d, b.y * d);
     }
   }
 }
 
-cudaError_t nufft_pad(const double2 *small, double2 *fine, const NufftGeom &g, int n_elem, const double *dec,
-                      cudaStream_t st) {
+cudaError_t nufft_pad(const double2 *small, double2 *fine, const NufftGeom &g, int n_elem, int copies,
+                      const double *dec, cudaStream_t st) {
   const size_t cells2 = (size_t)g.n2[0] * g.n2[1] * g.n2[2];
   cudaError_t e = cudaMemsetAsync(fine, 0, cells2 * n_elem * sizeof(double2), st);
   if (e != cudaSuccess) return e;
   const int threads = 128;
   dim3 grid((unsigned)std::min((g.n1[0] + threads - 1) / threads, 8), (unsigned)g.n1[1],
             (unsigned)std::min(n_elem * g.n1[2], 65535));
-  nufft_scatter_kernel<<<grid, threads, 0, st>>>(small, fine, g, n_elem, dec);
+  nufft_scatter_kernel<<<grid, threads, 0, st>>>(small, fine, g, n_elem, std::max(copies, 1), dec);
   return cudaGetLastError();
 }
 

@@ -69,14 +69,17 @@ double nufft_key_to_double(unsigned long long k);
 unsigned long long nufft_double_to_key(double d);
 
 // Step 1.  atoms: element-sorted FP64 records; seg: n_elem + 1 segment starts;
-// grid (zeroed): [n_elem][n1z][n1y][n1x].  An atom whose stencil leaves the
-// grid is skipped and sets err[0].
+// grid (zeroed): `copies` x [n_elem][n1z][n1y][n1x], atom j adding into copy
+// j mod copies (several copies spread the updates of one cell when the grid is
+// small next to the atom count).  An atom whose stencil leaves the grid is
+// skipped and sets err[0].
 cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_atoms, const NufftGeom &g,
-                         double2 *grid, int *err, cudaStream_t st);
-// Step 2: zero `fine` and scatter the deconvolved spreading grid into it.
-// dec: 1 / phi2hat per spreading-grid index, x then y then z.
-cudaError_t nufft_pad(const double2 *small, double2 *fine, const NufftGeom &g, int n_elem, const double *dec,
-                      cudaStream_t st);
+                         double2 *grid, int copies, int *err, cudaStream_t st);
+// Step 2: zero `fine` and scatter the deconvolved spreading grid (the sum of
+// its copies) into it.  dec: 1 / phi2hat per spreading-grid index, x then y
+// then z.
+cudaError_t nufft_pad(const double2 *small, double2 *fine, const NufftGeom &g, int n_elem, int copies,
+                      const double *dec, cudaStream_t st);
 // Step 3b: FP32 element-interleaved copy of the FFT output for step 4
 // (nufft_pack_groups(n_elem) x cells2 x nufft_pack_halves(n_elem) float4).
 int nufft_pack_halves(int n_elem);
