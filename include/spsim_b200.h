@@ -336,7 +336,8 @@ int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
 /* The reference-shaped calls (include/spsim.h) and
  * spsim_b200_structure_factor_host keep device scratch between calls on the
  * calling thread (grow-only buffers, the last molecule while its atom arrays
- * stay byte-identical, a reusable plan); this frees it for the current device.
+ * stay byte-identical, a reusable plan), and the NUFFT forwards keep their
+ * grids and FFT plans per device; this frees both for the current device.
  * No reference counterpart: spsim allocates and frees per call. */
 void spsim_b200_release_scratch(void);
 

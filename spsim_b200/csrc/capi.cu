@@ -1230,10 +1230,14 @@ static int host_session_qset(int64_t npix, const float *hkl, spsim_b200_qset **o
 }
 
 // Frees this thread's host-call session and scratch plan (called by
-// spsim_b200_release_scratch after a device synchronisation).
+// spsim_b200_release_scratch after a device synchronisation), and the
+// device's NUFFT grids and plans.
+static void nufft_release(int dev);
+
 extern "C" void spsim_internal_release_host_session(void) {
   int dev = -1;
   cudaGetDevice(&dev);
+  nufft_release(dev);
   if (g_host.device == dev) {
     if (g_host.mol) spsim_b200_molecule_destroy(g_host.mol);
     if (g_host.qs) spsim_b200_qset_destroy(g_host.qs);
@@ -1666,6 +1670,18 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   g_last_nufft_w[1] = g.w2;
   for (int d = 0; d < 3; ++d) g_last_nufft_n2[d] = g.n2[d];
   return SPSIM_OK;
+}
+
+static void nufft_release(int dev) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_nufft.find(dev);
+  if (it == g_nufft.end()) return;
+  NufftCtx &c = it->second;
+  if (c.fft_yx) cufftDestroy(c.fft_yx);
+  if (c.fft_z) cufftDestroy(c.fft_z);
+  if (c.h_keys) cudaFreeHost(c.h_keys);
+  if (c.done) cudaEventDestroy(c.done);
+  g_nufft.erase(it);  // the grids' DevBufs free themselves
 }
 
 // Sticky error word of this device's NUFFT context (atoms outside the grid).

@@ -188,3 +188,20 @@ def test_orientation_batch_matches_oracle_and_single_calls(cuda):
         Fs, _ = core.forward_nufft(mol, qs, rot=r, B=10.0)
         core.synchronize()
         assert np.abs(_np(Fs) - _np(F[i])).max() < 2e-6 * np.abs(F64).max()
+
+
+def test_release_scratch_frees_and_rebuilds_the_grids(cuda):
+    # spsim_b200_release_scratch drops the device's NUFFT grids and FFT plans;
+    # the next forward builds them again
+    from spsim_b200._native import lib
+
+    g = golden("sf_small.npz")
+    mol = core.Molecule(g["Z"], g["pos"])
+    qs = core.QSet.from_list(g["hkl"])
+    F1, _ = core.forward_nufft(mol, qs)
+    core.synchronize()
+    F1 = _np(F1)
+    lib().spsim_b200_release_scratch()
+    F2, _ = core.forward_nufft(mol, qs)
+    core.synchronize()
+    assert np.abs(_np(F2) - F1).max() <= 1e-6 * np.abs(F1).max()
