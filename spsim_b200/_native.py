@@ -128,6 +128,8 @@ _SIGNATURES = {
                                           POINTER(c_int)]),
     "spsim_b200_clear_tuning": (c_int, []),
     "spsim_b200_set_legacy_precision": (None, [c_int]),
+    "spsim_b200_set_legacy_nufft_eps": (None, [c_double]),
+    "spsim_b200_get_legacy_nufft_eps": (c_double, []),
     "spsim_b200_get_legacy_precision": (c_int, []),
     "spsim_b200_set_noise_seed": (None, [c_uint64]),
 }

@@ -301,6 +301,16 @@ def set_noise_seed(seed):
     _native.lib().spsim_b200_set_noise_seed(int(seed))
 
 
+def set_nufft_eps(eps):
+    """Relative error of the NUFFT structure factor behind compute_pattern_on_list_by_nfft
+    and use_nfft_for_sf (default 1e-8)."""
+    _native.lib().spsim_b200_set_legacy_nufft_eps(float(eps))
+
+
+def get_nufft_eps():
+    return _native.lib().spsim_b200_get_legacy_nufft_eps()
+
+
 def _floats(a):
     if isinstance(a, np.ndarray):
         a = np.ascontiguousarray(a, np.float32)

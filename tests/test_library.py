@@ -78,3 +78,15 @@ def test_invalid_arguments_rejected_before_device_use():
         _native.SPSIM_ERR_INVALID_ARG
     p = _native.ChainParams(nx=4, ny=4, nz=1, binning_x=0, binning_y=1, binning_z=1)
     assert L.spsim_b200_thomson(ctypes.byref(p), None, None) == _native.SPSIM_ERR_INVALID_ARG
+
+
+def test_legacy_nufft_eps_setting():
+    # the relative error used by compute_pattern_on_list_by_nfft / use_nfft_for_sf
+    from spsim_b200 import spsim as S
+
+    assert S.get_nufft_eps() == 1e-8
+    try:
+        S.set_nufft_eps(1e-10)
+        assert S.get_nufft_eps() == 1e-10
+    finally:
+        S.set_nufft_eps(1e-8)
