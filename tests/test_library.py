@@ -78,6 +78,10 @@ def test_invalid_arguments_rejected_before_device_use():
         _native.SPSIM_ERR_INVALID_ARG
     p = _native.ChainParams(nx=4, ny=4, nz=1, binning_x=0, binning_y=1, binning_z=1)
     assert L.spsim_b200_thomson(ctypes.byref(p), None, None) == _native.SPSIM_ERR_INVALID_ARG
+    # the NUFFT forwards: NULL handles, and a batch outside [1, 65535] patterns
+    assert L.spsim_b200_forward_nufft(None, None, None, 0.0, 1e-8, None, None, None) == _native.SPSIM_ERR_INVALID_ARG
+    assert L.spsim_b200_forward_nufft_batch(None, None, 0, None, 0.0, 1e-8, None, None, None) == \
+        _native.SPSIM_ERR_INVALID_ARG
 
 
 def test_legacy_nufft_eps_setting():
