@@ -159,16 +159,20 @@ int spsim_b200_structure_factor_host_spectrum(int natoms, const int32_t *Z, cons
  * The same F(q) = sum_e f_e(|q|) sum_{j in e} w_j exp(-2 pi i q.r_j) as
  * spsim_b200_forward, computed per element as a type-3 non-uniform FFT
  * (atoms spread onto a real-space grid, one batched 3-D FFT, interpolation at
- * every pixel's q; FP64 grids) in O(atoms w^3 + grid log grid + pixels w^3)
+ * every pixel's q; FP64 spreading and FFT, an FP32 copy of the FFT grid for
+ * the interpolation) in O(atoms w^3 + grid log grid + pixels w^3)
  * instead of O(atoms x pixels).  Replaces the reference's NNFFT path
  * (compute_pattern_on_list_by_nfft, src/diffraction.c:528-675, dispatched by
  * compute_sf when use_nfft_for_sf is set, src/spsim.c:119-123), which runs
  * the NFFT library with a cut-off of m = 2.
- * eps: requested relative L2 error of F against the exact sum, in
- * [1e-14, 1e-2]; it sets the kernel width w = ceil(-log10 eps) + 1 grid points
- * (interpolation) and w + 1 (spreading), up to 15.  The grid follows the
- * bounding box of R q and the molecule's radius: (4 S_d |r - c|max * 2 + w)
- * * 2 points per axis (S_d: half-width of the q box along d).
+ * eps: target relative L2 error of F against the exact sum, in
+ * [1e-14, 1e-2] (measured errors come out within a few eps, and not below the
+ * complex64 output's ~3e-8); it sets the interpolation kernel width
+ * w = ceil(-log10 eps) + 1 grid points (up to 15) and the spreading width
+ * w + 3 (up to 16).  The grids follow the bounding box of R q and the
+ * molecule's radius r_b: about 6 S_d r_b + w + 5 spreading points per axis
+ * (S_d: half-width of the q box along d) and twice that, rounded up to a size
+ * with factors 2, 3, 5, 7, for the FFT.
  * Not supported: per-atom B factors (SPSIM_ERR_INVALID_ARG).  F_dev, I_dev
  * as spsim_b200_forward; enqueued on `stream` after a one-time read-back of
  * the q box per (q set, rotation); atoms that moved outside the creation-time

@@ -41,7 +41,7 @@ def test_small_molecule_meets_requested_eps(cuda, eps):
     _check_F(_np(F), F64, eps)
     assert np.allclose(_np(I), np.abs(_np(F)) ** 2, rtol=1e-5, atol=1e-6 * I64.max())
     w1, w2, n2 = core.last_nufft_grid()
-    assert w2 == min(max(int(np.ceil(-np.log10(eps))) + 1, 4), 15) and w1 == min(w2 + 4, 16)
+    assert w2 == min(max(int(np.ceil(-np.log10(eps))) + 1, 4), 15) and w1 == min(w2 + 3, 16)
     assert all(n % 2 == 0 and n >= 2 * (w2 + 3) for n in n2)
 
 
