@@ -518,8 +518,8 @@ def _nufft_mode(core, mol, qs, rot, terms, sub_rows, I64, eps=1e-8, steps=5):
             "kernel_widths": [w1, w2], "fft_grid": list(n2),
             "accuracy": {"floored_max_rel": float(np.max(np.abs(In - I64) / den)),
                          "l2_rel": float(np.linalg.norm(In - I64) / np.linalg.norm(I64))},
-            "note": "type-3 NUFFT per element (spread, pad, cuFFT Z2Z, interpolate; FP64 grids), "
-                    "a different algorithm from the direct sum the headline value times"}
+            "note": "type-3 NUFFT per element (spread, pad, cuFFT Z2Z, interpolate; FP64 spreading and FFT, "
+                    "FP32 interpolation grid), a different algorithm from the direct sum the headline value times"}
 
 
 def _e2e(args, w, Z, pos, terms, world, dist=None):
