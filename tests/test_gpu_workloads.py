@@ -1,0 +1,124 @@
+"""The batched workloads at their stated sizes, against the FP64 oracle.
+
+  orientations_20k  20,000 atoms, 256^2 pixels of 150 um at 0.2 m, 0.2 nm,
+                    4,096 Haar rotations in ONE batched forward
+  uneven_64         64 molecules of 500..100,000 atoms, each on its own
+                    detector (128^2 .. 1024^2) and wavelength, in one batched
+                    forward after the batch autotuner has picked the tile shape
+  adjoint_5k        5,000 atoms, 512^2 pixels, 256 orientations, per-atom
+                    occupancies and B factors: forward + adjoint over the whole
+                    batch, dL/dI non-zero on a pixel subset
+
+The GPU runs the whole workload; the oracle checks a subset of each output
+(whole detector rows), which the FP32 path must meet at its tolerance: floored
+maximum relative |F|^2 error 1e-5, L2 1e-6 (tests/test_gpu_sf.py); gradients
+1e-4 relative L2 against the oracle's analytic FP64 vector-Jacobian product
+(itself checked against FP64 central differences, tests/test_oracle_adjoint.py).
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import intensity_errors
+from oracle import oracle as O
+from spsim_b200 import core, synth
+
+pytestmark = pytest.mark.gpu
+
+F32_TOL = (1e-5, 1e-6)
+
+
+def _rows(nx, ny, nrows):
+    """Pixel indices of `nrows` evenly spaced whole detector rows."""
+    rows = np.unique(np.linspace(0, ny - 1, nrows).round().astype(np.int64))
+    return (rows[:, None] * nx + np.arange(nx)[None, :]).reshape(-1)
+
+
+def test_orientations_20k_4096_rotations_in_one_batch(cuda):
+    w = synth.WORKLOADS["orientations_20k"]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    d = w["det"]
+    R = synth.haar_rotations(w["n_orient"], w["rot_seed"])
+    assert len(R) == 4096
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(**d)
+    I = torch.empty(len(R), qs.npix, device="cuda")
+    core.forward_batch(mol, qs, rots=R, precision="f32", I=list(I.unbind(0)), want_F=False)
+    torch.cuda.synchronize()
+    core.synchronize()
+    assert core.kernel_name() == "sf_dpair_kernel"
+    q0 = O.hkl_detector(**d)
+    sel = _rows(d["nx"], d["ny"], 4)
+    for k in (0, 1, 2047, 4095):
+        _, I64 = O.structure_factor(Z, pos.astype(np.float64), q0[sel] @ R[k].T)
+        e_max, e_l2 = intensity_errors(I[k, sel].cpu().numpy(), I64)
+        print("orientation %d: floored max %.3g  L2 %.3g" % (k, e_max, e_l2))
+        assert e_max < F32_TOL[0] and e_l2 < F32_TOL[1], (k, e_max, e_l2)
+
+
+def test_uneven_64_molecules_in_one_batch_after_autotune(cuda):
+    specs = synth.uneven_batch()
+    mols, qsets, atoms = [], [], []
+    for m in specs:
+        Zm, pm = synth.random_molecule(m["natoms"], m["radius"], m["seed"])
+        mols.append(core.Molecule(Zm, pm))
+        qsets.append(core.QSet.from_detector(**m["det"]))
+        atoms.append((Zm, pm))
+    try:
+        tuned = core.autotune_batch(mols, qsets, precision="f32")
+        _, I = core.forward_batch(mols, qsets, precision="f32", want_F=False)
+        torch.cuda.synchronize()
+        core.synchronize()
+        assert core.last_variant()[:2] == tuned[:2]
+    finally:
+        core.clear_tuning()
+    n = np.array([m["natoms"] for m in specs])
+    big = [i for i, m in enumerate(specs) if m["det"]["nx"] == 1024]
+    assert big, "the seeded batch holds a 1024^2 detector"
+    picks = sorted({int(n.argmin()), int(n.argmax()), big[0]})
+    for i in picks:
+        d = specs[i]["det"]
+        Zm, pm = atoms[i]
+        sel = _rows(d["nx"], d["ny"], 16)
+        q = O.hkl_detector(**d)[sel]
+        _, I64 = O.structure_factor(Zm, pm.astype(np.float64), q)
+        e_max, e_l2 = intensity_errors(I[i][sel].cpu().numpy(), I64)
+        print("molecule %d (%d atoms, %d^2): floored max %.3g  L2 %.3g" % (i, n[i], d["nx"], e_max, e_l2))
+        assert e_max < F32_TOL[0] and e_l2 < F32_TOL[1], (i, e_max, e_l2)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_adjoint_5k_512sq_256_orientations(cuda):
+    w = synth.WORKLOADS["adjoint_5k"]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    d = w["det"]
+    R = synth.haar_rotations(w["n_orient"], w["rot_seed"])
+    assert len(R) == 256
+    rng = np.random.Generator(np.random.PCG64(w["seed"]))
+    occ = rng.uniform(0.5, 1.0, len(Z)).astype(np.float32)
+    bfac = rng.uniform(0.0, 30.0, len(Z)).astype(np.float32)
+    mol = core.Molecule(Z, pos, occ=occ, bfac=bfac)
+    qs = core.QSet.from_detector(**d)
+    F = torch.empty(len(R), qs.npix, dtype=torch.complex64, device="cuda")
+    I = torch.empty(len(R), qs.npix, device="cuda")
+    core.forward_batch(mol, qs, rots=R, precision="f32", F=list(F.unbind(0)), I=list(I.unbind(0)))
+    # dL/dI on 16 whole rows of every 16th orientation, zero elsewhere: the
+    # adjoint still runs over every atom x pixel term of the batch
+    pats = np.arange(0, len(R), 16)
+    sel = _rows(d["nx"], d["ny"], 16)
+    g = rng.normal(size=(len(pats), len(sel))).astype(np.float32)
+    G = torch.zeros(len(R), qs.npix, device="cuda")
+    G[torch.from_numpy(pats)[:, None].cuda(), torch.from_numpy(sel)[None, :].cuda()] = torch.from_numpy(g).cuda()
+    dpos, docc, dB = core.adjoint(mol, qs, F.reshape(-1), G.reshape(-1), rots=R, precision="f32")
+    torch.cuda.synchronize()
+    core.synchronize()
+    q0 = O.hkl_detector(**d)[sel]
+    q = np.concatenate([q0 @ R[k].T for k in pats])
+    dp, do, db = O.structure_factor_vjp(Z, pos.astype(np.float64), q, g.reshape(-1).astype(np.float64), occ=occ,
+                                        bfac=bfac)
+    errs = (_rel(dpos.cpu().numpy(), dp), _rel(docc.cpu().numpy(), do), _rel(dB.cpu().numpy(), db))
+    print("adjoint_5k gradient rel. L2 (pos, occ, B):", errs)
+    assert max(errs) < 1e-4, errs
