@@ -24,6 +24,22 @@ namespace spsim {
 // gave them up to 252 registers and cost 5 %).
 __host__ __device__ constexpr int sf_min_blocks(int mode) { return mode == PREC_MODE_POLY ? 1 : 0; }
 
+// Bounded waits on the atom-tile ring.  A wait that runs out sets the error
+// word, drains (bounded) the copies this CTA still has in flight and returns.
+// g_copy_stall is the test hook behind spsim_b200_debug_stall_first_copy:
+// while it is set, each CTA arms the barrier of its first tile without issuing
+// that tile's copy (a barrier that nothing completes) and its waits give up
+// after kStallWaitCycles, so the exit path runs in milliseconds and without a
+// fault; read once per CTA at launch.
+__device__ int g_copy_stall = 0;
+constexpr long long kWaitCyclesDefault = 4000000000LL;  // ~2 s at 2 GHz
+constexpr long long kStallWaitCycles = 20000000LL;      // ~10 ms
+
+cudaError_t set_copy_stall(int on) {
+  const int v = on ? 1 : 0;
+  return cudaMemcpyToSymbol(g_copy_stall, &v, sizeof(int));
+}
+
 // ---------------------------------------------------------------------------
 // form factors
 
@@ -141,7 +157,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_f32_kernel(const S
 
   uint32_t g_issue = 0;  // tiles issued by this CTA (meaningful in thread 0)
   uint32_t g_cons = 0;   // tiles consumed by this CTA (uniform)
-  const long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
+  const bool stall = g_copy_stall != 0;
+  const long long kWaitCycles = stall ? kStallWaitCycles : kWaitCyclesDefault;
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(queue, 1);
@@ -194,7 +211,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_f32_kernel(const S
         const uint32_t st = g_issue % RING_STAGES;
         const uint32_t bytes = (uint32_t)td.count * 32u;
         mbar_arrive_expect_tx(&full_bar[st], bytes);
-        bulk_copy_g2s(&ring[st][0], atoms + 2 * (long long)td.atom_begin, bytes, &full_bar[st]);
+        if (!(stall && g_issue == 0))  // the stall hook skips the CTA's first copy
+          bulk_copy_g2s(&ring[st][0], atoms + 2 * (long long)td.atom_begin, bytes, &full_bar[st]);
         ++g_issue;
       }
     }
@@ -294,7 +312,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_f32x2_kernel(const
   __syncthreads();
 
   uint32_t g_issue = 0, g_cons = 0;
-  const long long kWaitCycles = 4000000000LL;
+  const bool stall = g_copy_stall != 0;
+  const long long kWaitCycles = stall ? kStallWaitCycles : kWaitCyclesDefault;
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(queue, 1);
@@ -357,7 +376,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_f32x2_kernel(const
         const uint32_t st = g_issue % RING_STAGES;
         const uint32_t bytes = (uint32_t)td.count * 64u;
         mbar_arrive_expect_tx(&full_bar[st], bytes);
-        bulk_copy_g2s(&ring[st][0], atoms2 + 4 * (long long)td.atom_begin, bytes, &full_bar[st]);
+        if (!(stall && g_issue == 0))  // the stall hook skips the CTA's first copy
+          bulk_copy_g2s(&ring[st][0], atoms2 + 4 * (long long)td.atom_begin, bytes, &full_bar[st]);
         ++g_issue;
       }
     }
@@ -524,7 +544,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dphase_kernel(cons
   __syncthreads();
 
   uint32_t g_issue = 0, g_cons = 0;
-  const long long kWaitCycles = 4000000000LL;
+  const bool stall = g_copy_stall != 0;
+  const long long kWaitCycles = stall ? kStallWaitCycles : kWaitCyclesDefault;
   const double M52 = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
   // FIXW: pixel q pre-scaled by 2 (half-cycle reduction) and the phase summed onto kWordBase
   constexpr double kQScale = (FIXW && MODE == PREC_MODE_POLY) ? 2.0 : 1.0;
@@ -569,7 +590,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dphase_kernel(cons
         const uint32_t st = g_issue % RING_STAGES;
         const uint32_t bytes = (uint32_t)td.count * (uint32_t)sizeof(AtomD);
         mbar_arrive_expect_tx(&full_bar[st], bytes);
-        bulk_copy_g2s(&ring[st][0], atomsd + td.atom_begin, bytes, &full_bar[st]);
+        if (!(stall && g_issue == 0))  // the stall hook skips the CTA's first copy
+          bulk_copy_g2s(&ring[st][0], atomsd + td.atom_begin, bytes, &full_bar[st]);
         ++g_issue;
       }
     }
@@ -746,7 +768,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
   __syncthreads();
 
   uint32_t g_issue = 0, g_cons = 0;
-  const long long kWaitCycles = 4000000000LL;
+  const bool stall = g_copy_stall != 0;
+  const long long kWaitCycles = stall ? kStallWaitCycles : kWaitCyclesDefault;
   const double M52 = 6755399441055744.0;  // 1.5 * 2^52
   constexpr double kQScale = (FIXW && MODE == PREC_MODE_POLY) ? 2.0 : 1.0;
   constexpr double kWordBase = MODE == PREC_MODE_POLY ? PHASE_WORD_BASE_HALF : PHASE_WORD_BASE;
@@ -800,7 +823,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
         const uint32_t st = g_issue % RING_STAGES;
         const uint32_t bytes = (uint32_t)td.count * (uint32_t)sizeof(AtomD);
         mbar_arrive_expect_tx(&full_bar[st], bytes);
-        bulk_copy_g2s(&ring[st][0], atomsd + td.atom_begin, bytes, &full_bar[st]);
+        if (!(stall && g_issue == 0))  // the stall hook skips the CTA's first copy
+          bulk_copy_g2s(&ring[st][0], atomsd + td.atom_begin, bytes, &full_bar[st]);
         ++g_issue;
       }
     }

@@ -15,6 +15,8 @@ cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix,
 cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
                           const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st,
                           bool fixw = false, bool narrow = false);
+// The bounded-wait test hook (see g_copy_stall in sf_kernels.cu), current device.
+cudaError_t set_copy_stall(int on);
 int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw = false, bool narrow = false);
 bool sf_f32_variant_exists(int mode, int nt, int p, int packed);
 cudaError_t launch_sf_f64(const SfPattern *pats, int pattern, long long npix, cudaStream_t st);
