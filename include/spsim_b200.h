@@ -200,20 +200,23 @@ int spsim_b200_structure_factor_host_nufft(int natoms, const int32_t *Z, const f
                                            int64_t npix, const float *hkl, double eps, float *F_host, float *I_host);
 
 /* ---- allocation-free variant (no counterpart in the reference) ------------
- * The same computation, arguments and results as
- * spsim_b200_structure_factor_host, for callers that may not allocate device
- * memory while they run: applications that hand out all device memory from
- * their own fixed budget or pool, and services that cannot afford a
- * cudaMalloc / cudaFree (which synchronise the whole device) on every call.
- * It calls no cudaMalloc, cudaFree or other allocating routine: its device
- * scratch is one static 64 MiB array per GPU (held by every GPU that loads
- * the library, until the process exits) and its host staging a static
- * 48 MiB array.  A call needs about 96 bytes per atom plus (40 + 8 x number of
- * elements) bytes per pixel of scratch; larger calls return
- * SPSIM_ERR_INVALID_ARG and print the sizes.  The first call on a device looks
- * up that device's address of the array, so make it before any stream capture.
- * Calls share the array: they are serialised and synchronised before
- * returning; calls that overlapped on the GPU would race. */
+ * The computation, arguments and results of spsim_b200_structure_factor_host
+ * (the same kernels, chosen by the same rules as its untuned defaults, and the
+ * same phase-range limit: SPSIM_ERR_RANGE beyond 2^48 cycles), for callers
+ * that may not allocate device memory while they run: applications that hand
+ * out all device memory from their own fixed budget or pool, and services
+ * that cannot afford a cudaMalloc / cudaFree (which synchronise the whole
+ * device) on every call.  It calls no cudaMalloc, cudaFree or other allocating
+ * routine: its device scratch is one static 64 MiB array per GPU (held by
+ * every GPU that loads the library, until the process exits) and its host
+ * staging a static 16 MiB array.  A call needs about 160 bytes per atom plus
+ * (40 + 8 x number of elements) bytes per pixel of scratch, e.g. 100,000 atoms
+ * on a 256 x 256 detector; larger calls return SPSIM_ERR_INVALID_ARG, with the
+ * sizes in spsim_b200_last_error().  The first call on a device looks up that
+ * device's address of the array, so make it before any stream capture;
+ * cudaDeviceReset between calls is not supported.  Calls share the array: they
+ * are serialised and synchronised before returning; calls that overlapped on
+ * the GPU would race. */
 int spsim_b200_structure_factor_host_noalloc(int natoms, const int32_t *Z, const float *pos, const float *occ,
                                              const float *bfac, float B, int delta_atoms, const float *beam,
                                              int64_t npix, const float *hkl, int precision, float *F_host,
@@ -323,6 +326,18 @@ int spsim_b200_crystal_lattice_sum(int64_t npix, const float *hkl_dev, const flo
  * refined positions outside the molecule's bounds) are recorded in device
  * flags; spsim_b200_synchronize waits for `stream` and reports them. */
 int spsim_b200_synchronize(void *stream);
+
+/* Test hook for the bounded device waits (no reference counterpart; spsim has
+ * no device-side waits).  While `on` is set for the current device, every
+ * structure-factor kernel (the direct FP32 forms, not the plain FP64 kernel)
+ * arms the barrier of its first atom tile without issuing the tile's copy, so
+ * that its first wait runs out after ~10 ms instead of ~2 s: the kernel sets
+ * its error word, waits for its copies still in flight and returns, and the
+ * forward reports SPSIM_ERR_TIMEOUT (the synchronous calls directly, the others
+ * through spsim_b200_synchronize).  Nothing faults and the context stays
+ * usable; with the hook off again the next forward runs normally.  Waits for
+ * the device to go idle before it changes the setting. */
+int spsim_b200_debug_stall_first_copy(int on);
 
 /* Per-launch timing of the structure-factor kernel with CUDA events recorded
  * on the launching stream.  While enabled, forwards run as direct launches

@@ -115,6 +115,9 @@ _SIGNATURES = {
     "spsim_b200_hkl_for_detector": (
         c_int, [c_int, c_int, c_float, c_float, c_float, c_float, c_float, c_float, c_int, _P, _P]),
     "spsim_b200_synchronize": (c_int, [_P]),
+    "spsim_b200_debug_stall_first_copy": (c_int, [c_int]),
+    "spsim_b200_structure_factor_host_noalloc": (
+        c_int, [c_int, _P, _P, _P, _P, c_float, c_int, _P, c_int64, _P, c_int, _P, _P]),
     "spsim_b200_timing_enable": (c_int, [c_int]),
     "spsim_b200_timing_read": (c_int, [POINTER(c_double), c_int, POINTER(c_int)]),
     "spsim_b200_last_forward_stats": (c_int, [POINTER(c_double), POINTER(c_double)]),

@@ -37,6 +37,10 @@ static int fail(int status, const char *fmt, ...) {
   return status;
 }
 
+// Records a failure of the allocation-free entry point (noalloc.cu), so that
+// spsim_b200_last_error() reports it like every other call's.
+int spsim_internal_fail(int status, const char *msg) { return fail(status, "%s", msg); }
+
 #define CUDA_TRY(expr)                                                                            \
   do {                                                                                            \
     cudaError_t _e = (expr);                                                                      \
@@ -104,12 +108,10 @@ extern "C" int spsim_b200_init(int device) {
 // directory; every row gets a1 = -1 and rows present in the file are replaced.
 
 static float g_atomsf[SPSIM_B200_N_ELEMENTS][9];
-static bool g_atomsf_loaded = false;
+static std::once_flag g_atomsf_once;
 
-static void load_atomsf_table() {
-  if (g_atomsf_loaded) return;
+static void read_atomsf_table() {
   memcpy(g_atomsf, spsim_b200_atomsf_default, sizeof(g_atomsf));
-  g_atomsf_loaded = true;
   FILE *f = fopen("atomsf.lib", "r");
   if (!f) return;
   for (int i = 0; i < SPSIM_B200_N_ELEMENTS; ++i) g_atomsf[i][0] = -1;
@@ -141,6 +143,9 @@ static void load_atomsf_table() {
   }
   fclose(f);
 }
+
+// The table is read once per process, by whichever thread uses it first.
+static void load_atomsf_table() { std::call_once(g_atomsf_once, read_atomsf_table); }
 
 // Row Z of the coefficient table in use (the ./atomsf.lib override applied);
 // internal, shared with the allocation-free entry point in noalloc.cu.
@@ -1793,6 +1798,16 @@ extern "C" int spsim_b200_synchronize(void *stream) {
   int dev = 0;
   CUDA_TRY(cudaGetDevice(&dev));
   return nufft_check_flags(dev);
+}
+
+extern "C" int spsim_b200_debug_stall_first_copy(int on) {
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(g_mu);
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(set_copy_stall(on));
+  return SPSIM_OK;
 }
 
 extern "C" int spsim_b200_timing_enable(int enable) {
