@@ -57,6 +57,73 @@ def scatt_factor(q_len, Z, B=0.0):
     return oracle_lib().oracle_scatt_factor(float(q_len), int(Z), float(B))
 
 
+def atomsf_table():
+    """The oracle's coefficient table in use: float32 (100, 9), rows a1..a4, b1..b4, c."""
+    L = oracle_lib()
+    L.oracle_get_atomsf_row.argtypes = [c_int, c_void_p]
+    out = np.zeros((100, 9), np.float32)
+    for z in range(100):
+        L.oracle_get_atomsf_row(z, _p(out[z]))
+    return out
+
+
+def set_atomsf_table(table):
+    """Replace every row of the oracle's coefficient table."""
+    L = oracle_lib()
+    L.oracle_set_atomsf_row.argtypes = [c_int, c_void_p]
+    t = np.ascontiguousarray(table, np.float32).reshape(100, 9)
+    for z in range(100):
+        L.oracle_set_atomsf_row(z, _p(t[z]))
+
+
+def reset_atomsf_table():
+    """Back to the compiled-in table."""
+    oracle_lib().oracle_reset_atomsf()
+
+
+def atomsf_lib_table(path, base=None):
+    """The coefficient table spsim uses when ./atomsf.lib exists
+    (src/diffraction.c:118-177, fill_ff_tables): starting from the compiled-in
+    table, every row's a1 is set to -1; after the leading comment lines (those
+    starting with "AD") the file holds 5-line records: a name line; a line with
+    Z (read by %d from its start) and c (read by %f from column 24 on); a1..a4
+    and b1..b4 in 16-column fields on the next two lines; one more line.  A
+    record replaces row Z only the first time Z appears (a1 still -1)."""
+    t = np.array(atomsf_table() if base is None else base, np.float32)
+    t[:, 0] = -1.0
+    lines = open(path).read().splitlines(keepends=True)
+    i = 0
+    while i < len(lines) and lines[i].startswith("AD"):
+        i += 1
+
+    def num(s, conv):
+        tok = s.split()
+        try:
+            return conv(tok[0]) if tok else None
+        except ValueError:
+            return None
+
+    while i < len(lines):  # lines[i]: the record's name line (a blank line counts)
+        if i + 3 >= len(lines):
+            break
+        zl, al, bl = lines[i + 1], lines[i + 2], lines[i + 3]
+        z = num(zl, int)
+        if z is None or not 0 <= z < 100:
+            break
+        if t[z, 0] == -1.0:
+            c = num(zl[23:], float)
+            if c is not None:
+                t[z, 8] = c
+            for k in range(4):
+                a, b = num(al[16 * k:], float), num(bl[16 * k:], float)
+                if a is not None:
+                    t[z, k] = a
+                if b is not None:
+                    t[z, 4 + k] = b
+        i += 5
+    return t
+
+
 def hkl_detector(nx, ny, width, height, distance, wavelength, center_x=0.0, center_y=0.0, spherical=False):
     q = np.empty((nx * ny, 3), np.float64)
     L = oracle_lib()
@@ -75,7 +142,7 @@ def structure_factor(Z, pos, q, occ=None, bfac=None, B=0.0, delta_atoms=False, b
     bfac = np.ascontiguousarray(bfac, np.float64) if bfac is not None else None
     n = q.shape[0]
     fr, fi, I = np.empty(n), np.empty(n), np.empty(n)
-    beam = beam or (0.0, 0.0, 0.0)
+    beam = (0.0, 0.0, 0.0) if beam is None else tuple(float(b) for b in beam)
     L = oracle_lib()
     L.oracle_structure_factor.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double,
                                           c_double, c_double, ctypes.c_long, c_void_p, c_void_p, c_void_p, c_void_p,
@@ -96,7 +163,7 @@ def structure_factor_spectrum(Z, pos, q, wavelength, bandwidth, samples, occ=Non
     q = np.ascontiguousarray(q, np.float64).reshape(-1, 3)
     occ = np.ascontiguousarray(occ, np.float64) if occ is not None else None
     bfac = np.ascontiguousarray(bfac, np.float64) if bfac is not None else None
-    beam = beam or (0.0, 0.0, 0.0)
+    beam = (0.0, 0.0, 0.0) if beam is None else tuple(float(b) for b in beam)
     n = q.shape[0]
     Fr, Fi, I = np.zeros(n), np.zeros(n), np.zeros(n)
     L.oracle_structure_factor_spectrum.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int,

@@ -47,6 +47,13 @@ void oracle_set_atomsf_row(int Z, const float *coeffs9) {
 
 void oracle_reset_atomsf(void) { g_atomsf_ready = 0; ensure_table(); }
 
+/* Row Z of the coefficient table in use. */
+void oracle_get_atomsf_row(int Z, float *coeffs9) {
+  ensure_table();
+  if (Z < 0 || Z >= SPSIM_B200_N_ELEMENTS) return;
+  memcpy(coeffs9, g_atomsf[Z], 9 * sizeof(float));
+}
+
 /* src/diffraction.c:183-193: f(|q|) = sum_i a_i exp(-(b_i+B) d^2/4) + c exp(-B d^2/4),
  * d = |q| * 1e-10 (1/m -> 1/Angstrom).  Here in FP64 throughout. */
 double oracle_scatt_factor(double q_len, int Z, double B) {
