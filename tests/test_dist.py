@@ -113,6 +113,54 @@ def test_sharded_orientation_batch_gather_equals_single_process():
     np.testing.assert_allclose(res["full.npy"], ref, rtol=1e-12)
 
 
+def _sharded_pixel_slabs(rank, world, out):
+    from oracle import oracle as O
+
+    Z, pos, R, q0 = _case()
+    q = (q0 @ R[0].T)[:61]  # 61 pixels: uneven slabs, the last rank takes the remainder
+
+    def slab(s, e):  # stands in for a GPU forward over the pixel slab
+        F, I = O.structure_factor(Z, pos.astype(np.float64), q[s:e], nthreads=1)
+        return torch.from_numpy(np.stack([F.real, F.imag, I], axis=1))
+
+    full, local, (s, e) = D.sharded_pixels(q.shape[0], slab)
+    np.save(os.path.join(out, "range_%d.npy" % rank), np.array([s, e, local.shape[0]]))
+    if rank == 0:
+        np.save(os.path.join(out, "full.npy"), full.numpy())
+    else:
+        assert full is None
+
+
+def test_one_pattern_split_in_pixel_slabs_equals_single_process():
+    # spsim's MPI split of one HKL list (src/mpi.c:30-48) and the gather to the
+    # master (src/mpi.c:96-117), on three gloo ranks
+    from oracle import oracle as O
+
+    res = _run(_sharded_pixel_slabs, world=3)
+    Z, pos, R, q0 = _case()
+    q = (q0 @ R[0].T)[:61]
+    assert [list(res["range_%d.npy" % r]) for r in range(3)] == [[0, 20, 20], [20, 40, 20], [40, 61, 21]]
+    F, I = O.structure_factor(Z, pos.astype(np.float64), q)
+    np.testing.assert_allclose(res["full.npy"], np.stack([F.real, F.imag, I], axis=1), rtol=1e-12, atol=0)
+
+
+def _balanced_gather(rank, world, out):
+    costs = [5.0, 1.0, 1.0, 1.0, 1.0]  # rank 0 takes unit 0, rank 1 the other four
+    local = D.forward_sharded(len(costs), lambda i: torch.full((3,), float(i)), costs=costs)
+    np.save(os.path.join(out, "mine_%d.npy" % rank), np.array(sorted(local)))
+    full = D.gather_to(local, len(costs), (3,), torch.float32)
+    if rank == 0:
+        np.save(os.path.join(out, "full.npy"), full.numpy())
+
+
+def test_gather_of_cost_balanced_units():
+    # non-contiguous unit sets of different sizes per rank, reassembled in order on rank 0
+    res = _run(_balanced_gather)
+    mine = [list(res["mine_%d.npy" % r]) for r in range(2)]
+    assert mine == [[0], [1, 2, 3, 4]]
+    np.testing.assert_array_equal(res["full.npy"], np.repeat(np.arange(5, dtype=np.float32)[:, None], 3, axis=1))
+
+
 def _gradient_allreduce(rank, world, out):
     from oracle import oracle as O
 
