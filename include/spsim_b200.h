@@ -227,7 +227,11 @@ int spsim_b200_structure_factor_host_noalloc(int natoms, const int32_t *Z, const
  * npat*npix) and the forward's F (device, complex64, npat*npix), accumulates
  * dL/dpos (double, 3 per atom, caller's atom order), dL/docc and dL/dB (double
  * per atom; NULL to skip) on `stream`.  Phases are recomputed, nothing of size
- * atoms x pixels is stored.  The outputs are overwritten. */
+ * atoms x pixels is stored.  The outputs are overwritten.  The form-factor
+ * table, atom blocks and work items of a (molecule, q set, pattern count, B,
+ * precision) are built on the first call and reused by the next ones, which
+ * allocate nothing; calls that share such a plan run in call order, whatever
+ * their streams. */
 int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int npat,
                        const double *rot, float B, int precision, const float *F_dev, const float *G_dev,
                        double *dpos_dev, double *docc_dev, double *dB_dev, void *stream);
@@ -355,9 +359,11 @@ int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
 /* The reference-shaped calls (include/spsim.h) and
  * spsim_b200_structure_factor_host keep device scratch between calls on the
  * calling thread (grow-only buffers, the last molecule while its atom arrays
- * stay byte-identical, a reusable plan), and the NUFFT forwards keep their
- * grids and FFT plans per device; this frees both for the current device.
- * No reference counterpart: spsim allocates and frees per call. */
+ * stay byte-identical, a reusable plan), the NUFFT forwards keep their grids
+ * and FFT plans per device, and the adjoint keeps its last few plans (form
+ * factors, atom blocks, work items, rotations); this frees all of them for the
+ * current device.  No reference counterpart: spsim allocates and frees per
+ * call. */
 void spsim_b200_release_scratch(void);
 
 /* Seed of the random positions get_Molecule_from_formula draws (the reference

@@ -1235,14 +1235,16 @@ static int host_session_qset(int64_t npix, const float *hkl, spsim_b200_qset **o
 }
 
 // Frees this thread's host-call session and scratch plan (called by
-// spsim_b200_release_scratch after a device synchronisation), and the
-// device's NUFFT grids and plans.
+// spsim_b200_release_scratch after a device synchronisation), the device's
+// NUFFT grids and plans, and its cached adjoint plans.
 static void nufft_release(int dev);
+static void adjoint_release(int dev);
 
 extern "C" void spsim_internal_release_host_session(void) {
   int dev = -1;
   cudaGetDevice(&dev);
   nufft_release(dev);
+  adjoint_release(dev);
   if (g_host.device == dev) {
     if (g_host.mol) spsim_b200_molecule_destroy(g_host.mol);
     if (g_host.qs) spsim_b200_qset_destroy(g_host.qs);
@@ -2140,6 +2142,32 @@ extern "C" int spsim_b200_binned_outputs(const spsim_b200_chain_params *p, const
 // ---------------------------------------------------------------------------
 // adjoint
 
+// Adjoint plans: the form-factor table, the atom blocks and the work items of
+// one (molecule, q set, pattern count, B, kernel mode) are built on the first
+// call and reused; only the rotations are uploaded again, when they change.
+struct AdjPlan {
+  unsigned long long mol_id = 0, qs_id = 0;
+  int npat = 0, mode = 0, device = 0;
+  float B = 0;
+  int n_items = 0;
+  DevBuf ff, blocks, items, rot;
+  std::vector<double> host_rot;  // the rotations as last uploaded
+  // recorded after each call's launch: the next call, on whatever stream,
+  // waits for it before it rewrites the rotations the last launch reads
+  cudaEvent_t done = nullptr;
+  ~AdjPlan() {
+    if (done) cudaEventDestroy(done);
+  }
+};
+static std::vector<std::unique_ptr<AdjPlan>> g_adj_plans;  // most recent last
+static const size_t kMaxAdjPlans = 4;
+
+static void adjoint_release(int dev) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (size_t i = g_adj_plans.size(); i-- > 0;)
+    if (g_adj_plans[i]->device == dev) g_adj_plans.erase(g_adj_plans.begin() + i);
+}
+
 extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int npat,
                                   const double *rot, float B, int precision, const float *F_dev, const float *G_dev,
                                   double *dpos_dev, double *docc_dev, double *dB_dev, void *stream) {
@@ -2180,90 +2208,127 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
   if (dB_dev) CUDA_TRY(cudaMemsetAsync(dB_dev, 0, (size_t)m->natoms_in * sizeof(double), st));
   if (m->n_kept == 0 || total == 0) return SPSIM_OK;
 
-  // atom blocks x pixel chunks.  The FP64-phase adjoint's blocks are
-  // consecutive runs of the element-sorted atoms that may span two element
-  // segments (each thread's atoms stay in one), so short segments do not leave
-  // blocks mostly empty; the other adjoints take one element per block.
-  const int block_atoms =
-      precision == SPSIM_PREC_FP64 ? ADJ_THREADS : (dphase ? ADJ_DPHASE_BLOCK_ATOMS : ADJ_BLOCK_ATOMS);
-  std::vector<AdjBlock> blocks;
-  {
-    struct Seg {
-      int elem, begin, end;
-    };
-    std::vector<Seg> segs;
-    int e = -1, seg0 = 0;
-    for (size_t k = 0; k <= m->tiles.size(); ++k) {
-      const bool end = k == m->tiles.size();
-      if (end || m->tiles[k].elem != e) {
-        if (e >= 0) segs.push_back({e, seg0, m->tiles[k - 1].atom_begin + m->tiles[k - 1].count});
-        if (!end) {
-          e = m->tiles[k].elem;
-          seg0 = m->tiles[k].atom_begin;
-        }
-      }
-    }
-    if (dphase) {
-      size_t s0 = 0;
-      int a = segs.empty() ? 0 : segs[0].begin;
-      while (s0 < segs.size()) {
-        AdjBlock b = {a, std::min(a + block_atoms, segs[s0].end), segs[s0].elem, -1, 0, 0};
-        b.split = b.atom_end;
-        if (b.atom_end == segs[s0].end && b.atom_end - a < block_atoms && s0 + 1 < segs.size()) {
-          // fill the rest of the block from the next segment (segments are contiguous)
-          b.elem2 = segs[s0 + 1].elem;
-          b.split = segs[s0 + 1].begin;
-          b.atom_end = std::min(a + block_atoms, segs[s0 + 1].end);
-        }
-        blocks.push_back(b);
-        a = b.atom_end;
-        while (s0 < segs.size() && a >= segs[s0].end) ++s0;
-      }
-    } else {
-      for (const Seg &sg : segs)
-        for (int a = sg.begin; a < sg.end; a += block_atoms)
-          blocks.push_back({a, std::min(a + block_atoms, sg.end), sg.elem, -1, std::min(a + block_atoms, sg.end), 0});
-    }
-  }
   // mode 4: the FP64-phase adjoint with the fixed-point phase word (phases within 2^17 cycles)
   const bool fixw = dphase && qmax * m->rbound < std::ldexp(1.0, 17);
   const int mode =
       precision == SPSIM_PREC_FP64 ? 2 : (precision == SPSIM_PREC_F32_FAST ? 1 : (dphase ? (fixw ? 4 : 3) : 0));
-  // pixel chunks per block so that the equal-cost CTAs fill at most four whole
-  // waves of the resident slots (a last wave of a few CTAs would leave the GPU
-  // idle for one item's length: 1,190 CTAs on 592 slots ran as three waves)
-  const long long slots = (long long)num_sms() * std::max(1, adjoint_occupancy(mode, m->per_atom_b != 0));
-  long long nchunk = std::max<long long>(1, 4 * slots / (long long)blocks.size());
-  long long chunk = (total + nchunk - 1) / nchunk;
-  chunk = (chunk + 255) / 256 * 256;
-  std::vector<AdjItem> items;
-  for (size_t b = 0; b < blocks.size(); ++b)
-    for (long long p0 = 0; p0 < total; p0 += chunk) items.push_back({(int)b, 0, p0, std::min(total, p0 + chunk)});
-
-  void *d_ff = nullptr, *d_blocks = nullptr, *d_items = nullptr, *d_rot = nullptr;
-  CUDA_TRY(cudaMallocAsync(&d_ff, std::max<size_t>((size_t)m->n_elem * npix, 1) * sizeof(double), st));
-  CUDA_TRY(cudaMallocAsync(&d_blocks, blocks.size() * sizeof(AdjBlock), st));
-  CUDA_TRY(cudaMallocAsync(&d_items, items.size() * sizeof(AdjItem), st));
-  CUDA_TRY(cudaMemcpyAsync(d_blocks, blocks.data(), blocks.size() * sizeof(AdjBlock), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(AdjItem), cudaMemcpyHostToDevice, st));
-  if (rot) {
-    CUDA_TRY(cudaMallocAsync(&d_rot, 9 * (size_t)npat * sizeof(double), st));
-    CUDA_TRY(cudaMemcpyAsync(d_rot, rot, 9 * (size_t)npat * sizeof(double), cudaMemcpyHostToDevice, st));
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_mu);
+  AdjPlan *pl = nullptr;
+  for (size_t i = 0; i < g_adj_plans.size(); ++i) {
+    AdjPlan &c = *g_adj_plans[i];
+    if (c.mol_id == m->id && c.qs_id == qs->id && c.npat == npat && c.B == B && c.mode == mode &&
+        c.device == dev) {
+      std::unique_ptr<AdjPlan> keep = std::move(g_adj_plans[i]);
+      g_adj_plans.erase(g_adj_plans.begin() + i);
+      g_adj_plans.push_back(std::move(keep));
+      pl = g_adj_plans.back().get();
+      break;
+    }
   }
-  CUDA_TRY(launch_ff_table(qs->d_hkl, qs->d_q64, npix, m->n_elem, m->d_coeffs, (double)B, m->delta_atoms,
-                           (double *)d_ff, st));
+  if (!pl) {
+    std::unique_ptr<AdjPlan> np(new AdjPlan());
+    np->mol_id = m->id;
+    np->qs_id = qs->id;
+    np->npat = npat;
+    np->B = B;
+    np->mode = mode;
+    np->device = dev;
+    // atom blocks x pixel chunks.  The FP64-phase adjoint's blocks are
+    // consecutive runs of the element-sorted atoms that may span two element
+    // segments (each thread's atoms stay in one), so short segments do not leave
+    // blocks mostly empty; the other adjoints take one element per block.
+    const int block_atoms =
+        precision == SPSIM_PREC_FP64 ? ADJ_THREADS : (dphase ? ADJ_DPHASE_BLOCK_ATOMS : ADJ_BLOCK_ATOMS);
+    std::vector<AdjBlock> blocks;
+    {
+      struct Seg {
+        int elem, begin, end;
+      };
+      std::vector<Seg> segs;
+      int e = -1, seg0 = 0;
+      for (size_t k = 0; k <= m->tiles.size(); ++k) {
+        const bool end = k == m->tiles.size();
+        if (end || m->tiles[k].elem != e) {
+          if (e >= 0) segs.push_back({e, seg0, m->tiles[k - 1].atom_begin + m->tiles[k - 1].count});
+          if (!end) {
+            e = m->tiles[k].elem;
+            seg0 = m->tiles[k].atom_begin;
+          }
+        }
+      }
+      if (dphase) {
+        size_t s0 = 0;
+        int a = segs.empty() ? 0 : segs[0].begin;
+        while (s0 < segs.size()) {
+          AdjBlock b = {a, std::min(a + block_atoms, segs[s0].end), segs[s0].elem, -1, 0, 0};
+          b.split = b.atom_end;
+          if (b.atom_end == segs[s0].end && b.atom_end - a < block_atoms && s0 + 1 < segs.size()) {
+            // fill the rest of the block from the next segment (segments are contiguous)
+            b.elem2 = segs[s0 + 1].elem;
+            b.split = segs[s0 + 1].begin;
+            b.atom_end = std::min(a + block_atoms, segs[s0 + 1].end);
+          }
+          blocks.push_back(b);
+          a = b.atom_end;
+          while (s0 < segs.size() && a >= segs[s0].end) ++s0;
+        }
+      } else {
+        for (const Seg &sg : segs)
+          for (int a = sg.begin; a < sg.end; a += block_atoms)
+            blocks.push_back({a, std::min(a + block_atoms, sg.end), sg.elem, -1, std::min(a + block_atoms, sg.end), 0});
+      }
+    }
+    // pixel chunks per block so that the equal-cost CTAs fill at most four whole
+    // waves of the resident slots (a last wave of a few CTAs would leave the GPU
+    // idle for one item's length: 1,190 CTAs on 592 slots ran as three waves)
+    const long long slots = (long long)num_sms() * std::max(1, adjoint_occupancy(mode, m->per_atom_b != 0));
+    long long nchunk = std::max<long long>(1, 4 * slots / (long long)blocks.size());
+    long long chunk = (total + nchunk - 1) / nchunk;
+    chunk = (chunk + 255) / 256 * 256;
+    std::vector<AdjItem> items;
+    for (size_t b = 0; b < blocks.size(); ++b)
+      for (long long p0 = 0; p0 < total; p0 += chunk) items.push_back({(int)b, 0, p0, std::min(total, p0 + chunk)});
+    np->n_items = (int)items.size();
+    CUDA_TRY(np->ff.ensure(std::max<size_t>((size_t)m->n_elem * npix, 1) * sizeof(double)));
+    CUDA_TRY(np->blocks.ensure(blocks.size() * sizeof(AdjBlock)));
+    CUDA_TRY(np->items.ensure(items.size() * sizeof(AdjItem)));
+    CUDA_TRY(np->rot.ensure(9 * (size_t)npat * sizeof(double)));
+    CUDA_TRY(cudaMemcpyAsync(np->blocks.p, blocks.data(), blocks.size() * sizeof(AdjBlock), cudaMemcpyHostToDevice,
+                             st));
+    CUDA_TRY(cudaMemcpyAsync(np->items.p, items.data(), items.size() * sizeof(AdjItem), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(launch_ff_table(qs->d_hkl, qs->d_q64, npix, m->n_elem, m->d_coeffs, (double)B, m->delta_atoms,
+                             (double *)np->ff.p, st));
+    CUDA_TRY(cudaEventCreateWithFlags(&np->done, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(np->done, st));
+    if (g_adj_plans.size() >= kMaxAdjPlans) {
+      cudaDeviceSynchronize();  // the evicted plan's buffers may still be in use
+      g_adj_plans.erase(g_adj_plans.begin());
+    }
+    g_adj_plans.push_back(std::move(np));
+    pl = g_adj_plans.back().get();
+  }
+  CUDA_TRY(cudaStreamWaitEvent(st, pl->done, 0));
+  // this call's rotations, uploaded when they differ from the last call's
+  if (rot && (pl->host_rot.size() != 9 * (size_t)npat ||
+              memcmp(pl->host_rot.data(), rot, 9 * (size_t)npat * sizeof(double)) != 0)) {
+    pl->host_rot.assign(rot, rot + 9 * (size_t)npat);
+    CUDA_TRY(cudaMemcpyAsync(pl->rot.p, pl->host_rot.data(), 9 * (size_t)npat * sizeof(double),
+                             cudaMemcpyHostToDevice, st));
+  }
   AdjParams prm;
   memset(&prm, 0, sizeof(prm));
   prm.atoms = m->d_atoms;
   prm.atomsd = m->d_atomsd;
   prm.perm = m->d_perm;
   prm.wbase = m->d_wbase;
-  prm.blocks = (const AdjBlock *)d_blocks;
-  prm.items = (const AdjItem *)d_items;
+  prm.blocks = (const AdjBlock *)pl->blocks.p;
+  prm.items = (const AdjItem *)pl->items.p;
   prm.hkl = qs->d_hkl;
   prm.q64 = qs->d_q64;
-  prm.rot = (const double *)d_rot;
-  prm.ff = (const double *)d_ff;
+  prm.rot = rot ? (const double *)pl->rot.p : nullptr;
+  prm.ff = (const double *)pl->ff.p;
   prm.F = (const float2 *)F_dev;
   prm.G = G_dev;
   prm.npix = npix;
@@ -2282,15 +2347,11 @@ extern "C" int spsim_b200_adjoint(const spsim_b200_molecule *m, const spsim_b200
     CUDA_TRY(cudaEventCreate(&e1));
     CUDA_TRY(cudaEventRecord(e0, st));
   }
-  CUDA_TRY(launch_adjoint(mode, prm, (int)items.size(), st));
+  CUDA_TRY(launch_adjoint(mode, prm, pl->n_items, st));
+  CUDA_TRY(cudaEventRecord(pl->done, st));
   if (g_timing) {
     CUDA_TRY(cudaEventRecord(e1, st));
-    std::lock_guard<std::mutex> lk(g_mu);
     g_timing_events.push_back({e0, e1});
   }
-  cudaFreeAsync(d_ff, st);
-  cudaFreeAsync(d_blocks, st);
-  cudaFreeAsync(d_items, st);
-  if (d_rot) cudaFreeAsync(d_rot, st);
   return SPSIM_OK;
 }
