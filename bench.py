@@ -87,7 +87,7 @@ def _cpu_sample(Z, pos, hkl_all, pool, nproc, target_s, vector=True):
     path = "vector_compute_pattern_on_list" if vector else "compute_pattern_on_list"
     desc = "%d evenly spaced pixels of the 1024x1024 detector x %d atoms, %s, %d processes over contiguous " \
            "slabs (src/mpi.c:30-48)" % (npix, n_atoms, path, nproc)
-    return npix * n_atoms / wall, desc
+    return npix * n_atoms / wall, desc, wall
 
 
 def _make_workload(rank=0):
@@ -118,16 +118,20 @@ def run_reference(args):
     w, Z, pos = _make_workload()
     hkl = _hkl_host(w)
     with ctx.Pool(nproc) as pool:
-        vals = []
+        vals, walls = [], []
         for i in range(args.warmup + args.steps):
-            v, desc = _cpu_sample(Z, pos, hkl, pool, nproc, target_s=2.0)
+            v, desc, wall = _cpu_sample(Z, pos, hkl, pool, nproc, target_s=2.0)
             if i >= args.warmup:
                 vals.append(v)
+                walls.append(wall)
     value = float(statistics.median(vals))
     terms = float(w["natoms"]) * w["det"]["nx"] * w["det"]["ny"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": terms / value * 1e3,
+        "steps": args.steps, "warmup": args.warmup,
+        # a step is one bounded pixel sample of the workload (terms/s is intensive)
+        "ms_per_step": float(statistics.median(walls)) * 1e3,
+        "ms_per_full_pattern_extrapolated": terms / value * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload_desc(), "precision": "reference float path (SSE sincos_ps)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": _ref_kind(), "sample": desc},
@@ -188,15 +192,31 @@ class ClockSampler:
 
 
 _PROBE = {}
+PROBE_SRC = os.path.join(ROOT, "pipe_probe.cu")
+PROBE_EXE = os.path.join(ROOT, "_build", "pipe_probe")
+
+
+def _build_probe():
+    """Compile pipe_probe.cu for sm_100a into _build/ (once; a few seconds)."""
+    if os.path.exists(PROBE_EXE) and os.path.getmtime(PROBE_EXE) >= os.path.getmtime(PROBE_SRC):
+        return True
+    os.makedirs(os.path.dirname(PROBE_EXE), exist_ok=True)
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    try:
+        r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-I", ROOT, "-o", PROBE_EXE,
+                            PROBE_SRC], capture_output=True, text=True, timeout=300)
+    except (OSError, subprocess.TimeoutExpired):
+        return False
+    return r.returncode == 0
 
 
 def measured_pipe_peaks():
     """FP32-FMA lane-ops/s and MUFU ops/s measured on this GPU by the pipe probe
-    (spsim_b200/csrc/tools/pipe_probe.cu), or None when it is not built."""
+    (pipe_probe.cu), or None when it cannot be built or run."""
     if "v" not in _PROBE:
         _PROBE["v"] = None
-        exe = os.path.join(ROOT, "spsim_b200", "_lib", "pipe_probe")
-        if os.path.exists(exe):
+        exe = PROBE_EXE
+        if _build_probe():
             try:
                 out = subprocess.run([exe], capture_output=True, text=True, timeout=120).stdout
                 for line in out.splitlines():
@@ -259,14 +279,14 @@ def balanced_bound(kernel, prec, probe):
     t_xu = mix.get("xu", 0) / rate["xu"] if mix.get("xu") else 0.0
     return {"terms_per_s": 1.0 / max(t_issue, t_xu), "mix_per_term": mix,
             "model": "1 / max(sum_p ops_p / rate_p over FP32, FP64, IMAD, ALU; XU ops / XU rate), rates from "
-                     "spsim_b200/_lib/pipe_probe"}
+                     "pipe_probe.cu"}
 
 
 def _peaks(props):
     probe = measured_pipe_peaks()
     if probe and probe.get("fma_lane_ops_per_s") and probe.get("mufu_ops_per_s"):
         p_fma, p_mufu = probe["fma_lane_ops_per_s"], probe["mufu_ops_per_s"]
-        src = "measured by spsim_b200/_lib/pipe_probe at %s MHz (%d SMs)" % (probe.get("clock_mhz"), probe.get("sms"))
+        src = "measured by pipe_probe.cu at %s MHz (%d SMs)" % (probe.get("clock_mhz"), probe.get("sms"))
         return min(p_fma / OPS_PER_TERM_FMA, p_mufu / OPS_PER_TERM_MUFU), p_mufu, p_fma, probe.get("clock_mhz"), src
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     src = "nominal"
@@ -421,7 +441,7 @@ def run_b200(args):
         if rank == 0:
             line["e2e"] = e2e
     if rank == 0 and pool is not None:
-        v, desc = _cpu_sample(Z, pos, _hkl_host(w), pool, nproc, target_s=12.0)
+        v, desc, _ = _cpu_sample(Z, pos, _hkl_host(w), pool, nproc, target_s=12.0)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nproc, "kind": _ref_kind(), "sample": desc}
         pool.close()
     if rank == 0:
@@ -430,7 +450,18 @@ def run_b200(args):
             f["f32_speedup"] = line["roofline"]["achieved"] / f["kernel_terms_per_s"] if line["roofline"]["achieved"] else None
             if line.get("f32_fast", {}).get("kernel_terms_per_s"):
                 f["f32_fast_speedup"] = line["f32_fast"]["kernel_terms_per_s"] / f["kernel_terms_per_s"]
-        line["backward_forward_ratio"] = _adjoint_ratio(prec) if not args.no_adjoint else None
+        # the batched workloads at their stated sizes (single-GPU extras: the
+        # other ranks of a multi-GPU run would wait on them at the final barrier)
+        batched = {}
+        if world == 1 and not args.no_batched:
+            batched["orientations_20k"] = batched_orientations(prec, line["roofline"]["peak"])
+            batched["uneven_64"] = batched_uneven(prec, line["roofline"]["peak"])
+        if not args.no_adjoint:
+            batched["adjoint_5k"] = batched_adjoint(prec)
+        if batched:
+            line["batched"] = batched
+        line["backward_forward_ratio"] = batched["adjoint_5k"]["backward_forward_ratio"] if "adjoint_5k" in batched \
+            else None
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -581,37 +612,6 @@ def _e2e(args, w, Z, pos, terms, world, dist=None):
             "steps": nsteps, "note": "reference semantics: no ADC clamp (extension) in this call"}
 
 
-def _adjoint_ratio(prec):
-    """Adjoint / forward time on the refinement shape (5,000 atoms, 512^2 pixels,
-    8 orientations), both timed with CUDA events."""
-    import torch
-
-    from spsim_b200 import core, synth
-
-    w = synth.WORKLOADS["adjoint_5k"]
-    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
-    d = w["det"]
-    mol = core.Molecule(Z, pos, occ=np.ones(len(Z), np.float32))
-    qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
-    R = synth.haar_rotations(8, w["rot_seed"])
-    F, I = core.forward_batch([mol] * 8, [qs] * 8, rots=R, precision=prec)
-    Fc = torch.cat(F)
-    G = torch.rand(Fc.numel(), device="cuda")
-    ta, tb = [], []
-    for it in range(4):
-        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        a.record()
-        core.forward_batch([mol] * 8, [qs] * 8, rots=R, precision=prec, F=F, I=I)
-        b.record()
-        core.adjoint(mol, qs, Fc, G, rots=R, precision=prec)
-        c.record()
-        torch.cuda.synchronize()
-        if it:
-            ta.append(a.elapsed_time(b))
-            tb.append(b.elapsed_time(c))
-    return statistics.median(tb) / statistics.median(ta)
-
-
 PROFILE_VARIANTS = {"f32": (128, 8, 3), "f32_fast": (128, 8, 2)}  # the untuned defaults on the 1024^2 workload
 
 
@@ -701,19 +701,10 @@ def sweep():
     return 0
 
 
-def workloads(prec, n_orient=512):
-    """The batched workloads, each timed with CUDA events (one JSON line each):
-    orientations_20k  20,000 atoms, 256^2 pixels, n_orient Haar rotations in one
-                      persistent launch (graph-replayed) vs a loop of single-pattern calls
-    uneven_64         64 molecules of 500..100,000 atoms on 128^2..1024^2 detectors
-    adjoint_5k        5,000 atoms, 512^2 pixels, 256 orientations: adjoint / forward"""
+def _event_timer(stream):
+    """ev_time(fn, reps): fn() once untimed, then the median of `reps` runs,
+    each bracketed by CUDA events on `stream` (the launching stream)."""
     import torch
-
-    from spsim_b200 import core, synth
-
-    R0 = _peaks(torch.cuda.get_device_properties(0))[0]
-    stream = torch.cuda.Stream()
-    stream.wait_stream(torch.cuda.current_stream())
 
     def ev_time(fn, reps=3):
         fn()
@@ -728,44 +719,76 @@ def workloads(prec, n_orient=512):
             ts.append(a.elapsed_time(b))
         return statistics.median(ts)
 
-    # orientations
+    return ev_time
+
+
+def batched_orientations(prec, R0, n_orient=None, reps=2, nufft=True):
+    """orientations_20k: 20,000 atoms, 256^2 pixels of 150 um at 0.2 m, 0.2 nm,
+    n_orient Haar rotations (4,096 by default) in one persistent launch
+    (graph-replayed on a side stream), against a loop of single-pattern calls
+    (64 timed, scaled to n_orient), and the same orientations by the NUFFT batch."""
+    import torch
+
+    from spsim_b200 import core, synth
+
     w = synth.WORKLOADS["orientations_20k"]
+    n_orient = n_orient or w["n_orient"]
     Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
     d = w["det"]
     mol = core.Molecule(Z, pos)
     qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
     R = synth.haar_rotations(n_orient, w["rot_seed"])
     terms = float(len(Z)) * qs.npix * n_orient
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    ev_time = _event_timer(stream)
+    Iall = torch.empty(n_orient, qs.npix, device="cuda")
+    I = list(Iall.unbind(0))
     with torch.cuda.stream(stream):
-        F, I = core.forward_batch([mol] * n_orient, [qs] * n_orient, rots=R, precision=prec, want_F=False)
-        t_batch = ev_time(lambda: core.forward_batch([mol] * n_orient, [qs] * n_orient, rots=R, precision=prec,
-                                                     I=I, want_F=False))
+        t_batch = ev_time(lambda: core.forward_batch(mol, qs, rots=R, precision=prec, I=I, want_F=False,
+                                                     stream=stream), reps=reps)
+        kname = _kernel_key()
         nloop = min(n_orient, 64)
         Iloop = torch.empty(qs.npix, device="cuda")
-        t_loop = ev_time(lambda: [core.forward(mol, qs, rot=R[i], precision=prec, I=Iloop, want_F=False)
-                                  for i in range(nloop)], reps=2) * n_orient / nloop
-    print(json.dumps({"workload": "orientations_20k", "precision": prec, "orientations": n_orient,
-                      "batch_ms": t_batch, "terms_per_s": terms / t_batch * 1e3, "frac_of_R": terms / t_batch * 1e3 / R0,
-                      "loop_of_single_calls_ms": t_loop, "batch_speedup": t_loop / t_batch}), flush=True)
-    del F, I
-    # the same orientations by the NUFFT batch (one grid for every rotation)
-    with torch.cuda.stream(stream):
-        Fn, In = core.forward_nufft_batch(mol, qs, R, stream=stream, want_F=False)
-        t_nufft = ev_time(lambda: core.forward_nufft_batch(mol, qs, R, I=In, want_F=False, stream=stream))
-        errs = []
-        for i in range(4):
-            _, I64 = core.forward(mol, qs, rot=R[i], precision="fp64")
-            I64 = I64.double()
-            errs.append(float(((In[i].double() - I64).abs() / torch.clamp(I64, min=1e-3 * float(I64.mean()))).max()))
-        torch.cuda.synchronize()
-    w1, w2, n2 = core.last_nufft_grid()
-    print(json.dumps({"workload": "orientations_20k", "method": "nufft_batch", "orientations": n_orient,
-                      "batch_ms": t_nufft, "equivalent_terms_per_s": terms / t_nufft * 1e3,
-                      "speedup_vs_direct_batch": t_batch / t_nufft, "kernel_widths": [w1, w2], "fft_grid": list(n2),
-                      "floored_max_rel_vs_fp64_first4": max(errs)}), flush=True)
-    del Fn, In
+        t_loop = ev_time(lambda: [core.forward(mol, qs, rot=R[i], precision=prec, I=Iloop, want_F=False,
+                                               stream=stream) for i in range(nloop)], reps=2) * n_orient / nloop
+    out = {"workload": "orientations_20k: 20,000 atoms, 256^2 pixels of 150 um at 0.2 m, 0.2 nm, %d Haar rotations "
+                       "in one batched forward (graph-replayed)" % n_orient,
+           "precision": prec, "orientations": n_orient, "kernel": kname, "batch_ms": t_batch,
+           "terms_per_s": terms / t_batch * 1e3, "frac_of_R": terms / t_batch * 1e3 / R0,
+           "loop_of_single_calls_ms": t_loop, "batch_speedup": t_loop / t_batch}
+    del Iall, I
+    if nufft:
+        with torch.cuda.stream(stream):
+            Fn, In = core.forward_nufft_batch(mol, qs, R, stream=stream, want_F=False)
+            t_nufft = ev_time(lambda: core.forward_nufft_batch(mol, qs, R, I=In, want_F=False, stream=stream),
+                              reps=reps)
+            errs = []
+            for i in range(4):
+                _, I64 = core.forward(mol, qs, rot=R[i], precision="fp64", stream=stream)
+                I64 = I64.double()
+                errs.append(float(((In[i].double() - I64).abs() /
+                                   torch.clamp(I64, min=1e-3 * float(I64.mean()))).max()))
+            stream.synchronize()
+        w1, w2, n2 = core.last_nufft_grid()
+        out["nufft_batch"] = {"ms": t_nufft, "equivalent_terms_per_s": terms / t_nufft * 1e3,
+                              "speedup_vs_direct_batch": t_batch / t_nufft, "kernel_widths": [w1, w2],
+                              "fft_grid": list(n2), "floored_max_rel_vs_fp64_first4": max(errs),
+                              "note": "type-3 NUFFT, one grid for every rotation: a different algorithm from the "
+                                      "direct sum"}
+        del In
+    return out
 
-    # uneven molecules
+
+def batched_uneven(prec, R0, reps=3):
+    """uneven_64: 64 molecules of 500..100,000 atoms on their own 128^2..1024^2
+    detectors and wavelengths, in one batched forward; the batch autotuner
+    picks the tile shape first (its choice and the untuned default's time are
+    reported)."""
+    import torch
+
+    from spsim_b200 import core, synth
+
     mols, qsets, cost = [], [], 0.0
     for m in synth.uneven_batch():
         Zm, pm = synth.random_molecule(m["natoms"], m["radius"], m["seed"])
@@ -774,36 +797,72 @@ def workloads(prec, n_orient=512):
         qsets.append(core.QSet.from_detector(dm["nx"], dm["ny"], dm["width"], dm["height"], dm["distance"],
                                              dm["wavelength"]))
         cost += float(len(Zm)) * qsets[-1].npix
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    ev_time = _event_timer(stream)
     with torch.cuda.stream(stream):
-        F, I = core.forward_batch(mols, qsets, precision=prec, want_F=False)
-        t_d = ev_time(lambda: core.forward_batch(mols, qsets, precision=prec, I=I, want_F=False))
-        # the autotuner picks the tile shape for this batch (kept for its size class)
-        tuned = core.autotune_batch(mols, qsets, precision=prec, stream=stream)
-        t_u = ev_time(lambda: core.forward_batch(mols, qsets, precision=prec, I=I, want_F=False))
-    print(json.dumps({"workload": "uneven_64", "precision": prec, "terms": cost, "batch_ms": t_u,
-                      "terms_per_s": cost / t_u * 1e3, "frac_of_R": cost / t_u * 1e3 / R0,
-                      "autotuned_variant": {"threads": tuned[0], "pixels_per_thread": tuned[1], "form": tuned[2]},
-                      "untuned_default_ms": t_d}), flush=True)
-    del mols, qsets, F, I
+        F, I = core.forward_batch(mols, qsets, precision=prec, want_F=False, stream=stream)
+        t_d = ev_time(lambda: core.forward_batch(mols, qsets, precision=prec, I=I, want_F=False, stream=stream),
+                      reps=reps)
+        try:
+            tuned = core.autotune_batch(mols, qsets, precision=prec, stream=stream)
+            t_u = ev_time(lambda: core.forward_batch(mols, qsets, precision=prec, I=I, want_F=False, stream=stream),
+                          reps=reps)
+        finally:
+            core.clear_tuning()
+    return {"workload": "uneven_64: 64 molecules, 500..100,000 atoms (log-uniform), 128^2..1024^2 detectors, "
+                        "lambda 0.1..0.3 nm, one batched forward after autotuning",
+            "precision": prec, "terms": cost, "batch_ms": t_u, "terms_per_s": cost / t_u * 1e3,
+            "frac_of_R": cost / t_u * 1e3 / R0,
+            "autotuned_variant": {"threads": tuned[0], "pixels_per_thread": tuned[1], "form": tuned[2]},
+            "untuned_default_ms": t_d}
 
-    # adjoint
+
+def batched_adjoint(prec, reps=3):
+    """adjoint_5k: 5,000 atoms, 512^2 pixels of 75 um at 0.15 m, 0.25 nm, 256
+    orientations, per-atom occupancies and B factors: the batched forward and
+    the adjoint (dL/dpos, dL/docc, dL/dB for a given dL/dI), each timed with
+    CUDA events; their ratio is the metric's backward/forward time ratio."""
+    import torch
+
+    from spsim_b200 import core, synth
+
     w = synth.WORKLOADS["adjoint_5k"]
     Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
     d = w["det"]
-    mol = core.Molecule(Z, pos, occ=np.ones(len(Z), np.float32), bfac=np.zeros(len(Z), np.float32))
+    rng = np.random.Generator(np.random.PCG64(w["seed"]))
+    mol = core.Molecule(Z, pos, occ=rng.uniform(0.5, 1.0, len(Z)).astype(np.float32),
+                        bfac=rng.uniform(0.0, 30.0, len(Z)).astype(np.float32))
     qs = core.QSet.from_detector(d["nx"], d["ny"], d["width"], d["height"], d["distance"], d["wavelength"])
     R = synth.haar_rotations(w["n_orient"], w["rot_seed"])
     terms = float(len(Z)) * qs.npix * len(R)
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    ev_time = _event_timer(stream)
     with torch.cuda.stream(stream):
-        F, I = core.forward_batch([mol] * len(R), [qs] * len(R), rots=R, precision=prec)
-        Fc = torch.cat(F)
-        G = torch.rand(Fc.numel(), device="cuda")
-        t_f = ev_time(lambda: core.forward_batch([mol] * len(R), [qs] * len(R), rots=R, precision=prec, F=F, I=I))
-        t_b = ev_time(lambda: core.adjoint(mol, qs, Fc, G, rots=R, precision=prec, stream=stream))
-    print(json.dumps({"workload": "adjoint_5k", "precision": prec, "orientations": len(R), "forward_ms": t_f,
-                      "adjoint_ms": t_b, "backward_forward_ratio": t_b / t_f,
-                      "forward_terms_per_s": terms / t_f * 1e3, "adjoint_terms_per_s": terms / t_b * 1e3}),
-          flush=True)
+        Fall = torch.empty(len(R), qs.npix, dtype=torch.complex64, device="cuda")
+        Iall = torch.empty(len(R), qs.npix, device="cuda")
+        F, I = list(Fall.unbind(0)), list(Iall.unbind(0))
+        G = torch.rand(len(R) * qs.npix, device="cuda")
+        t_f = ev_time(lambda: core.forward_batch(mol, qs, rots=R, precision=prec, F=F, I=I, stream=stream), reps=reps)
+        t_b = ev_time(lambda: core.adjoint(mol, qs, Fall.reshape(-1), G, rots=R, precision=prec, stream=stream),
+                      reps=reps)
+    return {"workload": "adjoint_5k: 5,000 atoms, 512^2 pixels, 256 orientations, per-atom occupancies and B "
+                        "factors: batched forward and adjoint",
+            "precision": prec, "orientations": len(R), "forward_ms": t_f, "adjoint_ms": t_b,
+            "backward_forward_ratio": t_b / t_f, "forward_terms_per_s": terms / t_f * 1e3,
+            "adjoint_terms_per_s": terms / t_b * 1e3}
+
+
+def workloads(prec, n_orient=None):
+    """The batched workloads, one JSON line each (batched_orientations,
+    batched_uneven, batched_adjoint)."""
+    import torch
+
+    R0 = _peaks(torch.cuda.get_device_properties(0))[0]
+    print(json.dumps(batched_orientations(prec, R0, n_orient)), flush=True)
+    print(json.dumps(batched_uneven(prec, R0)), flush=True)
+    print(json.dumps(batched_adjoint(prec)), flush=True)
     return 0
 
 
@@ -817,6 +876,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched orientation and uneven workloads")
     ap.add_argument("--no-modes", action="store_true", help="skip the f32_fast / fp64 / accuracy extras")
     ap.add_argument("--profile-case", default=None,
                     help="comma-separated precisions: one forward each on the 20,000-atom x 256^2 case, or "

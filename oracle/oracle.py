@@ -46,7 +46,7 @@ def ref_lib():
     global _ref
     if _ref is None:
         if not ref_available():
-            raise ImportError("reference library not built: make -C oracle ref (needs the spsim tree)")
+            raise ImportError("reference library not built: make -C oracle ref REF=<spsim tree>")
         _ref = ctypes.CDLL(REF_LIB)
     return _ref
 

@@ -5,11 +5,12 @@
 // structure-factor inner loop in isolation (term32, term64), and
 // stores one value per thread; the host prints lane-operations per clock per SM
 // and a JSON line with the measured FP32-FMA and MUFU rates (ops/s) that
-// bench.py uses as the measured peak of R = min(P_FMA/5, P_MUFU/2).
+// bench.py uses as the measured peak of R = min(P_FMA/5, P_MUFU/2); bench.py
+// builds it (nvcc, sm_100a) into _build/pipe_probe on first use.
 #include <cstdio>
 #include <cstring>
 #include <cuda_runtime.h>
-#include "../sincos_poly.h"
+#include "spsim_b200/csrc/sincos_poly.h"
 #define N_IT 4096
 __global__ void k_ffma(float *out, float b, float c) {
   float a[16];

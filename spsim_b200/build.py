@@ -8,8 +8,7 @@ hidden by a linker version script, so the library neither exports nor binds
 to another CUDA runtime loaded in the same process (PyTorch's, for example).
 
 Also builds spsim_b200/_lib/spsim, the spsim command-line program on the
-library (host/spsim_main.c), and spsim_b200/_lib/pipe_probe, the
-pipe-throughput probe bench.py runs for the measured FMA / MUFU peaks.
+library (host/spsim_main.c).
 
 Usage: python -m spsim_b200.build [--force] [--verbose]
 """
@@ -116,10 +115,6 @@ def build(force=False, verbose=False):
     csrc = os.path.join(CSRC, "host", "spsim_main.c")
     if force or _newer(cli, [csrc, out]):
         _run(["gcc"] + CC_FLAGS + ["-o", cli, csrc, "-L" + LIBDIR, "-l:" + LIBNAME, "-Wl,-rpath,$ORIGIN"], verbose)
-    probe = os.path.join(LIBDIR, "pipe_probe")
-    psrc = os.path.join(CSRC, "tools", "pipe_probe.cu")
-    if force or _newer(probe, [psrc]):
-        _run([NVCC] + ARCH + ["-O3", "-o", probe, psrc], verbose)
     return out
 
 

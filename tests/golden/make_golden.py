@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from spsim's own sources.
 
 Runs only where the reference tree and oracle/_ref/libspsim_ref.so (built by
-`make -C oracle ref`) are present; the fixtures are committed so that the
+`make -C oracle ref REF=<spsim tree>`) are present; the fixtures are committed so that the
 tests need neither.  Every array here is produced by spsim's own C code
 (compiled unchanged against oracle/refstub), never by this project's code:
 
@@ -243,7 +243,9 @@ def config():
 
 def atomsf_table():
     """The reference's compiled-in coefficient table, read from its own source."""
-    ref = os.environ.get("SPSIM_REFERENCE", "/root/reference")
+    ref = os.environ.get("SPSIM_REFERENCE")
+    if not ref:
+        sys.exit("set SPSIM_REFERENCE to the spsim source tree")
     import re
     text = open(os.path.join(ref, "include", "atomsf.cdata")).read()
     rows = [[float(v) for v in r.split(",")] for r in re.findall(r"\{([^{}]*)\}", text)]
@@ -252,7 +254,7 @@ def atomsf_table():
 
 if __name__ == "__main__":
     if not O.ref_available():
-        sys.exit("build the reference first: make -C oracle ref")
+        sys.exit("build the reference first: make -C oracle ref REF=<spsim tree>")
     sf_small()
     sf_plain1k()
     chain()
