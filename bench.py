@@ -240,6 +240,12 @@ MIX = {
     "sf_dpair_kernel+word": {"fp32": 15.5, "dfma": 1.5, "imad": 0.5, "alu": 0.5, "xu": 0.375, "i2f": 0.5},
     # second pixels on the NARROW polynomial: one FMA fewer per second-pixel term
     "sf_dpair_kernel+word+narrow": {"fp32": 15.0, "dfma": 1.5, "imad": 0.5, "alu": 0.5, "xu": 0.375, "i2f": 0.5},
+    # a quarter of the terms FP64-anchored (13 FP32: scale, DHALF, sums); the
+    # other three step from the anchor in one 3-FMA chain (16 with NARROW, 17
+    # with WIDER); the two-pixel step always WIDER
+    "sf_dquad_kernel+word": {"fp32": 16.0, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 0.375, "i2f": 0.25},
+    "sf_dquad_kernel+word+narrow": {"fp32": 15.5, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 0.375,
+                                    "i2f": 0.25},
     # FP64 phase + reduction, DHALF poly
     "sf_dphase_kernel": {"fp32": 12, "dfma": 6, "imad": 1, "xu": 1},
     "sf_dphase_kernel+word/f32": {"fp32": 13, "dfma": 3, "imad": 1, "alu": 1, "i2f": 1},
@@ -612,7 +618,7 @@ def _e2e(args, w, Z, pos, terms, world, dist=None):
             "steps": nsteps, "note": "reference semantics: no ADC clamp (extension) in this call"}
 
 
-PROFILE_VARIANTS = {"f32": (128, 8, 3), "f32_fast": (128, 8, 2)}  # the untuned defaults on the 1024^2 workload
+PROFILE_VARIANTS = {"f32": (128, 8, 4), "f32_fast": (128, 8, 2)}  # the untuned defaults on the 1024^2 workload
 
 
 def profile_case(precisions):
@@ -684,7 +690,9 @@ def sweep():
     for prec in ("f32", "f32_fast"):
         for v in [(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1),
                   (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2), (128, 4, 3), (128, 8, 3),
-                  (128, 12, 3), (256, 4, 3)]:
+                  (128, 12, 3), (256, 4, 3), (128, 8, 4), (128, 16, 4), (256, 8, 4)]:
+            if v[2] == 4 and prec != "f32":
+                continue
             core.set_variant(*v)
             for _ in range(2):
                 core.forward(mol, qs, precision=prec, F=F, I=I)
@@ -695,6 +703,7 @@ def sweep():
                 torch.cuda.synchronize()
             ms = statistics.median(t.ms)
             print(json.dumps({"precision": prec, "threads": v[0], "pixels_per_thread": v[1], "form": v[2],
+                              "ran": list(core.last_variant()), "kernel": _kernel_key(),
                               "ms": ms, "terms_per_s": terms / ms * 1e3, "frac_of_R": terms / ms * 1e3 / R}),
                   flush=True)
     core.set_variant(-1)

@@ -380,10 +380,15 @@ void spsim_b200_set_formula_seed(unsigned long long seed);
  *      (SPSIM_ERR_RANGE); the SPSIM_PREC_F32_FAST default
  *   3  form 2 on the first pixel of each neighbour pair (pixels 2m, 2m+1),
  *      the second pixel's phase as the first's plus (q_b - q_a).r in FP32;
- *      the SPSIM_PREC_F32 default, used where |q_b - q_a| |r|max <= 1/8
- *      cycle for every pair of the q set (detector rows of even width), else
- *      form 2
- * Forms 2 and 3 read the reduced phase from a fixed-point phase word (three
+ *      used where |q_b - q_a| |r|max <= 1/8 cycle for every pair of the q
+ *      set (detector rows of even width)
+ *   4  form 2 on the second pixel of each neighbour quad (pixels 4m..4m+3),
+ *      the other three as its phase plus (q - q_a).r in FP32 (SPSIM_PREC_F32
+ *      only); the SPSIM_PREC_F32 default, used where every one-pixel step
+ *      from a quad's anchor stays within 1/8 cycle of |r|max and every
+ *      two-pixel step within 0.16 cycle (detector rows of width divisible by
+ *      4), else form 3, else form 2
+ * Forms 2, 3 and 4 read the reduced phase from a fixed-point phase word (three
  * FP64 FMAs) while |q|max |r - centre|max < 2^17 cycles, and reduce by FP64
  * rounding (six FP64 operations, up to 2^48 cycles) beyond.
  * threads < 0 restores automatic choice; autotune times every compiled
@@ -393,14 +398,14 @@ int spsim_b200_set_variant(int threads, int pixels_per_thread, int form);
 /* The kernel variant the last forward on this thread ran: threads per CTA,
  * pixels per thread and form (-1 for the plain FP64 kernel). */
 int spsim_b200_last_variant(int *threads, int *pixels_per_thread, int *form);
-/* Whether the last forward on this thread (forms 2 and 3) took the phase from
+/* Whether the last forward on this thread (forms 2, 3 and 4) took the phase from
  * the fixed-point phase word (1) or reduced it by FP64 rounding (0); 0 for the
  * other forms and the plain FP64 kernel.  No reference counterpart. */
 int spsim_b200_last_phase_word(int *on);
 /* Whether the last forward on this thread ran the neighbour-pair form with
- * every pair's step within 0.07 cycle, so that its second pixels took the
- * shorter NARROW sin/cos polynomial (1), or not (0).  No reference
- * counterpart. */
+ * every pair's step within 0.07 cycle, or the neighbour-quad form with every
+ * one-pixel step within 0.07 cycle, so that those pixels took the shorter
+ * NARROW sin/cos polynomial (1), or not (0).  No reference counterpart. */
 int spsim_b200_last_pair_narrow(int *on);
 int spsim_b200_autotune(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int precision, void *stream,
                         int *best_threads, int *best_pixels_per_thread, int *best_form);

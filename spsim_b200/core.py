@@ -384,8 +384,10 @@ def last_forward_stats():
 
 FORMS = {0: "compensated FP32, one pixel per lane", 1: "compensated FP32, pixel pairs (f32x2)",
          2: "FP64 phase, FP32 sin/cos on pixel pairs (f32x2)",
-         3: "FP64 phase on the first pixel of neighbour pairs, FP32 step to the second"}
-KERNELS = {-1: "sf_f64_kernel", 0: "sf_f32_kernel", 1: "sf_f32x2_kernel", 2: "sf_dphase_kernel", 3: "sf_dpair_kernel"}
+         3: "FP64 phase on the first pixel of neighbour pairs, FP32 step to the second",
+         4: "FP64 phase on the second pixel of neighbour quads, FP32 steps to the other three"}
+KERNELS = {-1: "sf_f64_kernel", 0: "sf_f32_kernel", 1: "sf_f32x2_kernel", 2: "sf_dphase_kernel", 3: "sf_dpair_kernel",
+           4: "sf_dquad_kernel"}
 
 
 def last_variant():
@@ -396,7 +398,7 @@ def last_variant():
 
 
 def last_phase_word():
-    """True when the last forward on this thread (forms 2, 3) took its phases
+    """True when the last forward on this thread (forms 2, 3, 4) took its phases
     from the fixed-point phase word rather than FP64 rounding."""
     on = c_int(0)
     check(lib().spsim_b200_last_phase_word(byref(on)))
@@ -405,7 +407,8 @@ def last_phase_word():
 
 def last_pair_narrow():
     """True when the last forward on this thread ran the neighbour-pair form
-    (3) with every pair's step within 0.07 cycle, its second pixels on the
+    (3) with every pair's step within 0.07 cycle, or the neighbour-quad form
+    (4) with every one-pixel step within 0.07 cycle, those pixels on the
     shorter NARROW sin/cos polynomial."""
     on = c_int(0)
     check(lib().spsim_b200_last_pair_narrow(byref(on)))
@@ -417,7 +420,7 @@ def kernel_name():
     return KERNELS[last_variant()[2]]
 
 
-def set_variant(threads=-1, pixels_per_thread=-1, form=3):
+def set_variant(threads=-1, pixels_per_thread=-1, form=4):
     """Force an FP32 kernel variant: threads per CTA, pixels per thread and the
     kernel form (FORMS); threads < 0 returns to automatic choice."""
     check(lib().spsim_b200_set_variant(int(threads), int(pixels_per_thread), int(form)))

@@ -434,11 +434,21 @@ struct spsim_b200_qset {
   double *d_q64 = nullptr;
   double qmax = 0;
   double pair_step = 0;  // largest |q[2m+1] - q[2m]| (the pixel-pair form's admission test)
+  double quad_step1 = 0, quad_step2 = 0;  // largest one- and two-pixel steps from a quad's anchor (the quad form's)
   ~spsim_b200_qset() {
     cudaFree(d_hkl);
     cudaFree(d_q64);
   }
 };
+
+static cudaError_t set_steps(spsim_b200_qset *q, const float *hkl, const double *q64) {
+  double st[3];
+  cudaError_t e = qset_steps(hkl, q64, q->npix, st);
+  q->pair_step = st[0];
+  q->quad_step1 = st[1];
+  q->quad_step2 = st[2];
+  return e;
+}
 
 extern "C" int spsim_b200_qset_from_list(int64_t npix, const float *hkl, int memory, spsim_b200_qset **out) {
   if (!out) return fail(SPSIM_ERR_INVALID_ARG, "out is NULL");
@@ -469,7 +479,7 @@ extern "C" int spsim_b200_qset_from_list(int64_t npix, const float *hkl, int mem
     qm2 = std::max(qm2, a * a + b * b + c * c);
   }
   q->qmax = std::sqrt(qm2);
-  CUDA_TRY(pair_step(q->d_hkl, nullptr, q->npix, &q->pair_step));
+  CUDA_TRY(set_steps(q.get(), q->d_hkl, nullptr));
   *out = q.release();
   return SPSIM_OK;
 }
@@ -529,7 +539,7 @@ extern "C" int spsim_b200_qset_from_detector(int nx, int ny, float width, float 
                         q->d_q64, 0));
   CUDA_TRY(cudaDeviceSynchronize());
   q->qmax = detector_qmax(nx, ny, width, height, distance, center_x, center_y, wavelength, spherical);
-  CUDA_TRY(pair_step(nullptr, q->d_q64, q->npix, &q->pair_step));
+  CUDA_TRY(set_steps(q.get(), nullptr, q->d_q64));
   *out = q.release();
   return SPSIM_OK;
 }
@@ -618,6 +628,7 @@ static const size_t kMaxPlans = 8;
 static int g_force_nt = -1, g_force_p = -1, g_force_pk = 3;
 struct Variant {
   int nt, p, packed;
+  int p_fallback = 0;  // pixels per thread where form 4 or 3 is not admitted (0: p's nearest)
 };
 static std::map<long long, Variant> g_tuned;  // size class -> kernel variant
 static bool g_timing = false;
@@ -652,7 +663,18 @@ static Variant choose_variant(double terms, long long total_npix, int precision)
   // there are enough pixel tiles to fill every SM several times (fastest on
   // both the 50,000- and the 5,000-atom workloads)
   if (precision == SPSIM_PREC_F32_FAST) return {128, total_npix >= (1LL << 20) ? 8 : 4, 2};
-  return {128, total_npix >= (1LL << 20) ? 8 : 4, 3};  // falls back to form 2 where a q set is not admitted
+  // FP32: the neighbour-quad form (8 pixels per thread), falling back to the
+  // pair form and then to form 2 where a q set is not admitted, there with 4
+  // pixels per thread below 2^20 pixels
+  return {128, 8, 4, total_npix >= (1LL << 20) ? 8 : 4};
+}
+
+// The variant of `form` nearest to (nt, p): p itself where compiled, else 8, else 4.
+static Variant fit_variant(int precision, int nt, int p, int form) {
+  const int mode = precision == SPSIM_PREC_F32_FAST ? 1 : 0;
+  for (int pp : {p, 8, 4})
+    if (sf_f32_variant_exists(mode, nt, pp, form)) return {nt, pp, form};
+  return {128, 4, form};
 }
 
 static bool is_orthonormal(const double *R) {
@@ -707,6 +729,31 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
 
   Variant var = {128, 4, 1};
   if (precision != SPSIM_PREC_FP64) var = choose_variant(terms, total_npix, precision);
+  if (var.packed == 4) {
+    // neighbour-quad form (FP32 polynomial only): every pattern needs its
+    // one-pixel steps within 1/8 cycle and its two-pixel steps within 0.16
+    // cycle of the molecule's bound
+    bool ok = precision == SPSIM_PREC_F32;
+    double max_step1 = 0.0;
+    for (int i = 0; i < npat && ok; ++i) {
+      double scale = spec ? std::fabs(spec->qscale[i]) : 1.0;
+      if (rot && !is_orthonormal(rot + 9 * (size_t)i)) {
+        double fro = 0;
+        for (int k = 0; k < 9; ++k) fro += rot[9 * (size_t)i + k] * rot[9 * (size_t)i + k];
+        scale *= std::sqrt(fro);
+      }
+      const double s1 = qsets[i]->quad_step1 * scale * mols[i]->rbound;
+      const double s2 = qsets[i]->quad_step2 * scale * mols[i]->rbound;
+      ok = s1 <= (1.0 / 8) * (1.0 - 1e-9) && s2 <= 0.16 * (1.0 - 1e-9);
+      max_step1 = std::max(max_step1, s1);
+    }
+    pl.narrow = ok && max_step1 <= 0.07 * (1.0 - 1e-6);
+    if (!ok) {
+      const int pf = var.p_fallback;
+      var = fit_variant(precision, var.nt, pf ? pf : var.p, 3);
+      var.p_fallback = pf;
+    }
+  }
   if (var.packed == 3) {
     // neighbour-pair form: every pattern needs |q_b - q_a| |r|max <= 1/8 cycle
     bool ok = true;
@@ -722,11 +769,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
       max_step = std::max(max_step, qsets[i]->pair_step * scale * mols[i]->rbound);
     }
     pl.narrow = ok && max_step <= 0.07 * (1.0 - 1e-6);
-    if (!ok) {
-      var.packed = 2;
-      const int mode = precision == SPSIM_PREC_F32_FAST ? 1 : 0;
-      if (!sf_f32_variant_exists(mode, var.nt, var.p, 2)) var.p = 8;  // form 2 has no 12-pixel variant
-    }
+    if (!ok) var = fit_variant(precision, var.nt, var.p_fallback ? var.p_fallback : var.p, 2);
   }
   const int nt = var.nt, ppt = var.p;
   pl.nt = var.nt;
@@ -1037,7 +1080,7 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
   g_last_variant[1] = pl->precision == SPSIM_PREC_FP64 ? 1 : pl->ppt;
   g_last_variant[2] = pl->precision == SPSIM_PREC_FP64 ? -1 : pl->packed;
   g_last_phase_word = pl->precision != SPSIM_PREC_FP64 && pl->fixw ? 1 : 0;
-  g_last_pair_narrow = pl->precision == SPSIM_PREC_F32 && pl->packed == 3 && pl->fixw && pl->narrow ? 1 : 0;
+  g_last_pair_narrow = pl->precision == SPSIM_PREC_F32 && pl->packed >= 3 && pl->fixw && pl->narrow ? 1 : 0;
   CUDA_TRY(refresh_rotations(*pl, rot, stream));
   if (g_timing || !cache || stream == nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1159,7 +1202,7 @@ struct HostSession {
   std::vector<unsigned char> mol_inputs;  // natoms, Z, pos, occ, bfac, delta_atoms, beam, as passed
   spsim_b200_qset *qs = nullptr;
   DevBuf *F = nullptr, *I = nullptr;
-  DevBuf *stats = nullptr;  // two words for the device q-set statistics
+  DevBuf *stats = nullptr;  // four words for the device q-set statistics
 };
 static thread_local HostSession g_host;
 static thread_local spsim_b200_molecule *g_shot_mol = nullptr;  // set by spsim_internal_shot_molecule
@@ -1229,7 +1272,7 @@ static int host_session_qset(int64_t npix, const float *hkl, spsim_b200_qset **o
     qm2 = std::max(qm2, a * a + b * b + c * c);
   }
   q->qmax = std::sqrt(qm2);
-  CUDA_TRY(pair_step(q->d_hkl, nullptr, q->npix, &q->pair_step));
+  CUDA_TRY(set_steps(q, q->d_hkl, nullptr));
   *out = q;
   return SPSIM_OK;
 }
@@ -1320,8 +1363,12 @@ static int host_session_qset_device(int64_t npix, const float *hkl_dev, cudaStre
   if (npix)
     CUDA_TRY(cudaMemcpyAsync(q->d_hkl, hkl_dev, 3 * npix * sizeof(float), cudaMemcpyDeviceToDevice, stream));
   if (!g_host.stats) g_host.stats = new DevBuf();
-  CUDA_TRY(g_host.stats->ensure(2 * sizeof(unsigned long long)));
-  CUDA_TRY(qset_stats(q->d_hkl, npix, (unsigned long long *)g_host.stats->p, &q->qmax, &q->pair_step, stream));
+  CUDA_TRY(g_host.stats->ensure(4 * sizeof(unsigned long long)));
+  double steps[3];
+  CUDA_TRY(qset_stats(q->d_hkl, npix, (unsigned long long *)g_host.stats->p, &q->qmax, steps, stream));
+  q->pair_step = steps[0];
+  q->quad_step1 = steps[1];
+  q->quad_step2 = steps[2];
   *out = q;
   return SPSIM_OK;
 }
@@ -1867,7 +1914,9 @@ extern "C" int spsim_b200_set_variant(int threads, int pixels_per_thread, int pa
     g_force_pk = 3;
     return SPSIM_OK;
   }
-  if (!sf_f32_variant_exists(0, threads, pixels_per_thread, packed) ||
+  // form 4 exists for SPSIM_PREC_F32 only; FP32_FAST forwards ignore a forced
+  // variant they have not compiled
+  if (!sf_f32_variant_exists(0, threads, pixels_per_thread, packed) &&
       !sf_f32_variant_exists(1, threads, pixels_per_thread, packed))
     return fail(SPSIM_ERR_INVALID_ARG, "no compiled variant with %d threads x %d pixels (packed %d)", threads,
                 pixels_per_thread, packed);
@@ -1893,7 +1942,8 @@ static int autotune_impl(int npat, const spsim_b200_molecule *const *mols, const
   if (precision == SPSIM_PREC_FP64) return fail(SPSIM_ERR_INVALID_ARG, "the FP64 kernel has a single variant");
   const int cand[][3] = {{128, 2, 0}, {128, 4, 0}, {256, 4, 0}, {128, 2, 1}, {128, 4, 1}, {256, 4, 1},
                          {128, 6, 1}, {128, 2, 2}, {128, 4, 2}, {256, 4, 2}, {128, 6, 2}, {128, 8, 2},
-                         {128, 4, 3}, {128, 8, 3}, {128, 12, 3}, {256, 4, 3}};
+                         {128, 4, 3}, {128, 8, 3}, {128, 12, 3}, {256, 4, 3}, {128, 8, 4}, {128, 16, 4},
+                         {256, 8, 4}};
   float *dI = nullptr;
   CUDA_TRY(cudaMalloc(&dI, std::max<long long>(total, 1) * sizeof(float)));
   std::vector<float *> I(npat), F(npat, nullptr);
@@ -1910,6 +1960,7 @@ static int autotune_impl(int npat, const spsim_b200_molecule *const *mols, const
   const bool saved_timing = g_timing;
   int st = SPSIM_OK;
   for (auto &c : cand) {
+    if (!sf_f32_variant_exists(precision == SPSIM_PREC_F32_FAST ? 1 : 0, c[0], c[1], c[2])) continue;
     g_force_nt = c[0];
     g_force_p = c[1];
     g_force_pk = c[2];

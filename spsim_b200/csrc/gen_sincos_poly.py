@@ -18,6 +18,9 @@ The domains generated:
                              step of at most 1/8 cycle)
   NARROW: |y| <= 0.32       (the same where every step is at most 0.07 cycle:
                              one sine coefficient fewer at WIDE's accuracy)
+  WIDER: |y| <= 0.41        (the pixels of a neighbour quad two steps from the
+                             anchor: DHALF plus a step of at most 0.16 cycle;
+                             WIDE's degrees at WIDE's accuracy)
 Degrees are the smallest whose float32 evaluation stays near the float32
 rounding floor (a higher sine degree on HALF only adds rounding error).
 
@@ -130,6 +133,7 @@ def main():
     emit("DHALF", 0.25, 4, 4, out)
     emit("WIDE", 0.375, 5, 5, out)
     emit("NARROW", 0.32, 4, 5, out)
+    emit("WIDER", 0.41, 5, 5, out)
     out += ["#endif", ""]
     print("\n".join(out))
 

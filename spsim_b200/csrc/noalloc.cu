@@ -154,32 +154,50 @@ extern "C" int spsim_b200_structure_factor_host_noalloc(int natoms, const int32_
   int n_tiles = 0;
   for (int e = 0; e < n_elem; ++e) n_tiles += (seg[e + 1] - seg[e] + TILE_ATOMS - 1) / TILE_ATOMS;
 
-  // ---- q set: largest |q| and largest neighbour-pair step (as the q-set handles measure them)
-  double qm2 = 0, step2 = 0;
+  // ---- q set: largest |q| and the neighbour steps (as the q-set handles
+  // measure them): of pixel pairs 2m, 2m+1, and from each quad's anchor 4m+1
+  // (4m where that is the quad's only pixel) to its one-pixel neighbours 4m,
+  // 4m+2 and to 4m+3
+  double qm2 = 0, pair2 = 0, quad1 = 0, quad2 = 0;
+  auto d2 = [&](long long i, long long j) {
+    double s2 = 0;
+    for (int k = 0; k < 3; ++k) {
+      const double d = (double)hkl[3 * j + k] - (double)hkl[3 * i + k];
+      s2 += d * d;
+    }
+    return s2;
+  };
   for (long long i = 0; i < npix; ++i) {
     const double a = hkl[3 * i], b = hkl[3 * i + 1], cc = hkl[3 * i + 2];
     qm2 = std::max(qm2, a * a + b * b + cc * cc);
-    if (i & 1) {
-      double d2 = 0;
-      for (int k = 0; k < 3; ++k) {
-        const double d = (double)hkl[3 * i + k] - (double)hkl[3 * (i - 1) + k];
-        d2 += d * d;
-      }
-      step2 = std::max(step2, d2);
-    }
+    if (i & 1) pair2 = std::max(pair2, d2(i - 1, i));
+    const long long qb = i & ~3LL;
+    if ((i & 3) == 0 && i + 1 < npix) quad1 = std::max(quad1, d2(i + 1, i));
+    if ((i & 3) == 2) quad1 = std::max(quad1, d2(qb + 1, i));
+    if ((i & 3) == 3) quad2 = std::max(quad2, d2(qb + 1, i));
   }
-  const double qmax = std::sqrt(qm2), pair_step = std::sqrt(step2);
+  const double qmax = std::sqrt(qm2);
 
   // ---- kernel form: the untuned allocating call's choice.  FP32: the
-  // neighbour-pair form (3) where every pair's step is within 1/8 cycle, else
-  // the FP64-phase form (2); FP32_FAST: form 2; 8 pixels per thread from 2^20
-  // pixels; the fixed-point phase word below 2^17 cycles, FP64 rounding up to 2^48.
+  // neighbour-quad form (4, 8 pixels per thread) where every one-pixel step
+  // from a quad's anchor is within 1/8 cycle and every two-pixel step within
+  // 0.16, else the neighbour-pair form (3) where every pair's step is within
+  // 1/8 cycle, else the FP64-phase form (2); FP32_FAST: form 2; forms 2 and 3
+  // with 8 pixels per thread from 2^20 pixels, 4 below; the fixed-point phase
+  // word below 2^17 cycles, FP64 rounding up to 2^48.
   const bool fp32 = precision != SPSIM_PREC_FP64;
   const int mode = precision == SPSIM_PREC_F32_FAST ? PREC_MODE_MUFU : PREC_MODE_POLY;
-  const int NT = 128, P = npix >= (1LL << 20) ? 8 : 4;
-  const double max_step = pair_step * rbound;
-  const int form = (precision == SPSIM_PREC_F32 && max_step <= (1.0 / 8) * (1.0 - 1e-9)) ? 3 : 2;
-  const bool narrow = form == 3 && max_step <= 0.07 * (1.0 - 1e-6);
+  const double s_pair = std::sqrt(pair2) * rbound, s_q1 = std::sqrt(quad1) * rbound, s_q2 = std::sqrt(quad2) * rbound;
+  int form = 2;
+  bool narrow = false;
+  if (precision == SPSIM_PREC_F32 && s_q1 <= (1.0 / 8) * (1.0 - 1e-9) && s_q2 <= 0.16 * (1.0 - 1e-9)) {
+    form = 4;
+    narrow = s_q1 <= 0.07 * (1.0 - 1e-6);
+  } else if (precision == SPSIM_PREC_F32 && s_pair <= (1.0 / 8) * (1.0 - 1e-9)) {
+    form = 3;
+    narrow = s_pair <= 0.07 * (1.0 - 1e-6);
+  }
+  const int NT = 128, P = (form == 4 || npix >= (1LL << 20)) ? 8 : 4;
   const bool perb = bfac != nullptr;
   const double qr = qmax * rbound;
   const bool fixw = qr < std::ldexp(1.0, 17);

@@ -185,6 +185,39 @@ __device__ __forceinline__ void sincos_dhalf_poly2(float2 y, float2 &S, float2 &
   C = pc;
 }
 
+// the NARROW pair (|y| <= 0.32 cycle) on two phases
+__device__ __forceinline__ void sincos_narrow_poly2(float2 y, float2 &S, float2 &C) {
+  const float2 z = mul2(y, y);
+  float2 ps = fma2(z, f2(SPSIM_NARROW_S4), f2(SPSIM_NARROW_S3));
+  ps = fma2(z, ps, f2(SPSIM_NARROW_S2));
+  ps = fma2(z, ps, f2(SPSIM_NARROW_S1));
+  ps = fma2(z, ps, f2(SPSIM_NARROW_S0));
+  float2 pc = fma2(z, f2(SPSIM_NARROW_C5), f2(SPSIM_NARROW_C4));
+  pc = fma2(z, pc, f2(SPSIM_NARROW_C3));
+  pc = fma2(z, pc, f2(SPSIM_NARROW_C2));
+  pc = fma2(z, pc, f2(SPSIM_NARROW_C1));
+  pc = fma2(z, pc, f2(SPSIM_NARROW_C0));
+  S = mul2(y, ps);
+  C = pc;
+}
+
+// the WIDER pair (|y| <= 0.41 cycle) on two phases
+__device__ __forceinline__ void sincos_wider_poly2(float2 y, float2 &S, float2 &C) {
+  const float2 z = mul2(y, y);
+  float2 ps = fma2(z, f2(SPSIM_WIDER_S5), f2(SPSIM_WIDER_S4));
+  ps = fma2(z, ps, f2(SPSIM_WIDER_S3));
+  ps = fma2(z, ps, f2(SPSIM_WIDER_S2));
+  ps = fma2(z, ps, f2(SPSIM_WIDER_S1));
+  ps = fma2(z, ps, f2(SPSIM_WIDER_S0));
+  float2 pc = fma2(z, f2(SPSIM_WIDER_C5), f2(SPSIM_WIDER_C4));
+  pc = fma2(z, pc, f2(SPSIM_WIDER_C3));
+  pc = fma2(z, pc, f2(SPSIM_WIDER_C2));
+  pc = fma2(z, pc, f2(SPSIM_WIDER_C1));
+  pc = fma2(z, pc, f2(SPSIM_WIDER_C0));
+  S = mul2(y, ps);
+  C = pc;
+}
+
 // (-1)^k w for an integer k whose bit 0 sits in bit 0 of kbits: one integer
 // multiply-add, w_bits + kbits * 2^31 (adding 2^31 flips the sign bit).  The
 // multiplier comes in as a register (m31 = 2^31, a kernel argument) so the

@@ -1018,6 +1018,276 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
 }
 
 // ---------------------------------------------------------------------------
+// FP64-anchored pixel quads.  Pixels 4m .. 4m+3 of a q set are neighbours on a
+// detector row.  Pixel 4m+1 (the anchor) takes the FP64 phase and exact
+// half-cycle reduction of the pair form (|y_a| <= 1/4, sign (-1)^k); each of
+// the other three is y = y_a + (q - q_a).r in FP32, the step's three products
+// summed onto y_a in one FMA chain, with the anchor's sign.  The host admits a
+// q set when, for every quad, the one-pixel steps (4m and 4m+2 from the anchor)
+// stay within 1/8 cycle of the molecule's bound (0.07 for NARROW) and the
+// two-pixel step (4m+3) within 0.16 cycle, so that |y| <= 0.41 stays inside
+// the WIDER polynomial's domain (the one-pixel steps' |y| <= 0.32 inside
+// NARROW's).  Against the pair form: 3 DFMA per four terms instead of per two,
+// and one FP32 operation fewer per stepped pixel.  A partial last quad (q sets
+// whose length is not a multiple of 4) anchors on its first pixel when that is
+// the only one.  Threads hold P pixels as P/4 quads; the corresponding pixels
+// of two quads share each packed f32x2 instruction.  FP32 polynomial sin/cos
+// only (the MUFU forms gain nothing from anchors).
+
+// Anchor of quad base qb and the pixel of slot s (0 = anchor, 1..3 = qb, qb+2,
+// qb+3), or -1 where the slot holds no pixel of the q set.
+__device__ __forceinline__ long long quad_anchor(long long qb, long long npix) { return qb + 1 < npix ? qb + 1 : qb; }
+__device__ __forceinline__ long long quad_pixel(long long qb, int slot, long long npix) {
+  const long long pa = quad_anchor(qb, npix);
+  const long long p = slot == 0 ? pa : slot == 1 ? qb : qb + slot;
+  return (p < npix && (slot == 0 || p != pa)) ? p : -1;
+}
+
+template <int NT, int P, bool PERB, bool FIXW, bool NARROW>
+__global__ void __launch_bounds__(NT, sf_min_blocks(PREC_MODE_POLY)) sf_dquad_kernel(
+    const SfPattern *__restrict__ pats, const WorkItem *__restrict__ items, int n_items, int *__restrict__ queue,
+    int *__restrict__ err, uint32_t m31) {
+  static_assert(P % 8 == 0, "pixels per thread must be a multiple of 8 (two quads per packed instruction)");
+  constexpr int NQ = P / 4;    // quads per thread
+  constexpr int NQP = P / 8;   // packed pairs of quads
+  __shared__ __align__(128) float4 ring[RING_STAGES][2 * TILE_ATOMS];
+  __shared__ __align__(16) double2 sacc[P * NT];  // per-thread FP64 pixel sums of the current work item
+  __shared__ __align__(8) uint64_t full_bar[RING_STAGES];
+  __shared__ int s_item;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < RING_STAGES; ++s) mbar_init(&full_bar[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  uint32_t g_issue = 0, g_cons = 0;
+  const bool stall = g_copy_stall != 0;
+  const long long kWaitCycles = stall ? kStallWaitCycles : kWaitCyclesDefault;
+  const double M52 = 6755399441055744.0;  // 1.5 * 2^52
+  constexpr double kQScale = FIXW ? 2.0 : 1.0;
+  constexpr double kWordBase = PHASE_WORD_BASE_HALF;
+  // per-atom B factors with the phase word: the weight folded into the exponent
+  constexpr bool LOGW = PERB && FIXW;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const WorkItem wi = items[it];
+    const SfPattern &pt = pats[wi.pattern];
+    const long long npix = pt.npix;
+    const AtomD *__restrict__ atomsd = pt.atomsd;
+    const TileDesc *__restrict__ tiles = pt.tiles;
+
+    // quad g of this thread: pixels qb .. qb + 3, qb = pix0 + 4 g NT
+    const long long pix0 = (long long)wi.pixel_tile * (NT * P) + 4 * tid;
+    double qx[NQ], qy[NQ], qz[NQ];
+    float dqx[NQ][3], dqy[NQ][3], dqz[NQ][3], s2[NQ][4];
+#pragma unroll
+    for (int g = 0; g < NQ; ++g) {
+      const long long qb = pix0 + 4LL * g * NT;
+      double a[3] = {0.0, 0.0, 0.0};
+      if (qb < npix) load_q(pt, quad_anchor(qb, npix), a);
+      qx[g] = kQScale * a[0];
+      qy[g] = kQScale * a[1];
+      qz[g] = kQScale * a[2];
+      s2[g][0] = (float)(-0.25 * (a[0] * a[0] + a[1] * a[1] + a[2] * a[2]) * 1e-20 * pt.s2scale * 1.4426950408889634);
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const long long p = quad_pixel(qb, s + 1, npix);
+        double b[3] = {a[0], a[1], a[2]};
+        if (p >= 0) load_q(pt, p, b);
+        dqx[g][s] = (float)(b[0] - a[0]);
+        dqy[g][s] = (float)(b[1] - a[1]);
+        dqz[g][s] = (float)(b[2] - a[2]);
+        s2[g][s + 1] =
+            (float)(-0.25 * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) * 1e-20 * pt.s2scale * 1.4426950408889634);
+      }
+    }
+    // float-float element sums: [pair of quads][slot]
+    float2 shc[NQP][4], slc[NQP][4], shs[NQP][4], sls[NQP][4];
+#pragma unroll
+    for (int j = 0; j < NQP; ++j)
+#pragma unroll
+      for (int h = 0; h < 4; ++h) shc[j][h] = slc[j][h] = shs[j][h] = sls[j][h] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < P; ++i) sacc[i * NT + tid] = make_double2(0.0, 0.0);
+
+    const int k0 = wi.k0, k1 = wi.k1;
+    if (tid == 0) {
+      for (int k = k0; k < k1 && k < k0 + RING_STAGES; ++k) {
+        const TileDesc td = tiles[k];
+        const uint32_t st = g_issue % RING_STAGES;
+        const uint32_t bytes = (uint32_t)td.count * (uint32_t)sizeof(AtomD);
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        if (!(stall && g_issue == 0))  // the stall hook skips the CTA's first copy
+          bulk_copy_g2s(&ring[st][0], atomsd + td.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+    }
+
+    for (int k = k0; k < k1; ++k) {
+      const uint32_t st = g_cons % RING_STAGES;
+      const uint32_t par = (g_cons / RING_STAGES) & 1u;
+      const bool ok = mbar_wait_bounded(&full_bar[st], par, kWaitCycles);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicOr(err, 1);
+          for (uint32_t g = g_cons; g < g_issue; ++g)
+            mbar_wait_bounded(&full_bar[g % RING_STAGES], (g / RING_STAGES) & 1u, kWaitCycles);
+        }
+        return;
+      }
+      const TileDesc td = tiles[k];
+      const float4 *__restrict__ ta = ring[st];
+      // atoms in groups of 2 x ATOM_GROUP (the last group of a tile may be
+      // ATOM_GROUP): FP32 sums within a group, Fast2Sum after it
+      for (int a = 0; a < td.count; a += 2 * ATOM_GROUP) {
+        float2 bc[NQP][4], bs[NQP][4];
+#pragma unroll
+        for (int j = 0; j < NQP; ++j)
+#pragma unroll
+          for (int h = 0; h < 4; ++h) bc[j][h] = bs[j][h] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int g = 0; g < 2 * ATOM_GROUP; ++g) {
+          if (g == ATOM_GROUP && a + ATOM_GROUP >= td.count) break;
+          const float4 d0 = ta[2 * (a + g)], d1 = ta[2 * (a + g) + 1];
+          const double rx = __hiloint2double(__float_as_int(d0.y), __float_as_int(d0.x));
+          const double ry = __hiloint2double(__float_as_int(d0.w), __float_as_int(d0.z));
+          const double rz = __hiloint2double(__float_as_int(d1.y), __float_as_int(d1.x));
+          const float W = d1.z;
+          const float2 fx = f2(__double2float_rn(rx)), fy = f2(__double2float_rn(ry)), fz = f2(__double2float_rn(rz));
+          // LOGW: W exp2(b s2) as exp2(b s2 + log2|W|), the sign of W as one more
+          // half cycle in the phase word (its parity bit flips every pixel's sign)
+          const float lw = LOGW ? lg2_approx(fabsf(W)) : 0.0f;
+          const double wbase = LOGW && W < 0.0f ? kWordBase + 1.0 : kWordBase;
+#pragma unroll
+          for (int j = 0; j < NQP; ++j) {
+            float ya[2];
+            uint32_t kb[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int m = 2 * j + h;
+              if (FIXW) {
+                const double t = phase_word(qx[m], qy[m], qz[m], rx, ry, rz, wbase);
+                reduce_phase_word<PREC_MODE_POLY>(t, ya[h], kb[h]);
+              } else {
+                double u = qx[m] * rx;
+                u = fma(qy[m], ry, u);
+                u = fma(qz[m], rz, u);
+                const double t = fma(u, 2.0, M52);
+                ya[h] = __double2float_rn(fma(t - M52, -0.5, u));
+                kb[h] = (uint32_t)__double2loint(t);
+              }
+            }
+            // anchors' reduced phases in cycles, then the stepped pixels
+            float2 Y[4];
+            Y[0] = FIXW ? mul2(make_float2(ya[0], ya[1]), f2(word_to_cycles<PREC_MODE_POLY>()))
+                        : make_float2(ya[0], ya[1]);
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+              float2 y = fma2(make_float2(dqx[2 * j][s], dqx[2 * j + 1][s]), fx, Y[0]);
+              y = fma2(make_float2(dqy[2 * j][s], dqy[2 * j + 1][s]), fy, y);
+              Y[s + 1] = fma2(make_float2(dqz[2 * j][s], dqz[2 * j + 1][s]), fz, y);
+            }
+            float2 ws[4];
+            if (PERB) {
+#pragma unroll
+              for (int h = 0; h < 4; ++h) {
+                const float w0 = LOGW ? ex2_approx(fmaf(d1.w, s2[2 * j][h], lw)) : W * ex2_approx(d1.w * s2[2 * j][h]);
+                const float w1 =
+                    LOGW ? ex2_approx(fmaf(d1.w, s2[2 * j + 1][h], lw)) : W * ex2_approx(d1.w * s2[2 * j + 1][h]);
+                ws[h] = make_float2(sign_by_parity(w0, kb[0], m31), sign_by_parity(w1, kb[1], m31));
+              }
+            } else {
+              ws[0] = make_float2(sign_by_parity(W, kb[0], m31), sign_by_parity(W, kb[1], m31));
+              ws[1] = ws[2] = ws[3] = ws[0];
+            }
+            float2 S, C;
+            sincos_dhalf_poly2(Y[0], S, C);
+            bc[j][0] = fma2(ws[0], C, bc[j][0]);
+            bs[j][0] = fma2(ws[0], S, bs[j][0]);
+#pragma unroll
+            for (int h = 1; h < 3; ++h) {  // one pixel from the anchor
+              if (NARROW)
+                sincos_narrow_poly2(Y[h], S, C);
+              else
+                sincos_wider_poly2(Y[h], S, C);
+              bc[j][h] = fma2(ws[h], C, bc[j][h]);
+              bs[j][h] = fma2(ws[h], S, bs[j][h]);
+            }
+            sincos_wider_poly2(Y[3], S, C);  // two pixels from the anchor
+            bc[j][3] = fma2(ws[3], C, bc[j][3]);
+            bs[j][3] = fma2(ws[3], S, bs[j][3]);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < NQP; ++j)
+#pragma unroll
+          for (int h = 0; h < 4; ++h) {
+            ff_accumulate2(shc[j][h], slc[j][h], bc[j][h]);
+            ff_accumulate2(shs[j][h], sls[j][h], bs[j][h]);
+          }
+      }
+      if (td.last || k == k1 - 1) {
+        const double *__restrict__ ffe = pt.ff + (long long)td.elem * npix;
+#pragma unroll
+        for (int j = 0; j < NQP; ++j)
+#pragma unroll
+          for (int h = 0; h < 4; ++h)      // slot: anchor, then the stepped pixels
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {  // which quad of the packed two
+              const int g = 2 * j + e;
+              const long long p = quad_pixel(pix0 + 4LL * g * NT, h, npix);
+              if (p >= 0) {
+                const double f = ffe[p];
+                const double re = e ? (double)shc[j][h].y + (double)slc[j][h].y : (double)shc[j][h].x + (double)slc[j][h].x;
+                const double sm = e ? (double)shs[j][h].y + (double)sls[j][h].y : (double)shs[j][h].x + (double)sls[j][h].x;
+                double2 v = sacc[(4 * g + h) * NT + tid];
+                v.x = fma(f, re, v.x);
+                v.y = fma(-f, sm, v.y);
+                sacc[(4 * g + h) * NT + tid] = v;
+              }
+            }
+#pragma unroll
+        for (int j = 0; j < NQP; ++j)
+#pragma unroll
+          for (int h = 0; h < 4; ++h) shc[j][h] = slc[j][h] = shs[j][h] = sls[j][h] = make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+      if (tid == 0 && k + RING_STAGES < k1) {
+        const TileDesc tn = tiles[k + RING_STAGES];
+        const uint32_t bytes = (uint32_t)tn.count * (uint32_t)sizeof(AtomD);
+        mbar_arrive_expect_tx(&full_bar[st], bytes);
+        bulk_copy_g2s(&ring[st][0], atomsd + tn.atom_begin, bytes, &full_bar[st]);
+        ++g_issue;
+      }
+      ++g_cons;
+    }
+    const bool whole = k0 == 0 && k1 == pt.n_tiles;
+#pragma unroll
+    for (int g = 0; g < NQ; ++g)
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const long long p = quad_pixel(pix0 + 4LL * g * NT, h, npix);
+        if (p >= 0) {
+          const double2 v = sacc[(4 * g + h) * NT + tid];
+          if (whole) {
+            pt.acc[p] = v;
+          } else {
+            atomicAdd(&pt.acc[p].x, v.x);
+            atomicAdd(&pt.acc[p].y, v.y);
+          }
+        }
+      }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // plain FP64 forward: one thread per pixel, atoms read as warp-uniform loads
 
 __global__ void __launch_bounds__(256) sf_f64_kernel(const SfPattern *__restrict__ pats, int pattern) {
@@ -1306,7 +1576,9 @@ cudaError_t launch_ff_table(const float *hkl, const double *q64, long long npix,
 template <int MODE, int NT, int P, bool PERB, int PK, bool FW, bool NW = false>
 static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, int n_items, int *queue, int *err,
                                 int grid, cudaStream_t st) {
-  if constexpr (PK == 3)
+  if constexpr (PK == 4)
+    sf_dquad_kernel<NT, P, PERB, FW, NW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
+  else if constexpr (PK == 3)
     sf_dpair_kernel<MODE, NT, P, PERB, FW, NW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
   else if constexpr (PK == 2)
     sf_dphase_kernel<MODE, NT, P, PERB, FW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
@@ -1320,7 +1592,9 @@ static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, in
 template <int MODE, int NT, int P, bool PERB, int PK, bool FW, bool NW = false>
 static int occupancy_t() {
   int n = 0;
-  if constexpr (PK == 3)
+  if constexpr (PK == 4)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dquad_kernel<NT, P, PERB, FW, NW>, NT, 0);
+  else if constexpr (PK == 3)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dpair_kernel<MODE, NT, P, PERB, FW, NW>, NT, 0);
   else if constexpr (PK == 2)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dphase_kernel<MODE, NT, P, PERB, FW>, NT, 0);
@@ -1363,16 +1637,19 @@ static int occupancy_t() {
   X(1, 128, 4, 3)             \
   X(1, 128, 8, 3)             \
   X(1, 128, 12, 3)            \
-  X(1, 256, 4, 3)
+  X(1, 256, 4, 3)             \
+  X(0, 128, 8, 4)             \
+  X(0, 128, 16, 4)            \
+  X(0, 256, 8, 4)
 
-// fixw selects the fixed-point phase word in the FP64-phase forms (2, 3);
-// the compensated forms ignore it.
+// fixw selects the fixed-point phase word in the FP64-phase forms (2, 3, 4),
+// narrow the NARROW polynomial of forms 3 and 4; the compensated forms ignore both.
 cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const SfPattern *pats,
                           const WorkItem *items, int n_items, int *queue, int *err, int grid, cudaStream_t st,
                           bool fixw, bool narrow) {
 #define X(M, N, PP, PK)                                                                                   \
   if (mode == M && nt == N && p == PP && packed == PK) {                                                  \
-    if (narrow && fixw && PK == 3 && M == PREC_MODE_POLY)                                                 \
+    if (narrow && fixw && PK >= 3 && M == PREC_MODE_POLY)                                                 \
       return perb ? launch_f32_t<M, N, PP, true, PK, true, true>(pats, items, n_items, queue, err, grid, st) \
                   : launch_f32_t<M, N, PP, false, PK, true, true>(pats, items, n_items, queue, err, grid, st); \
     if (fixw && PK >= 2)                                                                                  \
@@ -1389,7 +1666,7 @@ cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const 
 int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw, bool narrow) {
 #define X(M, N, PP, PK)                                                                          \
   if (mode == M && nt == N && p == PP && packed == PK) {                                         \
-    if (narrow && fixw && PK == 3 && M == PREC_MODE_POLY)                                        \
+    if (narrow && fixw && PK >= 3 && M == PREC_MODE_POLY)                                        \
       return perb ? occupancy_t<M, N, PP, true, PK, true, true>()                                \
                   : occupancy_t<M, N, PP, false, PK, true, true>();                              \
     if (fixw && PK >= 2)                                                                         \
@@ -1476,37 +1753,50 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long *out) 
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) pair_step_kernel(const float *__restrict__ hkl, const double *__restrict__ q64,
-                                                        long long npix, unsigned long long *__restrict__ out) {
-  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double n = 0.0;
-  if (2 * m + 1 < npix) {
-    double d[3];
-    for (int c = 0; c < 3; ++c)
-      d[c] = hkl ? (double)hkl[3 * (2 * m + 1) + c] - (double)hkl[3 * (2 * m) + c]
-                 : q64[3 * (2 * m + 1) + c] - q64[3 * (2 * m) + c];
-    n = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-  }
-  block_max_to(n, out);
+// Neighbour steps of one quad of pixels 4m .. 4m+3 (the pair and quad
+// forms' admission tests): st[0] = largest |q[2i+1] - q[2i]| of its two pairs,
+// st[1] = largest |q - q_a| over its one-pixel neighbours of the anchor q_a
+// (q[4m+1], or q[4m] where that is the quad's only pixel), st[2] = |q[4m+3] - q_a|.
+__device__ __forceinline__ void quad_steps(const float *__restrict__ hkl, const double *__restrict__ q64,
+                                           long long npix, long long m, double st[3]) {
+  st[0] = st[1] = st[2] = 0.0;
+  const long long qb = 4 * m;
+  double q[4][3];
+  const int n = (int)(npix - qb < 4 ? npix - qb : 4);
+  for (int i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) q[i][c] = hkl ? (double)hkl[3 * (qb + i) + c] : q64[3 * (qb + i) + c];
+  auto dist = [&](int a, int b) {
+    const double d0 = q[b][0] - q[a][0], d1 = q[b][1] - q[a][1], d2 = q[b][2] - q[a][2];
+    return sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  };
+  if (n >= 2) st[0] = dist(0, 1), st[1] = dist(1, 0);
+  if (n >= 3) st[1] = fmax(st[1], dist(1, 2));
+  if (n >= 4) st[0] = fmax(st[0], dist(2, 3)), st[2] = dist(1, 3);
 }
 
-cudaError_t pair_step(const float *hkl, const double *q64, long long npix, double *step) {
-  *step = 0.0;
+__global__ void __launch_bounds__(256) qset_steps_kernel(const float *__restrict__ hkl, const double *__restrict__ q64,
+                                                         long long npix, unsigned long long *__restrict__ out) {
+  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double st[3] = {0.0, 0.0, 0.0};
+  if (4 * m < npix) quad_steps(hkl, q64, npix, m, st);
+  block_max_to(st[0], out);
+  block_max_to(st[1], out + 1);
+  block_max_to(st[2], out + 2);
+}
+
+cudaError_t qset_steps(const float *hkl, const double *q64, long long npix, double steps[3]) {
+  steps[0] = steps[1] = steps[2] = 0.0;
   if (npix < 2) return cudaSuccess;
-  unsigned long long *d = nullptr, h = 0;
-  cudaError_t e = cudaMalloc(&d, sizeof(*d));
+  unsigned long long *d = nullptr, h[3] = {0, 0, 0};
+  cudaError_t e = cudaMalloc(&d, sizeof(h));
   if (e != cudaSuccess) return e;
-  if ((e = cudaMemset(d, 0, sizeof(*d))) == cudaSuccess) {
-    const long long pairs = npix / 2;
-    pair_step_kernel<<<(unsigned)((pairs + 255) / 256), 256>>>(hkl, q64, npix, d);
-    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  if ((e = cudaMemset(d, 0, sizeof(h))) == cudaSuccess) {
+    const long long quads = (npix + 3) / 4;
+    qset_steps_kernel<<<(unsigned)((quads + 255) / 256), 256>>>(hkl, q64, npix, d);
+    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
   }
   cudaFree(d);
-  if (e == cudaSuccess) {
-    double v;
-    memcpy(&v, &h, sizeof(v));
-    *step = v;
-  }
+  if (e == cudaSuccess) memcpy(steps, h, sizeof(h));
   return e;
 }
 
@@ -1538,42 +1828,39 @@ cudaError_t launch_rotate_hkl(long long n, const float R[9], float *hkl, cudaStr
   return cudaGetLastError();
 }
 
-// Largest |q|^2 and largest |q[2m+1] - q[2m]|^2 of a float HKL list, as the
-// bits of non-negative doubles (which order like integers) in out[0], out[1].
+// Largest |q| of a float HKL list and its neighbour steps (qset_steps), as
+// the bits of non-negative doubles (which order like integers) in out[0..3].
 __global__ void __launch_bounds__(256) qset_stats_kernel(const float *__restrict__ hkl, long long npix,
                                                          unsigned long long *__restrict__ out) {
   const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double qq = 0.0, dd = 0.0;
-  if (2 * m < npix) {
-    double a[3], b[3];
-    for (int c = 0; c < 3; ++c) a[c] = hkl[3 * (2 * m) + c];
-    qq = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
-    if (2 * m + 1 < npix) {
-      for (int c = 0; c < 3; ++c) b[c] = hkl[3 * (2 * m + 1) + c];
-      qq = fmax(qq, b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
-      dd = (b[0] - a[0]) * (b[0] - a[0]) + (b[1] - a[1]) * (b[1] - a[1]) + (b[2] - a[2]) * (b[2] - a[2]);
-    }
+  double qq = 0.0, st[3] = {0.0, 0.0, 0.0};
+  for (long long i = 4 * m; i < 4 * m + 4 && i < npix; ++i) {
+    const double a = hkl[3 * i], b = hkl[3 * i + 1], c = hkl[3 * i + 2];
+    qq = fmax(qq, a * a + b * b + c * c);
   }
+  if (4 * m < npix) quad_steps(hkl, nullptr, npix, m, st);
   block_max_to(qq, out);
-  block_max_to(dd, out + 1);
+  block_max_to(st[0], out + 1);
+  block_max_to(st[1], out + 2);
+  block_max_to(st[2], out + 3);
 }
 
-cudaError_t qset_stats(const float *hkl, long long npix, unsigned long long *scratch2, double *qmax, double *step,
+cudaError_t qset_stats(const float *hkl, long long npix, unsigned long long *scratch4, double *qmax, double steps[3],
                        cudaStream_t st) {
-  *qmax = *step = 0.0;
+  *qmax = steps[0] = steps[1] = steps[2] = 0.0;
   if (npix <= 0) return cudaSuccess;
-  cudaError_t e = cudaMemsetAsync(scratch2, 0, 2 * sizeof(unsigned long long), st);
+  cudaError_t e = cudaMemsetAsync(scratch4, 0, 4 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
-  const long long pairs = (npix + 1) / 2;
-  qset_stats_kernel<<<(unsigned)((pairs + 255) / 256), 256, 0, st>>>(hkl, npix, scratch2);
+  const long long quads = (npix + 3) / 4;
+  qset_stats_kernel<<<(unsigned)((quads + 255) / 256), 256, 0, st>>>(hkl, npix, scratch4);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  unsigned long long h[2] = {0, 0};
-  if ((e = cudaMemcpyAsync(h, scratch2, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+  unsigned long long h[4] = {0, 0, 0, 0};
+  if ((e = cudaMemcpyAsync(h, scratch4, sizeof(h), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-  double v[2];
+  double v[4];
   memcpy(v, h, sizeof(v));
   *qmax = sqrt(v[0]);
-  *step = sqrt(v[1]);
+  for (int k = 0; k < 3; ++k) steps[k] = v[k + 1];
   return cudaSuccess;
 }
 

@@ -28,12 +28,15 @@ cudaError_t launch_crystal(long long npix, const float *hkl, const double cell[9
                            float *I, cudaStream_t st);
 // q <- R q in float on a device HKL list, bit-identical to the reference's host loop.
 cudaError_t launch_rotate_hkl(long long n, const float R[9], float *hkl, cudaStream_t st);
-// Largest |q| and largest |q[2m+1] - q[2m]| of a device float HKL list
-// (scratch2: two device words; waits for `st`).
-cudaError_t qset_stats(const float *hkl, long long npix, unsigned long long *scratch2, double *qmax, double *step,
+// Neighbour steps of a q set (synchronous, small): steps[0] the largest
+// |q[2m+1] - q[2m]| (the pair form's admission), steps[1] the largest step from
+// a quad's anchor q[4m+1] to q[4m] or q[4m+2], steps[2] the largest to q[4m+3]
+// (the quad form's).
+cudaError_t qset_steps(const float *hkl, const double *q64, long long npix, double steps[3]);
+// Largest |q| and the neighbour steps of a device float HKL list (scratch4:
+// four device words; waits for `st`).
+cudaError_t qset_stats(const float *hkl, long long npix, unsigned long long *scratch4, double *qmax, double steps[3],
                        cudaStream_t st);
-// Largest |q[2m+1] - q[2m]| of a q set's pixel pairs (synchronous, small).
-cudaError_t pair_step(const float *hkl, const double *q64, long long npix, double *step);
 cudaError_t launch_finalize(const SfPattern *pats, int pattern0, int npat, long long max_npix, cudaStream_t st);
 cudaError_t launch_ewald(int nx, int ny, double width, double height, double distance, double cx, double cy,
                          double wavelength, int spherical, float *out32, double *out64, cudaStream_t st);

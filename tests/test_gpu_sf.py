@@ -218,13 +218,16 @@ def test_wide_phase_range_uses_fp64_rounding(cuda, precision):
 
 
 VARIANTS = [(128, 2, 0), (256, 4, 0), (128, 4, 1), (128, 6, 1), (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 8, 2),
-            (128, 4, 3), (128, 8, 3), (128, 12, 3), (256, 4, 3)]
+            (128, 4, 3), (128, 8, 3), (128, 12, 3), (256, 4, 3), (128, 8, 4), (128, 16, 4), (256, 8, 4)]
 
 
 @pytest.mark.parametrize("precision", ["f32", "f32_fast"])
 @pytest.mark.parametrize("variant", VARIANTS, ids=["%dx%d_form%d" % v for v in VARIANTS])
 def test_every_kernel_form_meets_tolerance(cuda, precision, variant):
-    # each compiled variant, forced, on the plain 1k workload and with per-atom B factors
+    # each compiled variant, forced, on the plain 1k workload (whole detector
+    # rows: pairs and quads are admitted) and with per-atom B factors
+    if variant[2] == 4 and precision != "f32":
+        pytest.skip("the neighbour-quad form is FP32-polynomial only")
     g = golden("sf_plain1k.npz")
     F64, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64))
     rng = np.random.Generator(np.random.PCG64(17))
@@ -233,7 +236,9 @@ def test_every_kernel_form_meets_tolerance(cuda, precision, variant):
     try:
         core.set_variant(*variant)
         F, I = _run(g["Z"], g["pos"], g["hkl"], precision)
+        assert core.last_variant() == variant
         Fb, Ib = _run(g["Z"], g["pos"], g["hkl"], precision, bfac=bfac)
+        assert core.last_variant() == variant
     finally:
         core.set_variant(-1)
     for got, want in ((I, I64), (Ib, I64b)):
@@ -241,15 +246,18 @@ def test_every_kernel_form_meets_tolerance(cuda, precision, variant):
         assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1], (variant, e_max, e_l2)
 
 
-def test_neighbour_pair_form_admission(cuda):
-    # a detector of even width is admitted to the neighbour-pair form; a random
-    # HKL list (no neighbour structure) falls back to the FP64-phase form; both
-    # stay within tolerance
+def test_neighbour_form_admission(cuda):
+    # a detector of width divisible by 4 is admitted to the neighbour-quad
+    # form, one of even width (6: quads straddle rows) to the neighbour-pair
+    # form; a random HKL list (no neighbour structure) falls back to the
+    # FP64-phase form; all stay within tolerance
     Z, pos = synth.random_molecule(2000, 3e-9, 31)
     d = dict(nx=64, ny=40, width=64 * 150e-6, height=40 * 150e-6, distance=0.1, wavelength=0.2e-9)
     q_det = O.hkl_detector(**d).astype(np.float32)
+    d6 = dict(nx=6, ny=400, width=6 * 150e-6, height=400 * 150e-6, distance=0.1, wavelength=0.2e-9)
+    q_det6 = O.hkl_detector(**d6).astype(np.float32)
     q_rand = np.random.Generator(np.random.PCG64(31)).normal(size=(2560, 3)).astype(np.float32) * 1e9
-    for q, kernel in ((q_det, "sf_dpair_kernel"), (q_rand, "sf_dphase_kernel")):
+    for q, kernel in ((q_det, "sf_dquad_kernel"), (q_det6, "sf_dpair_kernel"), (q_rand, "sf_dphase_kernel")):
         F, I = _run(Z, pos, q, "f32")
         assert core.kernel_name() == kernel and core.last_phase_word()
         _, I64 = O.structure_factor(Z, pos.astype(np.float64), q.astype(np.float64))
@@ -290,8 +298,79 @@ def test_neighbour_pair_step_selects_second_pixel_polynomial(cuda, step, narrow)
         assert not core.last_pair_narrow()  # the MUFU forms have no polynomial
 
 
+def _quads(rng, n, s1, s2, scale=1.5e9):
+    """A q list of n quads 4m..4m+3 around random anchors q_a = q[4m+1]: the
+    one-pixel neighbours at distance s1 (in 1/m), the two-pixel one at s2."""
+    qa = rng.normal(size=(n, 3)) * scale
+    u = rng.normal(size=(n, 3, 3))
+    u /= np.linalg.norm(u, axis=2, keepdims=True)
+    return np.stack([qa + u[:, 0] * s1, qa, qa + u[:, 1] * s1, qa + u[:, 2] * s2], axis=1).reshape(-1, 3)
+
+
+def _bound(pos):
+    p64 = pos.astype(np.float64)
+    c = 0.5 * (p64.min(0) + p64.max(0))
+    rmax = np.linalg.norm(p64 - c, axis=1).max()
+    return rmax + max(0.05 * rmax, 5e-10)
+
+
+@pytest.mark.parametrize("step1,step2,narrow", [(0.065, 0.155, True), (0.12, 0.155, False)])
+def test_neighbour_quad_steps_select_polynomials(cuda, step1, step2, narrow):
+    # quads whose one-pixel steps (times the molecule's bound) stay within
+    # 0.07 cycle take the NARROW polynomial for them, up to 1/8 the WIDER one;
+    # the two-pixel step always takes WIDER (up to 0.16); all within tolerance
+    # on the steepest steps the admission allows, with and without B factors
+    Z, pos = synth.random_molecule(3000, 3e-9, 43)
+    rb = _bound(pos)
+    rng = np.random.Generator(np.random.PCG64(44))
+    hkl = _quads(rng, 2048, step1 / rb, step2 / rb).astype(np.float32)
+    bfac = rng.uniform(0, 40, len(Z)).astype(np.float32)
+    for kw in ({}, {"bfac": bfac}):
+        _, I64 = O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64), **kw)
+        _, I = _run(Z, pos, hkl, "f32", **kw)
+        assert core.kernel_name() == "sf_dquad_kernel" and core.last_phase_word()
+        assert core.last_pair_narrow() == narrow
+        e_max, e_l2 = intensity_errors(I, I64)
+        assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (step1, kw.keys(), e_max, e_l2)
+
+
+def test_neighbour_quad_admission_limits(cuda):
+    # a two-pixel step beyond 0.16 cycle, or a one-pixel step beyond 1/8,
+    # sends the q set to the pair form (or form 2) instead
+    Z, pos = synth.random_molecule(1000, 2e-9, 45)
+    rb = _bound(pos)
+    rng = np.random.Generator(np.random.PCG64(46))
+    for s1, s2 in ((0.05, 0.17), (0.13, 0.1)):
+        hkl = _quads(rng, 512, s1 / rb, s2 / rb).astype(np.float32)
+        _, I64 = O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64))
+        _, I = _run(Z, pos, hkl, "f32")
+        assert core.kernel_name() != "sf_dquad_kernel", (s1, s2)
+        e_max, e_l2 = intensity_errors(I, I64)
+        assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1]
+
+
+@pytest.mark.parametrize("npix", [1, 2, 3, 5, 6, 7, 1021, 1022, 1023, 1029])
+def test_neighbour_quads_with_a_partial_last_quad(cuda, npix):
+    # q sets whose length is not a multiple of 4 (and tiles that end inside a
+    # quad): the last quad anchors on its first pixel when that is its only one
+    Z, pos = synth.random_molecule(700, 2e-9, 47)
+    d = dict(nx=64, ny=20, width=64 * 150e-6, height=20 * 150e-6, distance=0.1, wavelength=0.2e-9)
+    hkl = O.hkl_detector(**d)[:npix].astype(np.float32)
+    _, I64 = O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64))
+    for variant in ((128, 8, 4), (128, 16, 4), (256, 8, 4)):
+        try:
+            core.set_variant(*variant)
+            _, I = _run(Z, pos, hkl, "f32")
+            assert core.last_variant() == variant
+        finally:
+            core.set_variant(-1)
+        e_max, e_l2 = intensity_errors(I, I64)
+        assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (npix, variant, e_max, e_l2)
+
+
 CANDIDATES = {(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1), (128, 2, 2),
-              (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2), (128, 4, 3), (128, 8, 3), (128, 12, 3), (256, 4, 3)}
+              (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2), (128, 4, 3), (128, 8, 3), (128, 12, 3), (256, 4, 3),
+              (128, 8, 4), (128, 16, 4), (256, 8, 4)}
 
 
 def test_autotune_single_and_batch(cuda):
@@ -323,7 +402,7 @@ def test_autotune_single_and_batch(cuda):
     finally:
         core.clear_tuning()
     core.forward(mol, qs, precision="f32")
-    assert core.last_variant() == (128, 4, 3)  # the untuned default again
+    assert core.last_variant() == (128, 8, 4)  # the untuned default again
 
 
 @pytest.mark.parametrize("form", [2, 3])

@@ -23,8 +23,8 @@ from spsim_b200._native import SPSIM_ERR_TIMEOUT, SpsimError
 pytestmark = pytest.mark.gpu
 
 # one variant of each kernel form: compensated FP32 (0, 1), FP64 phase (2),
-# FP64-anchored neighbour pairs (3)
-FORMS = [(128, 4, 0), (128, 4, 1), (128, 4, 2), (128, 8, 3)]
+# FP64-anchored neighbour pairs (3) and quads (4)
+FORMS = [(128, 4, 0), (128, 4, 1), (128, 4, 2), (128, 8, 3), (128, 8, 4)]
 DET = dict(nx=64, ny=40, width=64 * 150e-6, height=40 * 150e-6, distance=0.1, wavelength=0.2e-9)
 
 

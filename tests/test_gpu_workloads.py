@@ -46,7 +46,7 @@ def test_orientations_20k_4096_rotations_in_one_batch(cuda):
     core.forward_batch(mol, qs, rots=R, precision="f32", I=list(I.unbind(0)), want_F=False)
     torch.cuda.synchronize()
     core.synchronize()
-    assert core.kernel_name() == "sf_dpair_kernel"
+    assert core.kernel_name() == "sf_dquad_kernel"
     q0 = O.hkl_detector(**d)
     sel = _rows(d["nx"], d["ny"], 4)
     for k in (0, 1, 2047, 4095):
