@@ -241,10 +241,12 @@ MIX = {
     # second pixels on the NARROW polynomial: one FMA fewer per second-pixel term
     "sf_dpair_kernel+word+narrow": {"fp32": 15.0, "dfma": 1.5, "imad": 0.5, "alu": 0.5, "xu": 0.375, "i2f": 0.5},
     # a quarter of the terms FP64-anchored (13 FP32: scale, DHALF, sums); the
-    # other three step from the anchor in one 3-FMA chain (16 with NARROW, 17
-    # with WIDER); the two-pixel step always WIDER
-    "sf_dquad_kernel+word": {"fp32": 16.0, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 0.375, "i2f": 0.25},
-    "sf_dquad_kernel+word+narrow": {"fp32": 15.5, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 0.375,
+    # other three step from the anchor in one 3-FMA chain: pixel 4m on a
+    # polynomial (16 FP32 with NARROW, 17 with WIDER), pixels 4m+2 and 4m+3 on
+    # MUFU (6 FP32: step, scale to radians, sums; 2 MUFU each); XU also takes
+    # the atom's FP64 -> FP32 conversions (3 per 8 terms)
+    "sf_dquad_kernel+word": {"fp32": 10.5, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 1.375, "i2f": 0.25},
+    "sf_dquad_kernel+word+narrow": {"fp32": 10.25, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 1.375,
                                     "i2f": 0.25},
     # FP64 phase + reduction, DHALF poly
     "sf_dphase_kernel": {"fp32": 12, "dfma": 6, "imad": 1, "xu": 1},
@@ -310,7 +312,7 @@ def _peaks(props):
     return min(p_fma / OPS_PER_TERM_FMA, p_mufu / OPS_PER_TERM_MUFU), p_mufu, p_fma, sm_max, src
 
 
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "sf_dpair_precision50k_traffic.md")
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "sf_dquad_precision50k_traffic.md")
 
 
 def _traffic_per_launch():

@@ -34,8 +34,10 @@ extern "C" {
 
 /* ---- precision of the structure-factor sum ----------------------------- */
 #define SPSIM_PREC_FP64 0        /* plain FP64 per-pixel kernel (FP64 phase, sincos, sum)      */
-#define SPSIM_PREC_F32 1         /* compensated FP32 phase, FMA-pipe minimax sin/cos,          */
-                                 /* float-float segment sums, FP64 cross-tile/element sum      */
+#define SPSIM_PREC_F32 1         /* FP64 (or compensated FP32) phase, FMA-pipe minimax sin/cos */
+                                 /* (MUFU for half of each neighbour quad's pixels), float-    */
+                                 /* float segment sums, FP64 cross-tile/element sum; <= 1e-5   */
+                                 /* relative |F|^2 error against FP64                          */
 #define SPSIM_PREC_F32_FAST 2    /* compensated FP32 phase, MUFU sin/cos, same summation        */
 
 /* ---- where caller buffers live ----------------------------------------- */
@@ -383,8 +385,9 @@ void spsim_b200_set_formula_seed(unsigned long long seed);
  *      used where |q_b - q_a| |r|max <= 1/8 cycle for every pair of the q
  *      set (detector rows of even width)
  *   4  form 2 on the second pixel of each neighbour quad (pixels 4m..4m+3),
- *      the other three as its phase plus (q - q_a).r in FP32 (SPSIM_PREC_F32
- *      only); the SPSIM_PREC_F32 default, used where every one-pixel step
+ *      the other three as its phase plus (q - q_a).r in FP32, sin/cos of
+ *      pixels 4m+2 and 4m+3 on MUFU (SPSIM_PREC_F32 only); the
+ *      SPSIM_PREC_F32 default, used where every one-pixel step
  *      from a quad's anchor stays within 1/8 cycle of |r|max and every
  *      two-pixel step within 0.16 cycle (detector rows of width divisible by
  *      4), else form 3, else form 2

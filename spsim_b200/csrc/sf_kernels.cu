@@ -1025,14 +1025,23 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
 // summed onto y_a in one FMA chain, with the anchor's sign.  The host admits a
 // q set when, for every quad, the one-pixel steps (4m and 4m+2 from the anchor)
 // stay within 1/8 cycle of the molecule's bound (0.07 for NARROW) and the
-// two-pixel step (4m+3) within 0.16 cycle, so that |y| <= 0.41 stays inside
-// the WIDER polynomial's domain (the one-pixel steps' |y| <= 0.32 inside
-// NARROW's).  Against the pair form: 3 DFMA per four terms instead of per two,
-// and one FP32 operation fewer per stepped pixel.  A partial last quad (q sets
-// whose length is not a multiple of 4) anchors on its first pixel when that is
-// the only one.  Threads hold P pixels as P/4 quads; the corresponding pixels
-// of two quads share each packed f32x2 instruction.  FP32 polynomial sin/cos
-// only (the MUFU forms gain nothing from anchors).
+// two-pixel step (4m+3) within 0.16 cycle, so that |y| <= 0.41.
+//
+// sin/cos of the four pixels go to two pipes: the anchor (DHALF) and pixel 4m
+// (NARROW, or WIDER for steps up to 1/8) on FMA-pipe polynomials, pixels 4m+2
+// and 4m+3 on the XU pipe (MUFU sin/cos of 2 pi y, |2 pi y| <= 2.6).  Per quad
+// that leaves ~51 FMA-pipe lane slots (FP32, the anchor's 3 DFMA and its
+// sign's IMAD) against ~6.5 XU operations (4 MUFU, the anchor's conversion,
+// the atom's three FP64 -> FP32 conversions per two quads), which the two
+// pipes take in about equal time; all four on polynomials leaves the XU pipe
+// idle and the FMA pipe the bound, three on MUFU makes XU the bound.  MUFU's
+// absolute error (~2^-21) on half the terms keeps the 50,000-atom workload's
+// floored maximum |F|^2 error at 3.2e-6 (2.1e-6 with polynomials only).
+// Against the pair form: 3 DFMA per four terms instead of per two, and one
+// FP32 operation fewer per stepped pixel.  A partial last quad (q sets whose
+// length is not a multiple of 4) anchors on its first pixel when that is the
+// only one.  Threads hold P pixels as P/4 quads; the corresponding pixels of
+// two quads share each packed f32x2 instruction.  SPSIM_PREC_F32 only.
 
 // Anchor of quad base qb and the pixel of slot s (0 = anchor, 1..3 = qb, qb+2,
 // qb+3), or -1 where the slot holds no pixel of the q set.
@@ -1210,18 +1219,20 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(PREC_MODE_POLY)) sf_dquad_ke
             sincos_dhalf_poly2(Y[0], S, C);
             bc[j][0] = fma2(ws[0], C, bc[j][0]);
             bs[j][0] = fma2(ws[0], S, bs[j][0]);
+            if (NARROW)
+              sincos_narrow_poly2(Y[1], S, C);
+            else
+              sincos_wider_poly2(Y[1], S, C);
+            bc[j][1] = fma2(ws[1], C, bc[j][1]);
+            bs[j][1] = fma2(ws[1], S, bs[j][1]);
 #pragma unroll
-            for (int h = 1; h < 3; ++h) {  // one pixel from the anchor
-              if (NARROW)
-                sincos_narrow_poly2(Y[h], S, C);
-              else
-                sincos_wider_poly2(Y[h], S, C);
+            for (int h = 2; h < 4; ++h) {  // pixels 4m+2, 4m+3: MUFU sin/cos on the XU pipe
+              const float2 x = mul2(Y[h], f2(6.28318530717958648f));
+              __sincosf(x.x, &S.x, &C.x);
+              __sincosf(x.y, &S.y, &C.y);
               bc[j][h] = fma2(ws[h], C, bc[j][h]);
               bs[j][h] = fma2(ws[h], S, bs[j][h]);
             }
-            sincos_wider_poly2(Y[3], S, C);  // two pixels from the anchor
-            bc[j][3] = fma2(ws[3], C, bc[j][3]);
-            bs[j][3] = fma2(ws[3], S, bs[j][3]);
           }
         }
 #pragma unroll

@@ -5,6 +5,8 @@ intensity, and L2 over the pattern; every path stores F and I as float32, so
 one float ulp, ~6e-8, is the floor):
   fp64      2e-7  / 1e-7
   f32       1e-5  / 1e-6     FP64 or compensated FP32 phase, FMA-pipe sin/cos
+                             (the neighbour-quad form: MUFU sin/cos for half
+                             of each quad's pixels)
   f32_fast  2e-4  / 1e-5     FP64 or compensated FP32 phase, MUFU sin/cos
 and against the reference's float results, its own error band (2e-5 / 2e-6).
 """
