@@ -1029,7 +1029,9 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
 //
 // sin/cos of the four pixels go to two pipes: the anchor (DHALF) and pixel 4m
 // (NARROW, or WIDER for steps up to 1/8) on FMA-pipe polynomials, pixels 4m+2
-// and 4m+3 on the XU pipe (MUFU sin/cos of 2 pi y, |2 pi y| <= 2.6).  Per quad
+// and 4m+3 on the XU pipe (MUFU sin/cos of 2 pi y, |2 pi y| <= 2.6); with
+// per-atom B factors, whose weight exp2 already issues one XU operation per
+// term, only pixel 4m+3 (pixel 4m+2 on the WIDER polynomial).  Per quad
 // that leaves ~51 FMA-pipe lane slots (FP32, the anchor's 3 DFMA and its
 // sign's IMAD) against ~6.5 XU operations (4 MUFU, the anchor's conversion,
 // the atom's three FP64 -> FP32 conversions per two quads), which the two
@@ -1219,14 +1221,20 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(PREC_MODE_POLY)) sf_dquad_ke
             sincos_dhalf_poly2(Y[0], S, C);
             bc[j][0] = fma2(ws[0], C, bc[j][0]);
             bs[j][0] = fma2(ws[0], S, bs[j][0]);
-            if (NARROW)
-              sincos_narrow_poly2(Y[1], S, C);
-            else
-              sincos_wider_poly2(Y[1], S, C);
-            bc[j][1] = fma2(ws[1], C, bc[j][1]);
-            bs[j][1] = fma2(ws[1], S, bs[j][1]);
+            // per-atom B factors already give the XU pipe one ex2 per term:
+            // there only pixel 4m+3 goes to MUFU (PERB: pixel 4m+2 on WIDER)
+            constexpr int kFirstMufu = PERB ? 3 : 2;
 #pragma unroll
-            for (int h = 2; h < 4; ++h) {  // pixels 4m+2, 4m+3: MUFU sin/cos on the XU pipe
+            for (int h = 1; h < kFirstMufu; ++h) {
+              if (NARROW && h == 1)
+                sincos_narrow_poly2(Y[h], S, C);
+              else
+                sincos_wider_poly2(Y[h], S, C);
+              bc[j][h] = fma2(ws[h], C, bc[j][h]);
+              bs[j][h] = fma2(ws[h], S, bs[j][h]);
+            }
+#pragma unroll
+            for (int h = kFirstMufu; h < 4; ++h) {  // MUFU sin/cos on the XU pipe
               const float2 x = mul2(Y[h], f2(6.28318530717958648f));
               __sincosf(x.x, &S.x, &C.x);
               __sincosf(x.y, &S.y, &C.y);
