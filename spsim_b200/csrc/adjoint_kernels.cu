@@ -292,7 +292,13 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
             reduce_phase_word<PREC_MODE_POLY>(t, y[h], kb[h]);
           }
           float2 S, C;
-          sincos_dhalf_poly2(mul2(make_float2(y[0], y[1]), f2(word_to_cycles<PREC_MODE_POLY>())), S, C);
+          if (j & 1) {  // every other atom pair on MUFU sin/cos (the XU pipe)
+            const float2 x = mul2(make_float2(y[0], y[1]), f2(6.28318530717958648f * word_to_cycles<PREC_MODE_POLY>()));
+            __sincosf(x.x, &S.x, &C.x);
+            __sincosf(x.y, &S.y, &C.y);
+          } else {
+            sincos_dhalf_poly2(mul2(make_float2(y[0], y[1]), f2(word_to_cycles<PREC_MODE_POLY>())), S, C);
+          }
           float2 zr, zn;
           if (PERB) {
             // the sign once, on the B-factor weight E, which then scales both
@@ -330,7 +336,13 @@ __global__ void __launch_bounds__(NT) adj_dphase_kernel(AdjParams prm, uint32_t 
           }
         }
         float2 S, C;
-        sincos_dhalf_poly2(make_float2(y[0], y[1]), S, C);
+        if (j & 1) {  // every other atom pair on MUFU sin/cos (the XU pipe)
+          const float2 x = mul2(make_float2(y[0], y[1]), f2(6.28318530717958648f));
+          __sincosf(x.x, &S.x, &C.x);
+          __sincosf(x.y, &S.y, &C.y);
+        } else {
+          sincos_dhalf_poly2(make_float2(y[0], y[1]), S, C);
+        }
         // H conj(A) e^{-2 pi i u} = (hr C - hi S) - i (hr S + hi C), times (-1)^k
         float2 zr = fma2(nhi, S, mul2(hr, C));
         float2 zn = fma2(hi, C, mul2(hr, S));  // = -Im
