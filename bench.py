@@ -241,13 +241,18 @@ MIX = {
     # second pixels on the NARROW polynomial: one FMA fewer per second-pixel term
     "sf_dpair_kernel+word+narrow": {"fp32": 15.0, "dfma": 1.5, "imad": 0.5, "alu": 0.5, "xu": 0.375, "i2f": 0.5},
     # a quarter of the terms FP64-anchored (13 FP32: scale, DHALF, sums); the
-    # other three step from the anchor in one 3-FMA chain: pixel 4m on a
-    # polynomial (16 FP32 with NARROW, 17 with WIDER), pixels 4m+2 and 4m+3 on
-    # MUFU (6 FP32: step, scale to radians, sums; 2 MUFU each); XU also takes
-    # the atom's FP64 -> FP32 conversions (3 per 8 terms)
-    "sf_dquad_kernel+word": {"fp32": 10.5, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 1.375, "i2f": 0.25},
-    "sf_dquad_kernel+word+narrow": {"fp32": 10.25, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 1.375,
-                                    "i2f": 0.25},
+    # other three step from the anchor in one 3-FMA chain (16 FP32 with NARROW,
+    # 17 with WIDER); the two-pixel step always WIDER
+    "sf_dquad_kernel+word/f32": {"fp32": 16.0, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 0.375, "i2f": 0.25},
+    "sf_dquad_kernel+word+narrow/f32": {"fp32": 15.5, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 0.375,
+                                        "i2f": 0.25},
+    # f32_fast: pixel 4m on a polynomial, pixels 4m+2 and 4m+3 on MUFU (6 FP32:
+    # step, scale to radians, sums; 2 MUFU each); XU also takes the atom's
+    # FP64 -> FP32 conversions (3 per 8 terms)
+    "sf_dquad_kernel+word/f32_fast": {"fp32": 10.5, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 1.375,
+                                      "i2f": 0.25},
+    "sf_dquad_kernel+word+narrow/f32_fast": {"fp32": 10.25, "dfma": 0.75, "imad": 0.25, "alu": 0.25, "xu": 1.375,
+                                             "i2f": 0.25},
     # FP64 phase + reduction, DHALF poly
     "sf_dphase_kernel": {"fp32": 12, "dfma": 6, "imad": 1, "xu": 1},
     "sf_dphase_kernel+word/f32": {"fp32": 13, "dfma": 3, "imad": 1, "alu": 1, "i2f": 1},
@@ -272,7 +277,7 @@ def balanced_bound(kernel, prec, probe):
     conversions) runs beside them, so the bound is the larger of the two."""
     if not probe or not probe.get("fma_lane_ops_per_s"):
         return None
-    mix = MIX.get(kernel) or MIX.get("%s/%s" % (kernel, prec))
+    mix = MIX.get("%s/%s" % (kernel, prec)) or MIX.get(kernel)
     if not mix:
         return None
     rate = {"fp32": probe["fma_lane_ops_per_s"], "dfma": probe.get("dfma_lane_ops_per_s"),
@@ -620,7 +625,7 @@ def _e2e(args, w, Z, pos, terms, world, dist=None):
             "steps": nsteps, "note": "reference semantics: no ADC clamp (extension) in this call"}
 
 
-PROFILE_VARIANTS = {"f32": (128, 8, 4), "f32_fast": (128, 8, 2)}  # the untuned defaults on the 1024^2 workload
+PROFILE_VARIANTS = {"f32": (128, 8, 4), "f32_fast": (128, 8, 4)}  # the untuned defaults on the 1024^2 workload
 
 
 def profile_case(precisions):
@@ -693,8 +698,6 @@ def sweep():
         for v in [(128, 2, 0), (128, 4, 0), (256, 4, 0), (128, 2, 1), (128, 4, 1), (256, 4, 1), (128, 6, 1),
                   (128, 2, 2), (128, 4, 2), (256, 4, 2), (128, 6, 2), (128, 8, 2), (128, 4, 3), (128, 8, 3),
                   (128, 12, 3), (256, 4, 3), (128, 8, 4), (128, 16, 4), (256, 8, 4)]:
-            if v[2] == 4 and prec != "f32":
-                continue
             core.set_variant(*v)
             for _ in range(2):
                 core.forward(mol, qs, precision=prec, F=F, I=I)

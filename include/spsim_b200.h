@@ -34,11 +34,11 @@ extern "C" {
 
 /* ---- precision of the structure-factor sum ----------------------------- */
 #define SPSIM_PREC_FP64 0        /* plain FP64 per-pixel kernel (FP64 phase, sincos, sum)      */
-#define SPSIM_PREC_F32 1         /* FP64 (or compensated FP32) phase, FMA-pipe minimax sin/cos */
-                                 /* (MUFU for half of each neighbour quad's pixels), float-    */
-                                 /* float segment sums, FP64 cross-tile/element sum; <= 1e-5   */
-                                 /* relative |F|^2 error against FP64                          */
-#define SPSIM_PREC_F32_FAST 2    /* compensated FP32 phase, MUFU sin/cos, same summation        */
+#define SPSIM_PREC_F32 1         /* FP64 (or compensated FP32) phase, FMA-pipe minimax sin/cos,*/
+                                 /* float-float segment sums, FP64 cross-tile/element sum;     */
+                                 /* <= 1e-5 relative |F|^2 error against FP64                  */
+#define SPSIM_PREC_F32_FAST 2    /* the same phase and sums, MUFU sin/cos (on neighbour quads   */
+                                 /* for half the pixels, the others on the polynomials)        */
 
 /* ---- where caller buffers live ----------------------------------------- */
 #define SPSIM_MEM_HOST 0
@@ -385,12 +385,13 @@ void spsim_b200_set_formula_seed(unsigned long long seed);
  *      used where |q_b - q_a| |r|max <= 1/8 cycle for every pair of the q
  *      set (detector rows of even width)
  *   4  form 2 on the second pixel of each neighbour quad (pixels 4m..4m+3),
- *      the other three as its phase plus (q - q_a).r in FP32, sin/cos of
- *      pixels 4m+2 and 4m+3 on MUFU (SPSIM_PREC_F32 only); the
- *      SPSIM_PREC_F32 default, used where every one-pixel step
- *      from a quad's anchor stays within 1/8 cycle of |r|max and every
- *      two-pixel step within 0.16 cycle (detector rows of width divisible by
- *      4), else form 3, else form 2
+ *      the other three as its phase plus (q - q_a).r in FP32 (with
+ *      SPSIM_PREC_F32_FAST the sin/cos of pixels 4m+2 and 4m+3 on MUFU, the
+ *      rest on FMA-pipe polynomials); the default of both FP32 precisions,
+ *      used where every one-pixel step from a quad's anchor stays within 1/8
+ *      cycle of |r|max and every two-pixel step within 0.16 cycle (detector
+ *      rows of width divisible by 4), else form 3 (SPSIM_PREC_F32), else
+ *      form 2
  * Forms 2, 3 and 4 read the reduced phase from a fixed-point phase word (three
  * FP64 FMAs) while |q|max |r - centre|max < 2^17 cycles, and reduce by FP64
  * rounding (six FP64 operations, up to 2^48 cycles) beyond.

@@ -662,10 +662,10 @@ static Variant choose_variant(double terms, long long total_npix, int precision)
   // neighbour step saves nothing); 8 pixels per thread (two CTAs per SM) once
   // there are enough pixel tiles to fill every SM several times (fastest on
   // both the 50,000- and the 5,000-atom workloads)
-  if (precision == SPSIM_PREC_F32_FAST) return {128, total_npix >= (1LL << 20) ? 8 : 4, 2};
-  // FP32: the neighbour-quad form (8 pixels per thread), falling back to the
+  // the neighbour-quad form (8 pixels per thread), falling back (FP32) to the
   // pair form and then to form 2 where a q set is not admitted, there with 4
-  // pixels per thread below 2^20 pixels
+  // pixels per thread below 2^20 pixels; FP32_FAST falls back to form 2 (its
+  // MUFU sin/cos gains nothing from pairs)
   return {128, 8, 4, total_npix >= (1LL << 20) ? 8 : 4};
 }
 
@@ -730,10 +730,9 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
   Variant var = {128, 4, 1};
   if (precision != SPSIM_PREC_FP64) var = choose_variant(terms, total_npix, precision);
   if (var.packed == 4) {
-    // neighbour-quad form (FP32 polynomial only): every pattern needs its
-    // one-pixel steps within 1/8 cycle and its two-pixel steps within 0.16
-    // cycle of the molecule's bound
-    bool ok = precision == SPSIM_PREC_F32;
+    // neighbour-quad form: every pattern needs its one-pixel steps within 1/8
+    // cycle and its two-pixel steps within 0.16 cycle of the molecule's bound
+    bool ok = precision != SPSIM_PREC_FP64;
     double max_step1 = 0.0;
     for (int i = 0; i < npat && ok; ++i) {
       double scale = spec ? std::fabs(spec->qscale[i]) : 1.0;
@@ -750,7 +749,7 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     pl.narrow = ok && max_step1 <= 0.07 * (1.0 - 1e-6);
     if (!ok) {
       const int pf = var.p_fallback;
-      var = fit_variant(precision, var.nt, pf ? pf : var.p, 3);
+      var = fit_variant(precision, var.nt, pf ? pf : var.p, precision == SPSIM_PREC_F32 ? 3 : 2);
       var.p_fallback = pf;
     }
   }
@@ -1080,7 +1079,11 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
   g_last_variant[1] = pl->precision == SPSIM_PREC_FP64 ? 1 : pl->ppt;
   g_last_variant[2] = pl->precision == SPSIM_PREC_FP64 ? -1 : pl->packed;
   g_last_phase_word = pl->precision != SPSIM_PREC_FP64 && pl->fixw ? 1 : 0;
-  g_last_pair_narrow = pl->precision == SPSIM_PREC_F32 && pl->packed >= 3 && pl->fixw && pl->narrow ? 1 : 0;
+  g_last_pair_narrow =
+      pl->precision != SPSIM_PREC_FP64 && (pl->packed == 4 || (pl->packed == 3 && pl->precision == SPSIM_PREC_F32)) &&
+              pl->fixw && pl->narrow
+          ? 1
+          : 0;
   CUDA_TRY(refresh_rotations(*pl, rot, stream));
   if (g_timing || !cache || stream == nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -178,19 +178,19 @@ extern "C" int spsim_b200_structure_factor_host_noalloc(int natoms, const int32_
   }
   const double qmax = std::sqrt(qm2);
 
-  // ---- kernel form: the untuned allocating call's choice.  FP32: the
+  // ---- kernel form: the untuned allocating call's choice.  The
   // neighbour-quad form (4, 8 pixels per thread) where every one-pixel step
   // from a quad's anchor is within 1/8 cycle and every two-pixel step within
-  // 0.16, else the neighbour-pair form (3) where every pair's step is within
-  // 1/8 cycle, else the FP64-phase form (2); FP32_FAST: form 2; forms 2 and 3
-  // with 8 pixels per thread from 2^20 pixels, 4 below; the fixed-point phase
-  // word below 2^17 cycles, FP64 rounding up to 2^48.
+  // 0.16, else (FP32 only) the neighbour-pair form (3) where every pair's step
+  // is within 1/8 cycle, else the FP64-phase form (2); forms 2 and 3 with 8
+  // pixels per thread from 2^20 pixels, 4 below; the fixed-point phase word
+  // below 2^17 cycles, FP64 rounding up to 2^48.
   const bool fp32 = precision != SPSIM_PREC_FP64;
   const int mode = precision == SPSIM_PREC_F32_FAST ? PREC_MODE_MUFU : PREC_MODE_POLY;
   const double s_pair = std::sqrt(pair2) * rbound, s_q1 = std::sqrt(quad1) * rbound, s_q2 = std::sqrt(quad2) * rbound;
   int form = 2;
   bool narrow = false;
-  if (precision == SPSIM_PREC_F32 && s_q1 <= (1.0 / 8) * (1.0 - 1e-9) && s_q2 <= 0.16 * (1.0 - 1e-9)) {
+  if (fp32 && s_q1 <= (1.0 / 8) * (1.0 - 1e-9) && s_q2 <= 0.16 * (1.0 - 1e-9)) {
     form = 4;
     narrow = s_q1 <= 0.07 * (1.0 - 1e-6);
   } else if (precision == SPSIM_PREC_F32 && s_pair <= (1.0 / 8) * (1.0 - 1e-9)) {

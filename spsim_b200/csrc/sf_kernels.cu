@@ -1027,23 +1027,28 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
 // stay within 1/8 cycle of the molecule's bound (0.07 for NARROW) and the
 // two-pixel step (4m+3) within 0.16 cycle, so that |y| <= 0.41.
 //
-// sin/cos of the four pixels go to two pipes: the anchor (DHALF) and pixel 4m
-// (NARROW, or WIDER for steps up to 1/8) on FMA-pipe polynomials, pixels 4m+2
-// and 4m+3 on the XU pipe (MUFU sin/cos of 2 pi y, |2 pi y| <= 2.6); with
-// per-atom B factors, whose weight exp2 already issues one XU operation per
-// term, only pixel 4m+3 (pixel 4m+2 on the WIDER polynomial).  Per quad
-// that leaves ~51 FMA-pipe lane slots (FP32, the anchor's 3 DFMA and its
-// sign's IMAD) against ~6.5 XU operations (4 MUFU, the anchor's conversion,
-// the atom's three FP64 -> FP32 conversions per two quads), which the two
-// pipes take in about equal time; all four on polynomials leaves the XU pipe
-// idle and the FMA pipe the bound, three on MUFU makes XU the bound.  MUFU's
-// absolute error (~2^-21) on half the terms keeps the 50,000-atom workload's
-// floored maximum |F|^2 error at 3.2e-6 (2.1e-6 with polynomials only).
+// SPSIM_PREC_F32 (HYB false): every pixel's sin/cos on FMA-pipe polynomials,
+// DHALF for the anchor, NARROW (or WIDER, for steps up to 1/8) for the
+// one-pixel steps, WIDER (|y| <= 0.41, 6 + 6 coefficients) for the two-pixel
+// step.  SPSIM_PREC_F32_FAST (HYB true): the work split between two pipes,
+// the anchor and pixel 4m on the polynomials, pixels 4m+2 and 4m+3 on the XU
+// pipe (MUFU sin/cos of 2 pi y, |2 pi y| <= 2.6); with per-atom B factors,
+// whose weight exp2 already issues one XU operation per term, only pixel
+// 4m+3.  Per quad that leaves ~51 FMA-pipe lane slots (FP32, the anchor's 3
+// DFMA and its sign's IMAD) against ~6.5 XU operations (4 MUFU, the anchor's
+// conversion, the atom's three FP64 -> FP32 conversions per two quads), which
+// the two pipes take in about equal time (2.07e12 against 1.78e12 terms/s on
+// the 50,000-atom workload).  MUFU's error is a bias of ~2e-7 over wide
+// ranges of its argument rather than zero-mean noise, so a pixel whose sin/cos
+// all come from MUFU carries it into |F|^2: the floored maximum error of the
+// 50,000-atom workload is 3.2e-6 (2.1e-6 with polynomials only) but reaches
+// ~1.7e-5 on random neighbour quads at |q| ~ 1e10 1/m, beyond SPSIM_PREC_F32's
+// 1e-5; hence the split belongs to the fast mode.
 // Against the pair form: 3 DFMA per four terms instead of per two, and one
 // FP32 operation fewer per stepped pixel.  A partial last quad (q sets whose
 // length is not a multiple of 4) anchors on its first pixel when that is the
 // only one.  Threads hold P pixels as P/4 quads; the corresponding pixels of
-// two quads share each packed f32x2 instruction.  SPSIM_PREC_F32 only.
+// two quads share each packed f32x2 instruction.
 
 // Anchor of quad base qb and the pixel of slot s (0 = anchor, 1..3 = qb, qb+2,
 // qb+3), or -1 where the slot holds no pixel of the q set.
@@ -1054,7 +1059,7 @@ __device__ __forceinline__ long long quad_pixel(long long qb, int slot, long lon
   return (p < npix && (slot == 0 || p != pa)) ? p : -1;
 }
 
-template <int NT, int P, bool PERB, bool FIXW, bool NARROW>
+template <int NT, int P, bool PERB, bool FIXW, bool NARROW, bool HYB>
 __global__ void __launch_bounds__(NT, sf_min_blocks(PREC_MODE_POLY)) sf_dquad_kernel(
     const SfPattern *__restrict__ pats, const WorkItem *__restrict__ items, int n_items, int *__restrict__ queue,
     int *__restrict__ err, uint32_t m31) {
@@ -1221,12 +1226,12 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(PREC_MODE_POLY)) sf_dquad_ke
             sincos_dhalf_poly2(Y[0], S, C);
             bc[j][0] = fma2(ws[0], C, bc[j][0]);
             bs[j][0] = fma2(ws[0], S, bs[j][0]);
-            // per-atom B factors already give the XU pipe one ex2 per term:
-            // there only pixel 4m+3 goes to MUFU (PERB: pixel 4m+2 on WIDER)
-            constexpr int kFirstMufu = PERB ? 3 : 2;
+            // HYB: pixels 4m+2 and 4m+3 on MUFU; per-atom B factors already give
+            // the XU pipe one ex2 per term, so there only pixel 4m+3
+            constexpr int kFirstMufu = !HYB ? 4 : (PERB ? 3 : 2);
 #pragma unroll
             for (int h = 1; h < kFirstMufu; ++h) {
-              if (NARROW && h == 1)
+              if (NARROW && h < 3)
                 sincos_narrow_poly2(Y[h], S, C);
               else
                 sincos_wider_poly2(Y[h], S, C);
@@ -1596,7 +1601,8 @@ template <int MODE, int NT, int P, bool PERB, int PK, bool FW, bool NW = false>
 static cudaError_t launch_f32_t(const SfPattern *pats, const WorkItem *items, int n_items, int *queue, int *err,
                                 int grid, cudaStream_t st) {
   if constexpr (PK == 4)
-    sf_dquad_kernel<NT, P, PERB, FW, NW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
+    sf_dquad_kernel<NT, P, PERB, FW, NW, MODE == PREC_MODE_MUFU><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err,
+                                                                              0x80000000u);
   else if constexpr (PK == 3)
     sf_dpair_kernel<MODE, NT, P, PERB, FW, NW><<<grid, NT, 0, st>>>(pats, items, n_items, queue, err, 0x80000000u);
   else if constexpr (PK == 2)
@@ -1612,7 +1618,8 @@ template <int MODE, int NT, int P, bool PERB, int PK, bool FW, bool NW = false>
 static int occupancy_t() {
   int n = 0;
   if constexpr (PK == 4)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dquad_kernel<NT, P, PERB, FW, NW>, NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dquad_kernel<NT, P, PERB, FW, NW, MODE == PREC_MODE_MUFU>, NT,
+                                                  0);
   else if constexpr (PK == 3)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sf_dpair_kernel<MODE, NT, P, PERB, FW, NW>, NT, 0);
   else if constexpr (PK == 2)
@@ -1659,7 +1666,10 @@ static int occupancy_t() {
   X(1, 256, 4, 3)             \
   X(0, 128, 8, 4)             \
   X(0, 128, 16, 4)            \
-  X(0, 256, 8, 4)
+  X(0, 256, 8, 4)             \
+  X(1, 128, 8, 4)             \
+  X(1, 128, 16, 4)            \
+  X(1, 256, 8, 4)
 
 // fixw selects the fixed-point phase word in the FP64-phase forms (2, 3, 4),
 // narrow the NARROW polynomial of forms 3 and 4; the compensated forms ignore both.
@@ -1668,7 +1678,7 @@ cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const 
                           bool fixw, bool narrow) {
 #define X(M, N, PP, PK)                                                                                   \
   if (mode == M && nt == N && p == PP && packed == PK) {                                                  \
-    if (narrow && fixw && PK >= 3 && M == PREC_MODE_POLY)                                                 \
+    if (narrow && fixw && (PK == 4 || (PK == 3 && M == PREC_MODE_POLY)))                                  \
       return perb ? launch_f32_t<M, N, PP, true, PK, true, true>(pats, items, n_items, queue, err, grid, st) \
                   : launch_f32_t<M, N, PP, false, PK, true, true>(pats, items, n_items, queue, err, grid, st); \
     if (fixw && PK >= 2)                                                                                  \
@@ -1685,7 +1695,7 @@ cudaError_t launch_sf_f32(int mode, int nt, int p, int packed, bool perb, const 
 int sf_f32_occupancy(int mode, int nt, int p, int packed, bool perb, bool fixw, bool narrow) {
 #define X(M, N, PP, PK)                                                                          \
   if (mode == M && nt == N && p == PP && packed == PK) {                                         \
-    if (narrow && fixw && PK >= 3 && M == PREC_MODE_POLY)                                        \
+    if (narrow && fixw && (PK == 4 || (PK == 3 && M == PREC_MODE_POLY)))                         \
       return perb ? occupancy_t<M, N, PP, true, PK, true, true>()                                \
                   : occupancy_t<M, N, PP, false, PK, true, true>();                              \
     if (fixw && PK >= 2)                                                                         \

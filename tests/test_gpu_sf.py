@@ -5,9 +5,9 @@ intensity, and L2 over the pattern; every path stores F and I as float32, so
 one float ulp, ~6e-8, is the floor):
   fp64      2e-7  / 1e-7
   f32       1e-5  / 1e-6     FP64 or compensated FP32 phase, FMA-pipe sin/cos
-                             (the neighbour-quad form: MUFU sin/cos for half
-                             of each quad's pixels)
-  f32_fast  2e-4  / 1e-5     FP64 or compensated FP32 phase, MUFU sin/cos
+  f32_fast  2e-4  / 1e-5     FP64 or compensated FP32 phase, MUFU sin/cos (the
+                             neighbour-quad form: for half of each quad's
+                             pixels, the others on the polynomials)
 and against the reference's float results, its own error band (2e-5 / 2e-6).
 """
 import numpy as np
@@ -228,8 +228,6 @@ VARIANTS = [(128, 2, 0), (256, 4, 0), (128, 4, 1), (128, 6, 1), (128, 2, 2), (12
 def test_every_kernel_form_meets_tolerance(cuda, precision, variant):
     # each compiled variant, forced, on the plain 1k workload (whole detector
     # rows: pairs and quads are admitted) and with per-atom B factors
-    if variant[2] == 4 and precision != "f32":
-        pytest.skip("the neighbour-quad form is FP32-polynomial only")
     g = golden("sf_plain1k.npz")
     F64, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), g["hkl"].astype(np.float64))
     rng = np.random.Generator(np.random.PCG64(17))
@@ -334,6 +332,23 @@ def test_neighbour_quad_steps_select_polynomials(cuda, step1, step2, narrow):
         assert core.last_pair_narrow() == narrow
         e_max, e_l2 = intensity_errors(I, I64)
         assert e_max < TOL["f32"][0] and e_l2 < TOL["f32"][1], (step1, kw.keys(), e_max, e_l2)
+
+
+def test_fast_mode_takes_the_split_pipe_quads(cuda):
+    # f32_fast on a detector q set runs the quad form with pixels 4m+2, 4m+3 on
+    # MUFU (all on polynomials in f32), within its tolerance, with and without
+    # per-atom B factors (one MUFU pixel per quad there)
+    Z, pos = synth.random_molecule(3000, 3e-9, 48)
+    d = dict(nx=64, ny=48, width=64 * 150e-6, height=48 * 150e-6, distance=0.1, wavelength=0.2e-9)
+    hkl = O.hkl_detector(**d).astype(np.float32)
+    bfac = np.random.Generator(np.random.PCG64(49)).uniform(0, 40, len(Z)).astype(np.float32)
+    for kw in ({}, {"bfac": bfac}):
+        _, I64 = O.structure_factor(Z, pos.astype(np.float64), hkl.astype(np.float64), **kw)
+        for precision in ("f32", "f32_fast"):
+            _, I = _run(Z, pos, hkl, precision, **kw)
+            assert core.kernel_name() == "sf_dquad_kernel" and core.last_pair_narrow()
+            e_max, e_l2 = intensity_errors(I, I64)
+            assert e_max < TOL[precision][0] and e_l2 < TOL[precision][1], (precision, kw.keys(), e_max, e_l2)
 
 
 def test_neighbour_quad_admission_limits(cuda):
