@@ -58,6 +58,13 @@ void free_stuff(Diffraction_Pattern *pattern, Options *opts);            /* src/
 void free_diffraction_pattern(Diffraction_Pattern *pattern);             /* src/spsim.c:353 */
 void free_output_in_options(Options *opts);                              /* src/spsim.c:363 */
 
+/* ---- output files: include/spsim.h:47-52 of spsim ----
+ * <basename>-NNNNN.cxi, an HDF5 file in the CXI image layout written without
+ * libspimage or the HDF5 library (see spsim_b200/csrc/host/cxi.c). */
+void output_array(char *basename, int index, float *array, SpRotation *rot, Options *opts);     /* src/spsim.c:146 */
+void output_carray(char *basename, int index, Complex *array, SpRotation *rot, Options *opts);  /* src/spsim.c:175 */
+void output_files(Diffraction_Pattern *pattern, Options *opts, int index);                     /* src/spsim.c:228 */
+
 /* ---- molecules: include/molecule.h:25-28 ---- */
 Molecule *alloc_mol(void);                                               /* src/molecule.c:394 */
 void add_atom_to_mol(Molecule *mol, int atomic_number, float x, float y, float z); /* src/molecule.c:402 */

@@ -35,7 +35,7 @@ CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-result", "-Werro
             "-I" + os.path.join(CUDA_HOME, "include")]
 
 CU_SOURCES = ["sf_kernels.cu", "chain_kernels.cu", "adjoint_kernels.cu", "nufft_kernels.cu", "capi.cu", "noalloc.cu"]
-C_SOURCES = ["host/config.c", "host/legacy.c", "host/molecule.c", "host/crystal.c"]
+C_SOURCES = ["host/config.c", "host/legacy.c", "host/molecule.c", "host/crystal.c", "host/cxi.c"]
 
 
 def lib_path():

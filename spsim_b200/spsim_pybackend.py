@@ -129,6 +129,9 @@ _PROTOS = {
     "get_my_loop_start_and_end": (None, [c_int, P(c_int), P(c_int)]),
     "syncronize_patterns": (None, [P(Diffraction_Pattern)]),
     "sum_patterns": (None, [P(Diffraction_Pattern)]),
+    "output_array": (None, [c_char_p, c_int, P(c_float), P(SpRotation), P(Options)]),
+    "output_carray": (None, [c_char_p, c_int, P(Complex), P(SpRotation), P(Options)]),
+    "output_files": (None, [P(Diffraction_Pattern), P(Options), c_int]),
 }
 
 _bound = {}
@@ -274,6 +277,25 @@ def add_atom_to_mol(mol, atomic_number, x, y, z):
 
 def free_mol(mol):
     _fn("free_mol")(mol)
+
+
+# ---- output files (src/spsim.c:146-279): <basename>-NNNNN.cxi
+def output_array(basename, index, array, rot, opts):
+    """array: a float32 numpy array of the detector's pixels (or a ctypes float pointer)."""
+    keep = np.ascontiguousarray(array, np.float32) if isinstance(array, np.ndarray) else None
+    ptr = keep.ctypes.data_as(P(c_float)) if keep is not None else array
+    _fn("output_array")(_path(basename), int(index), ptr, rot, opts)
+
+
+def output_carray(basename, index, array, rot, opts):
+    """array: a complex64 numpy array (or a ctypes Complex pointer)."""
+    keep = np.ascontiguousarray(array, np.complex64) if isinstance(array, np.ndarray) else None
+    ptr = keep.ctypes.data_as(P(Complex)) if keep is not None else array
+    _fn("output_carray")(_path(basename), int(index), ptr, rot, opts)
+
+
+def output_files(pattern, opts, index):
+    _fn("output_files")(pattern, opts, int(index))
 
 
 # ---- distribution (single-process semantics)

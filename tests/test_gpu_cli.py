@@ -1,13 +1,15 @@
 """The spsim command-line program on this library (spsim_b200/_lib/spsim,
 src/spsim.c:374-415): spsim.conf in, spsim.confout, molout.pdb and the output
-arrays out.  A PDB molecule with BIOMT operators checks the scattering
-factors the program writes against the FP64 oracle."""
+arrays out, as CXI files (read with the spec-based reader tests/h5read.py).
+A PDB molecule with BIOMT operators checks the scattering factors the
+program writes against the FP64 oracle."""
 import os
 import subprocess
 
 import numpy as np
 import pytest
 
+import h5read
 from conftest import GOLDEN, intensity_errors
 from oracle import oracle as O
 from spsim_b200 import spsim as S
@@ -40,6 +42,14 @@ output_solid_angles = 1;
 """
 
 
+def _data(tmp_path, name):
+    """The image of one CXI file (complex for the {r, i} compound)."""
+    f = h5read.read(str(tmp_path / name))
+    assert int(f["/cxi_version"]) == 150
+    a = f["/entry_1/image_1/data"]
+    return h5read.complex_of(a) if a.dtype.names else a
+
+
 def _run(tmp_path, conf):
     (tmp_path / "spsim.conf").write_text(conf)
     r = subprocess.run([CLI], cwd=tmp_path, capture_output=True, text=True, timeout=300)
@@ -69,10 +79,10 @@ def test_cli_formula_molecule(cuda, tmp_path):
                                    ("solid_angles", (ny, nx), np.float32),
                                    ("counts_out", (ny // 2, nx // 2), np.float32),
                                    ("noiseless_counts_out", (ny // 2, nx // 2), np.float32)):
-            a = np.load(tmp_path / ("%s-%05d.npy" % (name, k)))
+            a = _data(tmp_path, "%s-%05d.cxi" % (name, k))
             assert a.shape == shape and a.dtype == dtype and np.all(np.isfinite(a.view(np.float32)))
-    p0 = np.load(tmp_path / "photon_out-00000.npy")
-    p1 = np.load(tmp_path / "photon_out-00001.npy")
+    p0 = _data(tmp_path, "photon_out-00000.cxi")
+    p1 = _data(tmp_path, "photon_out-00001.cxi")
     assert not np.array_equal(p0, p1)  # independent noise per shot
 
 
@@ -103,6 +113,6 @@ def test_cli_pdb_molecule_scattering_factors(cuda, tmp_path, nfft):
     assert n == 1600
     q = O.hkl_detector(64, 48, 9.6e-3, 7.2e-3, 0.1, 2e-10)
     F64, I64 = O.structure_factor(Z, pos.astype(np.float64), q.astype(np.float32).astype(np.float64))
-    F = np.load(tmp_path / "scattering_factors-00000.npy").reshape(-1)
+    F = _data(tmp_path, "scattering_factors-00000.cxi").reshape(-1)
     e_max, e_l2 = intensity_errors(np.abs(F.astype(np.complex128)) ** 2, I64)
     assert e_max < 1e-5 and e_l2 < 1e-6, (e_max, e_l2)
