@@ -435,6 +435,7 @@ struct spsim_b200_qset {
   double qmax = 0;
   double pair_step = 0;  // largest |q[2m+1] - q[2m]| (the pixel-pair form's admission test)
   double quad_step1 = 0, quad_step2 = 0;  // largest one- and two-pixel steps from a quad's anchor (the quad form's)
+  int row = 0;           // pixels per detector row (q sets made from a detector), 0 for a list
   ~spsim_b200_qset() {
     cudaFree(d_hkl);
     cudaFree(d_q64);
@@ -534,6 +535,7 @@ extern "C" int spsim_b200_qset_from_detector(int nx, int ny, float width, float 
   q->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
   q->device = dev;
   q->npix = (long long)nx * ny;
+  q->row = nx;
   CUDA_TRY(cudaMalloc(&q->d_q64, 3 * q->npix * sizeof(double)));
   CUDA_TRY(launch_ewald(nx, ny, width, height, distance, center_x, center_y, wavelength, spherical, nullptr,
                         q->d_q64, 0));
@@ -1699,6 +1701,7 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   a.hkl = qs->d_hkl;
   a.q64 = qs->d_q64;
   a.npix = npix;
+  a.tile_nx = qs->row > 0 && npix % qs->row == 0 ? qs->row : 0;
   a.npat = npat;
   if (npat > 1 && rot) {
     CUDA_TRY(c.rots.ensure(9 * (size_t)npat * sizeof(double)));

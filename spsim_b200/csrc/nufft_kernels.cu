@@ -287,9 +287,24 @@ __device__ __forceinline__ void ld_cell32(const float4 *p, float4 &a, float4 &b)
                : "l"(p));
 }
 
+// Pixel tiles of a detector q list: a CTA takes 16 x 8 neighbouring pixels,
+// whose stencils share most grid cells (~14 x 12 x 10 cells of 32 bytes on the
+// 50,000-atom workload, so that three CTAs' working sets stay in L1), where
+// 128 pixels of one row would reach ~47 x 9 x 9.
+constexpr int INTERP_TX = 16, INTERP_TY = 8;
+
 template <int W, int H>
 __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant__ NufftInterp a) {
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long p;
+  if (a.tile_nx > 0) {
+    const int tiles_x = (a.tile_nx + INTERP_TX - 1) / INTERP_TX;
+    const long long x = (long long)(blockIdx.x % tiles_x) * INTERP_TX + threadIdx.x % INTERP_TX;
+    const long long y = (long long)(blockIdx.x / tiles_x) * INTERP_TY + threadIdx.x / INTERP_TX;
+    if (x >= a.tile_nx) return;
+    p = y * a.tile_nx + x;
+  } else {
+    p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  }
   if (p >= a.npix) return;
   const NufftGeom &g = a.g;
   const long long out = (long long)blockIdx.y * a.npix + p;
@@ -407,7 +422,13 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
 
 template <int W>
 static cudaError_t interp_t(const NufftInterp &a, cudaStream_t st) {
-  const dim3 grid((unsigned)((a.npix + 127) / 128), (unsigned)std::max(a.npat, 1));
+  static_assert(INTERP_TX * INTERP_TY == 128, "one tile per CTA of 128 threads");
+  long long blocks = (a.npix + 127) / 128;
+  if (a.tile_nx > 0) {
+    const long long rows = (a.npix + a.tile_nx - 1) / a.tile_nx;
+    blocks = ((a.tile_nx + INTERP_TX - 1) / INTERP_TX) * ((rows + INTERP_TY - 1) / INTERP_TY);
+  }
+  const dim3 grid((unsigned)blocks, (unsigned)std::max(a.npat, 1));
   if (a.halves == 1)
     nufft_interp_kernel<W, 1><<<grid, 128, 0, st>>>(a);
   else

@@ -43,6 +43,7 @@ struct NufftInterp {
   const float *hkl;   // AoS float3 q, or nullptr
   const double *q64;  // AoS double3 q, or nullptr
   long long npix;
+  int tile_nx;        // > 0: the q list is a detector of rows of tile_nx pixels, taken in 16 x 8 tiles
   int has_rot;
   double rot[9];      // q' = R q (row-major)
   int npat;           // patterns (blockIdx.y); outputs [npat][npix]
