@@ -34,7 +34,8 @@ CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-result", "-Werro
             "-ffp-contract=off",
             "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["sf_kernels.cu", "chain_kernels.cu", "adjoint_kernels.cu", "nufft_kernels.cu", "capi.cu", "noalloc.cu"]
+CU_SOURCES = ["sf_kernels.cu", "chain_kernels.cu", "adjoint_kernels.cu", "nufft_kernels.cu", "nufft_fft.cu", "capi.cu",
+              "noalloc.cu"]
 C_SOURCES = ["host/config.c", "host/legacy.c", "host/molecule.c", "host/crystal.c", "host/cxi.c"]
 
 
@@ -107,8 +108,7 @@ def build(force=False, verbose=False):
         tmp = out + ".tmp"
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs +
              ["-Xlinker", "--version-script=" + vmap, "-Xlinker", "-Bsymbolic",
-              "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft",
-              "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64"), "-lrt", "-ldl", "-lpthread"],
+              "-lrt", "-ldl", "-lpthread"],
              verbose)
         shutil.move(tmp, out)
     cli = os.path.join(LIBDIR, "spsim")

@@ -18,7 +18,6 @@
 #include "sf_kernels.cuh"
 #include "nufft_kernels.cuh"
 
-#include <cufft.h>
 
 using namespace spsim;
 
@@ -1472,12 +1471,8 @@ extern "C" int spsim_b200_structure_factor_host_spectrum(int natoms, const int32
 // streams are ordered by the context's completion event.
 
 struct NufftCtx {
-  DevBuf small, fine, packed, dec, seg, keys, flags, rots;
-  // the FFT of the padded grid, element by element: 2-D (y, x) transforms of
-  // the planes that hold data (the n1z / 2 planes at either end of z), then
-  // the z transform of every (y, x) column
-  cufftHandle fft_yx = 0, fft_z = 0;
-  int fft_dims[4] = {0, 0, 0, 0};  // n2z, n2y, n2x, n1z
+  DevBuf small, fa, fb, packed, dec, tw, seg, keys, flags, rots;
+  FftAxis ax[3];  // the pruned FFT passes (twiddle tables in tw)
   std::vector<double> geom_key;
   unsigned long long seg_mol = 0;  // molecule whose segment table is on the device
   NufftGeom g;
@@ -1596,7 +1591,7 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
       }
     }
     const int w = nufft_width(eps);
-    const double sigma1 = 1.5, sigma2 = 2.0;
+    const double sigma1 = 1.5, sigma2 = 2.0;  // spreading-grid and FFT-grid upsampling
     NufftGeom g;
     std::memset(&g, 0, sizeof(g));
     g.w1 = std::min(w + 3, NUFFT_MAX_W);
@@ -1614,23 +1609,34 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
       if (n1 > 4096) return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: %.0f grid points along axis %d; use the direct sum", n1, d);
       g.n1[d] = (int)n1 + ((int)n1 & 1);
       g.n2[d] = fft_size((int)std::ceil(sigma2 * g.n1[d]));
+      if (g.n2[d] > NUFFT_FFT_MAX)
+        return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: FFT of %d points along axis %d; use the direct sum", g.n2[d], d);
       g.L[d] = g.h[d] * g.n2[d];
+      // the interpolation's stencils start at ceil(t - w/2), t = (q - cq) L,
+      // for t in [(lo - cq) L, (hi - cq) L]: the output box, 2 points of margin
+      const double tlo = (lo[d] - g.cq[d]) * g.L[d], thi = (hi[d] - g.cq[d]) * g.L[d];
+      g.pmin[d] = (int)std::floor(tlo - 0.5 * w) - 2;
+      g.m[d] = (int)std::ceil(thi - 0.5 * w) + w - 1 + 2 - g.pmin[d] + 1;
       cells1 *= (size_t)g.n1[d];
-      cells2 *= (size_t)g.n2[d];
+      cells2 *= (size_t)g.m[d];
     }
     // copies of the spreading grid while they stay small next to L2 (32 MB):
     // about 1,000 updates of one cell from 20,000 atoms on a 40 x 40 x 18 grid
     // otherwise serialise in the atomic units
     const size_t one1 = cells1 * n_elem * sizeof(double2);
     c.copies = (int)std::max<size_t>(1, std::min<size_t>(8, (32u << 20) / std::max<size_t>(one1, 1)));
-    const size_t bytes1 = one1 * c.copies, bytes2 = cells2 * n_elem * sizeof(double2);
+    // x pass output [E][n1z][n1y][m_x], y pass output [E][n1z][m_y][m_x],
+    // z pass output (the interpolation's FP32 grid) over the box
+    const size_t bytes1 = one1 * c.copies;
+    const size_t bytes_a = (size_t)n_elem * g.n1[2] * g.n1[1] * g.m[0] * sizeof(double2);
+    const size_t bytes_b = (size_t)n_elem * g.n1[2] * g.m[1] * g.m[0] * sizeof(double2);
     const size_t bytes3 = cells2 * nufft_pack_groups(n_elem) * nufft_pack_halves(n_elem) * sizeof(float4);
     size_t free_b = 0, total_b = 0;
     CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-    const size_t have = free_b + c.small.cap + c.fine.cap + c.packed.cap;
-    if (bytes1 + 2 * bytes2 + bytes3 > have / 10 * 9)  // cuFFT's work area about the size of the grid
+    const size_t have = free_b + c.small.cap + c.fa.cap + c.fb.cap + c.packed.cap;
+    if (bytes1 + bytes_a + bytes_b + bytes3 > have / 10 * 9)
       return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: grids of %.3g GB do not fit; use the direct sum",
-                  (bytes1 + 2.0 * bytes2 + bytes3) * 1e-9);
+                  (double)(bytes1 + bytes_a + bytes_b + bytes3) * 1e-9);
     // 1 / phi2hat per spreading-grid index, and psi1hat's trapezoid coefficients
     std::vector<double> dec;
     for (int d = 0; d < 3; ++d)
@@ -1638,30 +1644,25 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
         dec.push_back(1.0 / es_hat_host((double)(l - g.n1[d] / 2) / g.n2[d], g.w2, g.beta2, 0.01));
     c.n_coef = (int)std::floor(0.5 * g.w1 / 0.25) + 1;
     for (int k = 0; k < c.n_coef; ++k) c.psi_a[k] = 0.25 * (k == 0 ? 1.0 : 2.0) * es_host(0.25 * k, g.w1, g.beta1);
+    // twiddle tables of the three transforms, after dec in one upload
+    std::vector<double2> tw((size_t)g.n2[0] + g.n2[1] + g.n2[2]);
+    size_t tw_at[3];
+    for (int d = 0, at = 0; d < 3; at += g.n2[d], ++d) {
+      tw_at[d] = at;
+      nufft_fft_twiddles(g.n2[d], tw.data() + at);
+    }
     CUDA_TRY(c.small.ensure(bytes1));
-    CUDA_TRY(c.fine.ensure(bytes2));
+    CUDA_TRY(c.fa.ensure(bytes_a));
+    CUDA_TRY(c.fb.ensure(bytes_b));
     CUDA_TRY(c.packed.ensure(bytes3));
     CUDA_TRY(c.dec.ensure(dec.size() * sizeof(double)));
+    CUDA_TRY(c.tw.ensure(tw.size() * sizeof(double2)));
     CUDA_TRY(cudaMemcpyAsync(c.dec.p, dec.data(), dec.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    const int dims[4] = {g.n2[2], g.n2[1], g.n2[0], g.n1[2]};
-    if (!c.fft_yx || std::memcmp(dims, c.fft_dims, sizeof(dims)) != 0) {
-      if (c.fft_yx) cufftDestroy(c.fft_yx);
-      if (c.fft_z) cufftDestroy(c.fft_z);
-      c.fft_yx = c.fft_z = 0;
-      int nyx[2] = {dims[1], dims[2]}, nz[1] = {dims[0]};
-      const int plane = dims[1] * dims[2];
-      bool ok = cufftPlanMany(&c.fft_yx, 2, nyx, nullptr, 1, plane, nullptr, 1, plane, CUFFT_Z2Z, dims[3] / 2) ==
-                CUFFT_SUCCESS;
-      ok = ok && cufftPlanMany(&c.fft_z, 1, nz, nz, plane, 1, nz, plane, 1, CUFFT_Z2Z, plane) == CUFFT_SUCCESS;
-      if (!ok) {
-        if (c.fft_yx) cufftDestroy(c.fft_yx);
-        if (c.fft_z) cufftDestroy(c.fft_z);
-        c.fft_yx = c.fft_z = 0;
-        return fail(SPSIM_ERR_CUDA, "NUFFT: cuFFT plans for %d x %d x %d failed", dims[0], dims[1], dims[2]);
-      }
-      std::memcpy(c.fft_dims, dims, sizeof(dims));
-    }
-    // the read-back and the dec upload above are complete when this returns
+    CUDA_TRY(cudaMemcpyAsync(c.tw.p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+    for (int d = 0; d < 3; ++d)
+      if (nufft_fft_axis(g.n2[d], g.n1[d], g.pmin[d], g.m[d], (const double2 *)c.tw.p + tw_at[d], &c.ax[d]))
+        return fail(SPSIM_ERR_UNSUPPORTED, "NUFFT: no FFT pass for %d points", g.n2[d]);
+    // the read-back and the uploads above are complete when this returns
     CUDA_TRY(cudaStreamSynchronize(st));
     c.g = g;
     c.geom_key = key;
@@ -1680,21 +1681,9 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   CUDA_TRY(cudaMemsetAsync(c.small.p, 0, cells1 * n_elem * c.copies * sizeof(double2), st));
   CUDA_TRY(nufft_spread(m->d_atomsd, (const int *)c.seg.p, n_elem, m->n_padded, g, (double2 *)c.small.p, c.copies,
                         (int *)c.flags.p, st));
-  CUDA_TRY(nufft_pad((const double2 *)c.small.p, (double2 *)c.fine.p, g, n_elem, c.copies, (const double *)c.dec.p,
-                     st));
-  if (cufftSetStream(c.fft_yx, st) != CUFFT_SUCCESS || cufftSetStream(c.fft_z, st) != CUFFT_SUCCESS)
-    return fail(SPSIM_ERR_CUDA, "NUFFT: cufftSetStream failed");
-  const long long cells2 = (long long)g.n2[0] * g.n2[1] * g.n2[2];
-  const long long plane = (long long)g.n2[0] * g.n2[1];
-  for (int e = 0; e < n_elem; ++e) {
-    cufftDoubleComplex *base = (cufftDoubleComplex *)c.fine.p + e * cells2;
-    cufftDoubleComplex *upper = base + (long long)(g.n2[2] - g.n1[2] / 2) * plane;
-    if (cufftExecZ2Z(c.fft_yx, base, base, CUFFT_FORWARD) != CUFFT_SUCCESS ||
-        cufftExecZ2Z(c.fft_yx, upper, upper, CUFFT_FORWARD) != CUFFT_SUCCESS ||
-        cufftExecZ2Z(c.fft_z, base, base, CUFFT_FORWARD) != CUFFT_SUCCESS)
-      return fail(SPSIM_ERR_CUDA, "NUFFT: cuFFT execution failed");
-  }
-  CUDA_TRY(nufft_pack((const double2 *)c.fine.p, (float4 *)c.packed.p, cells2, n_elem, st));
+  CUDA_TRY(nufft_fft3((const double2 *)c.small.p, c.copies, (const double *)c.dec.p, g, n_elem, c.ax,
+                      (double2 *)c.fa.p, (double2 *)c.fb.p, (float4 *)c.packed.p, st));
+  const long long cells2 = (long long)g.m[0] * g.m[1] * g.m[2];
   NufftInterp a;
   std::memset(&a, 0, sizeof(a));
   a.g = g;
@@ -1737,8 +1726,6 @@ static void nufft_release(int dev) {
   auto it = g_nufft.find(dev);
   if (it == g_nufft.end()) return;
   NufftCtx &c = it->second;
-  if (c.fft_yx) cufftDestroy(c.fft_yx);
-  if (c.fft_z) cufftDestroy(c.fft_z);
   if (c.h_keys) cudaFreeHost(c.h_keys);
   if (c.done) cudaEventDestroy(c.done);
   g_nufft.erase(it);  // the grids' DevBufs free themselves

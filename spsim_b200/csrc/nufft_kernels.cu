@@ -1,6 +1,6 @@
 // Non-uniform FFT structure factor kernels for sm_100a: q-box bounds, atom
-// spreading, deconvolution/zero-padding and interpolation at the pixels' q.
-// The FFT between the last two steps is cuFFT's.  The transform replaces the
+// spreading and interpolation at the pixels' q.  The deconvolution, padding
+// and FFT between the two are the passes of nufft_fft.cu.  The transform replaces the
 // reference's per-element NNFFT (src/diffraction.c:528-675, dispatched from
 // src/spsim.c:119-123): atoms -> q list, unit atom weights, then the
 // form factor of |q| with the B factor (src/diffraction.c:390-400).
@@ -179,88 +179,10 @@ cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_a
   return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// step 2: deconvolution by phi2hat into the zeroed FFT grid.  Spreading-grid
-// index l holds mode m = l - n1/2, stored at FFT index m mod n2.
-
-__global__ void nufft_scatter_kernel(const double2 *__restrict__ small, double2 *__restrict__ fine, const NufftGeom g,
-                                     int n_elem, int copies, const double *__restrict__ dec) {
-  const int n1x = g.n1[0], n1y = g.n1[1], n1z = g.n1[2];
-  const int n2x = g.n2[0], n2y = g.n2[1], n2z = g.n2[2];
-  const double *decx = dec, *decy = dec + n1x, *decz = dec + n1x + n1y;
-  const int ly = blockIdx.y;
-  for (int ez = blockIdx.z; ez < n_elem * n1z; ez += gridDim.z) {
-    const int e = ez / n1z, lz = ez - e * n1z;
-    const int pz = lz - n1z / 2 < 0 ? lz - n1z / 2 + n2z : lz - n1z / 2;
-    const int py = ly - n1y / 2 < 0 ? ly - n1y / 2 + n2y : ly - n1y / 2;
-    const double dyz = decy[ly] * decz[lz];
-    const double2 *in = small + (((long long)e * n1z + lz) * n1y + ly) * n1x;
-    double2 *out = fine + (((long long)e * n2z + pz) * n2y + py) * n2x;
-    const long long copy_stride = (long long)n_elem * n1z * n1y * n1x;
-    for (int lx = blockIdx.x * blockDim.x + threadIdx.x; lx < n1x; lx += gridDim.x * blockDim.x) {
-      const int px = lx - n1x / 2 < 0 ? lx - n1x / 2 + n2x : lx - n1x / 2;
-      double2 b = in[lx];
-      for (int k = 1; k < copies; ++k) {
-        const double2 c = in[k * copy_stride + lx];
-        b.x += c.x;
-        b.y += c.y;
-      }
-      const double d = dyz * decx[lx];
-      out[px] = make_double2(b.x * d, b.y * d);
-    }
-  }
-}
-
-cudaError_t nufft_pad(const double2 *small, double2 *fine, const NufftGeom &g, int n_elem, int copies,
-                      const double *dec, cudaStream_t st) {
-  const size_t cells2 = (size_t)g.n2[0] * g.n2[1] * g.n2[2];
-  cudaError_t e = cudaMemsetAsync(fine, 0, cells2 * n_elem * sizeof(double2), st);
-  if (e != cudaSuccess) return e;
-  const int threads = 128;
-  dim3 grid((unsigned)std::min((g.n1[0] + threads - 1) / threads, 8), (unsigned)g.n1[1],
-            (unsigned)std::min(n_elem * g.n1[2], 65535));
-  nufft_scatter_kernel<<<grid, threads, 0, st>>>(small, fine, g, n_elem, std::max(copies, 1), dec);
-  return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
-// step 3b: the FFT output, FP64 [e][z][y][x], packed for the interpolation as
-// FP32 complex with the elements interleaved: [group][z][y][x][H float4], each
-// float4 holding two elements (re, im, re, im); absent elements are zero.  FP32
-// storage adds a relative error of ~4e-9 to F, below the rounding of the
-// complex64 output.
-
-template <int H>
-__global__ void nufft_pack_kernel(const double2 *__restrict__ fine, float4 *__restrict__ packed, long long cells2,
-                                  int n_elem, int n_groups) {
-  const long long total = cells2 * n_groups;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long grp = i / cells2, c = i - grp * cells2;
-#pragma unroll
-    for (int h = 0; h < H; ++h) {
-      const int e0 = (int)grp * 2 * H + 2 * h;
-      double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
-      if (e0 < n_elem) a = fine[(long long)e0 * cells2 + c];
-      if (e0 + 1 < n_elem) b = fine[(long long)(e0 + 1) * cells2 + c];
-      packed[i * H + h] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
-    }
-  }
-}
-
+// the interpolation's FP32 grid holds elements in groups of 2 x halves,
+// halves float4 (two elements each) per cell and group
 int nufft_pack_halves(int n_elem) { return n_elem <= 2 ? 1 : 2; }
 int nufft_pack_groups(int n_elem) { return (n_elem + 2 * nufft_pack_halves(n_elem) - 1) / (2 * nufft_pack_halves(n_elem)); }
-
-cudaError_t nufft_pack(const double2 *fine, float4 *packed, long long cells2, int n_elem, cudaStream_t st) {
-  const int H = nufft_pack_halves(n_elem), G = nufft_pack_groups(n_elem);
-  const long long total = cells2 * G;
-  const unsigned blocks = (unsigned)std::min<long long>((total + 255) / 256, 148 * 16);
-  if (H == 1)
-    nufft_pack_kernel<1><<<blocks, 256, 0, st>>>(fine, packed, cells2, n_elem, G);
-  else
-    nufft_pack_kernel<2><<<blocks, 256, 0, st>>>(fine, packed, cells2, n_elem, G);
-  return cudaGetLastError();
-}
 
 // ---------------------------------------------------------------------------
 // step 4: interpolation at each pixel's q, form factors, deconvolution by
@@ -294,7 +216,7 @@ __device__ __forceinline__ void ld_cell32(const float4 *p, float4 &a, float4 &b)
 constexpr int INTERP_TX = 16, INTERP_TY = 8;
 
 template <int W, int H>
-__global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant__ NufftInterp a) {
+__global__ void __launch_bounds__(128, W <= 11 ? 3 : 1) nufft_interp_kernel(const __grid_constant__ NufftInterp a) {
   long long p;
   if (a.tile_nx > 0) {
     const int tiles_x = (a.tile_nx + INTERP_TX - 1) / INTERP_TX;
@@ -325,7 +247,6 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
     q[1] = R[3] * h0 + R[4] * h1 + R[5] * h2;
     q[2] = R[6] * h0 + R[7] * h1 + R[8] * h2;
   }
-  const int n2x = g.n2[0], n2y = g.n2[1], n2z = g.n2[2];
   double t[3];
   int b[3];
   double D = 1.0;
@@ -334,8 +255,9 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
     t[d] = qp * g.L[d];
     const double p0 = ceil(t[d] - 0.5 * W);
     t[d] -= p0;  // stencil offsets: t - i, i = 0 .. W-1
-    const int s = (int)p0 % g.n2[d];
-    b[d] = s < 0 ? s + g.n2[d] : s;
+    // stencil start in the output box; the box holds every q of the list
+    // with a margin, the clamp only keeps the reads inside it
+    b[d] = min(max((int)p0 - g.pmin[d], 0), g.m[d] - W);
     D *= psi1_hat(g.h[d] * qp, a.psi_a, a.n_coef);
   }
   const double ihw = 2.0 / W;
@@ -346,15 +268,15 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
   for (int i = 0; i < W; ++i) {
     kx[i] = (float)es_kernel(t[0] - i, ihw, g.beta2);
     ky[i] = es_kernel(t[1] - i, ihw, g.beta2);
-    ix[i] = (b[0] + i >= n2x ? b[0] + i - n2x : b[0] + i) * H;
-    iy[i] = b[1] + i >= n2y ? b[1] + i - n2y : b[1] + i;
+    ix[i] = (b[0] + i) * H;
+    iy[i] = b[1] + i;
   }
   // |q| of the unrotated list for the form factors, as the direct path
   const double s2 = [&] {
     const double d = sqrt(h0 * h0 + h1 * h1 + h2 * h2) * 1e-10;
     return d * d * 0.25;
   }();
-  const long long row_stride = (long long)n2x * H, plane_stride = row_stride * n2y;
+  const long long row_stride = (long long)g.m[0] * H, plane_stride = row_stride * g.m[1];
   double fr = 0.0, fi = 0.0;
   for (int grp = 0; grp < a.n_groups; ++grp) {
     const float4 *gr = a.packed + (long long)grp * a.cell2 * H;
@@ -363,8 +285,7 @@ __global__ void __launch_bounds__(128) nufft_interp_kernel(const __grid_constant
     for (int k = 0; k < 4 * H; ++k) acc[k] = 0.0;
     for (int iz = 0; iz < W; ++iz) {
       const double kz = es_kernel(t[2] - iz, ihw, g.beta2);
-      const int zz = b[2] + iz >= n2z ? b[2] + iz - n2z : b[2] + iz;
-      const float4 *plane = gr + (long long)zz * plane_stride;
+      const float4 *plane = gr + (long long)(b[2] + iz) * plane_stride;
 #pragma unroll
       for (int jy = 0; jy < W; ++jy) {
         const float4 *row = plane + (long long)iy[jy] * row_stride;

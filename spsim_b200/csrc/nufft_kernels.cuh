@@ -7,8 +7,9 @@
 //               q box, h = 1 / (2 sigma1 S), S = half-width of the q box)
 //   2. pad      b_l / phi2hat((l - n1/2) / n2) into an n2 = sigma2 n1 grid at
 //               index (l - n1/2) mod n2, zeros elsewhere
-//   3. FFT      forward (e^{-2 pi i m p / n2}) over the n2 grid (cuFFT, batched
-//               over elements), then packed as FP32 with the elements interleaved
+//   3. FFT      forward (e^{-2 pi i m p / n2}) over the n2 grid: pruned x, y, z
+//               passes (steps 2 and 3 together, only the output box that step 4
+//               reads), written as FP32 with the elements interleaved
 //   4. interp   T(q') = sum_p g_p phi2(n2 h q' - p), F = e^{-2 pi i q.c}
 //               sum_e f_e T_e(q') / prod_d psi1hat(h_d q'_d)
 // psi1, phi2: "exponential of semicircle" kernels exp(beta (sqrt(1 - (2u/w)^2) - 1))
@@ -36,6 +37,45 @@ struct NufftGeom {
   double L[3];        // h n2: q' (1/m) -> FFT-grid coordinate
   double cq[3];       // centre of the q box (1/m)
   double center[3];   // molecule centre (m)
+  int pmin[3];        // FFT output box read by the interpolation: frequency indices
+  int m[3];           // pmin .. pmin + m - 1 (taken mod n2), m along each axis
+};
+
+// One axis of the pruned FFT passes (nufft_fft.cu)
+constexpr int NUFFT_FFT_MAX = 6144;  // longest transform: two FP64 lines in shared memory
+struct FftAxis {
+  int n;        // transform length (n2 along the axis)
+  int nin;      // input points: spreading-grid index l at frequency index (l - nin/2) mod n
+  int nout;     // output points: box index i from frequency index (p0 + i) mod n
+  int p0;
+  int ld;       // shared-memory line stride (double2): n + n/8 padding slots, 1 mod 8
+  int nst;      // Stockham stages and their radices (odd ones first)
+  int rad[16];
+  const double2 *tw;  // device: exp(-2 pi i k / n), k < n
+};
+struct FftPassX {
+  FftAxis ax;
+  const double2 *small;  // spreading grid, copies x [E][n1z][n1y][n1x]
+  long long copy_stride;
+  int copies;
+  const double *dec;     // 1 / phi2hat per spreading-grid index: x, then y, then z
+  int n1y, n1z;
+  long long lines;       // E n1z n1y
+  int per_cta;
+  double2 *out;          // [E][n1z][n1y][mx]
+};
+struct FftPassY {
+  FftAxis ax;
+  const double2 *in;     // [E][n1z][n1y][mx]
+  double2 *out;          // [E][n1z][my][mx]
+  int mx, per_cta;
+};
+struct FftPassZ {
+  FftAxis ax;
+  const double2 *in;     // [E][n1z][my][mx]
+  float2 *packed;        // [groups][mz][my][mx][slots]
+  int mx, my, n_elem, slots, n_groups;
+  int per_cta, per_elem;
 };
 
 struct NufftInterp {
@@ -48,8 +88,8 @@ struct NufftInterp {
   double rot[9];      // q' = R q (row-major)
   int npat;           // patterns (blockIdx.y); outputs [npat][npix]
   const double *rots; // device, 9 per pattern (row-major), or nullptr (then has_rot / rot)
-  const float4 *packed;  // [n_groups][n2z][n2y][n2x][halves] (nufft_pack)
-  long long cell2;       // n2x n2y n2z
+  const float4 *packed;  // [n_groups][m_z][m_y][m_x][halves] (the z pass of nufft_fft3)
+  long long cell2;       // box cells m_x m_y m_z
   int halves;            // float4 per cell and group (two elements each)
   int n_groups;
   int n_elem;
@@ -81,11 +121,16 @@ cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_a
 // then z.
 cudaError_t nufft_pad(const double2 *small, double2 *fine, const NufftGeom &g, int n_elem, int copies,
                       const double *dec, cudaStream_t st);
-// Step 3b: FP32 element-interleaved copy of the FFT output for step 4
-// (nufft_pack_groups(n_elem) x cells2 x nufft_pack_halves(n_elem) float4).
+// Steps 2-3 by the hand-written passes: x (with the sum of the spreading-grid
+// copies and the deconvolution), y, z (with the FP32 element-interleaved
+// output of nufft_pack_groups(n_elem) x box cells x nufft_pack_halves(n_elem)
+// float4).  fa: E n1z n1y m_x, fb: E n1z m_y m_x double2.
 int nufft_pack_halves(int n_elem);
 int nufft_pack_groups(int n_elem);
-cudaError_t nufft_pack(const double2 *fine, float4 *packed, long long cells2, int n_elem, cudaStream_t st);
+int nufft_fft_axis(int n, int nin, int pmin, int nout, const double2 *tw, FftAxis *ax);  // 0, or -1: n unsupported
+void nufft_fft_twiddles(int n, double2 *tw);  // host table exp(-2 pi i k / n)
+cudaError_t nufft_fft3(const double2 *small, int copies, const double *dec, const NufftGeom &g, int n_elem,
+                       const FftAxis ax[3], double2 *fa, double2 *fb, float4 *packed, cudaStream_t st);
 // Step 4.
 cudaError_t nufft_interp(const NufftInterp &a, cudaStream_t st);
 
