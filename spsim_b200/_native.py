@@ -135,6 +135,8 @@ _SIGNATURES = {
     "spsim_b200_get_legacy_nufft_eps": (c_double, []),
     "spsim_b200_get_legacy_precision": (c_int, []),
     "spsim_b200_set_noise_seed": (None, [c_uint64]),
+    "spsim_b200_set_shot_chunks": (None, [c_int]),
+    "spsim_b200_get_shot_chunks": (c_int, []),
 }
 
 _lock = threading.Lock()

@@ -688,6 +688,8 @@ static bool is_orthonormal(const double *R) {
   return true;
 }
 
+static thread_local long long g_split_pixels_hint = 0;  // pixels of the whole shot while a shot part is planned
+
 static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
                       const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
                       cudaStream_t stream, const Spectrum *spec) {
@@ -872,6 +874,9 @@ static int build_plan(Plan &pl, int npat, const spsim_b200_molecule *const *mols
     const long long slots = (long long)num_sms() * occ;
     long long total_ptiles = 0;
     for (int i = 0; i < npat; ++i) total_ptiles += (qsets[i]->npix + tile_pix - 1) / tile_pix;
+    // a row chunk of a pipelined shot splits its atoms as the whole shot
+    // would: the next chunk, on the other stream, fills this one's tail
+    if (g_split_pixels_hint > 0) total_ptiles = std::max(total_ptiles, (g_split_pixels_hint + tile_pix - 1) / tile_pix);
     // split atoms when pixel tiles alone cannot fill the GPU several times over
     const long long want = 6 * slots;
     std::vector<WorkItem> items;
@@ -1019,7 +1024,8 @@ static int check_flags(Plan &pl) {
 // waited for; spsim_internal_shot_check reads its error flags afterwards.
 static int run_forward(int npat, const spsim_b200_molecule *const *mols, const spsim_b200_qset *const *qsets,
                        const double *rot, float B, int precision, float *const *F_dev, float *const *I_dev,
-                       cudaStream_t stream, bool cache, const Spectrum *spec = nullptr, bool sync = true) {
+                       cudaStream_t stream, bool cache, const Spectrum *spec = nullptr, bool sync = true,
+                       Plan *scratch = nullptr) {
   if (npat < 0) return fail(SPSIM_ERR_INVALID_ARG, "npatterns < 0");
   if (npat == 0) return SPSIM_OK;
   if (!mols || !qsets) return fail(SPSIM_ERR_INVALID_ARG, "NULL molecule or q-set array");
@@ -1062,14 +1068,19 @@ static int run_forward(int npat, const spsim_b200_molecule *const *mols, const s
     g_plans.push_back(std::move(np));
     pl = g_plans.back().get();
   } else if (!pl) {
-    // one-shot calls rebuild the descriptors of this thread's scratch plan,
-    // whose device buffers only grow (no cudaMalloc / cudaFree per call)
+    // one-shot calls rebuild the descriptors of this thread's scratch plan (or
+    // the caller's), whose device buffers only grow (no cudaMalloc / cudaFree
+    // per call)
     OneShot &os = g_oneshot;
-    if (!os.plan || os.device != dev) {
-      os.plan = new Plan();  // a plan left on another device is kept, not freed, while its context may be busy
-      os.device = dev;
+    if (scratch) {
+      pl = scratch;
+    } else {
+      if (!os.plan || os.device != dev) {
+        os.plan = new Plan();  // a plan left on another device is kept, not freed, while its context may be busy
+        os.device = dev;
+      }
+      pl = os.plan;
     }
-    pl = os.plan;
     pl->key_ptrs = kp;
     pl->key_vals = kv;
     st = build_plan(*pl, npat, mols, qsets, rot, B, precision, F_dev, I_dev, stream, spec);
@@ -1207,6 +1218,12 @@ struct HostSession {
   spsim_b200_qset *qs = nullptr;
   DevBuf *F = nullptr, *I = nullptr;
   DevBuf *stats = nullptr;  // four words for the device q-set statistics
+  // the pipelined simulate_shot: per row chunk a view of qs (its pixels, the
+  // whole list's statistics) and a scratch plan; parts: chunks of this shot
+  std::vector<spsim_b200_qset *> views;
+  std::vector<Plan *> part_plans;
+  int parts = 0;
+  spsim_b200_qset *shot_q = nullptr;  // the shot's whole HKL list, borrowed (no copy)
 };
 static thread_local HostSession g_host;
 static thread_local spsim_b200_molecule *g_shot_mol = nullptr;  // set by spsim_internal_shot_molecule
@@ -1298,6 +1315,16 @@ extern "C" void spsim_internal_release_host_session(void) {
     delete g_host.F;
     delete g_host.I;
     delete g_host.stats;
+    // the shot's q sets borrow their lists: detach before deleting
+    for (spsim_b200_qset *v : g_host.views) {
+      v->d_hkl = nullptr;
+      delete v;
+    }
+    if (g_host.shot_q) {
+      g_host.shot_q->d_hkl = nullptr;
+      delete g_host.shot_q;
+    }
+    for (Plan *p : g_host.part_plans) delete p;
   }
   g_host = HostSession();
   g_shot_mol = nullptr;
@@ -1392,6 +1419,7 @@ extern "C" int spsim_internal_shot_molecule(int natoms, const int32_t *Z, const 
     g_host.device = dev;
   }
   g_shot_mol = nullptr;
+  g_host.parts = 0;
   spsim_b200_molecule *m = nullptr;
   st = host_session_molecule(natoms, Z, pos, nullptr, nullptr, delta_atoms, beam, &m);
   if (st) return st;
@@ -1426,6 +1454,72 @@ extern "C" int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z
                           false);
 }
 
+// The pipelined simulate_shot (monochromatic direct sum): the session q set
+// takes the whole HKL list once (its statistics decide the kernel form of
+// every chunk), then each row chunk [p0, p1) runs on a view of it with its own
+// scratch plan, on the caller's stream, not waited for.
+extern "C" int spsim_internal_shot_parts_begin(int64_t npix, const float *hkl_dev) {
+  if (npix < 0 || (npix > 0 && !hkl_dev)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (g_host.device != dev || !g_shot_mol || g_shot_mol != g_host.mol)
+    return fail(SPSIM_ERR_INVALID_ARG, "no shot molecule on this device");
+  // the caller's list stays put for the shot: borrowed, not copied (a device
+  // copy would queue behind the list's copy to the host on the copy engine)
+  if (!g_host.shot_q) g_host.shot_q = new spsim_b200_qset();
+  spsim_b200_qset *q = g_host.shot_q;
+  q->device = dev;
+  q->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
+  q->npix = npix;
+  q->d_hkl = const_cast<float *>(hkl_dev);
+  q->d_q64 = nullptr;
+  q->cap_bytes = 0;
+  if (!g_host.stats) g_host.stats = new DevBuf();
+  CUDA_TRY(g_host.stats->ensure(4 * sizeof(unsigned long long)));
+  double steps[3];
+  CUDA_TRY(qset_stats(q->d_hkl, npix, (unsigned long long *)g_host.stats->p, &q->qmax, steps, nullptr));
+  q->pair_step = steps[0];
+  q->quad_step1 = steps[1];
+  q->quad_step2 = steps[2];
+  g_host.parts = 0;
+  return SPSIM_OK;
+}
+
+extern "C" int spsim_internal_shot_part(int64_t p0, int64_t p1, float B, int precision, float *F_dev, float *I_dev,
+                                        void *stream) {
+  spsim_b200_qset *q = g_host.shot_q;
+  spsim_b200_molecule *m = g_host.mol;
+  if (!q || !m || g_shot_mol != m) return fail(SPSIM_ERR_INVALID_ARG, "shot parts without a prepared shot");
+  if (p0 < 0 || p1 > q->npix || p0 >= p1 || p0 % 4) return fail(SPSIM_ERR_INVALID_ARG, "bad shot part");
+  const int k = g_host.parts;
+  if ((int)g_host.views.size() <= k) {
+    g_host.views.push_back(new spsim_b200_qset());
+    g_host.part_plans.push_back(new Plan());
+  }
+  spsim_b200_qset *v = g_host.views[k];
+  v->device = q->device;
+  v->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
+  v->npix = p1 - p0;
+  v->d_hkl = q->d_hkl + 3 * p0;  // borrowed: views own no device memory
+  v->d_q64 = nullptr;
+  v->cap_bytes = 0;
+  v->qmax = q->qmax;
+  v->pair_step = q->pair_step;
+  v->quad_step1 = q->quad_step1;
+  v->quad_step2 = q->quad_step2;
+  g_host.parts = k + 1;
+  float *F[1] = {F_dev + 2 * p0};
+  float *I[1] = {I_dev + p0};
+  const spsim_b200_qset *qv = v;
+  const spsim_b200_molecule *mc = m;
+  g_split_pixels_hint = q->npix;
+  const int st = run_forward(1, &mc, &qv, nullptr, B, precision, F, I, (cudaStream_t)stream, false, nullptr, false,
+                             g_host.part_plans[k]);
+  g_split_pixels_hint = 0;
+  return st;
+}
+
 static int nufft_check_flags(int dev);
 
 extern "C" int spsim_internal_shot_check(void) {
@@ -1435,6 +1529,15 @@ extern "C" int spsim_internal_shot_check(void) {
     std::lock_guard<std::mutex> lk(g_mu);
     int st = nufft_check_flags(dev);
     if (st) return st;
+  }
+  if (g_host.parts > 0) {
+    const int n = g_host.parts;
+    g_host.parts = 0;
+    for (int k = 0; k < n; ++k) {
+      const int st = check_flags(*g_host.part_plans[k]);
+      if (st) return st;
+    }
+    return SPSIM_OK;
   }
   if (!g_oneshot.plan) return SPSIM_OK;
   return check_flags(*g_oneshot.plan);
@@ -2093,6 +2196,10 @@ static int chain_dev(const spsim_b200_chain_params *p, ChainDev *c) {
   c->maxv = p->maximum_value;
   c->seed = p->seed;
   c->pattern = p->pattern_index;
+  c->i0 = 0;
+  c->i1 = (long long)p->nx * p->ny * p->nz;
+  c->b0 = 0;
+  c->b1 = (long long)(p->nx / p->binning_x) * (p->ny / p->binning_y) * (p->nz / p->binning_z);
   return SPSIM_OK;
 }
 
@@ -2119,6 +2226,33 @@ extern "C" int spsim_b200_detector_chain(const spsim_b200_chain_params *p, const
     sel = (float *)g_chain_el.p;
   }
   CUDA_TRY(launch_chain(c, I_dev, o, sph, sel, (cudaStream_t)stream));
+  return SPSIM_OK;
+}
+
+// Rows [row0, row1) of a flat detector's fused chain (library-internal, the
+// pipelined simulate_shot): the pixels' and bins' values are those of the
+// whole-detector call, as every pixel keeps its index (Philox counter) and
+// row0 (and row1, unless it is ny) is a multiple of the y binning.
+extern "C" int spsim_internal_chain_rows(const spsim_b200_chain_params *p, const float *I_dev,
+                                         const spsim_b200_chain_outputs *out, int64_t row0, int64_t row1,
+                                         void *stream) {
+  ChainDev c;
+  int st = chain_dev(p, &c);
+  if (st) return st;
+  if (!out || !I_dev) return fail(SPSIM_ERR_INVALID_ARG, "outputs or intensities are NULL");
+  if (p->nz != 1 || row0 < 0 || row1 > p->ny || row0 > row1 || row0 % p->binning_y ||
+      (row1 != p->ny && row1 % p->binning_y))
+    return fail(SPSIM_ERR_INVALID_ARG, "chain rows [%lld, %lld) of %d", (long long)row0, (long long)row1, p->ny);
+  if (!c.unbinned && (!out->photons_per_pixel || !out->electrons_per_pixel))
+    return fail(SPSIM_ERR_INVALID_ARG, "binned chain rows need the photon and electron arrays");
+  const long long bnx = p->nx / p->binning_x;
+  c.i0 = row0 * p->nx;
+  c.i1 = row1 * p->nx;
+  c.b0 = row0 / p->binning_y * bnx;
+  c.b1 = std::min<long long>(row1 / p->binning_y, p->ny / p->binning_y) * bnx;
+  ChainOut o = {out->thomson_correction, out->solid_angle,  out->photons_per_pixel, out->photon_count,
+                out->electrons_per_pixel, out->real_output, out->noiseless_output};
+  CUDA_TRY(launch_chain(c, I_dev, o, nullptr, nullptr, (cudaStream_t)stream));
   return SPSIM_OK;
 }
 

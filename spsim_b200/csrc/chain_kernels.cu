@@ -140,9 +140,8 @@ __device__ __forceinline__ float solid_angle_factor(const ChainDev &c, int x, in
 // ---- fused chain -------------------------------------------------------------
 
 __global__ void chain_pixel_kernel(ChainDev c, const float *__restrict__ I, ChainOut o) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long n = (long long)c.nx * c.ny * c.nz;
-  if (i >= n) return;
+  const long long i = c.i0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.i1) return;
   const int x = (int)(i % c.nx);
   const int y = (int)((i / c.nx) % c.ny);
   const float T = thomson_factor(c, x, y);
@@ -174,9 +173,9 @@ __global__ void chain_pixel_kernel(ChainDev c, const float *__restrict__ I, Chai
 // Binned outputs (binning > 1): sums in the reference's loop order.
 __global__ void chain_bin_kernel(ChainDev c, const float *__restrict__ photons, const float *__restrict__ electrons,
                                  float *__restrict__ real_out, float *__restrict__ noiseless) {
-  const int bnx = c.nx / c.bx, bny = c.ny / c.by, bnz = c.nz / c.bz;
-  const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= (long long)bnx * bny * bnz) return;
+  const int bnx = c.nx / c.bx, bny = c.ny / c.by;
+  const long long b = c.b0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= c.b1) return;
   const int x = (int)(b % bnx), y = (int)((b / bnx) % bny), z = (int)(b / ((long long)bnx * bny));
   float acc_r = 0.0f, acc_n = 0.0f;
   for (int zi = 0; zi < c.bz; ++zi)
@@ -246,7 +245,7 @@ cudaError_t launch_electrons(const ChainDev &c, const float *cnt, float *out, cu
 
 cudaError_t launch_binned(const ChainDev &c, const float *electrons, const float *photons, float *real_out,
                           float *noiseless, cudaStream_t st) {
-  const long long nb = (long long)(c.nx / c.bx) * (c.ny / c.by) * (c.nz / c.bz);
+  const long long nb = c.b1 - c.b0;
   if (nb <= 0) return cudaSuccess;
   chain_bin_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(c, photons, electrons, real_out, noiseless);
   return cudaGetLastError();
@@ -254,7 +253,7 @@ cudaError_t launch_binned(const ChainDev &c, const float *electrons, const float
 
 cudaError_t launch_chain(const ChainDev &c, const float *I, const ChainOut &o, float *scratch_ph, float *scratch_el,
                          cudaStream_t st) {
-  const long long n = (long long)c.nx * c.ny * c.nz;
+  const long long n = c.i1 - c.i0;
   if (n <= 0) return cudaSuccess;
   ChainOut po = o;
   if (!c.unbinned) {
@@ -267,7 +266,7 @@ cudaError_t launch_chain(const ChainDev &c, const float *I, const ChainOut &o, f
   chain_pixel_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c, I, po);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || c.unbinned || (!o.noiseless && !o.real_out) || !I) return e;
-  const long long nb = (long long)(c.nx / c.bx) * (c.ny / c.by) * (c.nz / c.bz);
+  const long long nb = c.b1 - c.b0;
   if (nb <= 0) return cudaSuccess;
   chain_bin_kernel<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(c, po.photons, po.electrons, o.real_out,
                                                                  o.noiseless);

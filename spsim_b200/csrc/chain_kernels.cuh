@@ -24,6 +24,8 @@ struct ChainDev {
   float maxv;
   uint64_t seed;
   uint32_t pattern;
+  long long i0, i1;      // pixels [i0, i1) of the fused chain (row ranges of a pipelined shot)
+  long long b0, b1;      // bins [b0, b1) of the binning pass
 };
 
 struct ChainOut {

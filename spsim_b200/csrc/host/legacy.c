@@ -112,6 +112,11 @@ int spsim_internal_shot_structure_factor_nufft(int natoms, const int32_t *Z, con
                                                float *F_dev, float *I_dev);
 int spsim_internal_shot_check(void);
 int spsim_internal_shot_molecule(int natoms, const int32_t *Z, const float *pos, int delta_atoms, const float *beam);
+int spsim_internal_shot_parts_begin(int64_t npix, const float *hkl_dev);
+int spsim_internal_shot_part(int64_t p0, int64_t p1, float B, int precision, float *F_dev, float *I_dev,
+                             void *stream);
+int spsim_internal_chain_rows(const spsim_b200_chain_params *p, const float *I_dev,
+                              const spsim_b200_chain_outputs *out, int64_t row0, int64_t row1, void *stream);
 int spsim_internal_rotate_hkl(int64_t npix, const float R[9], float *hkl_dev);
 
 /* Pinned staging buffer of simulate_shot's device-to-host copies (grow-only,
@@ -120,6 +125,13 @@ static void *g_pinned = NULL;
 static size_t g_pinned_bytes = 0;
 static cudaStream_t g_copy_stream = NULL; /* non-blocking side stream of simulate_shot */
 static int g_copy_stream_device = -1;
+/* the pipelined simulate_shot's two compute streams (row chunks alternate) */
+static cudaStream_t g_comp_stream[2] = {NULL, NULL};
+static int g_comp_stream_device = -1;
+static int g_shot_chunks = 0; /* row chunks of simulate_shot: 0 automatic, 1 none */
+
+void spsim_b200_set_shot_chunks(int chunks) { g_shot_chunks = chunks < 0 ? 0 : chunks; }
+int spsim_b200_get_shot_chunks(void) { return g_shot_chunks; }
 
 static void *pinned_alloc(size_t bytes) {
   if (g_pinned && g_pinned_bytes >= bytes) return g_pinned;
@@ -147,6 +159,11 @@ void spsim_b200_release_scratch(void) {
   if (g_copy_stream && g_copy_stream_device == dev) cudaStreamDestroy(g_copy_stream);
   g_copy_stream = NULL;
   g_copy_stream_device = -1;
+  for (int k = 0; k < 2; k++) {
+    if (g_comp_stream[k] && g_comp_stream_device == dev) cudaStreamDestroy(g_comp_stream[k]);
+    g_comp_stream[k] = NULL;
+  }
+  g_comp_stream_device = -1;
   spsim_internal_release_host_session();
 }
 
@@ -592,6 +609,50 @@ void calculate_noiseless_detector_output(CCD *det, Experiment *experiment) {
 
 /* ------------------------------------------------------------ orchestration */
 
+/* simulate_shot's HKL list to the pinned staging buffer on the copy stream,
+ * after the work queued so far on the legacy stream; ev is recorded after it */
+static void queue_hkl_copy(cudaEvent_t ev, char *s_hkl, const float *d_hkl, size_t bytes) {
+  cudaEventRecord(ev, 0);
+  cudaStreamWaitEvent(g_copy_stream, ev, 0);
+  if (bytes) {
+    cudaError_t e = cudaMemcpyAsync(s_hkl, d_hkl, bytes, cudaMemcpyDeviceToHost, g_copy_stream);
+    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync HKL", e);
+  }
+  cudaEventRecord(ev, g_copy_stream);
+}
+
+/* Row chunks of the pipelined simulate_shot for a flat detector's direct,
+ * monochromatic structure factor (others: 1), as row boundaries rb[0..K].
+ * Automatic: 4 from 2^19 pixels on.  The last chunk, whose copies to the
+ * host nothing hides, gets a quarter of the others' rows.  Chunk rows are a
+ * multiple of the y binning and give a pixel count that is a multiple of 4
+ * (the neighbour-quad kernel's alignment). */
+enum { MAX_SHOT_CHUNKS = 8 };
+static int shot_row_chunks(const CCD *det, long long n, int nfft, int poly, int vol, long long *rb) {
+  rb[0] = 0;
+  rb[1] = det->ny;
+  if (vol || nfft || poly || n <= 0) return 1;
+  int k = g_shot_chunks > 0 ? g_shot_chunks : (n >= (1LL << 19) ? 4 : 1);
+  if (k > MAX_SHOT_CHUNKS) k = MAX_SHOT_CHUNKS;
+  if (k <= 1) return 1;
+  const int q = det->nx % 4 == 0 ? 1 : det->nx % 2 == 0 ? 2 : 4;
+  int unit = det->binning_y;
+  while (unit % q) unit += det->binning_y; /* lcm(binning_y, q) */
+  /* rows: k - 1 chunks of 4 parts and one of 1 part, in units */
+  const long long units = (det->ny + unit - 1) / unit, parts = 4LL * (k - 1) + 1;
+  long long last = units / parts;
+  if (last < 1) last = 1;
+  const long long rest = units - last;
+  if (rest < k - 1) return 1;
+  int chunks = 0;
+  for (int c = 0; c < k - 1; c++) {
+    const long long hi = rest * (c + 1) / (k - 1) * unit;
+    if (hi > rb[chunks]) rb[++chunks] = hi < det->ny ? hi : det->ny;
+  }
+  if (rb[chunks] < det->ny) rb[++chunks] = det->ny;
+  return chunks;
+}
+
 /* src/spsim.c:281-346 as one device pipeline with the reference's outputs:
  * the HKL list is computed and rotated on the device (bit-identical to
  * get_HKL_list and apply_orientation_to_HKL_list), the structure factor and
@@ -653,7 +714,9 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   cudaError_t e = cudaEventCreateWithFlags(&ev_hkl, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming);
   if (e != cudaSuccess) cuda_die("cudaEventCreate", e);
-  /* the HKL list goes down on a side stream, beside the structure factor */
+  /* the HKL list goes down on a side stream, beside the structure factor;
+   * it is queued once the structure factor's q-set statistics have come
+   * back, which would otherwise wait behind it on the copy engine */
   int cur_dev = 0;
   cudaGetDevice(&cur_dev);
   if (!g_copy_stream || g_copy_stream_device != cur_dev) { /* a stream left on another device is kept */
@@ -661,13 +724,6 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
     if (e != cudaSuccess) cuda_die("cudaStreamCreate", e);
     g_copy_stream_device = cur_dev;
   }
-  cudaEventRecord(ev_hkl, 0);
-  cudaStreamWaitEvent(g_copy_stream, ev_hkl, 0);
-  if (n > 0) {
-    e = cudaMemcpyAsync(s_hkl, d_hkl, b_hkl, cudaMemcpyDeviceToHost, g_copy_stream);
-    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync HKL", e);
-  }
-  cudaEventRecord(ev_hkl, g_copy_stream);
 
   /* structure factor (compute_sf, src/spsim.c:110-144): the CUDA dispatch decides the spectrum */
   const int spectrum = opts->use_cuda != 0 && opts->use_cuda != 2;
@@ -683,46 +739,105 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   }
   float *dF = (float *)dev_alloc(SLOT_SHOT_F, b_F > 0 ? b_F : 8);
   float *dI = (float *)dev_alloc(SLOT_SHOT_I, b_I > 0 ? b_I : 4);
-  if (opts->use_nfft_for_sf)
-    st = spsim_internal_shot_structure_factor_nufft(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
-                                                    opts->delta_atoms, n, d_hkl, g_nufft_eps, dF, dI);
-  else
-    st = spsim_internal_shot_structure_factor(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
-                                              opts->delta_atoms, beam, poly ? exp->wavelength : 0.0f,
-                                              poly ? exp->bandwidth : 0.0f, poly ? samples : 1, n, d_hkl,
-                                              g_precision, dF, dI);
-  if (st) die("simulate_shot structure factor", st);
-
-  /* F and |F|^2 go down ahead of the chain, so the host can copy them out
-   * while the chain's arrays are still in flight */
-  cudaEvent_t ev_fi;
-  e = cudaEventCreateWithFlags(&ev_fi, cudaEventDisableTiming);
-  if (e != cudaSuccess) cuda_die("cudaEventCreate", e);
-  if (n > 0) {
-    e = cudaMemcpyAsync(s_F, dF, b_F, cudaMemcpyDeviceToHost, 0);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(s_I, dI, b_I, cudaMemcpyDeviceToHost, 0);
-    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync F, I", e);
-  }
-  cudaEventRecord(ev_fi, 0);
-
-  /* detector chain on the device intensities (src/spsim.c:300-336) */
   spsim_b200_chain_params p = chain_params(det, exp);
   float *bufs[7];
   for (int k = 0; k < 5; k++) bufs[k] = (float *)dev_alloc(SLOT_SHOT_0 + k, sizeof(float) * np);
   bufs[5] = (float *)dev_alloc(SLOT_SHOT_0 + 5, sizeof(float) * nb);
   bufs[6] = (float *)dev_alloc(SLOT_SHOT_0 + 6, sizeof(float) * nb);
   spsim_b200_chain_outputs o = {bufs[0], bufs[1], bufs[2], bufs[3], bufs[4], bufs[5], bufs[6]};
-  st = spsim_b200_detector_chain(&p, dI, &o, NULL);
-  if (st) die("simulate_shot detector chain", st);
-  if (n > 0) {
-    for (int k = 0; k < 7 && e == cudaSuccess; k++) {
-      const size_t b = k < 5 ? b_I : b_nb;
-      if (b) e = cudaMemcpyAsync(s_chain + (k < 5 ? k * b_I : 5 * b_I + (k - 5) * b_nb), bufs[k], b,
-                                 cudaMemcpyDeviceToHost, 0);
+  long long rb[MAX_SHOT_CHUNKS + 1];
+  const int K = shot_row_chunks(det, n, opts->use_nfft_for_sf, poly, vol, rb);
+  const long long bnx = det->nx / det->binning_x;
+  cudaEvent_t ev_fi = NULL, ev_copied[MAX_SHOT_CHUNKS];
+
+  if (K == 1) {
+    if (opts->use_nfft_for_sf)
+      st = spsim_internal_shot_structure_factor_nufft(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
+                                                      opts->delta_atoms, n, d_hkl, g_nufft_eps, dF, dI);
+    else
+      st = spsim_internal_shot_structure_factor(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
+                                                opts->delta_atoms, beam, poly ? exp->wavelength : 0.0f,
+                                                poly ? exp->bandwidth : 0.0f, poly ? samples : 1, n, d_hkl,
+                                                g_precision, dF, dI);
+    if (st) die("simulate_shot structure factor", st);
+    queue_hkl_copy(ev_hkl, s_hkl, d_hkl, b_hkl);
+
+    /* F and |F|^2 go down ahead of the chain, so the host can copy them out
+     * while the chain's arrays are still in flight */
+    e = cudaEventCreateWithFlags(&ev_fi, cudaEventDisableTiming);
+    if (e != cudaSuccess) cuda_die("cudaEventCreate", e);
+    if (n > 0) {
+      e = cudaMemcpyAsync(s_F, dF, b_F, cudaMemcpyDeviceToHost, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(s_I, dI, b_I, cudaMemcpyDeviceToHost, 0);
+      if (e != cudaSuccess) cuda_die("cudaMemcpyAsync F, I", e);
     }
-    if (e != cudaSuccess) cuda_die("cudaMemcpyAsync outputs", e);
+    cudaEventRecord(ev_fi, 0);
+
+    /* detector chain on the device intensities (src/spsim.c:300-336) */
+    st = spsim_b200_detector_chain(&p, dI, &o, NULL);
+    if (st) die("simulate_shot detector chain", st);
+    if (n > 0) {
+      for (int k = 0; k < 7 && e == cudaSuccess; k++) {
+        const size_t b = k < 5 ? b_I : b_nb;
+        if (b) e = cudaMemcpyAsync(s_chain + (k < 5 ? k * b_I : 5 * b_I + (k - 5) * b_nb), bufs[k], b,
+                                   cudaMemcpyDeviceToHost, 0);
+      }
+      if (e != cudaSuccess) cuda_die("cudaMemcpyAsync outputs", e);
+    }
+    cudaEventRecord(ev_out, 0);
+  } else {
+    /* row chunks: chunk c's structure factor and chain run on one of two
+     * compute streams, its outputs go down on the copy stream and into the
+     * caller's arrays while chunk c + 1 computes */
+    st = spsim_internal_shot_parts_begin(n, d_hkl);
+    if (st) die("simulate_shot structure factor", st);
+    queue_hkl_copy(ev_hkl, s_hkl, d_hkl, b_hkl);
+    if (!g_comp_stream[0] || g_comp_stream_device != cur_dev) {
+      for (int k = 0; k < 2; k++) {
+        e = cudaStreamCreateWithFlags(&g_comp_stream[k], cudaStreamNonBlocking);
+        if (e != cudaSuccess) cuda_die("cudaStreamCreate", e);
+      }
+      g_comp_stream_device = cur_dev;
+    }
+    cudaEvent_t ev_ready;
+    e = cudaEventCreateWithFlags(&ev_ready, cudaEventDisableTiming);
+    if (e != cudaSuccess) cuda_die("cudaEventCreate", e);
+    cudaEventRecord(ev_ready, 0);
+    for (int c = 0; c < K; c++) {
+      const long long r0 = rb[c], r1 = rb[c + 1];
+      const long long p0 = r0 * det->nx, p1 = r1 * det->nx;
+      const long long b0 = r0 / det->binning_y * bnx;
+      const long long b1 = (r1 / det->binning_y < det->ny / det->binning_y ? r1 / det->binning_y
+                                                                            : det->ny / det->binning_y) * bnx;
+      cudaStream_t s = g_comp_stream[c & 1];
+      cudaStreamWaitEvent(s, ev_ready, 0);
+      st = spsim_internal_shot_part(p0, p1, opts->b_factor, g_precision, dF, dI, s);
+      if (st) die("simulate_shot structure factor", st);
+      st = spsim_internal_chain_rows(&p, dI, &o, r0, r1, s);
+      if (st) die("simulate_shot detector chain", st);
+      cudaEvent_t ev_part;
+      e = cudaEventCreateWithFlags(&ev_part, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_copied[c], cudaEventDisableTiming);
+      if (e != cudaSuccess) cuda_die("cudaEventCreate", e);
+      cudaEventRecord(ev_part, s);
+      cudaStreamWaitEvent(g_copy_stream, ev_part, 0);
+      cudaEventDestroy(ev_part); /* released once the wait has run */
+      e = cudaMemcpyAsync(s_F + sizeof(Complex) * p0, dF + 2 * p0, sizeof(Complex) * (p1 - p0),
+                          cudaMemcpyDeviceToHost, g_copy_stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s_I + sizeof(float) * p0, dI + p0, sizeof(float) * (p1 - p0), cudaMemcpyDeviceToHost,
+                            g_copy_stream);
+      for (int k = 0; k < 7 && e == cudaSuccess; k++) {
+        const long long lo = k < 5 ? p0 : b0, hi = k < 5 ? p1 : b1;
+        char *dst = s_chain + (k < 5 ? k * b_I : 5 * b_I + (k - 5) * b_nb) + sizeof(float) * lo;
+        if (hi > lo)
+          e = cudaMemcpyAsync(dst, bufs[k] + lo, sizeof(float) * (hi - lo), cudaMemcpyDeviceToHost, g_copy_stream);
+      }
+      if (e != cudaSuccess) cuda_die("cudaMemcpyAsync outputs", e);
+      cudaEventRecord(ev_copied[c], g_copy_stream);
+    }
+    cudaEventDestroy(ev_ready);
   }
-  cudaEventRecord(ev_out, 0);
 
   /* meanwhile on the host: the reference-owned outputs, first touched now */
   Diffraction_Pattern *pattern = (Diffraction_Pattern *)calloc(1, sizeof(Diffraction_Pattern));
@@ -750,18 +865,39 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   if (e != cudaSuccess) cuda_die("simulate_shot HKL copy", e);
   const HostCopy hk = {(char *)pattern->HKL_list, s_hkl, b_hkl};
   host_copy_batch(&hk, 1);
-  e = cudaEventSynchronize(ev_fi);
-  if (e != cudaSuccess) cuda_die("simulate_shot F, I", e);
-  host_copy_batch(out, 2);
-
-  e = cudaEventSynchronize(ev_out);
-  if (e != cudaSuccess) cuda_die("simulate_shot outputs", e);
+  if (K == 1) {
+    e = cudaEventSynchronize(ev_fi);
+    if (e != cudaSuccess) cuda_die("simulate_shot F, I", e);
+    host_copy_batch(out, 2);
+    e = cudaEventSynchronize(ev_out);
+    if (e != cudaSuccess) cuda_die("simulate_shot outputs", e);
+    cudaEventDestroy(ev_fi);
+    st = spsim_internal_shot_check();
+    if (st) die("simulate_shot structure factor", st);
+    host_copy_batch(out + 2, 7);
+  } else {
+    for (int c = 0; c < K; c++) {
+      const long long r0 = rb[c], r1 = rb[c + 1];
+      const long long p0 = r0 * det->nx, p1 = r1 * det->nx;
+      const long long b0 = r0 / det->binning_y * bnx;
+      const long long b1 = (r1 / det->binning_y < det->ny / det->binning_y ? r1 / det->binning_y
+                                                                            : det->ny / det->binning_y) * bnx;
+      e = cudaEventSynchronize(ev_copied[c]);
+      if (e != cudaSuccess) cuda_die("simulate_shot outputs", e);
+      cudaEventDestroy(ev_copied[c]);
+      HostCopy part[9];
+      for (int k = 0; k < 9; k++) {
+        const size_t el = k == 0 ? sizeof(Complex) : sizeof(float);
+        const long long lo = k < 7 ? p0 : b0, hi = k < 7 ? p1 : b1;
+        part[k] = (HostCopy){out[k].dst + el * lo, out[k].src + el * lo, hi > lo ? el * (size_t)(hi - lo) : 0};
+      }
+      host_copy_batch(part, 9);
+    }
+    st = spsim_internal_shot_check();
+    if (st) die("simulate_shot structure factor", st);
+  }
   cudaEventDestroy(ev_hkl);
-  cudaEventDestroy(ev_fi);
   cudaEventDestroy(ev_out);
-  st = spsim_internal_shot_check();
-  if (st) die("simulate_shot structure factor", st);
-  host_copy_batch(out + 2, 7);
   if (opts->verbosity_level > 0) /* src/diffraction.c:849-851 */
     printf("%g atoms.pixel/s\n", 1.0e6 * n * mol->natoms / (now_us() - t0));
   g_pattern_counter++;

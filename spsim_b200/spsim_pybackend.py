@@ -333,6 +333,15 @@ def get_nufft_eps():
     return _native.lib().spsim_b200_get_legacy_nufft_eps()
 
 
+def set_shot_chunks(chunks):
+    """Row chunks of simulate_shot (0: automatic, 1: none; see spsim_b200_set_shot_chunks)."""
+    _native.lib().spsim_b200_set_shot_chunks(int(chunks))
+
+
+def get_shot_chunks():
+    return _native.lib().spsim_b200_get_shot_chunks()
+
+
 def _floats(a):
     if isinstance(a, np.ndarray):
         a = np.ascontiguousarray(a, np.float32)

@@ -205,3 +205,136 @@ def test_simulate_shot_equals_step_by_step_sequence(cuda, tmp_path, use_cuda, ba
         S.free_mol(mol)
     finally:
         os.chdir(cwd)
+
+
+def _shot_arrays(shot, det, n, nb):
+    names = ["thomson_correction", "solid_angle", "photons_per_pixel", "photon_count", "electrons_per_pixel"]
+    out = {k: S.as_array(getattr(det, k), n).copy() for k in names}
+    for k in ("real_output", "noiseless_output"):
+        out[k] = S.as_array(getattr(det, k), nb).copy()
+    out["F"] = S.as_array(shot.contents.F, n).copy()
+    out["I"] = S.as_array(shot.contents.ints, n).copy()
+    out["hkl"] = S.as_array(shot.contents.HKL_list, 3 * n).copy()
+    return out
+
+
+@pytest.mark.parametrize("nx,ny,binning", [(96, 90, 1), (95, 91, 2), (64, 64, 2)], ids=["even", "odd_binned",
+                                                                                        "square_binned"])
+def test_simulate_shot_row_chunks_match_step_by_step(cuda, tmp_path, nx, ny, binning):
+    # the pipelined simulate_shot (three row chunks on two streams, each
+    # chunk's outputs copied while the next computes) against the reference's
+    # step-by-step sequence on the whole detector (no pattern counter step in
+    # between, so both draw the same noise streams): the HKL list and the
+    # geometry-only chain arrays bit for bit, |F|^2 within the FP32 tolerance
+    # of the one-pass result and of the FP64 oracle (the chunks split their
+    # atom ranges differently), the noise stages where the counts agree
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        opts = S.set_defaults()
+        S.read_options_file(os.path.join(GOLDEN, "config", "example.conf"), opts)
+        o = opts.contents
+        det = o.detector.contents
+        det.width, det.height = nx * det.pixel_width, ny * det.pixel_height
+        det.nx, det.ny, det.nz = nx, ny, 1
+        det.binning_x = det.binning_y = binning
+        det.readout_noise = 3.0
+        o.verbosity_level = 0
+        o.random_orientation = 0
+        o.euler_orientation[0], o.euler_orientation[1], o.euler_orientation[2] = 0.3, -1.1, 2.2
+        o.random_seed = 77
+        S.set_noise_seed(77)
+        g = golden("sf_small.npz")
+        mol = _mol(g["Z"], g["pos"])
+        n, nb = nx * ny, (nx // binning) * (ny // binning)
+
+        size = ctypes.c_int(0)
+        hkl = S.get_HKL_list(opts, ctypes.byref(size))
+        hp = ctypes.pointer(hkl)
+        rot = S.apply_orientation_to_HKL_list(hp, ctypes.byref(size), opts)
+        pat = S.compute_sf(mol, hp.contents, size.value, opts)
+        S.calculate_thomson_correction(o.detector, o.experiment)
+        S.calculate_pixel_solid_angle(o.detector)
+        S.calculate_photons_per_pixel(pat, opts)
+        S.generate_poisson_noise(o.detector)
+        S.calculate_electrons_per_pixel(o.detector, o.experiment)
+        S.calculate_real_detector_output(o.detector, o.experiment)
+        S.calculate_noiseless_detector_output(o.detector, o.experiment)
+        one = _shot_arrays(pat, det, n, nb)
+        S.free_diffraction_pattern(pat)
+        S.free_output_in_options(opts)
+
+        S.set_shot_chunks(3)
+        shot = S.simulate_shot(mol, opts)
+        S.set_shot_chunks(0)
+        ch = _shot_arrays(shot, det, n, nb)
+        S.free_stuff(shot, opts)
+
+        np.testing.assert_array_equal(ch["hkl"], one["hkl"])
+        np.testing.assert_allclose(ch["thomson_correction"], one["thomson_correction"], rtol=2.4e-7)
+        np.testing.assert_allclose(ch["solid_angle"], one["solid_angle"], rtol=2.4e-7)
+        e_max, e_l2 = intensity_errors(ch["I"], one["I"].astype(np.float64))
+        assert e_max < 1e-5 and e_l2 < 1e-6, (e_max, e_l2)
+        _, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), ch["hkl"].reshape(-1, 3).astype(np.float64))
+        e_max, e_l2 = intensity_errors(ch["I"], I64)
+        assert e_max < 1e-5 and e_l2 < 1e-6, (e_max, e_l2)
+        np.testing.assert_allclose(ch["photons_per_pixel"], one["photons_per_pixel"], rtol=2e-5)
+        same = ch["photon_count"] == one["photon_count"]
+        assert same.mean() > 0.995
+        np.testing.assert_allclose(ch["electrons_per_pixel"][same], one["electrons_per_pixel"][same], rtol=1e-6)
+        np.testing.assert_allclose(ch["noiseless_output"], one["noiseless_output"], rtol=2e-5, atol=1e-6)
+        if binning == 1:
+            np.testing.assert_allclose(ch["real_output"][same], one["real_output"][same], rtol=1e-5, atol=1e-3)
+        else:
+            # a bin's real output sums its pixels' electrons: compared where every pixel's count agrees
+            cnt = same.reshape(ny, nx)[: ny // binning * binning, : nx // binning * binning]
+            bins_same = cnt.reshape(ny // binning, binning, nx // binning, binning).all(axis=(1, 3)).reshape(-1)
+            assert bins_same.mean() > 0.98
+            np.testing.assert_allclose(ch["real_output"][bins_same], one["real_output"][bins_same], rtol=1e-5,
+                                       atol=1e-3)
+        S.free_mol(mol)
+    finally:
+        S.set_shot_chunks(0)
+        os.chdir(cwd)
+
+
+def test_simulate_shot_automatic_chunks_on_a_large_detector(cuda, tmp_path):
+    # 1024 x 512 pixels (2^19): simulate_shot pipelines four row chunks by
+    # default; every 29th row against the FP64 oracle, the chain's geometry
+    # arrays against the per-stage calls
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        assert S.get_shot_chunks() == 0
+        opts = S.set_defaults()
+        S.read_options_file(os.path.join(GOLDEN, "config", "example.conf"), opts)
+        o = opts.contents
+        det = o.detector.contents
+        nx, ny = 1024, 512
+        det.width, det.height = nx * det.pixel_width, ny * det.pixel_height
+        det.nx, det.ny, det.nz = nx, ny, 1
+        o.verbosity_level = 0
+        g = golden("sf_small.npz")
+        mol = _mol(g["Z"], g["pos"])
+        shot = S.simulate_shot(mol, opts)
+        n = nx * ny
+        I = S.as_array(shot.contents.ints, n).reshape(ny, nx)
+        hkl = S.as_array(shot.contents.HKL_list, 3 * n).reshape(ny, nx, 3)
+        rows = np.arange(0, ny, 29)
+        _, I64 = O.structure_factor(g["Z"], g["pos"].astype(np.float64), hkl[rows].reshape(-1, 3).astype(np.float64))
+        e_max, e_l2 = intensity_errors(I[rows].reshape(-1), I64)
+        assert e_max < 1e-5 and e_l2 < 1e-6, (e_max, e_l2)
+        T = S.as_array(det.thomson_correction, n).copy()
+        Om = S.as_array(det.solid_angle, n).copy()
+        ph = S.as_array(det.photons_per_pixel, n)
+        np.testing.assert_allclose(ph, (T * Om * I.reshape(-1) * np.float32(o.experiment.contents.beam_intensity)),
+                                   rtol=1e-6)
+        S.free_stuff(shot, opts)
+        S.calculate_thomson_correction(o.detector, o.experiment)
+        S.calculate_pixel_solid_angle(o.detector)
+        np.testing.assert_array_equal(S.as_array(det.thomson_correction, n), T)
+        np.testing.assert_array_equal(S.as_array(det.solid_angle, n), Om)
+        S.free_output_in_options(opts)
+        S.free_mol(mol)
+    finally:
+        os.chdir(cwd)
