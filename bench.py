@@ -562,7 +562,8 @@ def _nufft_mode(core, mol, qs, rot, terms, sub_rows, I64, eps=1e-8, steps=5):
             "kernel_widths": [w1, w2], "fft_grid": list(n2),
             "accuracy": {"floored_max_rel": float(np.max(np.abs(In - I64) / den)),
                          "l2_rel": float(np.linalg.norm(In - I64) / np.linalg.norm(I64))},
-            "note": "type-3 NUFFT per element (spread, pad, cuFFT Z2Z, interpolate; FP64 spreading and FFT, "
+            "note": "type-3 NUFFT per element (spread; pruned x, y, z FFT passes with the deconvolution and the "
+                    "FP32 packing fused; interpolate; FP64 spreading and FFT, "
                     "FP32 interpolation grid), a different algorithm from the direct sum the headline value times"}
 
 

@@ -169,7 +169,7 @@ def forward(mol, qs, rot=None, B=0.0, precision="f32", F=None, I=None, want_F=Tr
 
 def forward_nufft(mol, qs, rot=None, B=0.0, eps=1e-8, F=None, I=None, want_F=True, want_I=True, stream=None):
     """The structure factor of forward() by a type-3 non-uniform FFT per
-    element (FP64 grids, cuFFT), for large molecules: relative L2 error of F
+    element (FP64 grids and hand-written pruned FFT passes), for large molecules: relative L2 error of F
     about eps against the exact sum.  Replaces spsim's NNFFT path
     (src/diffraction.c:528-675).  Returns (F, I) like forward()."""
     _native.use_device(mol.device)
