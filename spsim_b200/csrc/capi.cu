@@ -1782,9 +1782,9 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   for (int d = 0; d < 3; ++d) g.center[d] = m->center[d];
   size_t cells1 = (size_t)g.n1[0] * g.n1[1] * g.n1[2];
   CUDA_TRY(cudaMemsetAsync(c.small.p, 0, cells1 * n_elem * c.copies * sizeof(double2), st));
-  CUDA_TRY(nufft_spread(m->d_atomsd, (const int *)c.seg.p, n_elem, m->n_padded, g, (double2 *)c.small.p, c.copies,
+  CUDA_TRY(nufft_spread(m->d_atomsd, (const int *)c.seg.p, n_elem, m->n_padded, g, (double *)c.small.p, c.copies,
                         (int *)c.flags.p, st));
-  CUDA_TRY(nufft_fft3((const double2 *)c.small.p, c.copies, (const double *)c.dec.p, g, n_elem, c.ax,
+  CUDA_TRY(nufft_fft3((const double *)c.small.p, c.copies, (const double *)c.dec.p, g, n_elem, c.ax,
                       (double2 *)c.fa.p, (double2 *)c.fb.p, (float4 *)c.packed.p, st));
   const long long cells2 = (long long)g.m[0] * g.m[1] * g.m[2];
   NufftInterp a;

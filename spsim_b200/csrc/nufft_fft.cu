@@ -225,27 +225,32 @@ constexpr int KL = 8;
 __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_x_kernel(const __grid_constant__ FftPassX a) {
   extern __shared__ double2 sm[];
   __shared__ double line_scale[FFT_MAX_LINES];
+  __shared__ long long line_at[FFT_MAX_LINES];  // offset of the line's real part in the spreading grid
   const FftAxis &ax = a.ax;
   const long long line0 = (long long)blockIdx.x * a.per_cta;
   const int nl = (int)min((long long)a.per_cta, a.lines - line0);
   double2 *b0 = sm, *b1 = sm + (long long)a.per_cta * ax.ld;
   if (threadIdx.x < nl) {
-    const long long line = line0 + threadIdx.x;
+    // line (e, lz, ly): real part at e 2 cells1 + (lz n1y + ly) n1x
+    const long long line = line0 + threadIdx.x, per_elem = (long long)a.n1z * a.n1y, e = line / per_elem;
     const int ly = (int)(line % a.n1y), lz = (int)((line / a.n1y) % a.n1z);
     line_scale[threadIdx.x] = a.dec[ax.nin + ly] * a.dec[ax.nin + a.n1y + lz];
+    line_at[threadIdx.x] = e * 2 * a.cells1 + (line - e * per_elem) * ax.nin;
   }
   zero_padding(b0, nl, ax);
   const int total = nl * ax.nin;
   const FastDiv dnin = fdiv_make(ax.nin);
-  const double2 *src = a.small + line0 * ax.nin;
+  __syncthreads();  // line_at
   for (int base = 0; base < total; base += KL * FFT_THREADS) {
     double2 v[KL];
 #pragma unroll
     for (int u = 0; u < KL; ++u) {
       const int i = base + u * FFT_THREADS + threadIdx.x;
       if (i < total) {
-        v[u] = src[i];
-        for (int k = 1; k < a.copies; ++k) v[u] = cadd(v[u], src[i + k * a.copy_stride]);
+        const int c = fdiv(i, dnin), lx = i - c * ax.nin;
+        const double *re = a.small + line_at[c] + lx;
+        v[u] = make_double2(re[0], re[a.cells1]);
+        for (int k = 1; k < a.copies; ++k) v[u] = cadd(v[u], make_double2(re[k * a.copy_stride], re[k * a.copy_stride + a.cells1]));
       }
     }
 #pragma unroll
@@ -420,7 +425,7 @@ static int lines_for(const FftAxis &ax, int cap) {
   return (int)std::max<size_t>(1, std::min<size_t>(cap, kSmemBudget / line));
 }
 
-cudaError_t nufft_fft3(const double2 *small, int copies, const double *dec, const NufftGeom &g, int n_elem,
+cudaError_t nufft_fft3(const double *small, int copies, const double *dec, const NufftGeom &g, int n_elem,
                        const FftAxis ax[3], double2 *fa, double2 *fb, float4 *packed, cudaStream_t st) {
   cudaError_t e = smem_opt_in();
   if (e != cudaSuccess) return e;
@@ -430,7 +435,8 @@ cudaError_t nufft_fft3(const double2 *small, int copies, const double *dec, cons
     p.ax = ax[0];
     p.small = small;
     p.copies = std::max(copies, 1);
-    p.copy_stride = (long long)n_elem * g.n1[0] * g.n1[1] * g.n1[2];
+    p.cells1 = (long long)g.n1[0] * g.n1[1] * g.n1[2];
+    p.copy_stride = 2 * (long long)n_elem * p.cells1;
     p.dec = dec;
     p.n1y = g.n1[1];
     p.n1z = g.n1[2];

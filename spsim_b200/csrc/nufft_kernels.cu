@@ -113,7 +113,7 @@ constexpr int SPREAD_WARPS = 8;
 __global__ void __launch_bounds__(32 * SPREAD_WARPS) nufft_spread_kernel(const AtomD *__restrict__ atoms,
                                                                          const int *__restrict__ seg, int n_elem,
                                                                          int n_atoms, const NufftGeom g,
-                                                                         double2 *__restrict__ grid, int copies,
+                                                                         double *__restrict__ grid, int copies,
                                                                          int *__restrict__ err) {
   __shared__ double kv[SPREAD_WARPS][3][NUFFT_MAX_W];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -148,10 +148,12 @@ __global__ void __launch_bounds__(32 * SPREAD_WARPS) nufft_spread_kernel(const A
   sincospi(2.0 * t, &sn, &cs);
   const double cr = (double)a.w * cs, ci = -(double)a.w * sn;
   const long long n1x = g.n1[0], n1y = g.n1[1];
-  // warps take the grid copies in turn: fewer updates of one cell in flight
+  // warps take the grid copies in turn: fewer updates of one cell in flight;
+  // real and imaginary parts in separate planes, so that a half-warp's
+  // atomics on one stencil row cover 96 contiguous bytes, not 192
   const long long cells1 = n1x * n1y * g.n1[2];
-  double2 *base = grid + ((long long)(j % copies) * n_elem + e) * cells1 + ((long long)l0[2] * n1y + l0[1]) * n1x +
-                  l0[0];
+  double *base = grid + 2 * ((long long)(j % copies) * n_elem + e) * cells1 + ((long long)l0[2] * n1y + l0[1]) * n1x +
+                 l0[0];
   // lane = (y parity, x offset): half-warps cover two stencil rows per step
   static_assert(NUFFT_MAX_W <= 16, "one stencil row per half-warp");
   const int ix = lane & 15, iy0 = lane >> 4;
@@ -159,19 +161,19 @@ __global__ void __launch_bounds__(32 * SPREAD_WARPS) nufft_spread_kernel(const A
     const double kxr = kv[warp][0][ix] * cr, kxi = kv[warp][0][ix] * ci;
     for (int iz = 0; iz < w; ++iz) {
       const double kz = kv[warp][2][iz];
-      double2 *plane = base + (long long)iz * n1y * n1x + ix;
+      double *plane = base + (long long)iz * n1y * n1x + ix;
       for (int iy = iy0; iy < w; iy += 2) {
         const double v = kz * kv[warp][1][iy];
-        double2 *p = plane + (long long)iy * n1x;
-        atomicAdd(&p->x, v * kxr);
-        atomicAdd(&p->y, v * kxi);
+        double *p = plane + (long long)iy * n1x;
+        atomicAdd(p, v * kxr);
+        atomicAdd(p + cells1, v * kxi);
       }
     }
   }
 }
 
 cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_atoms, const NufftGeom &g,
-                         double2 *grid, int copies, int *err, cudaStream_t st) {
+                         double *grid, int copies, int *err, cudaStream_t st) {
   if (n_atoms <= 0) return cudaSuccess;
   const unsigned blocks = (unsigned)((n_atoms + SPREAD_WARPS - 1) / SPREAD_WARPS);
   nufft_spread_kernel<<<blocks, 32 * SPREAD_WARPS, 0, st>>>(atoms, seg, n_elem, n_atoms, g, grid, std::max(copies, 1),

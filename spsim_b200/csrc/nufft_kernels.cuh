@@ -55,8 +55,9 @@ struct FftAxis {
 };
 struct FftPassX {
   FftAxis ax;
-  const double2 *small;  // spreading grid, copies x [E][n1z][n1y][n1x]
-  long long copy_stride;
+  const double *small;   // spreading grid, copies x [E][re, im][n1z][n1y][n1x]
+  long long copy_stride; // doubles between copies
+  long long cells1;      // n1x n1y n1z
   int copies;
   const double *dec;     // 1 / phi2hat per spreading-grid index: x, then y, then z
   int n1y, n1z;
@@ -110,12 +111,12 @@ double nufft_key_to_double(unsigned long long k);
 unsigned long long nufft_double_to_key(double d);
 
 // Step 1.  atoms: element-sorted FP64 records; seg: n_elem + 1 segment starts;
-// grid (zeroed): `copies` x [n_elem][n1z][n1y][n1x], atom j adding into copy
-// j mod copies (several copies spread the updates of one cell when the grid is
-// small next to the atom count).  An atom whose stencil leaves the grid is
-// skipped and sets err[0].
+// grid (zeroed, FP64): `copies` x [n_elem][re, im][n1z][n1y][n1x], atom j
+// adding into copy j mod copies (several copies spread the updates of one cell
+// when the grid is small next to the atom count).  An atom whose stencil
+// leaves the grid is skipped and sets err[0].
 cudaError_t nufft_spread(const AtomD *atoms, const int *seg, int n_elem, int n_atoms, const NufftGeom &g,
-                         double2 *grid, int copies, int *err, cudaStream_t st);
+                         double *grid, int copies, int *err, cudaStream_t st);
 // Step 2: zero `fine` and scatter the deconvolved spreading grid (the sum of
 // its copies) into it.  dec: 1 / phi2hat per spreading-grid index, x then y
 // then z.
@@ -129,7 +130,7 @@ int nufft_pack_halves(int n_elem);
 int nufft_pack_groups(int n_elem);
 int nufft_fft_axis(int n, int nin, int pmin, int nout, const double2 *tw, FftAxis *ax);  // 0, or -1: n unsupported
 void nufft_fft_twiddles(int n, double2 *tw);  // host table exp(-2 pi i k / n)
-cudaError_t nufft_fft3(const double2 *small, int copies, const double *dec, const NufftGeom &g, int n_elem,
+cudaError_t nufft_fft3(const double *small, int copies, const double *dec, const NufftGeom &g, int n_elem,
                        const FftAxis ax[3], double2 *fa, double2 *fb, float4 *packed, cudaStream_t st);
 // Step 4.
 cudaError_t nufft_interp(const NufftInterp &a, cudaStream_t st);
