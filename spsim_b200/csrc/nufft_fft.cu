@@ -110,11 +110,17 @@ struct Dft<5> : DftOdd<5> {};
 template <>
 struct Dft<7> : DftOdd<7> {};
 
-// Position i of a line in shared memory: one padding slot after every 8, so
-// that a stage with Ns = 1, whose thread j writes positions j R + t, stores
-// at a stride of 9 R / 8 slots (odd for R = 8) and spreads a quarter-warp's
-// 16-byte stores over all banks.  Lines are ld >= pad(n - 1) + 1 slots apart.
-__device__ __forceinline__ int pad(int i) { return i + (i >> 3); }
+// Position i of a line in shared memory.  A stage with Ns = 1 has thread j
+// write positions j R + t: for an odd first radix (every n with an odd
+// factor) that stride already spreads a quarter-warp's 16-byte stores over
+// all banks, and positions are plain (PAD false).  A power-of-two n starts
+// with R = 8: there one padding slot follows every 8 positions, so that the
+// stride becomes 9 slots (PAD true).  Lines are ld >= pos(n - 1) + 1 slots
+// apart.
+template <bool PAD>
+__device__ __forceinline__ int pad(int i) {
+  return PAD ? i + (i >> 3) : i;
+}
 
 // n / d for 0 <= n, n d < 2^32 by a multiply-high (the block-uniform d's
 // magic computed once per loop)
@@ -133,7 +139,7 @@ __device__ __forceinline__ int fdiv(int n, const FastDiv &f) { return f.d == 1 ?
 constexpr int FFT_THREADS = 256;
 constexpr int FFT_MAX_LINES = 64;  // lines of one block (x pass: its per-line scales)
 
-template <int R>
+template <int R, bool PAD>
 __device__ __forceinline__ void radix_stage(const double2 *__restrict__ src, double2 *__restrict__ dst, int lines,
                                             const FftAxis &ax, int Ns) {
   const int N = ax.n, Nr = N / R, tstep = N / (Ns * R), ld = ax.ld;
@@ -150,9 +156,10 @@ __device__ __forceinline__ void radix_stage(const double2 *__restrict__ src, dou
     const double2 *s = src + c * ld;
     double2 v[R];
 #pragma unroll
-    for (int t = 0; t < R; ++t) v[t] = s[pad(j + t * Nr)];
+    for (int t = 0; t < R; ++t) v[t] = s[pad<PAD>(j + t * Nr)];
     if (Ns > 1) {
-      // exp(-2 pi i t k / (Ns R)) as powers of the t = 1 twiddle
+      // exp(-2 pi i t k / (Ns R)) as powers of the t = 1 twiddle (R - 1 table
+      // loads per butterfly measured slower: the L1 path is the busier one)
       const double2 w1 = __ldg(ax.tw + k * tstep);
       double2 wt = w1;
       v[1] = cmul(v[1], w1);
@@ -166,23 +173,24 @@ __device__ __forceinline__ void radix_stage(const double2 *__restrict__ src, dou
     double2 *d = dst + c * ld;
     const int o = q * Ns * R + k;
 #pragma unroll
-    for (int t = 0; t < R; ++t) d[pad(o + t * Ns)] = v[t];
+    for (int t = 0; t < R; ++t) d[pad<PAD>(o + t * Ns)] = v[t];
   }
 }
 
 // all stages on `lines` lines of buffer a (b: the other buffer); returns the
 // buffer that holds the transforms.  Entered and left with the block in step.
+template <bool PAD>
 __device__ double2 *stockham(double2 *a, double2 *b, int lines, const FftAxis &ax) {
   int Ns = 1;
   for (int s = 0; s < ax.nst; ++s) {
     const int R = ax.rad[s];
     switch (R) {
-      case 8: radix_stage<8>(a, b, lines, ax, Ns); break;
-      case 4: radix_stage<4>(a, b, lines, ax, Ns); break;
-      case 2: radix_stage<2>(a, b, lines, ax, Ns); break;
-      case 3: radix_stage<3>(a, b, lines, ax, Ns); break;
-      case 5: radix_stage<5>(a, b, lines, ax, Ns); break;
-      default: radix_stage<7>(a, b, lines, ax, Ns); break;
+      case 8: radix_stage<8, PAD>(a, b, lines, ax, Ns); break;
+      case 4: radix_stage<4, PAD>(a, b, lines, ax, Ns); break;
+      case 2: radix_stage<2, PAD>(a, b, lines, ax, Ns); break;
+      case 3: radix_stage<3, PAD>(a, b, lines, ax, Ns); break;
+      case 5: radix_stage<5, PAD>(a, b, lines, ax, Ns); break;
+      default: radix_stage<7, PAD>(a, b, lines, ax, Ns); break;
     }
     __syncthreads();
     double2 *t = a;
@@ -194,25 +202,28 @@ __device__ double2 *stockham(double2 *a, double2 *b, int lines, const FftAxis &a
 }
 
 // zero the padding of `lines` lines: frequency indices [nin - nin/2, n - nin/2)
+template <bool PAD>
 __device__ __forceinline__ void zero_padding(double2 *buf, int lines, const FftAxis &ax) {
   const int nz = ax.n - ax.nin, first = ax.nin - ax.nin / 2;
   if (nz <= 0) return;
   const FastDiv dz = fdiv_make(nz);
   for (int i = threadIdx.x; i < lines * nz; i += FFT_THREADS) {
     const int c = fdiv(i, dz), q = i - c * nz;
-    buf[c * ax.ld + pad(first + q)] = make_double2(0.0, 0.0);
+    buf[c * ax.ld + pad<PAD>(first + q)] = make_double2(0.0, 0.0);
   }
 }
 
+template <bool PAD>
 __device__ __forceinline__ int in_pos(int l, const FftAxis &ax) {
   const int m = l - ax.nin / 2;
-  return pad(m < 0 ? m + ax.n : m);
+  return pad<PAD>(m < 0 ? m + ax.n : m);
 }
 
+template <bool PAD>
 __device__ __forceinline__ int out_pos(int o, const FftAxis &ax) {
   int p = ax.p0 + o;
   if (p >= ax.n) p %= ax.n;
-  return pad(p);
+  return pad<PAD>(p);
 }
 
 // Loads of a pass are issued KL per thread before any is stored to shared
@@ -222,6 +233,7 @@ constexpr int KL = 8;
 // x pass: lines (e, lz, ly) of the spreading grid (the sum of its copies),
 // times the separable deconvolution dec (x at the input, y z at the output:
 // the transform is linear); out [E n1z n1y][nout]
+template <bool PAD>
 __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_x_kernel(const __grid_constant__ FftPassX a) {
   extern __shared__ double2 sm[];
   __shared__ double line_scale[FFT_MAX_LINES];
@@ -237,7 +249,7 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_x_kernel(const __grid_c
     line_scale[threadIdx.x] = a.dec[ax.nin + ly] * a.dec[ax.nin + a.n1y + lz];
     line_at[threadIdx.x] = e * 2 * a.cells1 + (line - e * per_elem) * ax.nin;
   }
-  zero_padding(b0, nl, ax);
+  zero_padding<PAD>(b0, nl, ax);
   const int total = nl * ax.nin;
   const FastDiv dnin = fdiv_make(ax.nin);
   __syncthreads();  // line_at
@@ -259,17 +271,17 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_x_kernel(const __grid_c
       if (i < total) {
         const int c = fdiv(i, dnin), lx = i - c * ax.nin;
         const double d = a.dec[lx];
-        b0[c * ax.ld + in_pos(lx, ax)] = make_double2(v[u].x * d, v[u].y * d);
+        b0[c * ax.ld + in_pos<PAD>(lx, ax)] = make_double2(v[u].x * d, v[u].y * d);
       }
     }
   }
   __syncthreads();
-  const double2 *r = stockham(b0, b1, nl, ax);
+  const double2 *r = stockham<PAD>(b0, b1, nl, ax);
   double2 *out = a.out + line0 * ax.nout;
   const FastDiv dnout = fdiv_make(ax.nout);
   for (int i = threadIdx.x; i < nl * ax.nout; i += FFT_THREADS) {
     const int c = fdiv(i, dnout), o = i - c * ax.nout;
-    const double2 x = r[c * ax.ld + out_pos(o, ax)];
+    const double2 x = r[c * ax.ld + out_pos<PAD>(o, ax)];
     out[i] = make_double2(x.x * line_scale[c], x.y * line_scale[c]);
   }
 }
@@ -277,6 +289,7 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_x_kernel(const __grid_c
 // y pass: columns of [E n1z][n1y][mx], per_cta neighbouring columns of one
 // (e, lz) plane; out [E n1z][nout][mx].  Thread t takes column t mod nc and
 // rows t / nc + m (256 / nc).
+template <bool PAD>
 __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_y_kernel(const __grid_constant__ FftPassY a) {
   extern __shared__ double2 sm[];
   const FftAxis &ax = a.ax;
@@ -284,7 +297,7 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_y_kernel(const __grid_c
   const long long pl = blockIdx.x / tiles;  // (e, lz) plane
   const int x0 = (int)(blockIdx.x - pl * tiles) * a.per_cta, nc = min(a.per_cta, a.mx - x0);
   double2 *b0 = sm, *b1 = sm + a.per_cta * ax.ld;
-  zero_padding(b0, nc, ax);
+  zero_padding<PAD>(b0, nc, ax);
   const int c = threadIdx.x % nc, r0 = threadIdx.x / nc, step = FFT_THREADS / nc;
   const bool on = r0 < step;
   const double2 *in = a.in + pl * ax.nin * a.mx + x0 + c;
@@ -298,20 +311,21 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_y_kernel(const __grid_c
 #pragma unroll
     for (int u = 0; u < KL; ++u) {
       const int ly = base + u * step;
-      if (on && ly < ax.nin) b0[c * ax.ld + in_pos(ly, ax)] = v[u];
+      if (on && ly < ax.nin) b0[c * ax.ld + in_pos<PAD>(ly, ax)] = v[u];
     }
   }
   __syncthreads();
-  const double2 *r = stockham(b0, b1, nc, ax);
+  const double2 *r = stockham<PAD>(b0, b1, nc, ax);
   if (!on) return;
   double2 *out = a.out + pl * ax.nout * a.mx + x0 + c;
-  for (int o = r0; o < ax.nout; o += step) out[(long long)o * a.mx] = r[c * ax.ld + out_pos(o, ax)];
+  for (int o = r0; o < ax.nout; o += step) out[(long long)o * a.mx] = r[c * ax.ld + out_pos<PAD>(o, ax)];
 }
 
 // z pass: columns of [E][n1z][my][mx] for elements [e0, e0 + per_elem) and
 // per_cta neighbouring x of one y; out: the interpolation's FP32 grid,
 // float2 slots [group][nout][my][mx][slots], element e in group e / slots,
 // slot e mod slots; slots past the last element are written as zeros
+template <bool PAD>
 __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_z_kernel(const __grid_constant__ FftPassZ a) {
   extern __shared__ double2 sm[];
   const FftAxis &ax = a.ax;
@@ -320,7 +334,7 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_z_kernel(const __grid_c
   const int e0 = blockIdx.z * a.per_elem, ne = min(a.per_elem, a.n_elem - e0);
   const int lines = ne * nc;  // line l: element e0 + l / nc, column l mod nc
   double2 *b0 = sm, *b1 = sm + a.per_elem * a.per_cta * ax.ld;
-  zero_padding(b0, lines, ax);
+  zero_padding<PAD>(b0, lines, ax);
   const long long plane = (long long)a.my * a.mx;
   {
     const int l = threadIdx.x % lines, r0 = threadIdx.x / lines, step = FFT_THREADS / lines;
@@ -337,12 +351,12 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_z_kernel(const __grid_c
 #pragma unroll
       for (int u = 0; u < KL; ++u) {
         const int lz = base + u * step;
-        if (on && lz < ax.nin) b0[l * ax.ld + in_pos(lz, ax)] = v[u];
+        if (on && lz < ax.nin) b0[l * ax.ld + in_pos<PAD>(lz, ax)] = v[u];
       }
     }
   }
   __syncthreads();
-  const double2 *r = stockham(b0, b1, lines, ax);
+  const double2 *r = stockham<PAD>(b0, b1, lines, ax);
   // slots written by this block: its elements, and the empty slots after the
   // last element when the block holds it; thread t takes slot t mod nw of
   // column (t / nw) mod nc, outputs t / (nw nc) + m (256 / (nw nc))
@@ -356,7 +370,7 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_z_kernel(const __grid_c
   for (int o = o0; o < ax.nout; o += step) {
     float2 v = make_float2(0.0f, 0.0f);
     if (el < ne) {
-      const double2 d = r[(el * nc + c) * ax.ld + out_pos(o, ax)];
+      const double2 d = r[(el * nc + c) * ax.ld + out_pos<PAD>(o, ax)];
       v = make_float2((float)d.x, (float)d.y);
     }
     out[o * ostride] = v;
@@ -366,10 +380,13 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_z_kernel(const __grid_c
 // ---------------------------------------------------------------------------
 // host side
 
-// line stride: room for the padded positions, rounded up to 1 mod 8 so that
+// padded layout for powers of two (the transform's first radix is even)
+static bool pad_of(int n) { return (n & (n - 1)) == 0; }
+
+// line stride: room for the (padded) positions, rounded up to 1 mod 8 so that
 // neighbouring lines start 4 banks apart
 static int ld_of(int n) {
-  const int l = n + (n + 7) / 8;
+  const int l = pad_of(n) ? n + (n + 7) / 8 : n;
   return l + (9 - l % 8) % 8;
 }
 
@@ -381,6 +398,7 @@ int nufft_fft_axis(int n, int nin, int pmin, int nout, const double2 *tw, FftAxi
   a.nout = nout;
   a.p0 = ((pmin % n) + n) % n;
   a.ld = ld_of(n);
+  a.pad = pad_of(n) ? 1 : 0;
   a.tw = tw;
   a.nst = 0;
   int m = n;
@@ -403,15 +421,16 @@ void nufft_fft_twiddles(int n, double2 *tw) {
 }
 
 static constexpr size_t kSmemBudget = 110 * 1024;  // two blocks per SM
-static const size_t kSmemMax = 2 * (size_t)ld_of(NUFFT_FFT_MAX) * sizeof(double2);  // one line
+static const size_t kSmemMax = 2 * (size_t)std::max(ld_of(NUFFT_FFT_MAX), ld_of(4096)) * sizeof(double2);  // one line
 
 static cudaError_t smem_opt_in() {
   static thread_local int done_dev = -1;
   int dev;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev == done_dev) return e;
-  for (const void *f : {(const void *)nufft_fft_x_kernel, (const void *)nufft_fft_y_kernel,
-                        (const void *)nufft_fft_z_kernel}) {
+  for (const void *f : {(const void *)nufft_fft_x_kernel<false>, (const void *)nufft_fft_y_kernel<false>,
+                        (const void *)nufft_fft_z_kernel<false>, (const void *)nufft_fft_x_kernel<true>,
+                        (const void *)nufft_fft_y_kernel<true>, (const void *)nufft_fft_z_kernel<true>}) {
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
     if (e != cudaSuccess) return e;
   }
@@ -445,7 +464,10 @@ cudaError_t nufft_fft3(const double *small, int copies, const double *dec, const
     p.out = fa;
     const size_t smem = 2 * (size_t)p.per_cta * ax[0].ld * sizeof(double2);
     const long long blocks = (p.lines + p.per_cta - 1) / p.per_cta;
-    nufft_fft_x_kernel<<<(unsigned)blocks, FFT_THREADS, smem, st>>>(p);
+    if (p.ax.pad)
+      nufft_fft_x_kernel<true><<<(unsigned)blocks, FFT_THREADS, smem, st>>>(p);
+    else
+      nufft_fft_x_kernel<false><<<(unsigned)blocks, FFT_THREADS, smem, st>>>(p);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   {
@@ -457,7 +479,10 @@ cudaError_t nufft_fft3(const double *small, int copies, const double *dec, const
     p.per_cta = lines_for(ax[1], 16);
     const size_t smem = 2 * (size_t)p.per_cta * ax[1].ld * sizeof(double2);
     const long long blocks = (long long)((mx + p.per_cta - 1) / p.per_cta) * n_elem * g.n1[2];
-    nufft_fft_y_kernel<<<(unsigned)blocks, FFT_THREADS, smem, st>>>(p);
+    if (p.ax.pad)
+      nufft_fft_y_kernel<true><<<(unsigned)blocks, FFT_THREADS, smem, st>>>(p);
+    else
+      nufft_fft_y_kernel<false><<<(unsigned)blocks, FFT_THREADS, smem, st>>>(p);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   {
@@ -481,7 +506,10 @@ cudaError_t nufft_fft3(const double *small, int copies, const double *dec, const
     const size_t smem = 2 * (size_t)p.per_elem * p.per_cta * ax[2].ld * sizeof(double2);
     const dim3 grid((unsigned)((mx + p.per_cta - 1) / p.per_cta), (unsigned)my,
                     (unsigned)((n_elem + p.per_elem - 1) / p.per_elem));
-    nufft_fft_z_kernel<<<grid, FFT_THREADS, smem, st>>>(p);
+    if (p.ax.pad)
+      nufft_fft_z_kernel<true><<<grid, FFT_THREADS, smem, st>>>(p);
+    else
+      nufft_fft_z_kernel<false><<<grid, FFT_THREADS, smem, st>>>(p);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -48,7 +48,8 @@ struct FftAxis {
   int nin;      // input points: spreading-grid index l at frequency index (l - nin/2) mod n
   int nout;     // output points: box index i from frequency index (p0 + i) mod n
   int p0;
-  int ld;       // shared-memory line stride (double2): n + n/8 padding slots, 1 mod 8
+  int ld;       // shared-memory line stride (double2): n (+ n/8 padding slots), 1 mod 8
+  int pad;      // padded positions (powers of two)
   int nst;      // Stockham stages and their radices (odd ones first)
   int rad[16];
   const double2 *tw;  // device: exp(-2 pi i k / n), k < n
