@@ -205,3 +205,49 @@ def test_release_scratch_frees_and_rebuilds_the_grids(cuda):
     F2, _ = core.forward_nufft(mol, qs)
     core.synchronize()
     assert np.abs(_np(F2) - F1).max() <= 1e-6 * np.abs(F1).max()
+
+
+def _fft_size(n):
+    m = max(n, 2)
+    while True:
+        if m % 2 == 0:
+            r = m
+            for f in (2, 3, 5, 7):
+                while r % f == 0:
+                    r //= f
+            if r == 1:
+                return m
+        m += 1
+
+
+def test_power_of_two_transforms_and_nine_elements(cuda):
+    # the FFT passes take a padded shared-memory layout for power-of-two
+    # lengths and interleave elements in groups of four (the last group of
+    # nine elements holds one): a q box sized so that the transforms are 128
+    # (x) and 256 (y) long, by the grid sizing of the library restated here
+    # (n1 = ceil(2 r_bound 2 sigma1 S) + w1 + 2, even; n2 the next 2,3,5,7-smooth
+    # even size of 2 n1)
+    rng = np.random.Generator(np.random.PCG64(31))
+    Z = rng.choice([1, 6, 7, 8, 15, 16, 26, 30, 34], 600).astype(np.int32)
+    Z[:9] = [1, 6, 7, 8, 15, 16, 26, 30, 34]
+    pos = (rng.normal(size=(600, 3)) * 1.2e-9).astype(np.float32)
+    p = pos.astype(np.float64)
+    c = 0.5 * (p.min(0) + p.max(0))
+    rmax = np.sqrt(((p - c) ** 2).sum(1)).max()
+    X = rmax + max(0.05 * rmax, 5e-10)
+    S = np.array([49.5, 113.0, 30.0]) / (6.0 * X)
+    q = rng.uniform(-1.0, 1.0, size=(4000, 3)) * S
+    q[0], q[1] = -S, S  # the box's corners, so that its half-widths are S
+    hkl = q.astype(np.float32)
+    h = hkl.astype(np.float64)
+    half = 0.5 * (h.max(0) - h.min(0))
+    w2 = 9
+    n1 = np.ceil(2.0 * X * 2.0 * 1.5 * half) + (w2 + 3) + 2
+    n1 = n1 + n1 % 2
+    want = tuple(_fft_size(int(np.ceil(2.0 * v))) for v in n1)
+    assert want[0] == 128 and want[1] == 256
+    F, I = core.forward_nufft(core.Molecule(Z, pos), core.QSet.from_list(hkl), eps=1e-8)
+    core.synchronize()
+    assert core.last_nufft_grid()[2] == want
+    F64, _ = O.structure_factor(Z, pos.astype(np.float64), h)
+    _check_F(_np(F), F64, 1e-8)
