@@ -234,7 +234,7 @@ constexpr int KL = 8;
 // times the separable deconvolution dec (x at the input, y z at the output:
 // the transform is linear); out [E n1z n1y][nout]
 template <bool PAD>
-__global__ void __launch_bounds__(FFT_THREADS) nufft_fft_x_kernel(const __grid_constant__ FftPassX a) {
+__global__ void __launch_bounds__(FFT_THREADS, 3) nufft_fft_x_kernel(const __grid_constant__ FftPassX a) {
   extern __shared__ double2 sm[];
   __shared__ double line_scale[FFT_MAX_LINES];
   __shared__ long long line_at[FFT_MAX_LINES];  // offset of the line's real part in the spreading grid
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_x_kernel(const __grid_c
 // (e, lz) plane; out [E n1z][nout][mx].  Thread t takes column t mod nc and
 // rows t / nc + m (256 / nc).
 template <bool PAD>
-__global__ void __launch_bounds__(FFT_THREADS) nufft_fft_y_kernel(const __grid_constant__ FftPassY a) {
+__global__ void __launch_bounds__(FFT_THREADS, 3) nufft_fft_y_kernel(const __grid_constant__ FftPassY a) {
   extern __shared__ double2 sm[];
   const FftAxis &ax = a.ax;
   const int tiles = (a.mx + a.per_cta - 1) / a.per_cta;
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(FFT_THREADS) nufft_fft_y_kernel(const __grid_c
 // float2 slots [group][nout][my][mx][slots], element e in group e / slots,
 // slot e mod slots; slots past the last element are written as zeros
 template <bool PAD>
-__global__ void __launch_bounds__(FFT_THREADS) nufft_fft_z_kernel(const __grid_constant__ FftPassZ a) {
+__global__ void __launch_bounds__(FFT_THREADS, 3) nufft_fft_z_kernel(const __grid_constant__ FftPassZ a) {
   extern __shared__ double2 sm[];
   const FftAxis &ax = a.ax;
   const int x0 = blockIdx.x * a.per_cta, nc = min(a.per_cta, a.mx - x0);
@@ -420,7 +420,7 @@ void nufft_fft_twiddles(int n, double2 *tw) {
   }
 }
 
-static constexpr size_t kSmemBudget = 110 * 1024;  // two blocks per SM
+static constexpr size_t kSmemBudget = 72 * 1024;  // three blocks per SM
 static const size_t kSmemMax = 2 * (size_t)std::max(ld_of(NUFFT_FFT_MAX), ld_of(4096)) * sizeof(double2);  // one line
 
 static cudaError_t smem_opt_in() {
