@@ -182,6 +182,26 @@ struct DevBuf {
   }
 };
 
+// Grow-only pinned host buffer (not freed at exit: the process's end returns it).
+struct PinnedBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMallocHost(&p, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    else p = nullptr;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+static PinnedBuf g_upload_stage;  // molecule uploads, under g_mu
+
 struct spsim_b200_molecule {
   unsigned long long id = 0;
   int device = 0;
@@ -256,21 +276,21 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
   m->per_atom_b = bfac != nullptr;
   m->delta_atoms = delta_atoms;
 
-  // kept atoms, bounds
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  // kept atoms, bounds (in the positions' own type: the extremes are exact)
+  PosT lo[3] = {PosT(1e30), PosT(1e30), PosT(1e30)}, hi[3] = {PosT(-1e30), PosT(-1e30), PosT(-1e30)};
   int count[SPSIM_B200_N_ELEMENTS] = {0};
   for (int j = 0; j < natoms; ++j) {
     if (!Z[j]) continue;  // src/diffraction.c:830-832
     ++count[Z[j]];
     for (int k = 0; k < 3; ++k) {
-      lo[k] = std::min(lo[k], (double)pos[3 * j + k]);
-      hi[k] = std::max(hi[k], (double)pos[3 * j + k]);
+      lo[k] = std::min(lo[k], pos[3 * j + k]);
+      hi[k] = std::max(hi[k], pos[3 * j + k]);
     }
     ++m->n_kept;
   }
   if (m->n_kept > 0)
-    for (int k = 0; k < 3; ++k) m->center[k] = 0.5 * (lo[k] + hi[k]);
-  double rmax = 0;
+    for (int k = 0; k < 3; ++k) m->center[k] = 0.5 * ((double)lo[k] + (double)hi[k]);
+  double d2max = 0;  // the square root of the largest squared distance (sqrt is monotonic)
   for (int j = 0; j < natoms; ++j) {
     if (!Z[j]) continue;
     double d2 = 0;
@@ -278,8 +298,9 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
       const double d = (double)pos[3 * j + k] - m->center[k];
       d2 += d * d;
     }
-    rmax = std::max(rmax, std::sqrt(d2));
+    d2max = std::max(d2max, d2);
   }
+  const double rmax = std::sqrt(d2max);
   // room for refinement moves: 5% or 0.5 nm, whichever is larger
   m->rbound = rmax + std::max(0.05 * rmax, 5e-10);
   m->er = ceil_log2_bound(m->rbound);
@@ -366,18 +387,31 @@ static int molecule_create_impl(int natoms, const int32_t *Z, const PosT *pos, c
   const PosT *d_pos = (const PosT *)din;
   const float *d_occ = occ ? (const float *)(din + in_pos) : nullptr;
   const float *d_bfac = bfac ? (const float *)(din + in_pos + (occ ? in_occ : 0)) : nullptr;
-  if (natoms > 0) {
-    CUDA_TRY(cudaMemcpy(din, pos, 3 * (size_t)natoms * sizeof(PosT), cudaMemcpyHostToDevice));
-    if (occ) CUDA_TRY(cudaMemcpy((void *)d_occ, occ, (size_t)natoms * sizeof(float), cudaMemcpyHostToDevice));
-    if (bfac) CUDA_TRY(cudaMemcpy((void *)d_bfac, bfac, (size_t)natoms * sizeof(float), cudaMemcpyHostToDevice));
+  // the uploads go through one pinned staging buffer (grow-only, under g_mu;
+  // free again once the synchronisation below returns)
+  struct Up {
+    void *dst;
+    const void *src;
+    size_t bytes;
+  };
+  const Up ups[] = {{din, pos, natoms > 0 ? 3 * (size_t)natoms * sizeof(PosT) : 0},
+                    {(void *)d_occ, occ, occ && natoms > 0 ? (size_t)natoms * sizeof(float) : 0},
+                    {(void *)d_bfac, bfac, bfac && natoms > 0 ? (size_t)natoms * sizeof(float) : 0},
+                    {m->d_tiles, m->tiles.data(), m->tiles.size() * sizeof(TileDesc)},
+                    {m->d_perm, m->perm.data(), (size_t)n_pad * sizeof(int)},
+                    {m->d_wbase, wbase.data(), na * sizeof(float)},
+                    {m->d_coeffs, m->coeffs.data(), m->coeffs.size() * sizeof(float)}};
+  size_t stage_bytes = 0;
+  for (const Up &u : ups) stage_bytes += (u.bytes + 255) / 256 * 256;
+  CUDA_TRY(g_upload_stage.ensure(stage_bytes));
+  char *stage = (char *)g_upload_stage.p;
+  for (const Up &u : ups) {
+    if (!u.bytes) continue;
+    memcpy(stage, u.src, u.bytes);
+    CUDA_TRY(cudaMemcpyAsync(u.dst, stage, u.bytes, cudaMemcpyHostToDevice, nullptr));
+    stage += (u.bytes + 255) / 256 * 256;
   }
-  if (!m->tiles.empty())
-    CUDA_TRY(cudaMemcpy(m->d_tiles, m->tiles.data(), m->tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice));
-  if (n_pad) CUDA_TRY(cudaMemcpy(m->d_perm, m->perm.data(), n_pad * sizeof(int), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(m->d_wbase, wbase.data(), na * sizeof(float), cudaMemcpyHostToDevice));
-  if (!m->coeffs.empty())
-    CUDA_TRY(cudaMemcpy(m->d_coeffs, m->coeffs.data(), m->coeffs.size() * sizeof(float), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemset(m->d_flags, 0, 4 * sizeof(int)));
+  CUDA_TRY(cudaMemsetAsync(m->d_flags, 0, 4 * sizeof(int), nullptr));
   CUDA_TRY(launch_atoms_build<PosT>(m->d_atoms, m->d_atoms2, m->d_atomsd, m->d_perm, n_pad, d_pos, d_occ, d_bfac,
                                     m->d_wbase, m->center, (double)m->dr, (double)m->inv_dr, nullptr));
   // complete before return, so that work on any stream (non-blocking ones too) sees the records
@@ -1237,6 +1271,8 @@ static int host_session_molecule(int natoms, const int32_t *Z, const float *pos,
                                  int delta_atoms, const float *beam, spsim_b200_molecule **out) {
   std::vector<unsigned char> key;
   const size_t n = natoms > 0 ? (size_t)natoms : 0;
+  key.reserve(3 * sizeof(int) + n * (sizeof(int32_t) + 3 * sizeof(float) + (occ ? 4 : 0) + (bfac ? 4 : 0)) +
+              (beam ? 3 * sizeof(float) : 0));
   append_bytes(key, &natoms, sizeof(natoms));
   append_bytes(key, &delta_atoms, sizeof(delta_atoms));
   const int flags = (Z ? 1 : 0) | (pos ? 2 : 0) | (occ ? 4 : 0) | (bfac ? 8 : 0) | (beam ? 16 : 0);
@@ -1328,6 +1364,10 @@ extern "C" void spsim_internal_release_host_session(void) {
   }
   g_host = HostSession();
   g_shot_mol = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_upload_stage.release();
+  }
   if (g_oneshot.plan && g_oneshot.device == dev) delete g_oneshot.plan;
   g_oneshot = OneShot();
 }
