@@ -195,6 +195,11 @@ int spsim_b200_forward_nufft_batch(const spsim_b200_molecule *m, const spsim_b20
 /* Kernel widths (spreading, interpolation) and FFT grid (x, y, z) of the last
  * NUFFT forward on this thread. */
 int spsim_b200_last_nufft_grid(int *w_spread, int *w_interp, int *n2);
+/* Interpolation path of the NUFFT forwards (process-wide): 0 (default) lets
+ * q sets made from a detector walk each 16 x 8 pixel tile's grid region in
+ * shared memory together; 1 reads every pixel's stencil on its own.  Both
+ * give the same bits.  Other values: SPSIM_ERR_INVALID_ARG. */
+int spsim_b200_set_nufft_interp(int mode);
 /* The NUFFT structure factor of host arrays with unit atom weights (the
  * reference NNFFT's semantics: no illumination weights), host F (complex64)
  * and I out; synchronous. */

@@ -101,6 +101,7 @@ _SIGNATURES = {
     "spsim_b200_forward_nufft": (c_int, [_P, _P, _P, c_float, c_double, _P, _P, _P]),
     "spsim_b200_forward_nufft_batch": (c_int, [_P, _P, c_int, _P, c_float, c_double, _P, _P, _P]),
     "spsim_b200_last_nufft_grid": (c_int, [POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "spsim_b200_set_nufft_interp": (c_int, [c_int]),
     "spsim_b200_structure_factor_host_nufft": (
         c_int, [c_int, _P, _P, c_float, c_int, c_int64, _P, c_double, _P, _P]),
     "spsim_b200_adjoint": (c_int, [_P, _P, c_int, _P, c_float, c_int, _P, _P, _P, _P, _P, _P]),

@@ -204,6 +204,12 @@ def forward_nufft_batch(mol, qs, rots, B=0.0, eps=1e-8, F=None, I=None, want_F=T
     return (F if want_F else None), (I if want_I else None)
 
 
+def set_nufft_interp(mode):
+    """NUFFT interpolation path: 0 (default) the shared-memory tile path for
+    detector q sets, 1 per-pixel stencil reads everywhere (same bits)."""
+    check(lib().spsim_b200_set_nufft_interp(int(mode)))
+
+
 def last_nufft_grid():
     """(spreading width, interpolation width, (n2x, n2y, n2z)) of the last NUFFT forward on this thread."""
     a, b = c_int(0), c_int(0)

@@ -1898,6 +1898,13 @@ extern "C" int spsim_b200_forward_nufft_batch(const spsim_b200_molecule *m, cons
   return nufft_forward(m, qs, npatterns, rot, true, B, eps, F_dev, I_dev, (cudaStream_t)stream);
 }
 
+extern "C" int spsim_b200_set_nufft_interp(int mode) {
+  if (mode != 0 && mode != 1) return fail(SPSIM_ERR_INVALID_ARG, "NUFFT interpolation mode %d (0 or 1)", mode);
+  std::lock_guard<std::mutex> lk(g_mu);
+  nufft_set_interp_mode(mode);
+  return SPSIM_OK;
+}
+
 extern "C" int spsim_b200_last_nufft_grid(int *w_spread, int *w_interp, int *n2) {
   if (w_spread) *w_spread = g_last_nufft_w[0];
   if (w_interp) *w_interp = g_last_nufft_w[1];

@@ -133,7 +133,10 @@ int nufft_fft_axis(int n, int nin, int pmin, int nout, const double2 *tw, FftAxi
 void nufft_fft_twiddles(int n, double2 *tw);  // host table exp(-2 pi i k / n)
 cudaError_t nufft_fft3(const double *small, int copies, const double *dec, const NufftGeom &g, int n_elem,
                        const FftAxis ax[3], double2 *fa, double2 *fb, float4 *packed, cudaStream_t st);
-// Step 4.
+// Step 4.  Detector q sets (tile_nx > 0) take the tile path unless the mode is
+// 1 (the per-pixel path everywhere; both give the same bits).
 cudaError_t nufft_interp(const NufftInterp &a, cudaStream_t st);
+void nufft_set_interp_mode(int mode);
+int nufft_interp_mode();
 
 }  // namespace spsim

@@ -251,3 +251,29 @@ def test_power_of_two_transforms_and_nine_elements(cuda):
     assert core.last_nufft_grid()[2] == want
     F64, _ = O.structure_factor(Z, pos.astype(np.float64), h)
     _check_F(_np(F), F64, 1e-8)
+
+
+def test_tile_and_per_pixel_interpolation_give_the_same_bits(cuda):
+    # the tile path (a 16 x 8 pixel tile's grid region in shared memory, every
+    # pixel's x weights zero outside its stencil) against per-pixel stencil
+    # reads: identical F on a detector, a rotated detector (single calls and a
+    # batch) and a detector whose last tile row and column are partial
+    Z, pos = synth.random_molecule(4000, 5e-9, 41)
+    mol = core.Molecule(Z, pos)
+    try:
+        for nx, ny in ((96, 80), (77, 45)):
+            qs = core.QSet.from_detector(nx, ny, nx * 300e-6, ny * 300e-6, 0.09, 0.16e-9)
+            R = synth.haar_rotations(3, 43)
+            runs = {}
+            for mode in (1, 0):
+                core.set_nufft_interp(mode)
+                single = [core.forward_nufft(mol, qs, rot=r, eps=1e-8)[0] for r in (None, R[0])]
+                batch = core.forward_nufft_batch(mol, qs, R, eps=1e-8)[0]
+                core.synchronize()
+                runs[mode] = [_np(f) for f in single] + [_np(batch)]
+            for a, b in zip(runs[0], runs[1]):
+                np.testing.assert_array_equal(a, b)
+    finally:
+        core.set_nufft_interp(0)
+    with pytest.raises(Exception):
+        core.set_nufft_interp(2)
