@@ -367,7 +367,7 @@ int spsim_b200_last_forward_stats(double *terms, double *kernel_ms);
  * spsim_b200_structure_factor_host keep device scratch between calls on the
  * calling thread (grow-only buffers, the last molecule while its atom arrays
  * stay byte-identical, a reusable plan), the NUFFT forwards keep their grids
- * and FFT plans per device, and the adjoint keeps its last few plans (form
+ * and twiddle tables per device, and the adjoint keeps its last few plans (form
  * factors, atom blocks, work items, rotations); this frees all of them for the
  * current device.  No reference counterpart: spsim allocates and frees per
  * call. */

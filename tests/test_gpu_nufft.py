@@ -191,7 +191,7 @@ def test_orientation_batch_matches_oracle_and_single_calls(cuda):
 
 
 def test_release_scratch_frees_and_rebuilds_the_grids(cuda):
-    # spsim_b200_release_scratch drops the device's NUFFT grids and FFT plans;
+    # spsim_b200_release_scratch drops the device's NUFFT grids and twiddle tables;
     # the next forward builds them again
     from spsim_b200._native import lib
 
