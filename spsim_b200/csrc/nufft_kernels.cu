@@ -528,7 +528,9 @@ static cudaError_t interp_t(const NufftInterp &a, cudaStream_t st) {
     blocks = ((a.tile_nx + INTERP_TX - 1) / INTERP_TX) * ((rows + INTERP_TY - 1) / INTERP_TY);
   }
   const dim3 grid((unsigned)blocks, (unsigned)std::max(a.npat, 1));
-  if (a.tile_nx > 0 && g_interp_mode == 0) {
+  // a stencil wider than 11 points leaves no region of 1,728 points room to
+  // hold a tile's spread: such widths read per pixel
+  if constexpr (W <= 11) if (a.tile_nx > 0 && g_interp_mode == 0) {
     const size_t smem = (size_t)REGION_MAX_CELLS * a.halves * sizeof(float4);
     cudaError_t e;
     if (a.halves == 1) {
