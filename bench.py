@@ -469,6 +469,13 @@ def run_b200(args):
         if world == 1 and not args.no_batched:
             batched["orientations_20k"] = batched_orientations(prec, line["roofline"]["peak"])
             batched["uneven_64"] = batched_uneven(prec, line["roofline"]["peak"])
+            fp64 = line.get("fp64_plain", {}).get("kernel_terms_per_s")
+            if fp64:
+                # the batched forwards against the plain per-pattern FP64 kernel
+                o = batched["orientations_20k"]
+                o["vs_fp64_plain"] = o["terms_per_s"] / fp64
+                if "f32_fast" in o:
+                    o["f32_fast"]["vs_fp64_plain"] = o["f32_fast"]["terms_per_s"] / fp64
         if not args.no_adjoint:
             batched["adjoint_5k"] = batched_adjoint(prec)
         if batched:
@@ -767,11 +774,35 @@ def batched_orientations(prec, R0, n_orient=None, reps=2, nufft=True):
         Iloop = torch.empty(qs.npix, device="cuda")
         t_loop = ev_time(lambda: [core.forward(mol, qs, rot=R[i], precision=prec, I=Iloop, want_F=False,
                                                stream=stream) for i in range(nloop)], reps=2) * n_orient / nloop
+    def first4_error(Ib):
+        # floored max relative |F|^2 error of patterns 0..3 against the FP64 kernel
+        errs = []
+        with torch.cuda.stream(stream):
+            for i in range(4):
+                _, I64 = core.forward(mol, qs, rot=R[i], precision="fp64", stream=stream)
+                I64 = I64.double()
+                errs.append(float(((Ib[i].double() - I64).abs() /
+                                   torch.clamp(I64, min=1e-3 * float(I64.mean()))).max()))
+            stream.synchronize()
+        return max(errs)
+
     out = {"workload": "orientations_20k: 20,000 atoms, 256^2 pixels of 150 um at 0.2 m, 0.2 nm, %d Haar rotations "
                        "in one batched forward (graph-replayed)" % n_orient,
            "precision": prec, "orientations": n_orient, "kernel": kname, "batch_ms": t_batch,
            "terms_per_s": terms / t_batch * 1e3, "frac_of_R": terms / t_batch * 1e3 / R0,
-           "loop_of_single_calls_ms": t_loop, "batch_speedup": t_loop / t_batch}
+           "loop_of_single_calls_ms": t_loop, "batch_speedup": t_loop / t_batch,
+           "floored_max_rel_vs_fp64_first4": first4_error(Iall)}
+    if prec == "f32":
+        # the same batch in the fast mode (pixels 4m+2, 4m+3 of each neighbour
+        # quad on MUFU sin/cos), with its error on the same patterns
+        with torch.cuda.stream(stream):
+            t_fast = ev_time(lambda: core.forward_batch(mol, qs, rots=R, precision="f32_fast", I=I, want_F=False,
+                                                        stream=stream), reps=reps)
+        out["f32_fast"] = {"batch_ms": t_fast, "terms_per_s": terms / t_fast * 1e3,
+                           "frac_of_R": terms / t_fast * 1e3 / R0,
+                           "floored_max_rel_vs_fp64_first4": first4_error(Iall),
+                           "note": "measured here; the fast mode's MUFU bias can reach ~1.7e-5 on random "
+                                   "high-|q| neighbour quads, so SPSIM_PREC_F32 is the mode held to 1e-5 everywhere"}
     del Iall, I
     if nufft:
         with torch.cuda.stream(stream):

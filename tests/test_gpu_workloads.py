@@ -56,6 +56,31 @@ def test_orientations_20k_4096_rotations_in_one_batch(cuda):
         assert e_max < F32_TOL[0] and e_l2 < F32_TOL[1], (k, e_max, e_l2)
 
 
+def test_orientations_20k_fast_mode_batch(cuda):
+    # the same 4,096-orientation batch in SPSIM_PREC_F32_FAST (MUFU sin/cos for
+    # two pixels of each neighbour quad): within the FP32 tolerance on this
+    # workload, as the bench's batched f32_fast figure states (the mode is not
+    # held to it everywhere: on random high-|q| quads its MUFU bias reaches
+    # ~1.7e-5)
+    w = synth.WORKLOADS["orientations_20k"]
+    Z, pos = synth.random_molecule(w["natoms"], w["radius"], w["seed"])
+    d = w["det"]
+    R = synth.haar_rotations(w["n_orient"], w["rot_seed"])
+    mol = core.Molecule(Z, pos)
+    qs = core.QSet.from_detector(**d)
+    I = torch.empty(len(R), qs.npix, device="cuda")
+    core.forward_batch(mol, qs, rots=R, precision="f32_fast", I=list(I.unbind(0)), want_F=False)
+    torch.cuda.synchronize()
+    core.synchronize()
+    q0 = O.hkl_detector(**d)
+    sel = _rows(d["nx"], d["ny"], 4)
+    for k in (0, 1, 2047, 4095):
+        _, I64 = O.structure_factor(Z, pos.astype(np.float64), q0[sel] @ R[k].T)
+        e_max, e_l2 = intensity_errors(I[k, sel].cpu().numpy(), I64)
+        print("fast mode, orientation %d: floored max %.3g  L2 %.3g" % (k, e_max, e_l2))
+        assert e_max < F32_TOL[0] and e_l2 < F32_TOL[1], (k, e_max, e_l2)
+
+
 def test_uneven_64_molecules_in_one_batch_after_autotune(cuda):
     specs = synth.uneven_batch()
     mols, qsets, atoms = [], [], []
