@@ -218,9 +218,11 @@ def _shot_arrays(shot, det, n, nb):
     return out
 
 
-@pytest.mark.parametrize("nx,ny,binning", [(96, 90, 1), (95, 91, 2), (64, 64, 2)], ids=["even", "odd_binned",
-                                                                                        "square_binned"])
-def test_simulate_shot_row_chunks_match_step_by_step(cuda, tmp_path, nx, ny, binning):
+@pytest.mark.parametrize("nx,ny,binning,spherical,polarization",
+                         [(96, 90, 1, 0, 0), (95, 91, 2, 0, 0), (64, 64, 2, 0, 0), (80, 72, 1, 1, 3),
+                          (72, 81, 3, 0, 1)],
+                         ids=["even", "odd_binned", "square_binned", "spherical_unpolarised", "vertical_binned3"])
+def test_simulate_shot_row_chunks_match_step_by_step(cuda, tmp_path, nx, ny, binning, spherical, polarization):
     # the pipelined simulate_shot (three row chunks on two streams, each
     # chunk's outputs copied while the next computes) against the reference's
     # step-by-step sequence on the whole detector (no pattern counter step in
@@ -238,6 +240,8 @@ def test_simulate_shot_row_chunks_match_step_by_step(cuda, tmp_path, nx, ny, bin
         det.width, det.height = nx * det.pixel_width, ny * det.pixel_height
         det.nx, det.ny, det.nz = nx, ny, 1
         det.binning_x = det.binning_y = binning
+        det.spherical = spherical
+        o.experiment.contents.polarization = polarization
         det.readout_noise = 3.0
         o.verbosity_level = 0
         o.random_orientation = 0
