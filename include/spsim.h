@@ -112,10 +112,11 @@ int spsim_b200_get_legacy_precision(void);
 void spsim_b200_set_legacy_nufft_eps(double eps);
 double spsim_b200_get_legacy_nufft_eps(void);
 void spsim_b200_set_noise_seed(unsigned long long seed);
-/* Row chunks of simulate_shot on a flat detector with the direct,
- * monochromatic structure factor: chunk c's structure factor and detector
- * chain run while chunk c - 1's outputs are copied to the host, so that only
- * the last chunk's copies follow the computation.  0 (default): 4 chunks from
+/* Row chunks of simulate_shot on a flat detector with the direct
+ * monochromatic or the NUFFT structure factor: chunk c's structure factor
+ * (the NUFFT: its interpolation, the grid prepared once) and detector chain
+ * run while chunk c - 1's outputs are copied to the host, so that only the
+ * last chunk's copies follow the computation.  0 (default): 4 chunks from
  * 2^19 pixels on, none below; 1: none; at most 8.  Every output is that of
  * one whole-detector pass (each pixel keeps its noise stream; chunk rows are
  * a multiple of the y binning), up to the FP32 summation order of the

@@ -1322,6 +1322,7 @@ static int host_session_qset(int64_t npix, const float *hkl, spsim_b200_qset **o
   }
   q->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
   q->npix = npix;
+  q->row = 0;  // a list
   if (npix) CUDA_TRY(cudaMemcpy(q->d_hkl, hkl, 3 * npix * sizeof(float), cudaMemcpyHostToDevice));
   double qm2 = 0;
   for (long long i = 0; i < npix; ++i) {
@@ -1431,6 +1432,7 @@ static int host_session_qset_device(int64_t npix, const float *hkl_dev, cudaStre
   }
   q->id = __atomic_fetch_add(&g_next_id, 1, __ATOMIC_RELAXED);
   q->npix = npix;
+  q->row = 0;  // a list (callers that know the detector's rows set it)
   if (npix)
     CUDA_TRY(cudaMemcpyAsync(q->d_hkl, hkl_dev, 3 * npix * sizeof(float), cudaMemcpyDeviceToDevice, stream));
   if (!g_host.stats) g_host.stats = new DevBuf();
@@ -1616,7 +1618,8 @@ extern "C" int spsim_b200_structure_factor_host_spectrum(int natoms, const int32
 struct NufftCtx {
   DevBuf small, fa, fb, packed, dec, tw, seg, keys, flags, rots;
   FftAxis ax[3];  // the pruned FFT passes (twiddle tables in tw)
-  std::vector<double> geom_key;
+  std::vector<double> geom_key;   // inputs the q box was read for
+  std::vector<double> size_key;   // q box, bound, elements, eps the grids were sized for
   unsigned long long seg_mol = 0;  // molecule whose segment table is on the device
   NufftGeom g;
   int n_coef = 0;
@@ -1667,9 +1670,14 @@ static int nufft_width(double eps) {
 // npat patterns of one molecule and q set, pattern i rotated by rot[9 i] (or
 // none), outputs [npat][npix].  ball: size the grid for the ball |R q| <=
 // |q|max instead of the box of the rotated list, so that it holds for every
-// rotation (no read-back; the grid of a batch of orientations).
+// rotation (no read-back; the grid of a batch of orientations).  deferred:
+// prepare the grid (spread and FFT passes) and return the interpolation's
+// arguments there (F, I unset) instead of launching it; *deferred_empty is
+// set when there is nothing to interpolate (no atoms or no pixels: the
+// outputs are zeros).
 static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs, int npat, const double *rot,
-                         bool ball, float B, double eps, float *F_dev, float *I_dev, cudaStream_t st) {
+                         bool ball, float B, double eps, float *F_dev, float *I_dev, cudaStream_t st,
+                         NufftInterp *deferred = nullptr, bool *deferred_empty = nullptr) {
   if (!m || !qs) return fail(SPSIM_ERR_INVALID_ARG, "NULL handle");
   if (npat < 1 || npat > 65535) return fail(SPSIM_ERR_INVALID_ARG, "npatterns %d outside [1, 65535]", npat);
   if (!(eps >= 1e-14 && eps <= 1e-2)) return fail(SPSIM_ERR_INVALID_ARG, "eps %g outside [1e-14, 1e-2]", eps);
@@ -1680,6 +1688,7 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   if (st0) return st0;
   if (m->device != dev || qs->device != dev) return fail(SPSIM_ERR_INVALID_ARG, "handle belongs to another device");
   const long long npix = qs->npix;
+  if (deferred_empty) *deferred_empty = npix == 0 || m->n_kept == 0;
   if (npix == 0) return SPSIM_OK;
   if (m->n_kept == 0) {
     if (F_dev) CUDA_TRY(cudaMemsetAsync(F_dev, 0, 2 * npix * npat * sizeof(float), st));
@@ -1733,81 +1742,97 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
           return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: non-finite q in the list");
       }
     }
-    const int w = nufft_width(eps);
-    const double sigma1 = 1.5, sigma2 = 2.0;  // spreading-grid and FFT-grid upsampling
-    NufftGeom g;
-    std::memset(&g, 0, sizeof(g));
-    g.w1 = std::min(w + 3, NUFFT_MAX_W);
-    g.w2 = w;
-    g.beta1 = 0.97 * M_PI * g.w1 * (1.0 - 0.5 / sigma1);
-    g.beta2 = 0.97 * M_PI * g.w2 * (1.0 - 0.5 / sigma2);
-    const double X = m->rbound;
-    size_t cells1 = 1, cells2 = 1;
-    for (int d = 0; d < 3; ++d) {
-      g.cq[d] = 0.5 * (lo[d] + hi[d]);
-      const double S = std::max(0.5 * (hi[d] - lo[d]), 1e-3 / X);
-      g.h[d] = 1.0 / (2.0 * sigma1 * S);
-      g.inv_h[d] = 2.0 * sigma1 * S;
-      const double n1 = std::ceil(2.0 * X * g.inv_h[d]) + g.w1 + 2;
-      if (n1 > 4096) return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: %.0f grid points along axis %d; use the direct sum", n1, d);
-      g.n1[d] = (int)n1 + ((int)n1 & 1);
-      g.n2[d] = fft_size((int)std::ceil(sigma2 * g.n1[d]));
-      if (g.n2[d] > NUFFT_FFT_MAX)
-        return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: FFT of %d points along axis %d; use the direct sum", g.n2[d], d);
-      g.L[d] = g.h[d] * g.n2[d];
-      // the interpolation's stencils start at ceil(t - w/2), t = (q - cq) L,
-      // for t in [(lo - cq) L, (hi - cq) L]: the output box, 2 points of margin
-      const double tlo = (lo[d] - g.cq[d]) * g.L[d], thi = (hi[d] - g.cq[d]) * g.L[d];
-      g.pmin[d] = (int)std::floor(tlo - 0.5 * w) - 2;
-      g.m[d] = (int)std::ceil(thi - 0.5 * w) + w - 1 + 2 - g.pmin[d] + 1;
-      cells1 *= (size_t)g.n1[d];
-      cells2 *= (size_t)g.m[d];
+    // the grids follow from the q box, the molecule's bound, the elements and
+    // eps: an unchanged box (a new list of the same detector, say) keeps them
+    // (the molecule's bound enters only through the spreading grid's size n1)
+    std::vector<double> size_key = {lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], (double)n_elem, eps};
+    {
+      const int w1 = std::min(nufft_width(eps) + 3, NUFFT_MAX_W);
+      for (int d = 0; d < 3; ++d) {
+        const double S = std::max(0.5 * (hi[d] - lo[d]), 1e-3 / m->rbound);  // as below (a flat axis: from the bound)
+        size_key.push_back(S);
+        size_key.push_back(std::ceil(2.0 * m->rbound * (2.0 * 1.5 * S)) + w1 + 2);
+      }
     }
-    // copies of the spreading grid while they stay small next to L2 (32 MB):
-    // about 1,000 updates of one cell from 20,000 atoms on a 40 x 40 x 18 grid
-    // otherwise serialise in the atomic units
-    const size_t one1 = cells1 * n_elem * sizeof(double2);
-    c.copies = (int)std::max<size_t>(1, std::min<size_t>(8, (32u << 20) / std::max<size_t>(one1, 1)));
-    // x pass output [E][n1z][n1y][m_x], y pass output [E][n1z][m_y][m_x],
-    // z pass output (the interpolation's FP32 grid) over the box
-    const size_t bytes1 = one1 * c.copies;
-    const size_t bytes_a = (size_t)n_elem * g.n1[2] * g.n1[1] * g.m[0] * sizeof(double2);
-    const size_t bytes_b = (size_t)n_elem * g.n1[2] * g.m[1] * g.m[0] * sizeof(double2);
-    const size_t bytes3 = cells2 * nufft_pack_groups(n_elem) * nufft_pack_halves(n_elem) * sizeof(float4);
-    size_t free_b = 0, total_b = 0;
-    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-    const size_t have = free_b + c.small.cap + c.fa.cap + c.fb.cap + c.packed.cap;
-    if (bytes1 + bytes_a + bytes_b + bytes3 > have / 10 * 9)
-      return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: grids of %.3g GB do not fit; use the direct sum",
-                  (double)(bytes1 + bytes_a + bytes_b + bytes3) * 1e-9);
-    // 1 / phi2hat per spreading-grid index, and psi1hat's trapezoid coefficients
-    std::vector<double> dec;
-    for (int d = 0; d < 3; ++d)
-      for (int l = 0; l < g.n1[d]; ++l)
-        dec.push_back(1.0 / es_hat_host((double)(l - g.n1[d] / 2) / g.n2[d], g.w2, g.beta2, 0.01));
-    c.n_coef = (int)std::floor(0.5 * g.w1 / 0.25) + 1;
-    for (int k = 0; k < c.n_coef; ++k) c.psi_a[k] = 0.25 * (k == 0 ? 1.0 : 2.0) * es_host(0.25 * k, g.w1, g.beta1);
-    // twiddle tables of the three transforms, after dec in one upload
-    std::vector<double2> tw((size_t)g.n2[0] + g.n2[1] + g.n2[2]);
-    size_t tw_at[3];
-    for (int d = 0, at = 0; d < 3; at += g.n2[d], ++d) {
-      tw_at[d] = at;
-      nufft_fft_twiddles(g.n2[d], tw.data() + at);
+    if (size_key != c.size_key) {
+      c.size_key.clear();
+      const int w = nufft_width(eps);
+      const double sigma1 = 1.5, sigma2 = 2.0;  // spreading-grid and FFT-grid upsampling
+      NufftGeom g;
+      std::memset(&g, 0, sizeof(g));
+      g.w1 = std::min(w + 3, NUFFT_MAX_W);
+      g.w2 = w;
+      g.beta1 = 0.97 * M_PI * g.w1 * (1.0 - 0.5 / sigma1);
+      g.beta2 = 0.97 * M_PI * g.w2 * (1.0 - 0.5 / sigma2);
+      const double X = m->rbound;
+      size_t cells1 = 1, cells2 = 1;
+      for (int d = 0; d < 3; ++d) {
+        g.cq[d] = 0.5 * (lo[d] + hi[d]);
+        const double S = std::max(0.5 * (hi[d] - lo[d]), 1e-3 / X);
+        g.h[d] = 1.0 / (2.0 * sigma1 * S);
+        g.inv_h[d] = 2.0 * sigma1 * S;
+        const double n1 = std::ceil(2.0 * X * g.inv_h[d]) + g.w1 + 2;
+        if (n1 > 4096) return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: %.0f grid points along axis %d; use the direct sum", n1, d);
+        g.n1[d] = (int)n1 + ((int)n1 & 1);
+        g.n2[d] = fft_size((int)std::ceil(sigma2 * g.n1[d]));
+        if (g.n2[d] > NUFFT_FFT_MAX)
+          return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: FFT of %d points along axis %d; use the direct sum", g.n2[d], d);
+        g.L[d] = g.h[d] * g.n2[d];
+        // the interpolation's stencils start at ceil(t - w/2), t = (q - cq) L,
+        // for t in [(lo - cq) L, (hi - cq) L]: the output box, 2 points of margin
+        const double tlo = (lo[d] - g.cq[d]) * g.L[d], thi = (hi[d] - g.cq[d]) * g.L[d];
+        g.pmin[d] = (int)std::floor(tlo - 0.5 * w) - 2;
+        g.m[d] = (int)std::ceil(thi - 0.5 * w) + w - 1 + 2 - g.pmin[d] + 1;
+        cells1 *= (size_t)g.n1[d];
+        cells2 *= (size_t)g.m[d];
+      }
+      // copies of the spreading grid while they stay small next to L2 (32 MB):
+      // about 1,000 updates of one cell from 20,000 atoms on a 40 x 40 x 18 grid
+      // otherwise serialise in the atomic units
+      const size_t one1 = cells1 * n_elem * sizeof(double2);
+      c.copies = (int)std::max<size_t>(1, std::min<size_t>(8, (32u << 20) / std::max<size_t>(one1, 1)));
+      // x pass output [E][n1z][n1y][m_x], y pass output [E][n1z][m_y][m_x],
+      // z pass output (the interpolation's FP32 grid) over the box
+      const size_t bytes1 = one1 * c.copies;
+      const size_t bytes_a = (size_t)n_elem * g.n1[2] * g.n1[1] * g.m[0] * sizeof(double2);
+      const size_t bytes_b = (size_t)n_elem * g.n1[2] * g.m[1] * g.m[0] * sizeof(double2);
+      const size_t bytes3 = cells2 * nufft_pack_groups(n_elem) * nufft_pack_halves(n_elem) * sizeof(float4);
+      size_t free_b = 0, total_b = 0;
+      CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+      const size_t have = free_b + c.small.cap + c.fa.cap + c.fb.cap + c.packed.cap;
+      if (bytes1 + bytes_a + bytes_b + bytes3 > have / 10 * 9)
+        return fail(SPSIM_ERR_INVALID_ARG, "NUFFT: grids of %.3g GB do not fit; use the direct sum",
+                    (double)(bytes1 + bytes_a + bytes_b + bytes3) * 1e-9);
+      // 1 / phi2hat per spreading-grid index, and psi1hat's trapezoid coefficients
+      std::vector<double> dec;
+      for (int d = 0; d < 3; ++d)
+        for (int l = 0; l < g.n1[d]; ++l)
+          dec.push_back(1.0 / es_hat_host((double)(l - g.n1[d] / 2) / g.n2[d], g.w2, g.beta2, 0.01));
+      c.n_coef = (int)std::floor(0.5 * g.w1 / 0.25) + 1;
+      for (int k = 0; k < c.n_coef; ++k) c.psi_a[k] = 0.25 * (k == 0 ? 1.0 : 2.0) * es_host(0.25 * k, g.w1, g.beta1);
+      // twiddle tables of the three transforms, after dec in one upload
+      std::vector<double2> tw((size_t)g.n2[0] + g.n2[1] + g.n2[2]);
+      size_t tw_at[3];
+      for (int d = 0, at = 0; d < 3; at += g.n2[d], ++d) {
+        tw_at[d] = at;
+        nufft_fft_twiddles(g.n2[d], tw.data() + at);
+      }
+      CUDA_TRY(c.small.ensure(bytes1));
+      CUDA_TRY(c.fa.ensure(bytes_a));
+      CUDA_TRY(c.fb.ensure(bytes_b));
+      CUDA_TRY(c.packed.ensure(bytes3));
+      CUDA_TRY(c.dec.ensure(dec.size() * sizeof(double)));
+      CUDA_TRY(c.tw.ensure(tw.size() * sizeof(double2)));
+      CUDA_TRY(cudaMemcpyAsync(c.dec.p, dec.data(), dec.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+      CUDA_TRY(cudaMemcpyAsync(c.tw.p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+      for (int d = 0; d < 3; ++d)
+        if (nufft_fft_axis(g.n2[d], g.n1[d], g.pmin[d], g.m[d], (const double2 *)c.tw.p + tw_at[d], &c.ax[d]))
+          return fail(SPSIM_ERR_UNSUPPORTED, "NUFFT: no FFT pass for %d points", g.n2[d]);
+      // the read-back and the uploads above are complete when this returns
+      CUDA_TRY(cudaStreamSynchronize(st));
+      c.g = g;
+      c.size_key = size_key;
     }
-    CUDA_TRY(c.small.ensure(bytes1));
-    CUDA_TRY(c.fa.ensure(bytes_a));
-    CUDA_TRY(c.fb.ensure(bytes_b));
-    CUDA_TRY(c.packed.ensure(bytes3));
-    CUDA_TRY(c.dec.ensure(dec.size() * sizeof(double)));
-    CUDA_TRY(c.tw.ensure(tw.size() * sizeof(double2)));
-    CUDA_TRY(cudaMemcpyAsync(c.dec.p, dec.data(), dec.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(c.tw.p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
-    for (int d = 0; d < 3; ++d)
-      if (nufft_fft_axis(g.n2[d], g.n1[d], g.pmin[d], g.m[d], (const double2 *)c.tw.p + tw_at[d], &c.ax[d]))
-        return fail(SPSIM_ERR_UNSUPPORTED, "NUFFT: no FFT pass for %d points", g.n2[d]);
-    // the read-back and the uploads above are complete when this returns
-    CUDA_TRY(cudaStreamSynchronize(st));
-    c.g = g;
     c.geom_key = key;
   }
   if (c.seg_mol != m->id) {
@@ -1855,7 +1880,10 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   std::memcpy(a.psi_a, c.psi_a, sizeof(a.psi_a));
   a.F = (float2 *)F_dev;
   a.I = I_dev;
-  CUDA_TRY(nufft_interp(a, st));
+  if (deferred)
+    *deferred = a;
+  else
+    CUDA_TRY(nufft_interp(a, st));
   CUDA_TRY(cudaEventRecord(c.done, st));
   c.has_done = true;
   g_last_nufft_w[0] = g.w1;
@@ -1956,7 +1984,7 @@ extern "C" int spsim_b200_structure_factor_host_nufft(int natoms, const int32_t 
 // spsim_internal_shot_structure_factor.
 extern "C" int spsim_internal_shot_structure_factor_nufft(int natoms, const int32_t *Z, const float *pos, float B,
                                                           int delta_atoms, int64_t npix, const float *hkl_dev,
-                                                          double eps, float *F_dev, float *I_dev) {
+                                                          int row, double eps, float *F_dev, float *I_dev) {
   if (npix < 0 || (npix > 0 && !hkl_dev)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
   int dev;
   int st = current_device(&dev);
@@ -1974,7 +2002,67 @@ extern "C" int spsim_internal_shot_structure_factor_nufft(int natoms, const int3
   }
   st = host_session_qset_device(npix, hkl_dev, nullptr, &q);
   if (st) return st;
+  // a detector's rows: the interpolation takes its pixel-tile path
+  q->row = row > 0 && npix % row == 0 ? row : 0;
   return nufft_forward(m, q, 1, nullptr, false, B, eps, F_dev, I_dev, nullptr);
+}
+
+// The pipelined simulate_shot with the NUFFT structure factor: the grid is
+// prepared once (spread, FFT passes), then each whole-row chunk [p0, p1) is
+// interpolated on the legacy stream, in order, so that its detector chain and
+// copies overlap the next chunk's interpolation.
+static thread_local NufftInterp g_shot_interp;
+static thread_local bool g_shot_interp_empty = true;
+
+extern "C" int spsim_internal_shot_nufft_begin(int natoms, const int32_t *Z, const float *pos, float B,
+                                               int delta_atoms, int64_t npix, const float *hkl_dev, int row,
+                                               double eps) {
+  if (npix < 0 || (npix > 0 && !hkl_dev)) return fail(SPSIM_ERR_INVALID_ARG, "bad HKL list");
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  if (g_host.device != dev) {
+    g_host = HostSession();
+    g_host.device = dev;
+  }
+  spsim_b200_molecule *m = g_shot_mol;
+  g_shot_mol = nullptr;
+  spsim_b200_qset *q = nullptr;
+  if (!m || m != g_host.mol) {
+    st = host_session_molecule(natoms, Z, pos, nullptr, nullptr, delta_atoms, nullptr, &m);
+    if (st) return st;
+  }
+  st = host_session_qset_device(npix, hkl_dev, nullptr, &q);
+  if (st) return st;
+  q->row = row > 0 && npix % row == 0 ? row : 0;
+  g_shot_interp_empty = true;
+  return nufft_forward(m, q, 1, nullptr, false, B, eps, nullptr, nullptr, nullptr, &g_shot_interp,
+                       &g_shot_interp_empty);
+}
+
+extern "C" int spsim_internal_shot_nufft_part(int64_t p0, int64_t p1, float *F_dev, float *I_dev) {
+  NufftInterp a = g_shot_interp;
+  if (p0 < 0 || p1 > a.npix || p0 >= p1) return fail(SPSIM_ERR_INVALID_ARG, "bad NUFFT shot part");
+  if (g_shot_interp_empty) {
+    CUDA_TRY(cudaMemsetAsync(F_dev + 2 * p0, 0, 2 * (p1 - p0) * sizeof(float), nullptr));
+    CUDA_TRY(cudaMemsetAsync(I_dev + p0, 0, (p1 - p0) * sizeof(float), nullptr));
+    return SPSIM_OK;
+  }
+  int dev;
+  int st = current_device(&dev);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_nufft.find(dev);
+  if (it == g_nufft.end()) return fail(SPSIM_ERR_INVALID_ARG, "NUFFT shot part without a prepared grid");
+  if (a.hkl) a.hkl += 3 * p0;
+  if (a.q64) a.q64 += 3 * p0;
+  a.npix = p1 - p0;
+  if (a.tile_nx > 0 && (p0 % a.tile_nx || a.npix % a.tile_nx)) a.tile_nx = 0;
+  a.F = (float2 *)F_dev + p0;
+  a.I = I_dev + p0;
+  CUDA_TRY(nufft_interp(a, nullptr));
+  CUDA_TRY(cudaEventRecord(it->second.done, nullptr));
+  return SPSIM_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -108,11 +108,14 @@ int spsim_internal_shot_structure_factor(int natoms, const int32_t *Z, const flo
                                          int64_t npix, const float *hkl_dev, int precision, float *F_dev,
                                          float *I_dev);
 int spsim_internal_shot_structure_factor_nufft(int natoms, const int32_t *Z, const float *pos, float B,
-                                               int delta_atoms, int64_t npix, const float *hkl_dev, double eps,
-                                               float *F_dev, float *I_dev);
+                                               int delta_atoms, int64_t npix, const float *hkl_dev, int row,
+                                               double eps, float *F_dev, float *I_dev);
 int spsim_internal_shot_check(void);
 int spsim_internal_shot_molecule(int natoms, const int32_t *Z, const float *pos, int delta_atoms, const float *beam);
 int spsim_internal_shot_parts_begin(int64_t npix, const float *hkl_dev);
+int spsim_internal_shot_nufft_begin(int natoms, const int32_t *Z, const float *pos, float B, int delta_atoms,
+                                    int64_t npix, const float *hkl_dev, int row, double eps);
+int spsim_internal_shot_nufft_part(int64_t p0, int64_t p1, float *F_dev, float *I_dev);
 int spsim_internal_shot_part(int64_t p0, int64_t p1, float B, int precision, float *F_dev, float *I_dev,
                              void *stream);
 int spsim_internal_chain_rows(const spsim_b200_chain_params *p, const float *I_dev,
@@ -621,8 +624,9 @@ static void queue_hkl_copy(cudaEvent_t ev, char *s_hkl, const float *d_hkl, size
   cudaEventRecord(ev, g_copy_stream);
 }
 
-/* Row chunks of the pipelined simulate_shot for a flat detector's direct,
- * monochromatic structure factor (others: 1), as row boundaries rb[0..K].
+/* Row chunks of the pipelined simulate_shot for a flat detector's
+ * monochromatic structure factor, direct or NUFFT (others: 1), as row
+ * boundaries rb[0..K].
  * Automatic: 4 from 2^19 pixels on.  The last chunk, whose copies to the
  * host nothing hides, gets a quarter of the others' rows.  Chunk rows are a
  * multiple of the y binning and give a pixel count that is a multiple of 4
@@ -631,7 +635,7 @@ enum { MAX_SHOT_CHUNKS = 8 };
 static int shot_row_chunks(const CCD *det, long long n, int nfft, int poly, int vol, long long *rb) {
   rb[0] = 0;
   rb[1] = det->ny;
-  if (vol || nfft || poly || n <= 0) return 1;
+  if (vol || (poly && !nfft) || n <= 0) return 1;
   int k = g_shot_chunks > 0 ? g_shot_chunks : (n >= (1LL << 19) ? 4 : 1);
   if (k > MAX_SHOT_CHUNKS) k = MAX_SHOT_CHUNKS;
   if (k <= 1) return 1;
@@ -753,7 +757,7 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
   if (K == 1) {
     if (opts->use_nfft_for_sf)
       st = spsim_internal_shot_structure_factor_nufft(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
-                                                      opts->delta_atoms, n, d_hkl, g_nufft_eps, dF, dI);
+                                                      opts->delta_atoms, n, d_hkl, det->nx, g_nufft_eps, dF, dI);
     else
       st = spsim_internal_shot_structure_factor(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
                                                 opts->delta_atoms, beam, poly ? exp->wavelength : 0.0f,
@@ -787,9 +791,15 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
     cudaEventRecord(ev_out, 0);
   } else {
     /* row chunks: chunk c's structure factor and chain run on one of two
-     * compute streams, its outputs go down on the copy stream and into the
-     * caller's arrays while chunk c + 1 computes */
-    st = spsim_internal_shot_parts_begin(n, d_hkl);
+     * compute streams (the NUFFT: its grid prepared once, the chunks'
+     * interpolations in order on the legacy stream), its outputs go down on
+     * the copy stream and into the caller's arrays while chunk c + 1 computes */
+    const int nfft = opts->use_nfft_for_sf != 0;
+    if (nfft)
+      st = spsim_internal_shot_nufft_begin(mol->natoms, mol->atomic_number, mol->pos, opts->b_factor,
+                                           opts->delta_atoms, n, d_hkl, det->nx, g_nufft_eps);
+    else
+      st = spsim_internal_shot_parts_begin(n, d_hkl);
     if (st) die("simulate_shot structure factor", st);
     queue_hkl_copy(ev_hkl, s_hkl, d_hkl, b_hkl);
     if (!g_comp_stream[0] || g_comp_stream_device != cur_dev) {
@@ -809,9 +819,10 @@ Diffraction_Pattern *simulate_shot(Molecule *mol, Options *opts) {
       const long long b0 = r0 / det->binning_y * bnx;
       const long long b1 = (r1 / det->binning_y < det->ny / det->binning_y ? r1 / det->binning_y
                                                                             : det->ny / det->binning_y) * bnx;
-      cudaStream_t s = g_comp_stream[c & 1];
-      cudaStreamWaitEvent(s, ev_ready, 0);
-      st = spsim_internal_shot_part(p0, p1, opts->b_factor, g_precision, dF, dI, s);
+      cudaStream_t s = nfft ? (cudaStream_t)0 : g_comp_stream[c & 1];
+      if (s) cudaStreamWaitEvent(s, ev_ready, 0);
+      st = nfft ? spsim_internal_shot_nufft_part(p0, p1, dF, dI)
+                : spsim_internal_shot_part(p0, p1, opts->b_factor, g_precision, dF, dI, s);
       if (st) die("simulate_shot structure factor", st);
       st = spsim_internal_chain_rows(&p, dI, &o, r0, r1, s);
       if (st) die("simulate_shot detector chain", st);

@@ -218,11 +218,12 @@ def _shot_arrays(shot, det, n, nb):
     return out
 
 
-@pytest.mark.parametrize("nx,ny,binning,spherical,polarization",
-                         [(96, 90, 1, 0, 0), (95, 91, 2, 0, 0), (64, 64, 2, 0, 0), (80, 72, 1, 1, 3),
-                          (72, 81, 3, 0, 1)],
-                         ids=["even", "odd_binned", "square_binned", "spherical_unpolarised", "vertical_binned3"])
-def test_simulate_shot_row_chunks_match_step_by_step(cuda, tmp_path, nx, ny, binning, spherical, polarization):
+@pytest.mark.parametrize("nx,ny,binning,spherical,polarization,nfft",
+                         [(96, 90, 1, 0, 0, 0), (95, 91, 2, 0, 0, 0), (64, 64, 2, 0, 0, 0), (80, 72, 1, 1, 3, 0),
+                          (72, 81, 3, 0, 1, 0), (96, 90, 1, 0, 0, 1), (77, 70, 2, 0, 0, 1)],
+                         ids=["even", "odd_binned", "square_binned", "spherical_unpolarised", "vertical_binned3",
+                              "nufft", "nufft_odd_binned"])
+def test_simulate_shot_row_chunks_match_step_by_step(cuda, tmp_path, nx, ny, binning, spherical, polarization, nfft):
     # the pipelined simulate_shot (three row chunks on two streams, each
     # chunk's outputs copied while the next computes) against the reference's
     # step-by-step sequence on the whole detector (no pattern counter step in
@@ -242,6 +243,7 @@ def test_simulate_shot_row_chunks_match_step_by_step(cuda, tmp_path, nx, ny, bin
         det.binning_x = det.binning_y = binning
         det.spherical = spherical
         o.experiment.contents.polarization = polarization
+        o.use_nfft_for_sf = nfft  # the NUFFT: one grid, the chunks' interpolations in turn
         det.readout_noise = 3.0
         o.verbosity_level = 0
         o.random_orientation = 0
