@@ -2013,6 +2013,7 @@ extern "C" int spsim_internal_shot_structure_factor_nufft(int natoms, const int3
 // copies overlap the next chunk's interpolation.
 static thread_local NufftInterp g_shot_interp;
 static thread_local bool g_shot_interp_empty = true;
+static thread_local int64_t g_shot_npix = 0;  // pixels of the prepared shot (also when it has no atoms)
 
 extern "C" int spsim_internal_shot_nufft_begin(int natoms, const int32_t *Z, const float *pos, float B,
                                                int delta_atoms, int64_t npix, const float *hkl_dev, int row,
@@ -2036,13 +2037,14 @@ extern "C" int spsim_internal_shot_nufft_begin(int natoms, const int32_t *Z, con
   if (st) return st;
   q->row = row > 0 && npix % row == 0 ? row : 0;
   g_shot_interp_empty = true;
+  g_shot_npix = npix;
   return nufft_forward(m, q, 1, nullptr, false, B, eps, nullptr, nullptr, nullptr, &g_shot_interp,
                        &g_shot_interp_empty);
 }
 
 extern "C" int spsim_internal_shot_nufft_part(int64_t p0, int64_t p1, float *F_dev, float *I_dev) {
   NufftInterp a = g_shot_interp;
-  if (p0 < 0 || p1 > a.npix || p0 >= p1) return fail(SPSIM_ERR_INVALID_ARG, "bad NUFFT shot part");
+  if (p0 < 0 || p1 > g_shot_npix || p0 >= p1) return fail(SPSIM_ERR_INVALID_ARG, "bad NUFFT shot part");
   if (g_shot_interp_empty) {
     CUDA_TRY(cudaMemsetAsync(F_dev + 2 * p0, 0, 2 * (p1 - p0) * sizeof(float), nullptr));
     CUDA_TRY(cudaMemsetAsync(I_dev + p0, 0, (p1 - p0) * sizeof(float), nullptr));

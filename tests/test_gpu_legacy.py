@@ -304,6 +304,44 @@ def test_simulate_shot_row_chunks_match_step_by_step(cuda, tmp_path, nx, ny, bin
         os.chdir(cwd)
 
 
+@pytest.mark.parametrize("nfft", [0, 1])
+def test_simulate_shot_row_chunks_without_atoms(cuda, tmp_path, nfft):
+    # a molecule whose atoms are all Z = 0 (skipped, src/diffraction.c:830-832)
+    # through the pipelined shot, direct and NUFFT: every chunk's F and |F|^2
+    # are zeros, and the HKL list and geometry arrays those of one pass
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        opts = S.set_defaults()
+        S.read_options_file(os.path.join(GOLDEN, "config", "example.conf"), opts)
+        o = opts.contents
+        det = o.detector.contents
+        nx, ny = 64, 60
+        det.width, det.height = nx * det.pixel_width, ny * det.pixel_height
+        det.nx, det.ny, det.nz = nx, ny, 1
+        det.binning_x = det.binning_y = 1
+        o.use_nfft_for_sf = nfft
+        o.verbosity_level = 0
+        o.random_seed = 5
+        mol = _mol(np.zeros(5, np.int32), np.linspace(-1e-9, 1e-9, 15).reshape(5, 3))
+        n, nb = nx * ny, nx * ny
+        out = {}
+        for chunks in (1, 3):
+            S.set_shot_chunks(chunks)
+            shot = S.simulate_shot(mol, opts)
+            out[chunks] = _shot_arrays(shot, det, n, nb)
+            S.free_stuff(shot, opts)
+        ch, one = out[3], out[1]
+        assert not ch["F"].any() and not ch["I"].any()
+        assert not ch["photons_per_pixel"].any() and not ch["photon_count"].any()
+        np.testing.assert_array_equal(ch["hkl"], one["hkl"])
+        np.testing.assert_array_equal(ch["solid_angle"], one["solid_angle"])
+        S.free_mol(mol)
+    finally:
+        S.set_shot_chunks(0)
+        os.chdir(cwd)
+
+
 def test_simulate_shot_automatic_chunks_on_a_large_detector(cuda, tmp_path):
     # 1024 x 512 pixels (2^19): simulate_shot pipelines four row chunks by
     # default; every 29th row against the FP64 oracle, the chain's geometry
