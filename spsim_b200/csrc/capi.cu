@@ -7,7 +7,9 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <condition_variable>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -1628,8 +1630,20 @@ struct NufftCtx {
   unsigned long long *h_keys = nullptr;  // pinned bounds read-back
   cudaEvent_t done = nullptr;
   bool has_done = false;
+  // a pipelined shot's interpolation chunks read the grids after the call
+  // that prepared them has returned: from then until its last chunk is
+  // queued, other threads' NUFFT calls on the device wait
+  bool shot_open = false;
+  std::thread::id shot_owner;
 };
 static std::map<int, NufftCtx> g_nufft;
+static std::condition_variable g_nufft_cv;  // signalled when a shot releases its device's grids
+
+// under g_mu: no other thread's pipelined shot holds the device's grids
+static bool nufft_free_for_this_thread(int dev) {
+  const auto it = g_nufft.find(dev);
+  return it == g_nufft.end() || !it->second.shot_open || it->second.shot_owner == std::this_thread::get_id();
+}
 static thread_local int g_last_nufft_w[2] = {0, 0};
 static thread_local int g_last_nufft_n2[3] = {0, 0, 0};
 
@@ -1703,7 +1717,8 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
         for (int k = 0; k < 9; ++k) fro += rot[9 * (size_t)i + k] * rot[9 * (size_t)i + k];
         qball = std::max(qball, qs->qmax * std::sqrt(fro));
       }
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::unique_lock<std::mutex> lk(g_mu);
+  g_nufft_cv.wait(lk, [dev] { return nufft_free_for_this_thread(dev); });
   NufftCtx &c = g_nufft[dev];
   if (!c.h_keys) CUDA_TRY(cudaMallocHost(&c.h_keys, 6 * sizeof(unsigned long long)));
   if (!c.done) CUDA_TRY(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
@@ -1880,10 +1895,13 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
   std::memcpy(a.psi_a, c.psi_a, sizeof(a.psi_a));
   a.F = (float2 *)F_dev;
   a.I = I_dev;
-  if (deferred)
+  if (deferred) {
     *deferred = a;
-  else
+    c.shot_open = true;
+    c.shot_owner = std::this_thread::get_id();
+  } else {
     CUDA_TRY(nufft_interp(a, st));
+  }
   CUDA_TRY(cudaEventRecord(c.done, st));
   c.has_done = true;
   g_last_nufft_w[0] = g.w1;
@@ -1893,7 +1911,8 @@ static int nufft_forward(const spsim_b200_molecule *m, const spsim_b200_qset *qs
 }
 
 static void nufft_release(int dev) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::unique_lock<std::mutex> lk(g_mu);
+  g_nufft_cv.wait(lk, [dev] { return nufft_free_for_this_thread(dev); });
   auto it = g_nufft.find(dev);
   if (it == g_nufft.end()) return;
   NufftCtx &c = it->second;
@@ -2062,8 +2081,14 @@ extern "C" int spsim_internal_shot_nufft_part(int64_t p0, int64_t p1, float *F_d
   if (a.tile_nx > 0 && (p0 % a.tile_nx || a.npix % a.tile_nx)) a.tile_nx = 0;
   a.F = (float2 *)F_dev + p0;
   a.I = I_dev + p0;
-  CUDA_TRY(nufft_interp(a, nullptr));
-  CUDA_TRY(cudaEventRecord(it->second.done, nullptr));
+  const cudaError_t e = nufft_interp(a, nullptr);
+  const cudaError_t er = cudaEventRecord(it->second.done, nullptr);
+  if (p1 == g_shot_npix || e != cudaSuccess || er != cudaSuccess) {  // the last chunk: the grids are free again
+    it->second.shot_open = false;
+    g_nufft_cv.notify_all();
+  }
+  CUDA_TRY(e);
+  CUDA_TRY(er);
   return SPSIM_OK;
 }
 

@@ -277,3 +277,78 @@ def test_tile_and_per_pixel_interpolation_give_the_same_bits(cuda):
         core.set_nufft_interp(0)
     with pytest.raises(Exception):
         core.set_nufft_interp(2)
+
+
+def test_native_calls_on_another_thread_wait_for_a_pipelined_shot(cuda, tmp_path):
+    # simulate_shot with use_nfft_for_sf in four row chunks reads the device's
+    # NUFFT grids after the call that prepared them has returned; NUFFT
+    # forwards of another molecule on another detector (other grid sizes),
+    # issued meanwhile from this thread, wait until the shot's last chunk is
+    # queued.  Each thread's results against its own single-threaded ones.
+    import os
+    import threading
+
+    from conftest import GOLDEN
+    from spsim_b200 import spsim as S
+
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        opts = S.set_defaults()
+        S.read_options_file(os.path.join(GOLDEN, "config", "example.conf"), opts)
+        o = opts.contents
+        det = o.detector.contents
+        det.width, det.height = 256 * det.pixel_width, 256 * det.pixel_height
+        det.nx, det.ny, det.nz = 256, 256, 1
+        det.binning_x = det.binning_y = 1
+        o.use_nfft_for_sf = 1
+        o.verbosity_level = 0
+        g = golden("sf_small.npz")
+        smol = S.get_molecule_from_atoms(g["Z"], g["pos"])
+        n = 256 * 256
+        S.set_shot_chunks(4)
+
+        def shot_I():
+            shot = S.simulate_shot(smol, opts)
+            I = S.as_array(shot.contents.ints, n).copy()
+            S.free_stuff(shot, opts)
+            return I
+
+        I_ref = shot_I().astype(np.float64)
+        Z2, pos2 = synth.random_molecule(6000, 6e-9, 53)
+        mol2 = core.Molecule(Z2, pos2)
+        qs2 = core.QSet.from_detector(160, 144, 160 * 200e-6, 144 * 200e-6, 0.12, 0.18e-9)
+        F_ref, _ = core.forward_nufft(mol2, qs2, eps=1e-8)
+        core.synchronize()
+        F_ref = _np(F_ref)
+
+        shots, errors = [], []
+
+        def run_shots():
+            try:
+                for _ in range(4):
+                    shots.append(shot_I())
+            except Exception as e:  # reported below
+                errors.append(e)
+
+        t = threading.Thread(target=run_shots)
+        t.start()
+        forwards = []
+        while t.is_alive() or len(forwards) < 4:
+            F, _ = core.forward_nufft(mol2, qs2, eps=1e-8)
+            core.synchronize()
+            forwards.append(_np(F))
+            if len(forwards) >= 60:
+                break
+        t.join()
+        assert not errors, errors
+        assert len(shots) == 4
+        for I in shots:
+            e_max, e_l2 = intensity_errors(I, I_ref)
+            assert e_max < 1e-5 and e_l2 < 1e-6, (e_max, e_l2)
+        for F in forwards:
+            assert np.linalg.norm(F - F_ref) / np.linalg.norm(F_ref) < 1e-6
+        S.free_mol(smol)
+    finally:
+        S.set_shot_chunks(0)
+        os.chdir(cwd)
