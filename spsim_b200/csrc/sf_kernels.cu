@@ -933,8 +933,8 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(MODE)) sf_dpair_kernel(const
                 pc = fma2(zb, pc, f2(SPSIM_WIDE_C0));
               }
               const float2 Sb = mul2(Yb, ps);
-              const float2 wsa = make_float2(sign_by_parity(wa.x, kb[0], m31), sign_by_parity(wa.y, kb[1], m31));
-              const float2 wsb = PERB ? make_float2(sign_by_parity(wb.x, kb[0], m31), sign_by_parity(wb.y, kb[1], m31))
+              const float2 wsa = make_float2(sign_by_parity_alu(wa.x, kb[0]), sign_by_parity_alu(wa.y, kb[1]));
+              const float2 wsb = PERB ? make_float2(sign_by_parity_alu(wb.x, kb[0]), sign_by_parity_alu(wb.y, kb[1]))
                                       : wsa;
               bc[j][0] = fma2(wsa, Ca, bc[j][0]);
               bs[j][0] = fma2(wsa, Sa, bs[j][0]);
@@ -1216,10 +1216,12 @@ __global__ void __launch_bounds__(NT, sf_min_blocks(PREC_MODE_POLY)) sf_dquad_ke
                 const float w0 = LOGW ? ex2_approx(fmaf(d1.w, s2[2 * j][h], lw)) : W * ex2_approx(d1.w * s2[2 * j][h]);
                 const float w1 =
                     LOGW ? ex2_approx(fmaf(d1.w, s2[2 * j + 1][h], lw)) : W * ex2_approx(d1.w * s2[2 * j + 1][h]);
-                ws[h] = make_float2(sign_by_parity(w0, kb[0], m31), sign_by_parity(w1, kb[1], m31));
+                ws[h] = HYB ? make_float2(sign_by_parity(w0, kb[0], m31), sign_by_parity(w1, kb[1], m31))
+                            : make_float2(sign_by_parity_alu(w0, kb[0]), sign_by_parity_alu(w1, kb[1]));
               }
             } else {
-              ws[0] = make_float2(sign_by_parity(W, kb[0], m31), sign_by_parity(W, kb[1], m31));
+              ws[0] = HYB ? make_float2(sign_by_parity(W, kb[0], m31), sign_by_parity(W, kb[1], m31))
+                          : make_float2(sign_by_parity_alu(W, kb[0]), sign_by_parity_alu(W, kb[1]));
               ws[1] = ws[2] = ws[3] = ws[0];
             }
             float2 S, C;
