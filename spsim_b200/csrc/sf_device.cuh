@@ -233,8 +233,8 @@ __device__ __forceinline__ float sign_by_parity(float w, uint32_t kbits, uint32_
 // polynomial-only neighbour-quad and neighbour-pair kernels, whose FMA pipe
 // binds: on 50,000 atoms x 1024^2 0.3 % (quads) and 0.9 % (pairs) faster, on
 // 5,000 atoms x 512^2 x 256 orientations with per-atom B factors (a sign per
-// pixel) 3.8 % faster.  The split-pipe quads and the FP64-phase kernel keep
-// the multiply-add (0.4 % and 1.5 % slower with the shift).
+// pixel) 3.8 % faster.  The split-pipe quads, the FP64-phase kernel and the
+// adjoint keep the multiply-add (0.4 %, 1.5 % and 3 % slower with the shift).
 __device__ __forceinline__ float sign_by_parity_alu(float w, uint32_t kbits) {
   return __uint_as_float(__float_as_uint(w) ^ (kbits << 31));
 }
