@@ -133,7 +133,8 @@ static cudaStream_t g_comp_stream[2] = {NULL, NULL};
 static int g_comp_stream_device = -1;
 static int g_shot_chunks = 0; /* row chunks of simulate_shot: 0 automatic, 1 none */
 
-void spsim_b200_set_shot_chunks(int chunks) { g_shot_chunks = chunks < 0 ? 0 : chunks; }
+enum { MAX_SHOT_CHUNKS = 8 }; /* row chunks of simulate_shot, at most */
+void spsim_b200_set_shot_chunks(int chunks) { g_shot_chunks = chunks < 0 ? 0 : chunks > MAX_SHOT_CHUNKS ? MAX_SHOT_CHUNKS : chunks; }
 int spsim_b200_get_shot_chunks(void) { return g_shot_chunks; }
 
 static void *pinned_alloc(size_t bytes) {
@@ -631,7 +632,6 @@ static void queue_hkl_copy(cudaEvent_t ev, char *s_hkl, const float *d_hkl, size
  * host nothing hides, gets a quarter of the others' rows.  Chunk rows are a
  * multiple of the y binning and give a pixel count that is a multiple of 4
  * (the neighbour-quad kernel's alignment). */
-enum { MAX_SHOT_CHUNKS = 8 };
 static int shot_row_chunks(const CCD *det, long long n, int nfft, int poly, int vol, long long *rb) {
   rb[0] = 0;
   rb[1] = det->ny;

@@ -94,3 +94,17 @@ def test_legacy_nufft_eps_setting():
         assert S.get_nufft_eps() == 1e-10
     finally:
         S.set_nufft_eps(1e-8)
+
+
+def test_shot_chunk_setting_is_clamped():
+    # simulate_shot's row chunks: 0 automatic, 1 none, at most 8; negative
+    # values mean automatic (no device needed)
+    from spsim_b200 import spsim as S
+
+    assert S.get_shot_chunks() == 0
+    try:
+        for v, want in ((3, 3), (1, 1), (20, 8), (-5, 0)):
+            S.set_shot_chunks(v)
+            assert S.get_shot_chunks() == want
+    finally:
+        S.set_shot_chunks(0)
